@@ -1,0 +1,960 @@
+// hc_api.cu -- C-ABI of the B200 time-step engine (declared in include/hercules_b200.h).
+//
+// One handle owns one channel: its device state, one CUDA stream and the host
+// set-up that the reference's `drive` performs before the time loop
+// (src/module_navier_stokes.f90:53-129). hc_step issues, per RK sub-step,
+//   substep_begin -> momentum RHS -> r2c x -> c2c y -> column solve (3 Helmholtz +
+//   phi Poisson + projection) -> c2c y^-1 -> c2r x^-1 (+ p update)
+//   [-> temperature RHS -> FFT -> T column solve -> iFFT] -> divergence check
+// and per step the statistics/bulk-velocity/CFL pass and a one-block finaliser
+// that writes the step's diagnostics and the next step's scalars on the device.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+#include "../../include/hercules_b200.h"
+#include "hc_common.cuh"
+#include "hc_fd.cuh"
+#include "hc_fft.cuh"
+#include "hc_column.cuh"
+
+// ---------------------------------------------------------------------------
+// small device kernels for the scalar state
+// ---------------------------------------------------------------------------
+struct ScalarArgs {
+    DevScalars* sc;
+    int sub;               // 0-based sub-step
+    double dt;
+    int dp_opt;
+    double dpx_coef, um;
+    int is_ri_var;
+    double ri_str, ri_end;
+    int imax;
+};
+
+// screen_cpu_time's time_sim += dt (src/module_io.f90:68), update_ri
+// (src/module_parameters.f90:580-590) and update_dpx_drive (:594-613), which the
+// reference calls at the start of every sub-step's RHS.
+__global__ void k_substep_begin(ScalarArgs a)
+{
+    DevScalars* s = a.sc;
+    if (s->nan_flag) return;
+    if (a.sub == 0) {
+        s->step += 1;
+        s->time_sim = s->time_sim + a.dt;
+        if (a.is_ri_var == 1) s->got = a.ri_str + (a.ri_end - a.ri_str) * 1.0 / a.imax * s->step;
+    }
+    if (a.dp_opt == 1) s->dpx_drive = 1.0;
+    else if (a.dp_opt == 2) s->dpx_drive = s->dpx_drive - (s->ubar + a.um - 1.0) * a.dpx_coef;
+}
+
+struct FinalArgs {
+    DevScalars* sc;
+    const double* part_div;   // [3][nbd][3]
+    long long nbd;
+    int nsub;
+    const double* part_st;    // [nbs][2]
+    long long nbs;
+    double inv_n;             // 1/(nx ny nz) as the reference's sequential division
+    double nx, ny, nz, lz;
+    int dp_opt;
+    hc_diag* diag;            // diag[step - step_base]
+    int step_base;
+    int write_diag;
+    int cds;
+    double cfl_prev_dummy;
+};
+
+__device__ double block_sum_fixed(double v, double* sh)
+{
+    const int tid = threadIdx.x;
+    sh[tid] = v;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (tid < o) sh[tid] = sh[tid] + sh[tid + o];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+__device__ double block_max_fixed(double v, double* sh)
+{
+    const int tid = threadIdx.x;
+    sh[tid] = v;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (tid < o) sh[tid] = fmax(sh[tid], sh[tid + o]);
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+__device__ double block_absmax_fixed(double v, double* sh)
+{
+    const int tid = threadIdx.x;
+    sh[tid] = v;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (tid < o) sh[tid] = absmax_pick(sh[tid], sh[tid + o]);
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// End-of-step finaliser (one block of 256 threads, fixed reduction order).
+__global__ void __launch_bounds__(256) k_finalize(FinalArgs a)
+{
+    __shared__ double sh[256];
+    DevScalars* s = a.sc;
+    const int tid = threadIdx.x;
+    const bool halted_before = s->nan_flag != 0;
+    const double cfl_start = s->cfl;
+    double davg[3] = {0, 0, 0}, dmax[3] = {0, 0, 0};
+    int nan = 0;
+    for (int q = 0; q < a.nsub; ++q) {
+        const double* p = a.part_div + (long long)q * a.nbd * 3;
+        double sm = 0.0, mx = 0.0, nn = 0.0;
+        for (long long b = tid; b < a.nbd; b += blockDim.x) {
+            sm += p[3 * b];
+            mx = absmax_pick(mx, p[3 * b + 1]);
+            nn = fmax(nn, p[3 * b + 2]);
+        }
+        sm = block_sum_fixed(sm, sh);
+        mx = block_absmax_fixed(mx, sh);
+        nn = block_max_fixed(nn, sh);
+        davg[q] = sm / a.nx / a.ny / a.nz;
+        dmax[q] = a.cds == 3 ? fabs(mx) : mx;
+        if (nn != 0.0) nan = 1;
+    }
+    double ub = 0.0, cf = 0.0;
+    for (long long b = tid; b < a.nbs; b += blockDim.x) {
+        ub += a.part_st[2 * b];
+        cf = fmax(cf, a.part_st[2 * b + 1]);
+    }
+    ub = block_sum_fixed(ub, sh);
+    cf = block_max_fixed(cf, sh);
+    if (tid != 0) return;
+    if (halted_before) return;
+    for (int q = 0; q < a.nsub; ++q) {
+        s->div_avg[q] = davg[q];
+        s->div_max[q] = dmax[q];
+        if (fabs(dmax[q]) > fabs(s->div_hist)) s->div_hist = dmax[q];
+    }
+    if (a.dp_opt == 2) s->ubar = ub / a.lz / a.nx / a.ny;
+    s->cfl = cf;
+    if (nan) s->nan_flag = 1;
+    if (a.write_diag) {
+        hc_diag* d = a.diag + (s->step - a.step_base);
+        d->time_sim = s->time_sim;
+        d->cfl = cfl_start;
+        d->div_avg = davg[a.nsub - 1];
+        d->div_max = dmax[a.nsub - 1];
+        d->div_hist_max = s->div_hist;
+        d->ubar = a.dp_opt == 2 ? s->ubar : 0.0;
+        d->dpx_drive = s->dpx_drive;
+        d->got = s->got;
+        for (int q = 0; q < 3; ++q) {
+            d->div_avg_sub[q] = q < a.nsub ? davg[q] : 0.0;
+            d->div_max_sub[q] = q < a.nsub ? dmax[q] : 0.0;
+        }
+        d->nan_flag = nan;
+        d->step = s->step;
+    }
+}
+
+template <typename R>
+__global__ void k_convert_in(const double* src, R* dst, long long n)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (R)src[i];
+}
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+enum { F_U, F_V, F_W, F_P, F_T, F_FF, F_GG, F_HH, F_SS, F_QU, F_QV, F_QW, F_UHX, F_VHY, NFLD };
+
+struct hc_handle {
+    hc_params p;
+    int dev;
+    cudaStream_t st;
+    Geo g;
+    Phys ph;
+    size_t rsz;              // bytes of the storage type
+    void* fld[NFLD];
+    void* spec[4];
+    double* mean[11];
+    double* zbuf;            // 5*(nz+4)
+    double* coef;
+    ColCoef cc;
+    double* scratch;
+    ColScratch cs;
+    double* part_div;
+    double* part_st;
+    long long nbd, nbs;
+    DevScalars* sc;
+    hc_diag* diag_dev;
+    int diag_cap;
+    double2* twbuf;
+    FftPlan px, py;
+    double2* wpack;
+    int rows_x, tl_y;
+    size_t smem_x, smem_y;
+    double dpx_coef;
+    cudaEvent_t e0, e1;
+    double last_ms;
+    long long launches;
+    int initialized;
+    std::vector<double> zhost[5];
+};
+
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { fprintf(stderr, "hercules_b200: %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); return HC_ERR_CUDA; } } while (0)
+#define CKL() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) { fprintf(stderr, "hercules_b200: launch %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); return HC_ERR_CUDA; } ++h->launches; } while (0)
+
+static int factor_plan(int n, FftPlan* pl)
+{
+    pl->n = n;
+    pl->npass = 0;
+    int m = n;
+    const int rads[4] = {4, 2, 3, 5};
+    for (int q = 0; q < 4; ++q)
+        while (m % rads[q] == 0) {
+            if (pl->npass >= HC_MAX_PASS) return HC_ERR_UNSUPPORTED;
+            pl->rad[pl->npass++] = rads[q];
+            m /= rads[q];
+        }
+    return m == 1 ? HC_OK : HC_ERR_UNSUPPORTED;
+}
+
+// get_mesh_param (src/module_parameters.f90:432-508), Fortran k at [k-1]
+static void mesh_host(const hc_params* p, std::vector<double>* z)
+{
+    const int nz = p->nz, nka = nz + 4, kstr3 = 3, kend3 = nz + 2;
+    std::vector<double> zz(nka + 3, 0.0), dz(nka + 3, 0.0), lt(nka + 3, 0.0), lb(nka + 3, 0.0), dzt(nka + 3, 0.0), dzb(nka + 3, 0.0);
+    double zmin = 0.0, zmax = p->lz, zmean, coeff_a;
+    if (p->ochannel == 0) { zmean = 0.5 * (zmin + zmax); coeff_a = (2.0 + nz) * 0.5; }
+    else { zmean = zmin + zmax; coeff_a = (1.0 + nz) * 1.0; }
+    for (int k = 1; k <= nz + 1; ++k)
+        zz[k + 2] = zmean + (zmin - zmean) / tanh(2.0 * p->zstretch) * tanh(2.0 * p->zstretch * (k - coeff_a) / (1.0 - coeff_a));
+    for (int k = kstr3; k <= kend3; ++k) dz[k] = zz[k + 1] - zz[k];
+    dz[kstr3 - 1] = dz[kstr3]; dz[kend3 + 1] = dz[kend3];
+    dz[kstr3 - 2] = dz[kstr3]; dz[kend3 + 2] = dz[kend3];
+    for (int k = kstr3 - 1; k <= kend3 + 1; ++k) {
+        lt[k] = dz[k] / (dz[k] + dz[k + 1]);
+        lb[k] = dz[k] / (dz[k] + dz[k - 1]);
+        dzt[k] = 0.5 * (dz[k] + dz[k + 1]);
+        dzb[k] = 0.5 * (dz[k] + dz[k - 1]);
+    }
+    const std::vector<double>* src[5] = {&dz, &dzt, &dzb, &lt, &lb};
+    for (int q = 0; q < 5; ++q) {
+        z[q].assign(nka, 0.0);
+        for (int k = 1; k <= nka; ++k) z[q][k - 1] = (*src[q])[k];
+    }
+}
+
+// modified wavenumbers of the coefficient builders (src/module_poisson_solver.f90:71-102, 220-247)
+static double helm_sym(int cds, int l, int n, double h2, double dt, double dif, double L)
+{
+    const double th = 2.0 * HC_PI * l / n;
+    if (cds == 1) return 0.5 * dt * (2.0 * cos(th) - 2.0) * dif / h2;
+    if (cds == 2) return dt * (-2.0 * cos(2.0 * th) + 32.0 * cos(th) - 30.0) / 24.0 * dif / h2;
+    return 0.5 * dt * dif * (-(2.0 * HC_PI / L * l) * (2.0 * HC_PI / L * l));
+}
+static double pois_sym(int cds, int l, int n, double h2, double L)
+{
+    const double th = 2.0 * HC_PI * l / n;
+    if (cds == 1) return (2.0 * cos(th) - 2.0) / h2;
+    if (cds == 2) return (2.0 * cos(3.0 * th) - 108.0 * cos(2.0 * th) + 1566.0 * cos(th) - 1460.0) / 576.0 / h2;
+    return -(2.0 * HC_PI / L * l) * (2.0 * HC_PI / L * l);
+}
+
+static int build_tables(hc_handle* h)
+{
+    const hc_params& p = h->p;
+    const int nx = p.nx, ny = p.ny, nz = p.nz, nxh = nx / 2, cds = p.cds;
+    const double dx = h->g.dx, dy = h->g.dy, dx2 = h->g.dx2, dy2 = h->g.dy2, dt = p.dt, nu = p.nu, al = p.alpha;
+    // layout of the coefficient buffer
+    std::vector<double> buf;
+    auto put = [&](size_t n) { size_t o = buf.size(); buf.resize(o + n, 0.0); return o; };
+    size_t o_hx = put(nxh), o_hy = put(ny), o_hxt = put(nxh), o_hyt = put(ny), o_px = put(nxh), o_py = put(ny);
+    size_t o_dx = put(2 * nxh), o_dy = put(2 * ny), o_gx = put(2 * nxh), o_gy = put(2 * ny);
+    size_t o_lx = put(nxh), o_ly = put(ny);
+    size_t o_k[16];
+    for (int q = 0; q < 16; ++q) o_k[q] = put(nz);
+    auto lsig = [](int idx, int n) { return idx < n / 2 ? idx : idx - n; };
+    for (int l = 0; l < nxh; ++l) {
+        buf[o_hx + l] = helm_sym(cds, l, nx, dx2, dt, nu, p.lx);
+        buf[o_hxt + l] = helm_sym(cds, l, nx, dx2, dt, al, p.lx);
+        buf[o_px + l] = pois_sym(cds, l, nx, dx2, p.lx);
+    }
+    for (int mm = 0; mm < ny; ++mm) {
+        const int m = lsig(mm, ny);
+        buf[o_hy + mm] = helm_sym(cds, m, ny, dy2, dt, nu, p.ly);
+        buf[o_hyt + mm] = helm_sym(cds, m, ny, dy2, dt, al, p.ly);
+        buf[o_py + mm] = pois_sym(cds, m, ny, dy2, p.ly);
+    }
+    // divergence / gradient / second-derivative symbols of the staggered FD operators
+    auto fill_ops = [&](int idx, int n, double hh, size_t od, size_t og, size_t ol, int sgn_idx) {
+        const int l = sgn_idx;
+        const double th = 2.0 * HC_PI * l / n;
+        const double c1 = cos(th), s1 = sin(th), c2 = cos(2.0 * th), s2 = sin(2.0 * th);
+        double dre, dim, gre, gim, lap;
+        if (cds == 1) {
+            dre = (1.0 - c1) / hh; dim = s1 / hh;
+            gre = (c1 - 1.0) / hh; gim = s1 / hh;
+            lap = (2.0 * c1 - 2.0) / (hh * hh);
+        } else {
+            dre = (27.0 - 28.0 * c1 + c2) / (24.0 * hh); dim = (26.0 * s1 - s2) / (24.0 * hh);
+            gre = (-c2 + 28.0 * c1 - 27.0) / (24.0 * hh); gim = (26.0 * s1 - s2) / (24.0 * hh);
+            lap = (-2.0 * c2 + 32.0 * c1 - 30.0) / (12.0 * hh * hh);
+        }
+        buf[od + 2 * idx] = dre; buf[od + 2 * idx + 1] = dim;
+        buf[og + 2 * idx] = gre; buf[og + 2 * idx + 1] = gim;
+        buf[ol + idx] = lap;
+    };
+    for (int l = 0; l < nxh; ++l) fill_ops(l, nx, dx, o_dx, o_gx, o_lx, l);
+    for (int mm = 0; mm < ny; ++mm) fill_ops(mm, ny, dy, o_dy, o_gy, o_ly, lsig(mm, ny));
+    // per-k Thomas coefficients (interior level kk = Fortran k-3)
+    const std::vector<double>& DZ = h->zhost[0];
+    const std::vector<double>& DZT = h->zhost[1];
+    const std::vector<double>& DZB = h->zhost[2];
+    auto dz = [&](int kk) { return DZ[kk + 2]; };
+    auto dzt = [&](int kk) { return DZT[kk + 2]; };
+    auto dzb = [&](int kk) { return DZB[kk + 2]; };
+    double* au = &buf[o_k[0]]; double* cu = &buf[o_k[1]]; double* dgu = &buf[o_k[2]]; double* d0u = &buf[o_k[3]];
+    double* aw = &buf[o_k[4]]; double* cw = &buf[o_k[5]]; double* dgw = &buf[o_k[6]]; double* d0w = &buf[o_k[7]];
+    double* ap = &buf[o_k[8]]; double* cp = &buf[o_k[9]]; double* dgp = &buf[o_k[10]]; double* d0p = &buf[o_k[11]];
+    double* at = &buf[o_k[12]]; double* ct = &buf[o_k[13]]; double* dgt = &buf[o_k[14]]; double* d0t = &buf[o_k[15]];
+    for (int k = 0; k < nz; ++k) {
+        // u, v (get_u_eqn_coeff :198-278)
+        double a0 = -0.5 * dt * nu / dz(k) / dzb(k), c0 = -0.5 * dt * nu / dz(k) / dzt(k);
+        au[k] = k == 0 ? 0.0 : a0;
+        cu[k] = k == nz - 1 ? 0.0 : c0;
+        dgu[k] = -(k == 0 ? 0.0 : a0) - (k == nz - 1 ? 0.0 : c0);
+        d0u[k] = -a0 - c0;
+        if (k == 0) d0u[k] = d0u[k] - a0;
+        if (k == nz - 1) d0u[k] = p.ochannel == 0 ? d0u[k] - c0 : d0u[k] + c0;
+        // t (get_t_eqn_coeff :396-473)
+        double a0t = -0.5 * dt * al / dz(k) / dzb(k), c0t = -0.5 * dt * al / dz(k) / dzt(k);
+        at[k] = k == 0 ? 0.0 : a0t;
+        ct[k] = k == nz - 1 ? 0.0 : c0t;
+        dgt[k] = -(k == 0 ? 0.0 : a0t) - (k == nz - 1 ? 0.0 : c0t);
+        d0t[k] = -a0t - c0t;
+        if (k == 0) d0t[k] = d0t[k] - a0t;
+        if (k == nz - 1) d0t[k] = d0t[k] - c0t;
+        // p (get_p_eqn_coeff :49-118)
+        double a0p = 1.0 / dz(k) / dzb(k), c0p = 1.0 / dz(k) / dzt(k);
+        ap[k] = k == 0 ? 0.0 : a0p;
+        cp[k] = k == nz - 1 ? 0.0 : c0p;
+        dgp[k] = -(k == 0 ? 0.0 : a0p) - (k == nz - 1 ? 0.0 : c0p);
+        d0p[k] = -a0p - c0p;
+        if (k == 0) d0p[k] = d0p[k] + a0p;
+        if (k == nz - 1) d0p[k] = d0p[k] + c0p;
+        // w (get_w_eqn_coeff :304-370), rows 0..nz-2
+        if (k <= nz - 2) {
+            double a0w = -0.5 * dt * nu / dz(k) / dzt(k), c0w = -0.5 * dt * nu / dz(k + 1) / dzt(k);
+            aw[k] = k == 0 ? 0.0 : a0w;
+            cw[k] = k == nz - 2 ? 0.0 : c0w;
+            dgw[k] = -(k == 0 ? 0.0 : a0w) - (k == nz - 2 ? 0.0 : c0w);
+            d0w[k] = -a0w - c0w;
+        }
+    }
+    CK(cudaMalloc(&h->coef, buf.size() * sizeof(double)));
+    CK(cudaMemcpy(h->coef, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
+    double* b = h->coef;
+    ColCoef& c = h->cc;
+    c.hx = b + o_hx; c.hy = b + o_hy; c.hxt = b + o_hxt; c.hyt = b + o_hyt; c.px = b + o_px; c.py = b + o_py;
+    c.dx = (const double2*)(b + o_dx); c.dy = (const double2*)(b + o_dy);
+    c.gx = (const double2*)(b + o_gx); c.gy = (const double2*)(b + o_gy);
+    c.lx = b + o_lx; c.ly = b + o_ly;
+    c.au = b + o_k[0]; c.cu = b + o_k[1]; c.dgu = b + o_k[2]; c.d0u = b + o_k[3];
+    c.aw = b + o_k[4]; c.cw = b + o_k[5]; c.dgw = b + o_k[6]; c.d0w = b + o_k[7];
+    c.ap = b + o_k[8]; c.cp = b + o_k[9]; c.dgp = b + o_k[10]; c.d0p = b + o_k[11];
+    c.at = b + o_k[12]; c.ct = b + o_k[13]; c.dgt = b + o_k[14]; c.d0t = b + o_k[15];
+    return HC_OK;
+}
+
+static int upload_zgrid(hc_handle* h)
+{
+    const int nka = h->p.nz + 4;
+    for (int q = 0; q < 5; ++q)
+        CK(cudaMemcpy(h->zbuf + q * nka, h->zhost[q].data(), nka * sizeof(double), cudaMemcpyHostToDevice));
+    h->g.z.dz = h->zbuf; h->g.z.dz_t = h->zbuf + nka; h->g.z.dz_b = h->zbuf + 2 * nka;
+    h->g.z.l_t = h->zbuf + 3 * nka; h->g.z.l_b = h->zbuf + 4 * nka;
+    return HC_OK;
+}
+
+static int build_fft(hc_handle* h)
+{
+    const int nx = h->p.nx, ny = h->p.ny, nxh = nx / 2;
+    if (factor_plan(nxh, &h->px) != HC_OK || factor_plan(ny, &h->py) != HC_OK) return HC_ERR_UNSUPPORTED;
+    std::vector<double2> tw(nxh + ny + nxh);
+    for (int e = 0; e < nxh; ++e) tw[e] = make_double2(cos(2.0 * HC_PI * e / nxh), -sin(2.0 * HC_PI * e / nxh));
+    for (int e = 0; e < ny; ++e) tw[nxh + e] = make_double2(cos(2.0 * HC_PI * e / ny), -sin(2.0 * HC_PI * e / ny));
+    for (int e = 0; e < nxh; ++e) tw[nxh + ny + e] = make_double2(cos(2.0 * HC_PI * e / nx), -sin(2.0 * HC_PI * e / nx));
+    CK(cudaMalloc(&h->twbuf, tw.size() * sizeof(double2)));
+    CK(cudaMemcpy(h->twbuf, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    h->px.tw = h->twbuf;
+    h->py.tw = h->twbuf + nxh;
+    h->wpack = h->twbuf + nxh + ny;
+    const size_t c2 = 2 * h->rsz;     // bytes of one complex
+    h->rows_x = 2048 / nxh; if (h->rows_x < 1) h->rows_x = 1; if (h->rows_x > 64) h->rows_x = 64;
+    h->smem_x = 2 * (size_t)h->rows_x * nxh * c2;
+    h->tl_y = 2048 / ny; if (h->tl_y < 2) h->tl_y = 2; if (h->tl_y > 16) h->tl_y = 16; if (h->tl_y > nxh) h->tl_y = nxh;
+    h->smem_y = 2 * (size_t)h->tl_y * (ny + 1) * c2;
+    if (h->smem_x > 200 * 1024 || h->smem_y > 200 * 1024) return HC_ERR_UNSUPPORTED;
+    return HC_OK;
+}
+
+template <typename R> static int set_smem_attrs()
+{
+    CK(cudaFuncSetAttribute(k_fft_x_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(k_fft_x_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(k_fft_y<R, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(k_fft_y<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    return HC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+static dim3 pt_block() { return dim3(32, 8, 1); }
+static dim3 pt_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
+
+template <typename R> static Acc<R> make_acc(hc_handle* h)
+{
+    Acc<R> a;
+    a.f.u = (const R*)h->fld[F_U]; a.f.v = (const R*)h->fld[F_V]; a.f.w = (const R*)h->fld[F_W];
+    a.f.p = (const R*)h->fld[F_P]; a.f.t = (const R*)h->fld[F_T];
+    a.g = h->g;
+    a.um = (R)h->p.u_mrf; a.tbot = (R)h->p.tbot; a.ttop = (R)h->p.ttop;
+    a.closed = h->p.ochannel == 0;
+    return a;
+}
+
+template <typename R> static int fft_forward(hc_handle* h, const R* const* in, typename V2<R>::T* const* out, int nf)
+{
+    typedef typename V2<R>::T T2;
+    const int* halt = &h->sc->nan_flag;
+    FftXArgs<R> ax;
+    memset(&ax, 0, sizeof(ax));
+    for (int f = 0; f < nf; ++f) { ax.in[f] = in[f]; ax.out[f] = out[f]; }
+    ax.nrows = (long long)h->g.ny * h->g.nz;
+    ax.rows = h->rows_x; ax.pl = h->px; ax.wpack = h->wpack; ax.scale = 1.0 / h->p.nx; ax.halt = halt;
+    dim3 gx((unsigned)((ax.nrows + ax.rows - 1) / ax.rows), nf, 1);
+    k_fft_x_r2c<R><<<gx, 256, h->smem_x, h->st>>>(ax);
+    CKL();
+    FftYArgs<R> ay;
+    memset(&ay, 0, sizeof(ay));
+    for (int f = 0; f < nf; ++f) ay.data[f] = out[f];
+    ay.nxh = h->g.nxh; ay.ny = h->g.ny; ay.tl = h->tl_y; ay.pl = h->py; ay.scale = 1.0 / h->p.ny; ay.halt = halt;
+    dim3 gy((h->g.nxh + ay.tl - 1) / ay.tl, h->g.nz, nf);
+    k_fft_y<R, -1><<<gy, 256, h->smem_y, h->st>>>(ay);
+    CKL();
+    (void)sizeof(T2);
+    return HC_OK;
+}
+
+template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* const* in, R* const* out, const int* add, int nf)
+{
+    const int* halt = &h->sc->nan_flag;
+    FftYArgs<R> ay;
+    memset(&ay, 0, sizeof(ay));
+    for (int f = 0; f < nf; ++f) ay.data[f] = in[f];
+    ay.nxh = h->g.nxh; ay.ny = h->g.ny; ay.tl = h->tl_y; ay.pl = h->py; ay.scale = 1.0; ay.halt = halt;
+    dim3 gy((h->g.nxh + ay.tl - 1) / ay.tl, h->g.nz, nf);
+    k_fft_y<R, 1><<<gy, 256, h->smem_y, h->st>>>(ay);
+    CKL();
+    FftXInvArgs<R> ax;
+    memset(&ax, 0, sizeof(ax));
+    for (int f = 0; f < nf; ++f) { ax.in[f] = in[f]; ax.out[f] = out[f]; ax.add[f] = add[f]; }
+    ax.nrows = (long long)h->g.ny * h->g.nz;
+    ax.rows = h->rows_x; ax.pl = h->px; ax.wpack = h->wpack; ax.halt = halt;
+    dim3 gx((unsigned)((ax.nrows + ax.rows - 1) / ax.rows), nf, 1);
+    k_fft_x_c2r<R><<<gx, 256, h->smem_x, h->st>>>(ax);
+    CKL();
+    return HC_OK;
+}
+
+static const double RKC1[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+static const double RKC2[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+static const double RKC3[3] = {8.0 / 15.0, 2.0 / 15.0, 1.0 / 3.0};
+
+template <typename R> static int launch_stats(hc_handle* h, int accumulate)
+{
+    StatsArgs<R> s;
+    memset(&s, 0, sizeof(s));
+    s.f.u = (const R*)h->fld[F_U]; s.f.v = (const R*)h->fld[F_V]; s.f.w = (const R*)h->fld[F_W];
+    s.f.p = (const R*)h->fld[F_P]; s.f.t = (const R*)h->fld[F_T];
+    s.g = h->g;
+    if (h->p.cds != 3) { s.uhx_s = (const R*)h->fld[F_UHX]; s.vhy_s = (const R*)h->fld[F_VHY]; }
+    for (int q = 0; q < 11; ++q) s.mean[q] = h->mean[q];
+    s.accumulate = accumulate;
+    s.um = h->p.u_mrf; s.dt = h->p.dt;
+    s.part = h->part_st;
+    k_stats<R><<<pt_grid(h->g), pt_block(), 0, h->st>>>(s);
+    CKL();
+    return HC_OK;
+}
+
+static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base)
+{
+    FinalArgs f;
+    memset(&f, 0, sizeof(f));
+    f.sc = h->sc; f.part_div = h->part_div; f.nbd = h->nbd; f.nsub = nsub;
+    f.part_st = h->part_st; f.nbs = h->nbs;
+    f.nx = h->p.nx; f.ny = h->p.ny; f.nz = h->p.nz; f.lz = h->p.lz;
+    f.dp_opt = h->p.dp_opt; f.diag = h->diag_dev; f.step_base = step_base; f.write_diag = write_diag;
+    f.cds = h->p.cds;
+    k_finalize<<<1, 256, 0, h->st>>>(f);
+    CKL();
+    return HC_OK;
+}
+
+template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
+{
+    typedef typename V2<R>::T T2;
+    const hc_params& p = h->p;
+    const int* halt = &h->sc->nan_flag;
+    double rk_a, rk_b, rk_c;
+    if (p.dts == 2) { rk_a = RKC1[sub]; rk_b = RKC2[sub]; rk_c = RKC3[sub]; }
+    else { rk_a = 1.5; rk_b = -0.5; rk_c = 1.0; }
+    const int last = (p.dts == 2) ? (sub == 2) : 1;
+
+    ScalarArgs sa;
+    sa.sc = h->sc; sa.sub = sub; sa.dt = p.dt; sa.dp_opt = p.dp_opt; sa.dpx_coef = h->dpx_coef; sa.um = p.u_mrf;
+    sa.is_ri_var = p.is_ri_var; sa.ri_str = p.ri_str; sa.ri_end = p.ri_end; sa.imax = p.imax;
+    k_substep_begin<<<1, 1, 0, h->st>>>(sa);
+    CKL();
+
+    // momentum RHS
+    MomArgs<R> m;
+    m.a = make_acc<R>(h);
+    m.ff = (R*)h->fld[F_FF]; m.gg = (R*)h->fld[F_GG]; m.hh = (R*)h->fld[F_HH];
+    m.qu = (R*)h->fld[F_QU]; m.qv = (R*)h->fld[F_QV]; m.qw = (R*)h->fld[F_QW];
+    m.uhx_s = last ? (R*)h->fld[F_UHX] : nullptr; m.vhy_s = last ? (R*)h->fld[F_VHY] : nullptr;
+    m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph; m.sc = h->sc;
+    k_rhs_momentum<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
+    CKL();
+
+    T2* S[4] = {(T2*)h->spec[0], (T2*)h->spec[1], (T2*)h->spec[2], (T2*)h->spec[3]};
+    const R* qin[3] = {(const R*)h->fld[F_QU], (const R*)h->fld[F_QV], (const R*)h->fld[F_QW]};
+    int rc = fft_forward<R>(h, qin, S, 3);
+    if (rc) return rc;
+
+    ColArgs<R> ca;
+    ca.qu = S[0]; ca.qv = S[1]; ca.qw = S[2]; ca.psi = S[3];
+    ca.c = h->cc; ca.s = h->cs; ca.g = h->g;
+    ca.rk_c = rk_c; ca.dt = p.dt; ca.nu = p.nu;
+    {
+        const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
+        const int ks = 2, ke = p.nz + 1;   // Fortran kstr3, kend3 at array index k-1
+        double aa_u_zstr = -0.5 * rk_c * p.dt * p.nu / DZ[ks] / DZB[ks];
+        ca.bcu0 = 2.0 * aa_u_zstr * p.u_mrf;
+        ca.bcu1 = 0.0;
+        if (p.ochannel == 0) {
+            double cc_u_zend = -0.5 * rk_c * p.dt * p.nu / DZ[ke] / DZT[ke];
+            ca.bcu1 = 2.0 * cc_u_zend * p.u_mrf;
+        }
+    }
+    ca.halt = halt;
+    k_column_fd<R><<<(unsigned)((h->g.ncol + 127) / 128), 128, 0, h->st>>>(ca);
+    CKL();
+
+    R* outs[4] = {(R*)h->fld[F_U], (R*)h->fld[F_V], (R*)h->fld[F_W], (R*)h->fld[F_P]};
+    const int add[4] = {0, 0, 0, 1};
+    rc = fft_inverse<R>(h, S, outs, add, 4);
+    if (rc) return rc;
+
+    if (p.isscalar == 1) {
+        TempArgs<R> ta;
+        ta.a = make_acc<R>(h);
+        ta.ss = (R*)h->fld[F_SS]; ta.qt = (R*)h->fld[F_QU];
+        ta.rk_a = rk_a; ta.rk_b = rk_b; ta.rk_c = rk_c; ta.ph = h->ph;
+        k_rhs_temperature<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(ta);
+        CKL();
+        const R* tin[1] = {(const R*)h->fld[F_QU]};
+        rc = fft_forward<R>(h, tin, S, 1);
+        if (rc) return rc;
+        ColTArgs<R> ct;
+        ct.qt = S[0]; ct.c = h->cc; ct.s = h->cs; ct.g = h->g; ct.rk_c = rk_c; ct.halt = halt;
+        {
+            const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
+            const int ks = 2, ke = p.nz + 1;
+            double aa_t_zstr = -0.5 * rk_c * p.dt * p.alpha / DZ[ks] / DZB[ks];
+            double cc_t_zend = -0.5 * rk_c * p.dt * p.alpha / DZ[ke] / DZT[ke];
+            ct.bct0 = -2.0 * aa_t_zstr * p.tbot;
+            ct.bct1 = -2.0 * cc_t_zend * p.ttop;
+        }
+        k_column_t<R><<<(unsigned)((h->g.ncol + 127) / 128), 128, 0, h->st>>>(ct);
+        CKL();
+        R* tout[1] = {(R*)h->fld[F_T]};
+        const int add0[1] = {0};
+        rc = fft_inverse<R>(h, S, tout, add0, 1);
+        if (rc) return rc;
+    }
+
+    FieldsIn<R> fi;
+    fi.u = (const R*)h->fld[F_U]; fi.v = (const R*)h->fld[F_V]; fi.w = (const R*)h->fld[F_W];
+    fi.p = (const R*)h->fld[F_P]; fi.t = (const R*)h->fld[F_T];
+    k_div_check<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->nbd * 3);
+    CKL();
+    return HC_OK;
+}
+
+template <typename R, int CDS> static int step_fd(hc_handle* h, int step_base)
+{
+    const int nsub = h->p.dts == 2 ? 3 : 1;
+    for (int sub = 0; sub < nsub; ++sub) {
+        int rc = substep_fd<R, CDS>(h, sub);
+        if (rc) return rc;
+    }
+    int rc = launch_stats<R>(h, 1);
+    if (rc) return rc;
+    return launch_finalize(h, nsub, 1, step_base);
+}
+
+template <typename R> static int step_dispatch(hc_handle* h, int step_base)
+{
+    if (h->p.cds == 1) return step_fd<R, 1>(h, step_base);
+    if (h->p.cds == 2) return step_fd<R, 2>(h, step_base);
+    return HC_ERR_UNSUPPORTED;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* hc_error_string(int code)
+{
+    switch (code) {
+    case HC_OK: return "ok";
+    case HC_ERR_ARG: return "bad argument";
+    case HC_ERR_PARAM: return "parameter check failed";
+    case HC_ERR_CUDA: return "CUDA error";
+    case HC_ERR_NOMEM: return "device allocation failed";
+    case HC_ERR_NAN: return "NaN error";
+    case HC_ERR_STATE: return "call out of order";
+    case HC_ERR_UNSUPPORTED: return "option not supported";
+    case HC_ERR_SIZE: return "size beyond the documented maximum";
+    }
+    return "unknown error";
+}
+
+static void free_all(hc_handle* h)
+{
+    for (int q = 0; q < NFLD; ++q) if (h->fld[q]) cudaFree(h->fld[q]);
+    for (int q = 0; q < 4; ++q) if (h->spec[q]) cudaFree(h->spec[q]);
+    for (int q = 0; q < 11; ++q) if (h->mean[q]) cudaFree(h->mean[q]);
+    if (h->zbuf) cudaFree(h->zbuf);
+    if (h->coef) cudaFree(h->coef);
+    if (h->scratch) cudaFree(h->scratch);
+    if (h->part_div) cudaFree(h->part_div);
+    if (h->part_st) cudaFree(h->part_st);
+    if (h->sc) cudaFree(h->sc);
+    if (h->diag_dev) cudaFree(h->diag_dev);
+    if (h->twbuf) cudaFree(h->twbuf);
+    if (h->e0) cudaEventDestroy(h->e0);
+    if (h->e1) cudaEventDestroy(h->e1);
+    if (h->st) cudaStreamDestroy(h->st);
+}
+
+int hc_create(const hc_params* p, hc_handle** out)
+{
+    if (!p || !out) return HC_ERR_ARG;
+    *out = nullptr;
+    // initiate_parameters checks (src/module_parameters.f90:266-270) and this engine's limits
+    if (p->nx % 2 != 0 || p->ny % 2 != 0) return HC_ERR_PARAM;
+    if (p->nx < 8 || p->ny < 4 || p->nz < 3) return HC_ERR_PARAM;
+    if (p->cds < 1 || p->cds > 3 || (p->dts != 1 && p->dts != 2) || p->dt <= 0.0) return HC_ERR_PARAM;
+    if (p->isscalar != 0 && p->isscalar != 1) return HC_ERR_PARAM;
+    if (p->dp_opt < 1 || p->dp_opt > 3) return HC_ERR_PARAM;
+    if (p->precision != HC_PREC_FP64 && p->precision != HC_PREC_MIXED) return HC_ERR_PARAM;
+    if (p->cds == 3) return HC_ERR_UNSUPPORTED;
+    if (p->isdamp == 1) return HC_ERR_UNSUPPORTED;
+
+    hc_handle* h = new hc_handle();
+    memset((void*)&h->p, 0, sizeof(h->p));
+    h->p = *p;
+    for (int q = 0; q < NFLD; ++q) h->fld[q] = nullptr;
+    for (int q = 0; q < 4; ++q) h->spec[q] = nullptr;
+    for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
+    h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
+    h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
+    h->diag_cap = 0; h->last_ms = 0.0; h->launches = 0; h->initialized = 0;
+    int rc = HC_OK;
+#define FAIL(code) do { rc = (code); goto fail; } while (0)
+    {
+        if (cudaGetDevice(&h->dev) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        if (cudaEventCreate(&h->e0) != cudaSuccess || cudaEventCreate(&h->e1) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        h->rsz = p->precision == HC_PREC_MIXED ? sizeof(float) : sizeof(double);
+        Geo& g = h->g;
+        g.nx = p->nx; g.ny = p->ny; g.nz = p->nz; g.nxh = p->nx / 2;
+        g.nxy = (long long)p->nx * p->ny; g.n = g.nxy * p->nz; g.ncol = (long long)g.nxh * p->ny;
+        g.dx = p->lx / p->nx; g.dy = p->ly / p->ny; g.dx2 = g.dx * g.dx; g.dy2 = g.dy * g.dy;
+        Phys& ph = h->ph;
+        ph.dt = p->dt; ph.nu = p->nu; ph.alpha = p->alpha; ph.um = p->u_mrf; ph.fc = p->fc; ph.ug = p->ug;
+        ph.vg = p->vg; ph.t_ref = p->t_ref; ph.tbot = p->tbot; ph.ttop = p->ttop;
+        ph.cds = p->cds; ph.dp_opt = p->dp_opt; ph.isscalar = p->isscalar; ph.ochannel = p->ochannel; ph.dts = p->dts;
+        h->dpx_coef = p->nu * 1.0;
+        mesh_host(p, h->zhost);
+        const long long n = g.n;
+        for (int q = 0; q < NFLD; ++q) {
+            if (cudaMalloc(&h->fld[q], n * h->rsz) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+            if (cudaMemset(h->fld[q], 0, n * h->rsz) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        }
+        for (int q = 0; q < 4; ++q) {
+            if (cudaMalloc(&h->spec[q], g.ncol * g.nz * 2 * h->rsz) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+            if (cudaMemset(h->spec[q], 0, g.ncol * g.nz * 2 * h->rsz) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        }
+        for (int q = 0; q < 11; ++q) {
+            if (cudaMalloc(&h->mean[q], n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+            if (cudaMemset(h->mean[q], 0, n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        }
+        const long long cz = g.ncol * g.nz;
+        if (cudaMalloc(&h->scratch, cz * (3 * sizeof(double) + 4 * sizeof(double2))) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+        h->cs.bu = h->scratch; h->cs.bw = h->scratch + cz; h->cs.bp = h->scratch + 2 * cz;
+        h->cs.su = (double2*)(h->scratch + 3 * cz); h->cs.sv = h->cs.su + cz; h->cs.sw = h->cs.sv + cz; h->cs.sp = h->cs.sw + cz;
+        if (cudaMalloc(&h->zbuf, 5 * (p->nz + 4) * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+        if ((rc = upload_zgrid(h)) != HC_OK) goto fail;
+        if ((rc = build_tables(h)) != HC_OK) goto fail;
+        if ((rc = build_fft(h)) != HC_OK) goto fail;
+        rc = h->rsz == sizeof(float) ? set_smem_attrs<float>() : set_smem_attrs<double>();
+        if (rc != HC_OK) goto fail;
+        dim3 gr = pt_grid(g);
+        h->nbd = (long long)gr.x * gr.y * gr.z;
+        h->nbs = h->nbd;
+        if (cudaMalloc(&h->part_div, 3 * h->nbd * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+        if (cudaMemset(h->part_div, 0, 3 * h->nbd * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        if (cudaMalloc(&h->part_st, 2 * h->nbs * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+        if (cudaMalloc(&h->sc, sizeof(DevScalars)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+        DevScalars s0;
+        memset(&s0, 0, sizeof(s0));
+        s0.dpx_drive = p->dp_opt == 1 ? 1.0 : 0.0;
+        s0.got = p->got;
+        if (cudaMemcpy(h->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        h->diag_cap = 256;
+        if (cudaMalloc(&h->diag_dev, h->diag_cap * sizeof(hc_diag)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+    }
+    *out = h;
+    return HC_OK;
+fail:
+    free_all(h);
+    delete h;
+    return rc;
+#undef FAIL
+}
+
+int hc_destroy(hc_handle* h)
+{
+    if (!h) return HC_ERR_ARG;
+    cudaStreamSynchronize(h->st);
+    free_all(h);
+    delete h;
+    return HC_OK;
+}
+
+int hc_set_grid(hc_handle* h, const double* dz, const double* l_t, const double* l_b, const double* dz_t, const double* dz_b)
+{
+    if (!h || !dz || !l_t || !l_b || !dz_t || !dz_b) return HC_ERR_ARG;
+    if (h->initialized) return HC_ERR_STATE;
+    const int nka = h->p.nz + 4;
+    const double* src[5] = {dz, dz_t, dz_b, l_t, l_b};
+    for (int q = 0; q < 5; ++q) h->zhost[q].assign(src[q], src[q] + nka);
+    int rc = upload_zgrid(h);
+    if (rc) return rc;
+    cudaFree(h->coef);
+    h->coef = nullptr;
+    return build_tables(h);
+}
+
+int hc_get_grid(hc_handle* h, double* dz, double* l_t, double* l_b, double* dz_t, double* dz_b)
+{
+    if (!h) return HC_ERR_ARG;
+    double* dst[5] = {dz, dz_t, dz_b, l_t, l_b};
+    for (int q = 0; q < 5; ++q)
+        if (dst[q]) memcpy(dst[q], h->zhost[q].data(), (h->p.nz + 4) * sizeof(double));
+    return HC_OK;
+}
+
+static void* field_dev(hc_handle* h, int id, int* is_mean)
+{
+    *is_mean = 0;
+    switch (id) {
+    case HC_FIELD_U: return h->fld[F_U];
+    case HC_FIELD_V: return h->fld[F_V];
+    case HC_FIELD_W: return h->fld[F_W];
+    case HC_FIELD_P: return h->fld[F_P];
+    case HC_FIELD_T: return h->fld[F_T];
+    case HC_FIELD_FF: return h->fld[F_FF];
+    case HC_FIELD_GG: return h->fld[F_GG];
+    case HC_FIELD_HH: return h->fld[F_HH];
+    case HC_FIELD_SS: return h->fld[F_SS];
+    default: break;
+    }
+    if (id >= HC_FIELD_MEAN_U && id <= HC_FIELD_MEAN_TW) { *is_mean = 1; return h->mean[id - HC_FIELD_MEAN_U]; }
+    return nullptr;
+}
+
+int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, int ghost)
+{
+    if (!h || !host || ghost < 0 || ld1 < h->p.nx + 2 * ghost || ld2 < h->p.ny + 2 * ghost) return HC_ERR_ARG;
+    int is_mean;
+    void* d = field_dev(h, field_id, &is_mean);
+    if (!d) return HC_ERR_ARG;
+    const int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
+    const long long n = (long long)nx * ny * nz;
+    std::vector<double> tmp(n);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            memcpy(&tmp[((long long)k * ny + j) * nx], host + (size_t)ghost + (size_t)ld1 * ((size_t)(j + ghost) + (size_t)ld2 * (size_t)(k + ghost)), nx * sizeof(double));
+    if (is_mean || h->rsz == sizeof(double)) {
+        CK(cudaMemcpy(d, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> tf(n);
+        for (long long q = 0; q < n; ++q) tf[q] = (float)tmp[q];
+        CK(cudaMemcpy(d, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return HC_OK;
+}
+
+int hc_download(hc_handle* h, int field_id, double* host, int ld1, int ld2, int ghost)
+{
+    if (!h || !host || ghost < 0 || ld1 < h->p.nx + 2 * ghost || ld2 < h->p.ny + 2 * ghost) return HC_ERR_ARG;
+    if (field_id == HC_FIELD_PHI) return HC_ERR_UNSUPPORTED;
+    int is_mean;
+    void* d = field_dev(h, field_id, &is_mean);
+    if (!d) return HC_ERR_ARG;
+    CK(cudaStreamSynchronize(h->st));
+    const int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
+    const long long n = (long long)nx * ny * nz;
+    std::vector<double> tmp(n);
+    if (is_mean || h->rsz == sizeof(double)) {
+        CK(cudaMemcpy(tmp.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tf(n);
+        CK(cudaMemcpy(tf.data(), d, n * sizeof(float), cudaMemcpyDeviceToHost));
+        for (long long q = 0; q < n; ++q) tmp[q] = tf[q];
+    }
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            memcpy(host + (size_t)ghost + (size_t)ld1 * ((size_t)(j + ghost) + (size_t)ld2 * (size_t)(k + ghost)), &tmp[((long long)k * ny + j) * nx], nx * sizeof(double));
+    return HC_OK;
+}
+
+int hc_upload_dev(hc_handle* h, int field_id, const void* dev)
+{
+    if (!h || !dev) return HC_ERR_ARG;
+    int is_mean;
+    void* d = field_dev(h, field_id, &is_mean);
+    if (!d) return HC_ERR_ARG;
+    const size_t bytes = h->g.n * (is_mean ? sizeof(double) : h->rsz);
+    CK(cudaMemcpyAsync(d, dev, bytes, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return HC_OK;
+}
+
+int hc_download_dev(hc_handle* h, int field_id, void* dev)
+{
+    if (!h || !dev) return HC_ERR_ARG;
+    int is_mean;
+    void* d = field_dev(h, field_id, &is_mean);
+    if (!d) return HC_ERR_ARG;
+    const size_t bytes = h->g.n * (is_mean ? sizeof(double) : h->rsz);
+    CK(cudaMemcpyAsync(dev, d, bytes, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return HC_OK;
+}
+
+int hc_initialize(hc_handle* h)
+{
+    if (!h) return HC_ERR_ARG;
+    const hc_params& p = h->p;
+    // update_boundary_uvw sets w = 0 on the top wall before the loop (src/module_navier_stokes.f90:127)
+    CK(cudaMemsetAsync((char*)h->fld[F_W] + (size_t)(p.nz - 1) * h->g.nxy * h->rsz, 0, h->g.nxy * h->rsz, h->st));
+    DevScalars s0;
+    memset(&s0, 0, sizeof(s0));
+    s0.dpx_drive = p.dp_opt == 1 ? 1.0 : 0.0;
+    s0.got = p.is_ri_var == 1 ? p.ri_str + (p.ri_end - p.ri_str) * 1.0 / p.imax * 0 : p.got;
+    CK(cudaMemcpyAsync(h->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice, h->st));
+    // calculate_ubar (dp_opt=2) and the CFL of the initial fields
+    int rc = h->rsz == sizeof(float) ? launch_stats<float>(h, 0) : launch_stats<double>(h, 0);
+    if (rc) return rc;
+    rc = launch_finalize(h, 0, 0, 0);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->st));
+    h->initialized = 1;
+    return HC_OK;
+}
+
+int hc_step(hc_handle* h, int nsteps, hc_diag* out)
+{
+    if (!h || nsteps < 0) return HC_ERR_ARG;
+    if (!h->initialized) return HC_ERR_STATE;
+    DevScalars s;
+    CK(cudaMemcpy(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost));
+    if (s.nan_flag) return HC_ERR_NAN;
+    h->launches = 0;
+    CK(cudaEventRecord(h->e0, h->st));
+    int done = 0;
+    int rc = HC_OK;
+    float total_ms = 0.0f;
+    while (done < nsteps) {
+        const int chunk = (nsteps - done) < h->diag_cap ? (nsteps - done) : h->diag_cap;
+        const int base = s.step + done + 1;
+        for (int q = 0; q < chunk; ++q) {
+            rc = h->rsz == sizeof(float) ? step_dispatch<float>(h, base) : step_dispatch<double>(h, base);
+            if (rc) return rc;
+        }
+        if (out) CK(cudaMemcpyAsync(out + done, h->diag_dev, chunk * sizeof(hc_diag), cudaMemcpyDeviceToHost, h->st));
+        done += chunk;
+    }
+    CK(cudaEventRecord(h->e1, h->st));
+    CK(cudaEventSynchronize(h->e1));
+    CK(cudaEventElapsedTime(&total_ms, h->e0, h->e1));
+    h->last_ms = total_ms;
+    DevScalars s1;
+    CK(cudaMemcpy(&s1, h->sc, sizeof(s1), cudaMemcpyDeviceToHost));
+    if (s1.nan_flag) return HC_ERR_NAN;
+    return rc;
+}
+
+int hc_get_scalars(hc_handle* h, double* time_sim, double* dpx_drive, double* ubar, double* got, double* div_hist_max, int* step)
+{
+    if (!h) return HC_ERR_ARG;
+    DevScalars s;
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaMemcpy(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost));
+    if (time_sim) *time_sim = s.time_sim;
+    if (dpx_drive) *dpx_drive = s.dpx_drive;
+    if (ubar) *ubar = s.ubar;
+    if (got) *got = s.got;
+    if (div_hist_max) *div_hist_max = s.div_hist;
+    if (step) *step = s.step;
+    return HC_OK;
+}
+
+int hc_last_step_ms(hc_handle* h, double* ms)
+{
+    if (!h || !ms) return HC_ERR_ARG;
+    *ms = h->last_ms;
+    return HC_OK;
+}
+
+int hc_last_launch_count(hc_handle* h, long long* n)
+{
+    if (!h || !n) return HC_ERR_ARG;
+    *n = h->launches;
+    return HC_OK;
+}
+
+}  // extern "C"

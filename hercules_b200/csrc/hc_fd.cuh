@@ -1,0 +1,450 @@
+// hc_fd.cuh -- finite-difference stencil kernels (cds = 1: 2nd order, cds = 2: 4th order).
+//
+// One thread per interior grid point. Every interpolant the reference stores in a
+// separate array (uhx .. why, thx .. thz; src/module_tools.f90:410-512, with their
+// ghost values from src/module_boundary.f90:202-355) is recomputed in registers
+// from u, v, w, t, and every ghost cell is produced on load: periodic wrap in x, y
+// and the wall / top conditions in z.
+#pragma once
+#include "hc_common.cuh"
+
+template <typename R> struct FieldsIn {
+    const R* u; const R* v; const R* w; const R* p; const R* t;
+};
+
+template <typename R> __device__ __forceinline__ R ldf(const R* f, const Geo& g, int i, int j, int k)
+{
+    return __ldg(f + ((long long)k * g.ny + wrapi(j, g.ny)) * g.nx + wrapi(i, g.nx));
+}
+
+// ---- z ghost cells on load (update_boundary_uvw/p/t, src/module_boundary.f90:33-196) ----
+template <typename R> struct Acc {
+    FieldsIn<R> f;
+    Geo g;
+    R um, tbot, ttop;
+    int closed;   // ochannel == 0
+
+    __device__ __forceinline__ R U(int i, int j, int k) const {
+        if (k < 0) return -ldf(f.u, g, i, j, 0) - R(2) * um;
+        if (k >= g.nz) return closed ? -ldf(f.u, g, i, j, g.nz - 1) - R(2) * um : ldf(f.u, g, i, j, g.nz - 1);
+        return ldf(f.u, g, i, j, k);
+    }
+    __device__ __forceinline__ R V(int i, int j, int k) const {
+        if (k < 0) return -ldf(f.v, g, i, j, 0);
+        if (k >= g.nz) return closed ? -ldf(f.v, g, i, j, g.nz - 1) : ldf(f.v, g, i, j, g.nz - 1);
+        return ldf(f.v, g, i, j, k);
+    }
+    __device__ __forceinline__ R W(int i, int j, int k) const {
+        if (k < 0) return R(0);
+        if (k >= g.nz) return -ldf(f.w, g, i, j, g.nz - 2);
+        return ldf(f.w, g, i, j, k);          // level nz-1 is the top wall, stored as 0
+    }
+    __device__ __forceinline__ R P(int i, int j, int k) const {
+        k = k < 0 ? 0 : (k >= g.nz ? g.nz - 1 : k);
+        return ldf(f.p, g, i, j, k);
+    }
+    __device__ __forceinline__ R T(int i, int j, int k) const {
+        if (k < 0) return R(2) * tbot - ldf(f.t, g, i, j, 0);
+        if (k >= g.nz) return R(2) * ttop - ldf(f.t, g, i, j, g.nz - 1);
+        return ldf(f.t, g, i, j, k);
+    }
+    __device__ __forceinline__ R lt(int k) const { return (R)ldz(g.z.l_t, k); }
+
+    // ---- mid-point interpolants (get_interp_fields_uvwhxyz, src/module_tools.f90:410-468) ----
+    template <int CDS> __device__ __forceinline__ R uhx(int i, int j, int k) const {
+        if (CDS == 1) return R(0.5) * (U(i, j, k) + U(i - 1, j, k));
+        return (-U(i + 1, j, k) + R(9) * U(i, j, k) + R(9) * U(i - 1, j, k) - U(i - 2, j, k)) * R(0.0625);
+    }
+    template <int CDS> __device__ __forceinline__ R uhy(int i, int j, int k) const {
+        if (CDS == 1) return R(0.5) * (U(i, j + 1, k) + U(i, j, k));
+        return (-U(i, j + 2, k) + R(9) * U(i, j + 1, k) + R(9) * U(i, j, k) - U(i, j - 1, k)) * R(0.0625);
+    }
+    template <int CDS> __device__ __forceinline__ R vhx(int i, int j, int k) const {
+        if (CDS == 1) return R(0.5) * (V(i + 1, j, k) + V(i, j, k));
+        return (-V(i + 2, j, k) + R(9) * V(i + 1, j, k) + R(9) * V(i, j, k) - V(i - 1, j, k)) * R(0.0625);
+    }
+    template <int CDS> __device__ __forceinline__ R vhy(int i, int j, int k) const {
+        if (CDS == 1) return R(0.5) * (V(i, j, k) + V(i, j - 1, k));
+        return (-V(i, j + 1, k) + R(9) * V(i, j, k) + R(9) * V(i, j - 1, k) - V(i, j - 2, k)) * R(0.0625);
+    }
+    // whx/why: 0 on the wall ghost below and on the top wall (update_boundary_uvwhxyz :232-235, :281-282)
+    template <int CDS> __device__ __forceinline__ R whx(int i, int j, int k) const {
+        if (k < 0 || k >= g.nz - 1) return R(0);
+        if (CDS == 1) return R(0.5) * (W(i + 1, j, k) + W(i, j, k));
+        return (-W(i + 2, j, k) + R(9) * W(i + 1, j, k) + R(9) * W(i, j, k) - W(i - 1, j, k)) * R(0.0625);
+    }
+    template <int CDS> __device__ __forceinline__ R why(int i, int j, int k) const {
+        if (k < 0 || k >= g.nz - 1) return R(0);
+        if (CDS == 1) return R(0.5) * (W(i, j + 1, k) + W(i, j, k));
+        return (-W(i, j + 2, k) + R(9) * W(i, j + 1, k) + R(9) * W(i, j, k) - W(i, j - 1, k)) * R(0.0625);
+    }
+    // uhz/vhz: linear in z; wall value below, wall (closed) or surface value (open) on top
+    __device__ __forceinline__ R uhz(int i, int j, int k) const {
+        if (k < 0) return -um;
+        if (k >= g.nz - 1) return closed ? -um : U(i, j, g.nz - 1);
+        R l = lt(k);
+        return U(i, j, k + 1) * l + U(i, j, k) * (R(1) - l);
+    }
+    __device__ __forceinline__ R vhz(int i, int j, int k) const {
+        if (k < 0) return R(0);
+        if (k >= g.nz - 1) return closed ? R(0) : V(i, j, g.nz - 1);
+        R l = lt(k);
+        return V(i, j, k + 1) * l + V(i, j, k) * (R(1) - l);
+    }
+    // temperature interpolants (get_interp_fields_thxyz :473-512, update_boundary_thxyz :311-355)
+    template <int CDS> __device__ __forceinline__ R thx(int i, int j, int k) const {
+        if (CDS == 1) return R(0.5) * (T(i + 1, j, k) + T(i, j, k));
+        return (-T(i + 2, j, k) + R(9) * T(i + 1, j, k) + R(9) * T(i, j, k) - T(i - 1, j, k)) * R(0.0625);
+    }
+    template <int CDS> __device__ __forceinline__ R thy(int i, int j, int k) const {
+        if (CDS == 1) return R(0.5) * (T(i, j + 1, k) + T(i, j, k));
+        return (-T(i, j + 2, k) + R(9) * T(i, j + 1, k) + R(9) * T(i, j, k) - T(i, j - 1, k)) * R(0.0625);
+    }
+    __device__ __forceinline__ R thz(int i, int j, int k) const {
+        if (k < 0) return tbot;
+        if (k >= g.nz - 1) return ttop;
+        R l = lt(k);
+        return T(i, j, k + 1) * l + T(i, j, k) * (R(1) - l);
+    }
+};
+
+template <typename R> struct MomArgs {
+    Acc<R> a;
+    R* ff; R* gg; R* hh;          // histories, updated in place (old value read first)
+    R* qu; R* qv; R* qw;
+    R* uhx_s; R* vhy_s;           // stats snapshot of uhx, vhy (may be null)
+    double rk_a, rk_b, rk_c;
+    Phys ph;
+    const DevScalars* sc;
+};
+
+// get_momentum_cnvdiff (src/module_cnvdiff.f90:35-374)
+template <typename R, int CDS>
+__global__ void __launch_bounds__(256) k_rhs_momentum(MomArgs<R> m)
+{
+    const Acc<R>& A = m.a;
+    const Geo& g = A.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+
+    const R dx = (R)g.dx, dy = (R)g.dy, dx2 = (R)g.dx2, dy2 = (R)g.dy2;
+    const R dt = (R)m.ph.dt, nu = (R)m.ph.nu, um = A.um, fc = (R)m.ph.fc;
+    const R rka = (R)m.rk_a, rkb = (R)m.rk_b, rkc = (R)m.rk_c;
+    const R dz = (R)ldz(g.z.dz, k), dzt = (R)ldz(g.z.dz_t, k), dzb = (R)ldz(g.z.dz_b, k);
+    const R cdif = rkc * R(0.5) * dt * nu;
+    const R dpx = (R)m.sc->dpx_drive;
+
+    // ---------------- U ----------------
+    {
+        R uux, uvy, ux, uxx, uyy, dpdx;
+        if (CDS == 1) {
+            R h1 = A.template uhx<1>(i + 1, j, k), h0 = A.template uhx<1>(i, j, k);
+            uux = (h1 * h1 - h0 * h0) / dx;
+            uvy = (A.template uhy<1>(i, j, k) * A.template vhx<1>(i, j, k) -
+                   A.template uhy<1>(i, j - 1, k) * A.template vhx<1>(i, j - 1, k)) / dy;
+            ux = (h1 - h0) / dx;
+            uxx = (A.U(i + 1, j, k) - R(2) * A.U(i, j, k) + A.U(i - 1, j, k)) / dx2;
+            uyy = (A.U(i, j + 1, k) - R(2) * A.U(i, j, k) + A.U(i, j - 1, k)) / dy2;
+            dpdx = (A.P(i + 1, j, k) - A.P(i, j, k)) / dx;
+        } else {
+            R h2 = A.template uhx<2>(i + 2, j, k), h1 = A.template uhx<2>(i + 1, j, k);
+            R h0 = A.template uhx<2>(i, j, k), hm = A.template uhx<2>(i - 1, j, k);
+            uux = (-h2 * h2 + R(27) * h1 * h1 - R(27) * h0 * h0 + hm * hm) / R(24) / dx;
+            uvy = (-A.template uhy<2>(i, j + 1, k) * A.template vhx<2>(i, j + 1, k) +
+                   R(27) * A.template uhy<2>(i, j, k) * A.template vhx<2>(i, j, k) -
+                   R(27) * A.template uhy<2>(i, j - 1, k) * A.template vhx<2>(i, j - 1, k) +
+                   A.template uhy<2>(i, j - 2, k) * A.template vhx<2>(i, j - 2, k)) / R(24) / dy;
+            ux = (-h2 + R(27) * h1 - R(27) * h0 + hm) / R(24) / dx;
+            uxx = (-A.U(i + 2, j, k) + R(16) * A.U(i + 1, j, k) - R(30) * A.U(i, j, k) + R(16) * A.U(i - 1, j, k) - A.U(i - 2, j, k)) / R(12) / dx2;
+            uyy = (-A.U(i, j + 2, k) + R(16) * A.U(i, j + 1, k) - R(30) * A.U(i, j, k) + R(16) * A.U(i, j - 1, k) - A.U(i, j - 2, k)) / R(12) / dy2;
+            dpdx = (-A.P(i + 2, j, k) + R(27) * A.P(i + 1, j, k) - R(27) * A.P(i, j, k) + A.P(i - 1, j, k)) / R(24) / dx;
+        }
+        R uwz = (A.uhz(i, j, k) * A.template whx<CDS>(i, j, k) - A.uhz(i, j, k - 1) * A.template whx<CDS>(i, j, k - 1)) / dz;
+        R uc = A.U(i, j, k);
+        R uzz = ((A.U(i, j, k + 1) - uc) / dzt - (uc - A.U(i, j, k - 1)) / dzb) / dz;
+        R f;
+        if (m.ph.dp_opt == 3)
+            f = -uux - uvy - uwz - um * ux + fc * (R(0.5) * (A.template vhx<CDS>(i, j, k) + A.template vhx<CDS>(i, j - 1, k)) - (R)m.ph.vg);
+        else
+            f = -uux - uvy - uwz + dpx - um * ux;
+        R f0 = m.ff[id];
+        m.ff[id] = f;
+        m.qu[id] = uc + dt * (rka * f + rkb * f0) + cdif * (uxx + uyy + uzz) - rkc * dt * dpdx;
+        if (m.uhx_s) m.uhx_s[id] = A.template uhx<CDS>(i, j, k);
+    }
+    // ---------------- V ----------------
+    {
+        R vux, vvy, vx, vxx, vyy, dpdy;
+        if (CDS == 1) {
+            R h0 = A.template vhx<1>(i, j, k), hm = A.template vhx<1>(i - 1, j, k);
+            vux = (h0 * A.template uhy<1>(i, j, k) - hm * A.template uhy<1>(i - 1, j, k)) / dx;
+            R y1 = A.template vhy<1>(i, j + 1, k), y0 = A.template vhy<1>(i, j, k);
+            vvy = (y1 * y1 - y0 * y0) / dy;
+            vx = (h0 - hm) / dx;
+            vxx = (A.V(i + 1, j, k) - R(2) * A.V(i, j, k) + A.V(i - 1, j, k)) / dx2;
+            vyy = (A.V(i, j + 1, k) - R(2) * A.V(i, j, k) + A.V(i, j - 1, k)) / dy2;
+            dpdy = (A.P(i, j + 1, k) - A.P(i, j, k)) / dy;
+        } else {
+            R h1 = A.template vhx<2>(i + 1, j, k), h0 = A.template vhx<2>(i, j, k);
+            R hm = A.template vhx<2>(i - 1, j, k), hm2 = A.template vhx<2>(i - 2, j, k);
+            vux = (-h1 * A.template uhy<2>(i + 1, j, k) + R(27) * h0 * A.template uhy<2>(i, j, k) -
+                   R(27) * hm * A.template uhy<2>(i - 1, j, k) + hm2 * A.template uhy<2>(i - 2, j, k)) / R(24) / dx;
+            R y2 = A.template vhy<2>(i, j + 2, k), y1 = A.template vhy<2>(i, j + 1, k);
+            R y0 = A.template vhy<2>(i, j, k), ym = A.template vhy<2>(i, j - 1, k);
+            vvy = (-y2 * y2 + R(27) * y1 * y1 - R(27) * y0 * y0 + ym * ym) / R(24) / dy;
+            vx = (-h1 + R(27) * h0 - R(27) * hm + hm2) / R(24) / dx;
+            vxx = (-A.V(i + 2, j, k) + R(16) * A.V(i + 1, j, k) - R(30) * A.V(i, j, k) + R(16) * A.V(i - 1, j, k) - A.V(i - 2, j, k)) / R(12) / dx2;
+            vyy = (-A.V(i, j + 2, k) + R(16) * A.V(i, j + 1, k) - R(30) * A.V(i, j, k) + R(16) * A.V(i, j - 1, k) - A.V(i, j - 2, k)) / R(12) / dy2;
+            dpdy = (-A.P(i, j + 2, k) + R(27) * A.P(i, j + 1, k) - R(27) * A.P(i, j, k) + A.P(i, j - 1, k)) / R(24) / dy;
+        }
+        R vwz = (A.vhz(i, j, k) * A.template why<CDS>(i, j, k) - A.vhz(i, j, k - 1) * A.template why<CDS>(i, j, k - 1)) / dz;
+        R vc = A.V(i, j, k);
+        R vzz = ((A.V(i, j, k + 1) - vc) / dzt - (vc - A.V(i, j, k - 1)) / dzb) / dz;
+        R f;
+        if (m.ph.dp_opt == 3)
+            f = -vux - vvy - vwz - um * vx + fc * ((R)m.ph.ug - R(0.5) * (A.template uhy<CDS>(i, j, k) + A.template uhy<CDS>(i - 1, j, k)) - um);
+        else
+            f = -vux - vvy - vwz - um * vx;
+        R f0 = m.gg[id];
+        m.gg[id] = f;
+        m.qv[id] = vc + dt * (rka * f + rkb * f0) + cdif * (vxx + vyy + vzz) - rkc * dt * dpdy;
+        if (m.vhy_s) m.vhy_s[id] = A.template vhy<CDS>(i, j, k);
+    }
+    // ---------------- W (k <= nz-2; the top-wall level keeps its old hh, qw) ----------------
+    if (k <= g.nz - 2) {
+        R wux, wvy, wx, wxx, wyy;
+        if (CDS == 1) {
+            R h0 = A.template whx<1>(i, j, k), hm = A.template whx<1>(i - 1, j, k);
+            wux = (h0 * A.uhz(i, j, k) - hm * A.uhz(i - 1, j, k)) / dx;
+            wvy = (A.template why<1>(i, j, k) * A.vhz(i, j, k) - A.template why<1>(i, j - 1, k) * A.vhz(i, j - 1, k)) / dy;
+            wx = (h0 - hm) / dx;
+            wxx = (A.W(i + 1, j, k) - R(2) * A.W(i, j, k) + A.W(i - 1, j, k)) / dx2;
+            wyy = (A.W(i, j + 1, k) - R(2) * A.W(i, j, k) + A.W(i, j - 1, k)) / dy2;
+        } else {
+            R h1 = A.template whx<2>(i + 1, j, k), h0 = A.template whx<2>(i, j, k);
+            R hm = A.template whx<2>(i - 1, j, k), hm2 = A.template whx<2>(i - 2, j, k);
+            wux = (-h1 * A.uhz(i + 1, j, k) + R(27) * h0 * A.uhz(i, j, k) - R(27) * hm * A.uhz(i - 1, j, k) +
+                   hm2 * A.uhz(i - 2, j, k)) / R(24) / dx;
+            wvy = (-A.template why<2>(i, j + 1, k) * A.vhz(i, j + 1, k) + R(27) * A.template why<2>(i, j, k) * A.vhz(i, j, k) -
+                   R(27) * A.template why<2>(i, j - 1, k) * A.vhz(i, j - 1, k) + A.template why<2>(i, j - 2, k) * A.vhz(i, j - 2, k)) / R(24) / dy;
+            wx = (-h1 + R(27) * h0 - R(27) * hm + hm2) / R(24) / dx;
+            wxx = (-A.W(i + 2, j, k) + R(16) * A.W(i + 1, j, k) - R(30) * A.W(i, j, k) + R(16) * A.W(i - 1, j, k) - A.W(i - 2, j, k)) / R(12) / dx2;
+            wyy = (-A.W(i, j + 2, k) + R(16) * A.W(i, j + 1, k) - R(30) * A.W(i, j, k) + R(16) * A.W(i, j - 1, k) - A.W(i, j - 2, k)) / R(12) / dy2;
+        }
+        R wc = A.W(i, j, k), wp = A.W(i, j, k + 1), wm = A.W(i, j, k - 1);
+        R a1 = R(0.5) * (wc + wp); a1 = a1 * a1;
+        R a2 = R(0.5) * (wc + wm); a2 = a2 * a2;
+        R wwz = (a1 - a2) / dzt;
+        R dzp = (R)ldz(g.z.dz, k + 1);
+        R wzz = ((wp - wc) / dzp - (wc - wm) / dz) / dzt;
+        R f = -wux - wvy - wwz - um * wx;
+        if (m.ph.isscalar == 1) {
+            R l = A.lt(k);
+            f = f + (R)m.sc->got * ((R(1) - l) * A.T(i, j, k) + l * A.T(i, j, k + 1) - (R)m.ph.t_ref);
+        }
+        R dpdz = (A.P(i, j, k + 1) - A.P(i, j, k)) / dzt;
+        R f0 = m.hh[id];
+        m.hh[id] = f;
+        m.qw[id] = wc + dt * (rka * f + rkb * f0) + cdif * (wxx + wyy + wzz) - rkc * dt * dpdz;
+    }
+}
+
+template <typename R> struct TempArgs {
+    Acc<R> a;
+    R* ss; R* qt;
+    double rk_a, rk_b, rk_c;
+    Phys ph;
+};
+
+// get_temperature_cnvdiff (src/module_cnvdiff.f90:381-473); u, v, w are the
+// projected velocities of this sub-step, t the one from before it.
+template <typename R, int CDS>
+__global__ void __launch_bounds__(256) k_rhs_temperature(TempArgs<R> m)
+{
+    const Acc<R>& A = m.a;
+    const Geo& g = A.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+    const R dx = (R)g.dx, dy = (R)g.dy, dx2 = (R)g.dx2, dy2 = (R)g.dy2;
+    const R dt = (R)m.ph.dt, al = (R)m.ph.alpha, um = A.um;
+    const R dz = (R)ldz(g.z.dz, k), dzt = (R)ldz(g.z.dz_t, k), dzb = (R)ldz(g.z.dz_b, k);
+    R tux, tvy, tx, txx, tyy;
+    if (CDS == 1) {
+        R h0 = A.template thx<1>(i, j, k), hm = A.template thx<1>(i - 1, j, k);
+        tux = (h0 * A.U(i, j, k) - hm * A.U(i - 1, j, k)) / dx;
+        tvy = (A.template thy<1>(i, j, k) * A.V(i, j, k) - A.template thy<1>(i, j - 1, k) * A.V(i, j - 1, k)) / dy;
+        tx = (h0 - hm) / dx;
+        txx = (A.T(i + 1, j, k) - R(2) * A.T(i, j, k) + A.T(i - 1, j, k)) / dx2;
+        tyy = (A.T(i, j + 1, k) - R(2) * A.T(i, j, k) + A.T(i, j - 1, k)) / dy2;
+    } else {
+        R h1 = A.template thx<2>(i + 1, j, k), h0 = A.template thx<2>(i, j, k);
+        R hm = A.template thx<2>(i - 1, j, k), hm2 = A.template thx<2>(i - 2, j, k);
+        tux = (-h1 * A.U(i + 1, j, k) + R(27) * h0 * A.U(i, j, k) - R(27) * hm * A.U(i - 1, j, k) + hm2 * A.U(i - 2, j, k)) / R(24) / dx;
+        tvy = (-A.template thy<2>(i, j + 1, k) * A.V(i, j + 1, k) + R(27) * A.template thy<2>(i, j, k) * A.V(i, j, k) -
+               R(27) * A.template thy<2>(i, j - 1, k) * A.V(i, j - 1, k) + A.template thy<2>(i, j - 2, k) * A.V(i, j - 2, k)) / R(24) / dy;
+        tx = (-h1 + R(27) * h0 - R(27) * hm + hm2) / R(24) / dx;
+        txx = (-A.T(i + 2, j, k) + R(16) * A.T(i + 1, j, k) - R(30) * A.T(i, j, k) + R(16) * A.T(i - 1, j, k) - A.T(i - 2, j, k)) / R(12) / dx2;
+        tyy = (-A.T(i, j + 2, k) + R(16) * A.T(i, j + 1, k) - R(30) * A.T(i, j, k) + R(16) * A.T(i, j - 1, k) - A.T(i, j - 2, k)) / R(12) / dy2;
+    }
+    R twz = (A.thz(i, j, k) * A.W(i, j, k) - A.thz(i, j, k - 1) * A.W(i, j, k - 1)) / dz;
+    R tc = A.T(i, j, k);
+    R tzz = ((A.T(i, j, k + 1) - tc) / dzt - (tc - A.T(i, j, k - 1)) / dzb) / dz;
+    R s = -tux - tvy - twz - um * tx;
+    R s0 = m.ss[id];
+    m.ss[id] = s;
+    m.qt[id] = tc + dt * ((R)m.rk_a * s + (R)m.rk_b * s0) + (R)m.rk_c * R(0.5) * dt * al * (txx + tyy + tzz);
+}
+
+// ---------------------------------------------------------------------------
+// block reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// keep the value of larger magnitude (ties: the larger value), so that the
+// result does not depend on the reduction order
+__device__ __forceinline__ double absmax_pick(double a, double b)
+{
+    double fa = fabs(a), fb = fabs(b);
+    if (fb > fa || (fb == fa && b > a)) return b;
+    return a;
+}
+__device__ __forceinline__ double warp_absmax(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = absmax_pick(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Divergence check (screen_div_error, src/module_io.f90:85-206): per block
+// sum |div|, the signed div of largest magnitude, and a NaN flag.
+template <typename R, int CDS>
+__global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double* part)
+{
+    __shared__ double s_sum[8], s_max[8];
+    __shared__ int s_nan;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid == 0) s_nan = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    double d = 0.0, ad = 0.0;
+    if (i < g.nx && j < g.ny) {
+        double dudx, dvdy;
+        if (CDS == 1) {
+            dudx = ((double)ldf(f.u, g, i, j, k) - (double)ldf(f.u, g, i - 1, j, k)) / g.dx;
+            dvdy = ((double)ldf(f.v, g, i, j, k) - (double)ldf(f.v, g, i, j - 1, k)) / g.dy;
+        } else {
+            dudx = (-(double)ldf(f.u, g, i + 1, j, k) + 27.0 * (double)ldf(f.u, g, i, j, k) -
+                    27.0 * (double)ldf(f.u, g, i - 1, j, k) + (double)ldf(f.u, g, i - 2, j, k)) / 24.0 / g.dx;
+            dvdy = (-(double)ldf(f.v, g, i, j + 1, k) + 27.0 * (double)ldf(f.v, g, i, j, k) -
+                    27.0 * (double)ldf(f.v, g, i, j - 1, k) + (double)ldf(f.v, g, i, j - 2, k)) / 24.0 / g.dy;
+        }
+        double wc = (double)ldf(f.w, g, i, j, k);
+        double wm = k > 0 ? (double)ldf(f.w, g, i, j, k - 1) : 0.0;
+        double dwdz = (wc - wm) / ldz(g.z.dz, k);
+        d = dudx + dvdy + dwdz;
+        ad = fabs(d);
+        double uc = (double)ldf(f.u, g, i, j, k), vc = (double)ldf(f.v, g, i, j, k);
+        if (uc != uc || vc != vc || wc != wc) s_nan = 1;
+        if (d != d) { d = 0.0; ad = 0.0; s_nan = 1; }
+    }
+    double sm = warp_sum(ad), mx = warp_absmax(d);
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) { s_sum[wid] = sm; s_max[wid] = mx; }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x * blockDim.y) >> 5;
+        sm = lane < nw ? s_sum[lane] : 0.0;
+        mx = lane < nw ? s_max[lane] : 0.0;
+        sm = warp_sum(sm);
+        mx = warp_absmax(mx);
+        if (lane == 0) {
+            const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            part[3 * b + 0] = sm;
+            part[3 * b + 1] = mx;
+            part[3 * b + 2] = s_nan ? 1.0 : 0.0;
+        }
+    }
+}
+
+template <typename R> struct StatsArgs {
+    FieldsIn<R> f;
+    Geo g;
+    const R* uhx_s; const R* vhy_s;     // null on the spectral path: u, v used directly
+    double* mean[11];
+    int accumulate;
+    double um, dt;
+    double* part;                        // per block: sum u*dz, CFL max
+};
+
+// calculate_mean_fields (src/module_tools.f90:362-404 / src/module_spectral.f90:1012-1052)
+// fused with the bulk velocity sum of calculate_ubar (src/module_parameters.f90:513-546)
+// and the CFL of screen_cpu_time (src/module_io.f90:43-61) for the next step.
+template <typename R>
+__global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
+{
+    __shared__ double s_sum[8], s_cfl[8];
+    const Geo& g = s.g;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    double ub = 0.0, cfl = 0.0;
+    if (i < g.nx && j < g.ny) {
+        const long long id = ((long long)k * g.ny + j) * g.nx + i;
+        const double u = (double)s.f.u[id], v = (double)s.f.v[id], w = (double)s.f.w[id];
+        const double dzk = ldz(g.z.dz, k);
+        ub = u * dzk;
+        cfl = s.dt * fabs(u) / g.dx + s.dt * fabs(v) / g.dy + s.dt * fabs(w) / dzk;
+        if (s.accumulate) {
+            const double t = (double)s.f.t[id];
+            const double wm = k > 0 ? (double)s.f.w[id - g.nxy] : 0.0;
+            const double wc = 0.5 * (w + wm);
+            const double ux = s.uhx_s ? (double)s.uhx_s[id] : u;
+            const double vy = s.vhy_s ? (double)s.vhy_s[id] : v;
+            const double um = s.um;
+            s.mean[4][id] += (u + um) * (u + um);
+            s.mean[5][id] += v * v;
+            s.mean[6][id] += w * w;
+            s.mean[7][id] += wc * (ux + um);
+            s.mean[8][id] += wc * vy;
+            s.mean[9][id] += t * t;
+            s.mean[10][id] += t * 0.5 * (w + wm);
+            s.mean[0][id] += u + um;
+            s.mean[1][id] += v;
+            s.mean[2][id] += w;
+            s.mean[3][id] += t;
+        }
+    }
+    ub = warp_sum(ub);
+    cfl = warp_max(cfl);
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) { s_sum[wid] = ub; s_cfl[wid] = cfl; }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x * blockDim.y) >> 5;
+        ub = lane < nw ? s_sum[lane] : 0.0;
+        cfl = lane < nw ? s_cfl[lane] : 0.0;
+        ub = warp_sum(ub);
+        cfl = warp_max(cfl);
+        if (lane == 0) {
+            const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            s.part[2 * b + 0] = ub;
+            s.part[2 * b + 1] = cfl;
+        }
+    }
+}

@@ -1,0 +1,121 @@
+"""GPU parity: the CUDA engine against the CPU FP64 oracle on the same seeded
+inputs, through the C-ABI (ctypes).
+
+Tolerances (written per test): FP64 path <= 1e-10 relative (max-norm over the
+field, divided by the field's max) after 10 steps; FP32-mixed path <= 1e-5.
+"""
+import numpy as np
+import pytest
+
+from hercules_b200 import inputs
+from hercules_b200.params import (Params, config_channel_fd, config_ekman, PREC_MIXED, MEAN_NAMES)
+from parity_util import rel_err, run_pair
+
+FP64_TOL = 1e-10
+MIXED_TOL = 1e-5
+MIXED_P_TOL = 5e-3
+
+
+def small(**kw):
+    base = dict(lx=4.0, ly=3.0, lz=2.0, nx=32, ny=24, nz=17, zstretch=1.0, ochannel=0, dp_opt=1,
+                cds=2, dts=2, nu=1.0 / 300.0, alpha=1.0 / 300.0 / 0.71, dt=2e-3, imax=100)
+    base.update(kw)
+    return Params(**base)
+
+
+CASES = {
+    "fd4_closed_dp2": config_channel_fd(nx=32, ny=24, nz=17),
+    "fd2_closed_dp1": small(cds=1),
+    "fd4_open_scalar": small(ochannel=1, isscalar=1, got=0.5, tbot=-1.0, ttop=0.0),
+    "fd2_open_scalar": small(cds=1, ochannel=1, isscalar=1, got=1.0, tbot=-1.0, ttop=0.0),
+    "fd4_ab2_scalar": small(dts=1, isscalar=1, got=0.2),
+    "fd4_ekman": config_ekman(nx=32, ny=32, nz=17),
+    "fd4_umrf_scalar": small(u_mrf=0.4, isscalar=1, got=0.3, tbot=0.5, ttop=-0.25),
+    "fd4_open_umrf_rivar": small(ochannel=1, u_mrf=-0.2, isscalar=1, is_ri_var=1, ri_str=0.1, ri_end=2.0, imax=20),
+    "fd4_nonsquare_radix": small(nx=48, ny=40, nz=9),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_fd_fp64_parity_10_steps(name, oracle_lib, engine):
+    p = CASES[name]
+    fields = inputs.small_random(p, seed=7)
+    o, od, rc, c, gd = run_pair(p, fields, 10, oracle_lib, engine)
+    assert rc == 0
+    names = ["u", "v", "w", "p"] + (["t", "ss"] if p.isscalar else []) + ["ff", "gg", "hh"]
+    for f in names:
+        e = rel_err(c.download(f), o.get(f))
+        assert e <= FP64_TOL, f"{name}: field {f} rel err {e:.3e}"
+    for f in MEAN_NAMES:
+        b = o.get(f)
+        if np.max(np.abs(b)) == 0:
+            continue
+        e = rel_err(c.download(f), b)
+        assert e <= FP64_TOL, f"{name}: {f} rel err {e:.3e}"
+    for a, b in zip(gd, od):
+        assert a["step"] == b["step"]
+        assert abs(a["time_sim"] - b["time_sim"]) <= 1e-12
+        assert abs(a["cfl"] - b["cfl"]) <= FP64_TOL * max(1.0, abs(b["cfl"]))
+        assert abs(a["dpx_drive"] - b["dpx_drive"]) <= FP64_TOL * max(1.0, abs(b["dpx_drive"]))
+        assert abs(a["ubar"] - b["ubar"]) <= FP64_TOL * max(1.0, abs(b["ubar"]))
+        assert abs(a["got"] - b["got"]) <= 1e-12 * max(1.0, abs(b["got"]))
+        # divergence is round-off on both sides
+        assert a["div_avg"] < 1e-9 and abs(a["div_max"]) < 1e-8
+        assert a["nan_flag"] == 0
+    c.close()
+    o.close()
+
+
+@pytest.mark.gpu
+def test_config1_full_size_fp64_10_steps(oracle_lib, engine):
+    """96x64x64 closed channel, FD4, RK3, dp_opt=2 from the seeded Poiseuille+10% start."""
+    p = config_channel_fd()
+    fields = inputs.poiseuille_noise(p, seed=1)
+    o, od, rc, c, gd = run_pair(p, fields, 10, oracle_lib, engine)
+    assert rc == 0
+    for f in ["u", "v", "w", "p", "ff", "gg", "hh"] + MEAN_NAMES[:3] + MEAN_NAMES[4:9]:
+        e = rel_err(c.download(f), o.get(f))
+        assert e <= FP64_TOL, f"field {f} rel err {e:.3e}"
+    assert abs(gd[-1]["ubar"] - od[-1]["ubar"]) <= 1e-12
+    assert gd[-1]["div_avg"] < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["fd4_closed_dp2", "fd4_open_scalar"])
+def test_fd_mixed_precision_10_steps(name, oracle_lib, engine):
+    p = CASES[name].replace(precision=PREC_MIXED)
+    fields = inputs.small_random(p, seed=3)
+    o, od, rc, c, gd = run_pair(p, fields, 10, oracle_lib, engine)
+    assert rc == 0
+    for f in ["u", "v", "w"] + (["t"] if p.isscalar else []):
+        e = rel_err(c.download(f), o.get(f))
+        assert e <= MIXED_TOL, f"{name}: field {f} rel err {e:.3e}"
+    # Pressure: FP32 storage of u leaves a discrete divergence of ~1e-6 that every
+    # projection turns into phi; the pressure therefore carries ~1e-3 relative
+    # noise in the mixed mode (stated tolerance 5e-3, velocities above 1e-5).
+    pg, po = c.download("p"), o.get("p")
+    e = rel_err(pg - pg.mean(), po - po.mean())
+    assert e <= MIXED_P_TOL, f"{name}: p rel err {e:.3e}"
+    assert gd[-1]["div_avg"] < 1e-3
+
+
+@pytest.mark.gpu
+def test_nan_is_reported_not_fatal(oracle_lib, engine):
+    """A NaN planted in an input field ends hc_step with HC_ERR_NAN; the handle
+    and the context stay usable (reference: print + stop, src/module_io.f90:135-140)."""
+    p = small()
+    fields = inputs.small_random(p, seed=1)
+    fields["u"][3, 4, 5] = np.nan
+    c = engine.Channel(p)
+    c.load(fields)
+    c.initialize()
+    with pytest.raises(engine.HerculesError) as ei:
+        c.step(2)
+    assert ei.value.code == -5
+    c.close()
+    c2 = engine.Channel(p)
+    c2.load(inputs.small_random(p, seed=1))
+    c2.initialize()
+    d = c2.step(1)
+    assert d[0]["nan_flag"] == 0
