@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark of the HERCULES time step on B200: gridpoint-steps/s, mixed vs FP64.
+
+Workload: neutral closed channel, 4th-order FD horizontally, RK3, constant
+flow-rate forcing, tanh-stretched wall-normal grid, 512x384x256, seeded laminar
+Poiseuille + 10% uniform noise (synthetic: no dataset is involved).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A "step" is one full time step (3 RK sub-steps with 15 Helmholtz/Poisson column
+solves, 5 forward + 5 inverse 2-D FFT pairs, statistics). `value` is the
+FP32-mixed throughput summed over all ranks; the FP64 run of the same workload
+is reported beside it with the mixed-vs-FP64 error. N>1 runs independent
+replicas, one per GPU (the north star keeps one domain on one GPU), so the
+scaling is weak. --impl reference times the CPU restatement of the reference's
+step (the Fortran/MPI reference cannot be built in this image) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "channel_fd4_512x384x256": (512, 384, 256),
+    "channel_fd4_256x256x128": (256, 256, 128),
+    "channel_fd4_96x64x64": (96, 64, 64),
+}
+DEFAULT_WORKLOAD = "channel_fd4_512x384x256"
+# CPU samples of the same physics, sized for 10-30 s of host work
+CPU_SAMPLE_GRID = (512, 384, 32)
+REF_STEP_GRID = (256, 192, 32)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    lrank = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, lrank
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, idx: int):
+        self.idx = idx
+        self.p = None
+        self.path = os.path.join("/tmp", f"hc_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        seen = set()
+        for r in rows:
+            for nm, v in zip(names, r[2]):
+                if v.lower().startswith("active"):
+                    seen.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(seen), "samples": len(rows)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# algorithmic words per grid point per launch of each kernel (FD path, neutral);
+# physical fields and half spectra both count one word per point
+ALG_WORDS = {"rhs_momentum": 13, "fft_x_r2c": 6, "fft_y_fwd": 6, "column_fd": 7, "fft_y_inv": 8,
+             "fft_x_c2r": 9, "div_check": 3}
+
+
+def alg_bytes(kernel: str, npts: int, wbytes: int) -> float:
+    if kernel == "stats":
+        # reads u, v, w, t, uhx, vhy in the storage type; 11 FP64 accumulators RMW
+        return npts * (6 * wbytes + 22 * 8)
+    return ALG_WORDS.get(kernel, 0) * npts * wbytes
+
+
+def run_gpu(args, ws, rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from hercules_b200 import engine, inputs
+    from hercules_b200.params import config_channel_fd, PREC_FP64, PREC_MIXED
+
+    nx, ny, nz = WORKLOADS[args.workload]
+    npts = nx * ny * nz
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    chans = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        p = config_channel_fd(nx, ny, nz, precision=prec)
+        c = engine.Channel(p)
+        c.load(inputs.poiseuille_noise(p, seed=3))
+        c.initialize()
+        rc = c.step_nodiag(args.warmup)
+        assert rc == 0, rc
+        barrier()
+        clk = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+        with clk:
+            barrier()
+            rc = c.step_nodiag(args.steps)
+            barrier()
+        assert rc == 0, rc
+        ms = max_over_ranks(c.last_ms)
+        results[prec] = {"ms_per_step": ms / args.steps, "launches": c.last_launches,
+                         "value": ws * npts * args.steps / (ms * 1e-3), "clocks": clk.summary()}
+        chans[prec] = c
+
+    # mixed-vs-FP64 error after the same warmup+steps from the same seed
+    err = {}
+    for f in ("u", "v", "w"):
+        a = chans[PREC_MIXED].download(f)
+        b = chans[PREC_FP64].download(f)
+        err[f] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    pm = chans[PREC_MIXED].download("p")
+    pf = chans[PREC_FP64].download("p")
+    err["p"] = float(np.max(np.abs((pm - pm.mean()) - (pf - pf.mean()))) / np.max(np.abs(pf - pf.mean())))
+
+    # per-kernel CUDA-event profile of 2 steps of the headline (mixed) run
+    kern = {}
+    for prec, tag in ((PREC_MIXED, "mixed"), (PREC_FP64, "fp64")):
+        c = chans[prec]
+        c.set_profiling(True)
+        c.step_nodiag(2)
+        prof = c.kernel_profile()
+        c.set_profiling(False)
+        wb = 4 if prec == PREC_MIXED else 8
+        kern[tag] = {}
+        for k, v in prof.items():
+            avg = v["total_ms"] / max(v["launches"], 1)
+            b = alg_bytes(k, npts, wb)
+            kern[tag][k] = {"launches": v["launches"], "avg_ms": avg,
+                            "alg_gbs": (b / (avg * 1e-3) / 1e9) if b and avg > 0 else None}
+    for c in chans.values():
+        c.close()
+
+    # end-to-end through the public API with host buffers (mixed)
+    e2e = None
+    if not args.no_e2e:
+        p = config_channel_fd(nx, ny, nz, precision=PREC_MIXED)
+        host = inputs.poiseuille_noise(p, seed=3)
+        host = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in host.items()}
+        barrier()
+        t0 = time.perf_counter()
+        c = engine.Channel(p)
+        c.load(host)
+        c.initialize()
+        for _ in range(args.steps):
+            c.step(1)
+        outs = {f: c.download(f) for f in ("u", "v", "w", "p", "t")}
+        barrier()
+        t1 = time.perf_counter()
+        c.close()
+        el = max_over_ranks(t1 - t0)
+        from hercules_b200.params import HcDiag
+        import ctypes
+        e2e = {"value": ws * npts * args.steps / el, "unit": "gridpoint-steps/s",
+               "h2d_bytes_per_step": int(5 * npts * 8 / args.steps),
+               "d2h_bytes_per_step": int((5 * npts * 8) / args.steps + ctypes.sizeof(HcDiag)),
+               "includes": "create + upload of 5 host fields + initialize + K x (hc_step(1) with diag "
+                           "copy-back) + download of 5 fields, wall clock"}
+        del outs
+
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return results, err, kern, e2e
+
+
+def cpu_oracle_rate(grid, steps, warm=1):
+    """Time the CPU restatement of the reference step (OpenMP, all host cores)."""
+    from oracle import oracle as O
+    from hercules_b200 import inputs
+    from hercules_b200.params import config_channel_fd
+    nx, ny, nz = grid
+    p = config_channel_fd(nx, ny, nz)
+    o = O.Oracle(p)
+    o.load(inputs.poiseuille_noise(p, seed=3))
+    o.initialize()
+    o.step(warm)
+    t0 = time.perf_counter()
+    rc, _ = o.step(steps)
+    el = time.perf_counter() - t0
+    o.close()
+    return nx * ny * nz * steps / el, el
+
+
+def main():
+    args = parse()
+    ws, rank, lrank = dist_env()
+    if ws > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(lrank)
+    nx, ny, nz = WORKLOADS[args.workload]
+    ncores = os.cpu_count() or 1
+    hbm, peak_kind = peaks()
+    base = {"metric": "gridpoint-steps/s mixed vs FP64 at stated err (1 B200)", "unit": "gridpoint-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded Poiseuille + 10% uniform noise)"}
+    cfg = {"workload": args.workload, "grid": [nx, ny, nz], "physics": "neutral closed channel, FD4 horizontal, "
+           "FD2 vertical, RK3, dp_opt=2, nu=1/2800, dt=1e-3, zstretch=1", "parallelism": f"replicas x{args.gpus}",
+           "l2": "working set larger than L2 (one FP64 field 403 MB, FP32 201 MB)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle as O
+        O.build()
+        g = REF_STEP_GRID
+        from hercules_b200.params import config_channel_fd
+        rate_w, _ = cpu_oracle_rate(g, max(args.warmup, 1), warm=0) if args.warmup else (None, 0)
+        rate, el = cpu_oracle_rate(g, args.steps, warm=0)
+        line = dict(base)
+        line.update({"impl": "reference", "value": rate, "ms_per_step": el / args.steps * 1e3,
+                     "dtype": "f64", "config": dict(cfg, sample_grid=list(g)),
+                     "cpu_baseline": {"value": rate, "unit": "gridpoint-steps/s", "cores": ncores, "kind": "port",
+                                      "sample": f"{args.steps} steps of the same physics on {g[0]}x{g[1]}x{g[2]} "
+                                                "(the reference's Fortran/MPI code cannot be built here: no gfortran/MPI)"},
+                     "e2e": {"value": rate, "unit": "gridpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        print(json.dumps(line), flush=True)
+        return
+
+    results, err, kern, e2e = run_gpu(args, ws, rank)
+    if rank != 0:
+        return
+    from hercules_b200.params import PREC_FP64, PREC_MIXED
+    mixed, fp64 = results[PREC_MIXED], results[PREC_FP64]
+    # dominant kernel of the headline run and its roofline
+    km = kern["mixed"]
+    dom = max((k for k in km if ALG_WORDS.get(k) or k == "stats"), key=lambda k: km[k]["avg_ms"] * km[k]["launches"])
+    ach = km[dom]["alg_gbs"]
+    roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm if ach else None, "peak_kind": peak_kind, "traffic": None,
+            "alg_bytes_per_launch": alg_bytes(dom, nx * ny * nz, 4),
+            "step_frac_of_hbm": 580.0 * mixed["value"] / args.gpus / (hbm * 1e9),
+            "step_frac_fp64": 1048.0 * fp64["value"] / args.gpus / (hbm * 1e9)}
+    cpu = None
+    if not args.no_cpu_baseline and args.gpus == 1:
+        rate, el = cpu_oracle_rate(CPU_SAMPLE_GRID, 1)
+        cpu = {"value": rate, "unit": "gridpoint-steps/s", "cores": ncores, "kind": "port",
+               "sample": f"1 step of the same physics on {CPU_SAMPLE_GRID[0]}x{CPU_SAMPLE_GRID[1]}x{CPU_SAMPLE_GRID[2]} "
+                         f"({el:.1f} s, OpenMP)"}
+    line = dict(base)
+    line.update({"value": mixed["value"], "ms_per_step": mixed["ms_per_step"], "dtype": "f32 fields/FFT + f64 Thomas",
+                 "config": cfg, "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"]},
+                 "mixed_speedup_vs_fp64": fp64["ms_per_step"] / mixed["ms_per_step"],
+                 "err_vs_fp64": err, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                 "gpu_launches": int(mixed["launches"]), "clocks": mixed["clocks"], "clocks_fp64": fp64["clocks"],
+                 "kernels": kern})
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

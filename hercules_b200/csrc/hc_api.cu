@@ -20,6 +20,7 @@
 #include "hc_fd.cuh"
 #include "hc_fft.cuh"
 #include "hc_column.cuh"
+#include "hc_rhs_tiled.cuh"
 
 // ---------------------------------------------------------------------------
 // small device kernels for the scalar state
@@ -181,6 +182,13 @@ __global__ void k_convert_in(const double* src, R* dst, long long n)
 // ---------------------------------------------------------------------------
 enum { F_U, F_V, F_W, F_P, F_T, F_FF, F_GG, F_HH, F_SS, F_QU, F_QV, F_QW, F_UHX, F_VHY, NFLD };
 
+// kernel categories for the optional per-launch CUDA-event profile
+enum { K_BEGIN, K_RHS_MOM, K_FFT_X_FWD, K_FFT_Y_FWD, K_COLUMN, K_FFT_Y_INV, K_FFT_X_INV,
+       K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_NCAT };
+static const char* K_NAMES[K_NCAT] = {"substep_begin", "rhs_momentum", "fft_x_r2c", "fft_y_fwd", "column_fd",
+                                      "fft_y_inv", "fft_x_c2r", "rhs_temperature", "column_t", "div_check",
+                                      "stats", "finalize"};
+
 struct hc_handle {
     hc_params p;
     int dev;
@@ -198,14 +206,14 @@ struct hc_handle {
     ColScratch cs;
     double* part_div;
     double* part_st;
-    long long nbd, nbs;
+    long long nbd, nbs, stx, sty;
     DevScalars* sc;
     hc_diag* diag_dev;
     int diag_cap;
     double2* twbuf;
     FftPlan px, py;
     double2* wpack;
-    int rows_x, tl_y;
+    int rows_x, tl_y, col_threads;
     size_t smem_x, smem_y;
     double dpx_coef;
     cudaEvent_t e0, e1;
@@ -213,10 +221,56 @@ struct hc_handle {
     long long launches;
     int initialized;
     std::vector<double> zhost[5];
+    // profiling: an event pair per launch, summed per category at the end of hc_step
+    int prof;
+    int cur_cat;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_cat;
+    size_t ev_used;
+    double cat_ms[K_NCAT];
+    long long cat_n[K_NCAT];
 };
 
 #define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { fprintf(stderr, "hercules_b200: %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); return HC_ERR_CUDA; } } while (0)
-#define CKL() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) { fprintf(stderr, "hercules_b200: launch %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); return HC_ERR_CUDA; } ++h->launches; } while (0)
+#define CKL() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) { fprintf(stderr, "hercules_b200: launch %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); return HC_ERR_CUDA; } ++h->launches; prof_end(h); } while (0)
+
+// Start-of-launch marker (no-op unless profiling): records an event on the
+// handle's stream and remembers the category; CKL() records the matching end.
+static int prof_begin(hc_handle* h, int cat)
+{
+    if (!h->prof) return HC_OK;
+    if (h->ev_used + 2 > h->ev_pool.size()) {
+        for (int q = 0; q < 256; ++q) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return HC_ERR_CUDA;
+            h->ev_pool.push_back(e);
+        }
+        h->ev_cat.resize(h->ev_pool.size() / 2 + 1);
+    }
+    h->cur_cat = cat;
+    cudaEventRecord(h->ev_pool[h->ev_used], h->st);
+    return HC_OK;
+}
+static void prof_end(hc_handle* h)
+{
+    if (!h->prof) return;
+    cudaEventRecord(h->ev_pool[h->ev_used + 1], h->st);
+    h->ev_cat[h->ev_used / 2] = h->cur_cat;
+    h->ev_used += 2;
+}
+static int prof_collect(hc_handle* h)
+{
+    if (!h->prof || h->ev_used == 0) return HC_OK;
+    CK(cudaStreamSynchronize(h->st));
+    for (size_t q = 0; q < h->ev_used; q += 2) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, h->ev_pool[q], h->ev_pool[q + 1]));
+        h->cat_ms[h->ev_cat[q / 2]] += ms;
+        h->cat_n[h->ev_cat[q / 2]] += 1;
+    }
+    h->ev_used = 0;
+    return HC_OK;
+}
 
 static int factor_plan(int n, FftPlan* pl)
 {
@@ -405,9 +459,13 @@ static int build_fft(hc_handle* h)
     h->py.tw = h->twbuf + nxh;
     h->wpack = h->twbuf + nxh + ny;
     const size_t c2 = 2 * h->rsz;     // bytes of one complex
-    h->rows_x = 2048 / nxh; if (h->rows_x < 1) h->rows_x = 1; if (h->rows_x > 64) h->rows_x = 64;
+    h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : 2048 / nxh;
+    if (h->rows_x < 1) h->rows_x = 1; if (h->rows_x > 64) h->rows_x = 64;
     h->smem_x = 2 * (size_t)h->rows_x * nxh * c2;
-    h->tl_y = 2048 / ny; if (h->tl_y < 2) h->tl_y = 2; if (h->tl_y > 16) h->tl_y = 16; if (h->tl_y > nxh) h->tl_y = nxh;
+    h->col_threads = h->p.tile[3] > 0 ? h->p.tile[3] : 128;
+    if (h->col_threads < 32 || h->col_threads > 256 || (h->col_threads & 31)) return HC_ERR_PARAM;
+    h->tl_y = h->p.tile[1] > 0 ? h->p.tile[1] : 2048 / ny;
+    if (h->tl_y < 1) h->tl_y = 1; if (h->tl_y > 32) h->tl_y = 32; if (h->tl_y > nxh) h->tl_y = nxh;
     h->smem_y = 2 * (size_t)h->tl_y * (ny + 1) * c2;
     if (h->smem_x > 200 * 1024 || h->smem_y > 200 * 1024) return HC_ERR_UNSUPPORTED;
     return HC_OK;
@@ -419,6 +477,8 @@ template <typename R> static int set_smem_attrs()
     CK(cudaFuncSetAttribute(k_fft_x_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(k_fft_y<R, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(k_fft_y<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
+    CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     return HC_OK;
 }
 
@@ -449,6 +509,7 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     ax.nrows = (long long)h->g.ny * h->g.nz;
     ax.rows = h->rows_x; ax.pl = h->px; ax.wpack = h->wpack; ax.scale = 1.0 / h->p.nx; ax.halt = halt;
     dim3 gx((unsigned)((ax.nrows + ax.rows - 1) / ax.rows), nf, 1);
+    prof_begin(h, K_FFT_X_FWD);
     k_fft_x_r2c<R><<<gx, 256, h->smem_x, h->st>>>(ax);
     CKL();
     FftYArgs<R> ay;
@@ -456,6 +517,7 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     for (int f = 0; f < nf; ++f) ay.data[f] = out[f];
     ay.nxh = h->g.nxh; ay.ny = h->g.ny; ay.tl = h->tl_y; ay.pl = h->py; ay.scale = 1.0 / h->p.ny; ay.halt = halt;
     dim3 gy((h->g.nxh + ay.tl - 1) / ay.tl, h->g.nz, nf);
+    prof_begin(h, K_FFT_Y_FWD);
     k_fft_y<R, -1><<<gy, 256, h->smem_y, h->st>>>(ay);
     CKL();
     (void)sizeof(T2);
@@ -470,6 +532,7 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
     for (int f = 0; f < nf; ++f) ay.data[f] = in[f];
     ay.nxh = h->g.nxh; ay.ny = h->g.ny; ay.tl = h->tl_y; ay.pl = h->py; ay.scale = 1.0; ay.halt = halt;
     dim3 gy((h->g.nxh + ay.tl - 1) / ay.tl, h->g.nz, nf);
+    prof_begin(h, K_FFT_Y_INV);
     k_fft_y<R, 1><<<gy, 256, h->smem_y, h->st>>>(ay);
     CKL();
     FftXInvArgs<R> ax;
@@ -478,6 +541,7 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
     ax.nrows = (long long)h->g.ny * h->g.nz;
     ax.rows = h->rows_x; ax.pl = h->px; ax.wpack = h->wpack; ax.halt = halt;
     dim3 gx((unsigned)((ax.nrows + ax.rows - 1) / ax.rows), nf, 1);
+    prof_begin(h, K_FFT_X_INV);
     k_fft_x_c2r<R><<<gx, 256, h->smem_x, h->st>>>(ax);
     CKL();
     return HC_OK;
@@ -499,7 +563,8 @@ template <typename R> static int launch_stats(hc_handle* h, int accumulate)
     s.accumulate = accumulate;
     s.um = h->p.u_mrf; s.dt = h->p.dt;
     s.part = h->part_st;
-    k_stats<R><<<pt_grid(h->g), pt_block(), 0, h->st>>>(s);
+    prof_begin(h, K_STATS);
+    k_stats<R><<<dim3((unsigned)h->stx, (unsigned)h->sty), 256, 0, h->st>>>(s);
     CKL();
     return HC_OK;
 }
@@ -513,6 +578,7 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base
     f.nx = h->p.nx; f.ny = h->p.ny; f.nz = h->p.nz; f.lz = h->p.lz;
     f.dp_opt = h->p.dp_opt; f.diag = h->diag_dev; f.step_base = step_base; f.write_diag = write_diag;
     f.cds = h->p.cds;
+    prof_begin(h, K_FINAL);
     k_finalize<<<1, 256, 0, h->st>>>(f);
     CKL();
     return HC_OK;
@@ -531,18 +597,34 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     ScalarArgs sa;
     sa.sc = h->sc; sa.sub = sub; sa.dt = p.dt; sa.dp_opt = p.dp_opt; sa.dpx_coef = h->dpx_coef; sa.um = p.u_mrf;
     sa.is_ri_var = p.is_ri_var; sa.ri_str = p.ri_str; sa.ri_end = p.ri_end; sa.imax = p.imax;
+    prof_begin(h, K_BEGIN);
     k_substep_begin<<<1, 1, 0, h->st>>>(sa);
     CKL();
 
-    // momentum RHS
-    MomArgs<R> m;
-    m.a = make_acc<R>(h);
+    // momentum RHS (SMEM-tiled, marching in k)
+    RhsTArgs<R> m;
+    m.f.u = (const R*)h->fld[F_U]; m.f.v = (const R*)h->fld[F_V]; m.f.w = (const R*)h->fld[F_W];
+    m.f.p = (const R*)h->fld[F_P]; m.f.t = (const R*)h->fld[F_T];
+    m.g = h->g;
     m.ff = (R*)h->fld[F_FF]; m.gg = (R*)h->fld[F_GG]; m.hh = (R*)h->fld[F_HH];
     m.qu = (R*)h->fld[F_QU]; m.qv = (R*)h->fld[F_QV]; m.qw = (R*)h->fld[F_QW];
     m.uhx_s = last ? (R*)h->fld[F_UHX] : nullptr; m.vhy_s = last ? (R*)h->fld[F_VHY] : nullptr;
     m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph; m.sc = h->sc;
-    k_rhs_momentum<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
-    CKL();
+    m.with_t = p.isscalar == 1;
+    {
+        const int bx = (h->g.nx + RT_TX - 1) / RT_TX, by = (h->g.ny + RT_TY - 1) / RT_TY;
+        // enough blocks for ~4 per SM, chunks of 4..32 levels
+        long long want = 4LL * 148;
+        int kc = p.tile[2] > 0 ? p.tile[2] : (int)((long long)bx * by * p.nz / want);
+        if (p.tile[2] <= 0) { if (kc < 4) kc = 4; if (kc > 32) kc = 32; }
+        if (kc < 1) kc = 1;
+        if (kc > p.nz) kc = p.nz;
+        m.kchunk = kc;
+        dim3 gr(bx, by, (p.nz + kc - 1) / kc);
+        prof_begin(h, K_RHS_MOM);
+        k_rhs_momentum_tiled<R, CDS><<<gr, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
+        CKL();
+    }
 
     T2* S[4] = {(T2*)h->spec[0], (T2*)h->spec[1], (T2*)h->spec[2], (T2*)h->spec[3]};
     const R* qin[3] = {(const R*)h->fld[F_QU], (const R*)h->fld[F_QV], (const R*)h->fld[F_QW]};
@@ -565,7 +647,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
         }
     }
     ca.halt = halt;
-    k_column_fd<R><<<(unsigned)((h->g.ncol + 127) / 128), 128, 0, h->st>>>(ca);
+    prof_begin(h, K_COLUMN);
+    k_column_fd<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ca);
     CKL();
 
     R* outs[4] = {(R*)h->fld[F_U], (R*)h->fld[F_V], (R*)h->fld[F_W], (R*)h->fld[F_P]};
@@ -578,6 +661,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
         ta.a = make_acc<R>(h);
         ta.ss = (R*)h->fld[F_SS]; ta.qt = (R*)h->fld[F_QU];
         ta.rk_a = rk_a; ta.rk_b = rk_b; ta.rk_c = rk_c; ta.ph = h->ph;
+        prof_begin(h, K_RHS_T);
         k_rhs_temperature<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(ta);
         CKL();
         const R* tin[1] = {(const R*)h->fld[F_QU]};
@@ -593,7 +677,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
             ct.bct0 = -2.0 * aa_t_zstr * p.tbot;
             ct.bct1 = -2.0 * cc_t_zend * p.ttop;
         }
-        k_column_t<R><<<(unsigned)((h->g.ncol + 127) / 128), 128, 0, h->st>>>(ct);
+        prof_begin(h, K_COLUMN_T);
+        k_column_t<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ct);
         CKL();
         R* tout[1] = {(R*)h->fld[F_T]};
         const int add0[1] = {0};
@@ -604,7 +689,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     FieldsIn<R> fi;
     fi.u = (const R*)h->fld[F_U]; fi.v = (const R*)h->fld[F_V]; fi.w = (const R*)h->fld[F_W];
     fi.p = (const R*)h->fld[F_P]; fi.t = (const R*)h->fld[F_T];
-    k_div_check<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->nbd * 3);
+    prof_begin(h, K_DIV);
+    k_div_check<R, CDS><<<(unsigned)h->nbd, 256, 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->nbd * 3);
     CKL();
     return HC_OK;
 }
@@ -662,6 +748,7 @@ static void free_all(hc_handle* h)
     if (h->sc) cudaFree(h->sc);
     if (h->diag_dev) cudaFree(h->diag_dev);
     if (h->twbuf) cudaFree(h->twbuf);
+    for (size_t q = 0; q < h->ev_pool.size(); ++q) cudaEventDestroy(h->ev_pool[q]);
     if (h->e0) cudaEventDestroy(h->e0);
     if (h->e1) cudaEventDestroy(h->e1);
     if (h->st) cudaStreamDestroy(h->st);
@@ -690,6 +777,8 @@ int hc_create(const hc_params* p, hc_handle** out)
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
     h->diag_cap = 0; h->last_ms = 0.0; h->launches = 0; h->initialized = 0;
+    h->prof = 0; h->cur_cat = 0; h->ev_used = 0;
+    for (int q = 0; q < K_NCAT; ++q) { h->cat_ms[q] = 0.0; h->cat_n[q] = 0; }
     int rc = HC_OK;
 #define FAIL(code) do { rc = (code); goto fail; } while (0)
     {
@@ -730,9 +819,13 @@ int hc_create(const hc_params* p, hc_handle** out)
         if ((rc = build_fft(h)) != HC_OK) goto fail;
         rc = h->rsz == sizeof(float) ? set_smem_attrs<float>() : set_smem_attrs<double>();
         if (rc != HC_OK) goto fail;
-        dim3 gr = pt_grid(g);
-        h->nbd = (long long)gr.x * gr.y * gr.z;
-        h->nbs = h->nbd;
+        h->nbd = (g.n + 255) / 256;
+        if (h->nbd > RED_BLOCKS) h->nbd = RED_BLOCKS;
+        h->stx = (g.nxy + 255) / 256;
+        h->sty = (2 * RED_BLOCKS) / h->stx;
+        if (h->sty < 1) h->sty = 1;
+        if (h->sty > p->nz) h->sty = p->nz;
+        h->nbs = h->stx * h->sty;
         if (cudaMalloc(&h->part_div, 3 * h->nbd * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
         if (cudaMemset(h->part_div, 0, 3 * h->nbd * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
         if (cudaMalloc(&h->part_st, 2 * h->nbs * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
@@ -914,6 +1007,7 @@ int hc_step(hc_handle* h, int nsteps, hc_diag* out)
         for (int q = 0; q < chunk; ++q) {
             rc = h->rsz == sizeof(float) ? step_dispatch<float>(h, base) : step_dispatch<double>(h, base);
             if (rc) return rc;
+            if (h->prof && h->ev_used > 4096) { rc = prof_collect(h); if (rc) return rc; }
         }
         if (out) CK(cudaMemcpyAsync(out + done, h->diag_dev, chunk * sizeof(hc_diag), cudaMemcpyDeviceToHost, h->st));
         done += chunk;
@@ -922,6 +1016,8 @@ int hc_step(hc_handle* h, int nsteps, hc_diag* out)
     CK(cudaEventSynchronize(h->e1));
     CK(cudaEventElapsedTime(&total_ms, h->e0, h->e1));
     h->last_ms = total_ms;
+    rc = prof_collect(h);
+    if (rc) return rc;
     DevScalars s1;
     CK(cudaMemcpy(&s1, h->sc, sizeof(s1), cudaMemcpyDeviceToHost));
     if (s1.nan_flag) return HC_ERR_NAN;
@@ -954,6 +1050,30 @@ int hc_last_launch_count(hc_handle* h, long long* n)
 {
     if (!h || !n) return HC_ERR_ARG;
     *n = h->launches;
+    return HC_OK;
+}
+
+int hc_set_profiling(hc_handle* h, int enable)
+{
+    if (!h) return HC_ERR_ARG;
+    h->prof = enable ? 1 : 0;
+    for (int q = 0; q < K_NCAT; ++q) { h->cat_ms[q] = 0.0; h->cat_n[q] = 0; }
+    h->ev_used = 0;
+    return HC_OK;
+}
+
+int hc_kernel_profile(hc_handle* h, int max, char* names, double* total_ms, long long* launches, int* count)
+{
+    if (!h || !count) return HC_ERR_ARG;
+    int n = 0;
+    for (int q = 0; q < K_NCAT && n < max; ++q) {
+        if (h->cat_n[q] == 0) continue;
+        if (names) { strncpy(names + 32 * n, K_NAMES[q], 31); names[32 * n + 31] = 0; }
+        if (total_ms) total_ms[n] = h->cat_ms[q];
+        if (launches) launches[n] = h->cat_n[q];
+        ++n;
+    }
+    *count = n;
     return HC_OK;
 }
 

@@ -78,7 +78,7 @@ __device__ __forceinline__ double2 zscale(double2 a, double s) { return make_dou
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_column_fd(ColArgs<R> a)
+__global__ void __launch_bounds__(256) k_column_fd(ColArgs<R> a)
 {
     if (a.halt && *a.halt) return;
     const long long ncol = a.g.ncol;
@@ -244,7 +244,7 @@ template <typename R> struct ColTArgs {
 };
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_column_t(ColTArgs<R> a)
+__global__ void __launch_bounds__(256) k_column_t(ColTArgs<R> a)
 {
     if (a.halt && *a.halt) return;
     const long long ncol = a.g.ncol;

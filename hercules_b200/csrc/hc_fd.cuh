@@ -328,6 +328,19 @@ __device__ __forceinline__ double warp_max(double v)
     return v;
 }
 
+// Reductions use a fixed grid of at most RED_BLOCKS blocks that stride over the
+// points, so the partial results (and the order they are combined in) depend on
+// the grid size only: the sums are deterministic from run to run.
+#define RED_BLOCKS 1184
+
+__device__ __forceinline__ void decode_pt(long long q, const Geo& g, int& i, int& j, int& k)
+{
+    i = (int)(q % g.nx);
+    const long long r = q / g.nx;
+    j = (int)(r % g.ny);
+    k = (int)(r / g.ny);
+}
+
 // Divergence check (screen_div_error, src/module_io.f90:85-206): per block
 // sum |div|, the signed div of largest magnitude, and a NaN flag.
 template <typename R, int CDS>
@@ -335,48 +348,48 @@ __global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double*
 {
     __shared__ double s_sum[8], s_max[8];
     __shared__ int s_nan;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int tid = threadIdx.x;
     if (tid == 0) s_nan = 0;
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    double d = 0.0, ad = 0.0;
-    if (i < g.nx && j < g.ny) {
+    const double r24dx = 1.0 / (24.0 * g.dx), r24dy = 1.0 / (24.0 * g.dy), rdx = 1.0 / g.dx, rdy = 1.0 / g.dy;
+    double sm = 0.0, mx = 0.0;
+    int nan = 0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + tid; q < g.n; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode_pt(q, g, i, j, k);
         double dudx, dvdy;
+        const double uc = (double)f.u[q], vc = (double)f.v[q], wc = (double)f.w[q];
         if (CDS == 1) {
-            dudx = ((double)ldf(f.u, g, i, j, k) - (double)ldf(f.u, g, i - 1, j, k)) / g.dx;
-            dvdy = ((double)ldf(f.v, g, i, j, k) - (double)ldf(f.v, g, i, j - 1, k)) / g.dy;
+            dudx = (uc - (double)ldf(f.u, g, i - 1, j, k)) * rdx;
+            dvdy = (vc - (double)ldf(f.v, g, i, j - 1, k)) * rdy;
         } else {
-            dudx = (-(double)ldf(f.u, g, i + 1, j, k) + 27.0 * (double)ldf(f.u, g, i, j, k) -
-                    27.0 * (double)ldf(f.u, g, i - 1, j, k) + (double)ldf(f.u, g, i - 2, j, k)) / 24.0 / g.dx;
-            dvdy = (-(double)ldf(f.v, g, i, j + 1, k) + 27.0 * (double)ldf(f.v, g, i, j, k) -
-                    27.0 * (double)ldf(f.v, g, i, j - 1, k) + (double)ldf(f.v, g, i, j - 2, k)) / 24.0 / g.dy;
+            dudx = (-(double)ldf(f.u, g, i + 1, j, k) + 27.0 * uc - 27.0 * (double)ldf(f.u, g, i - 1, j, k) +
+                    (double)ldf(f.u, g, i - 2, j, k)) * r24dx;
+            dvdy = (-(double)ldf(f.v, g, i, j + 1, k) + 27.0 * vc - 27.0 * (double)ldf(f.v, g, i, j - 1, k) +
+                    (double)ldf(f.v, g, i, j - 2, k)) * r24dy;
         }
-        double wc = (double)ldf(f.w, g, i, j, k);
-        double wm = k > 0 ? (double)ldf(f.w, g, i, j, k - 1) : 0.0;
-        double dwdz = (wc - wm) / ldz(g.z.dz, k);
-        d = dudx + dvdy + dwdz;
-        ad = fabs(d);
-        double uc = (double)ldf(f.u, g, i, j, k), vc = (double)ldf(f.v, g, i, j, k);
-        if (uc != uc || vc != vc || wc != wc) s_nan = 1;
-        if (d != d) { d = 0.0; ad = 0.0; s_nan = 1; }
+        const double wm = k > 0 ? (double)f.w[q - g.nxy] : 0.0;
+        const double d = dudx + dvdy + (wc - wm) / ldz(g.z.dz, k);
+        if (uc != uc || vc != vc || wc != wc || d != d) { nan = 1; continue; }
+        sm += fabs(d);
+        mx = absmax_pick(mx, d);
     }
-    double sm = warp_sum(ad), mx = warp_absmax(d);
+    if (nan) s_nan = 1;
+    sm = warp_sum(sm);
+    mx = warp_absmax(mx);
     const int lane = tid & 31, wid = tid >> 5;
     if (lane == 0) { s_sum[wid] = sm; s_max[wid] = mx; }
     __syncthreads();
     if (wid == 0) {
-        const int nw = (blockDim.x * blockDim.y) >> 5;
+        const int nw = blockDim.x >> 5;
         sm = lane < nw ? s_sum[lane] : 0.0;
         mx = lane < nw ? s_max[lane] : 0.0;
         sm = warp_sum(sm);
         mx = warp_absmax(mx);
         if (lane == 0) {
-            const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-            part[3 * b + 0] = sm;
-            part[3 * b + 1] = mx;
-            part[3 * b + 2] = s_nan ? 1.0 : 0.0;
+            part[3 * blockIdx.x + 0] = sm;
+            part[3 * blockIdx.x + 1] = mx;
+            part[3 * blockIdx.x + 2] = s_nan ? 1.0 : 0.0;
         }
     }
 }
@@ -397,37 +410,41 @@ template <typename R> struct StatsArgs {
 template <typename R>
 __global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
 {
+    // blockIdx.x: 256 consecutive (i,j) points of a plane; blockIdx.y: a chunk of levels
     __shared__ double s_sum[8], s_cfl[8];
     const Geo& g = s.g;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+    const int tid = threadIdx.x;
+    const double rdx = 1.0 / g.dx, rdy = 1.0 / g.dy;
+    const long long ij = (long long)blockIdx.x * blockDim.x + tid;
+    const int kc = (g.nz + gridDim.y - 1) / gridDim.y;
+    const int k0 = blockIdx.y * kc, k1 = min(g.nz, k0 + kc);
     double ub = 0.0, cfl = 0.0;
-    if (i < g.nx && j < g.ny) {
-        const long long id = ((long long)k * g.ny + j) * g.nx + i;
-        const double u = (double)s.f.u[id], v = (double)s.f.v[id], w = (double)s.f.w[id];
-        const double dzk = ldz(g.z.dz, k);
-        ub = u * dzk;
-        cfl = s.dt * fabs(u) / g.dx + s.dt * fabs(v) / g.dy + s.dt * fabs(w) / dzk;
-        if (s.accumulate) {
-            const double t = (double)s.f.t[id];
-            const double wm = k > 0 ? (double)s.f.w[id - g.nxy] : 0.0;
-            const double wc = 0.5 * (w + wm);
-            const double ux = s.uhx_s ? (double)s.uhx_s[id] : u;
-            const double vy = s.vhy_s ? (double)s.vhy_s[id] : v;
-            const double um = s.um;
-            s.mean[4][id] += (u + um) * (u + um);
-            s.mean[5][id] += v * v;
-            s.mean[6][id] += w * w;
-            s.mean[7][id] += wc * (ux + um);
-            s.mean[8][id] += wc * vy;
-            s.mean[9][id] += t * t;
-            s.mean[10][id] += t * 0.5 * (w + wm);
-            s.mean[0][id] += u + um;
-            s.mean[1][id] += v;
-            s.mean[2][id] += w;
-            s.mean[3][id] += t;
+    if (ij < g.nxy) {
+        for (int k = k0; k < k1; ++k) {
+            const long long q = (long long)k * g.nxy + ij;
+            const double u = (double)s.f.u[q], v = (double)s.f.v[q], w = (double)s.f.w[q];
+            const double dzk = ldz(g.z.dz, k);
+            ub += u * dzk;
+            cfl = fmax(cfl, s.dt * fabs(u) * rdx + s.dt * fabs(v) * rdy + s.dt * fabs(w) / dzk);
+            if (s.accumulate) {
+                const double t = (double)s.f.t[q];
+                const double wm = k > 0 ? (double)s.f.w[q - g.nxy] : 0.0;
+                const double wc = 0.5 * (w + wm);
+                const double ux = s.uhx_s ? (double)s.uhx_s[q] : u;
+                const double vy = s.vhy_s ? (double)s.vhy_s[q] : v;
+                const double um = s.um;
+                s.mean[4][q] += (u + um) * (u + um);
+                s.mean[5][q] += v * v;
+                s.mean[6][q] += w * w;
+                s.mean[7][q] += wc * (ux + um);
+                s.mean[8][q] += wc * vy;
+                s.mean[9][q] += t * t;
+                s.mean[10][q] += t * 0.5 * (w + wm);
+                s.mean[0][q] += u + um;
+                s.mean[1][q] += v;
+                s.mean[2][q] += w;
+                s.mean[3][q] += t;
+            }
         }
     }
     ub = warp_sum(ub);
@@ -436,13 +453,13 @@ __global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
     if (lane == 0) { s_sum[wid] = ub; s_cfl[wid] = cfl; }
     __syncthreads();
     if (wid == 0) {
-        const int nw = (blockDim.x * blockDim.y) >> 5;
+        const int nw = blockDim.x >> 5;
         ub = lane < nw ? s_sum[lane] : 0.0;
         cfl = lane < nw ? s_cfl[lane] : 0.0;
         ub = warp_sum(ub);
         cfl = warp_max(cfl);
         if (lane == 0) {
-            const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            const long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
             s.part[2 * b + 0] = ub;
             s.part[2 * b + 1] = cfl;
         }

@@ -29,7 +29,8 @@ HC_ERRORS = {0: "ok", -1: "bad argument", -2: "parameter check failed", -3: "CUD
 # every entry point declared in include/hercules_b200.h
 ABI_SYMBOLS = ["hc_create", "hc_set_grid", "hc_get_grid", "hc_upload", "hc_download",
                "hc_initialize", "hc_step", "hc_get_scalars", "hc_upload_dev", "hc_download_dev",
-               "hc_last_step_ms", "hc_last_launch_count", "hc_destroy", "hc_error_string"]
+               "hc_last_step_ms", "hc_last_launch_count", "hc_set_profiling", "hc_kernel_profile",
+               "hc_destroy", "hc_error_string"]
 
 
 class HerculesError(RuntimeError):
@@ -62,6 +63,8 @@ def load_library(path: str = LIB_PATH):
     L.hc_download_dev.argtypes = [vp, ip, ctypes.c_void_p]
     L.hc_last_step_ms.argtypes = [vp, ctypes.POINTER(dp)]
     L.hc_last_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.hc_set_profiling.argtypes = [vp, ip]
+    L.hc_kernel_profile.argtypes = [vp, ip, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ip)]
     L.hc_destroy.argtypes = [vp]
     L.hc_error_string.argtypes = [ip]
     L.hc_error_string.restype = ctypes.c_char_p
@@ -181,6 +184,23 @@ class Channel:
         v = ctypes.c_longlong()
         _check(self._L.hc_last_launch_count(self.h, ctypes.byref(v)), "hc_last_launch_count")
         return v.value
+
+    def set_profiling(self, enable: bool) -> None:
+        _check(self._L.hc_set_profiling(self.h, 1 if enable else 0), "hc_set_profiling")
+
+    def kernel_profile(self) -> Dict[str, dict]:
+        """Per-kernel launch count and total CUDA-event time since profiling was enabled."""
+        mx = 32
+        names = ctypes.create_string_buffer(32 * mx)
+        ms = (ctypes.c_double * mx)()
+        nl = (ctypes.c_longlong * mx)()
+        cnt = ctypes.c_int()
+        _check(self._L.hc_kernel_profile(self.h, mx, names, ms, nl, ctypes.byref(cnt)), "hc_kernel_profile")
+        out = {}
+        for q in range(cnt.value):
+            nm = names.raw[32 * q:32 * q + 32].split(b"\0")[0].decode()
+            out[nm] = {"launches": nl[q], "total_ms": ms[q]}
+        return out
 
     @property
     def mixed(self) -> bool:

@@ -48,7 +48,8 @@ class HcParams(ctypes.Structure):
         ("is_ri_var", ctypes.c_int),
         ("ri_str", ctypes.c_double), ("ri_end", ctypes.c_double),
         ("precision", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("tile", ctypes.c_int * 4),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 
@@ -124,13 +125,19 @@ class Params:
     isyz2d: int = 0
     yz2d_id: List[int] = field(default_factory=list)
     intv_2d: int = 1000
-    # not a namelist entry: storage/arithmetic precision of the GPU path
+    # not namelist entries: storage/arithmetic precision of the GPU path and the
+    # kernel tile shapes (0 = automatic)
     precision: int = PREC_FP64
+    tile: List[int] = field(default_factory=lambda: [0, 0, 0, 0])
 
     def to_c(self) -> HcParams:
         c = HcParams()
         for name, _ in HcParams._fields_:
             if name == "reserved":
+                continue
+            if name == "tile":
+                for q, v in enumerate(self.tile[:4]):
+                    c.tile[q] = int(v)
                 continue
             setattr(c, name, getattr(self, name))
         return c

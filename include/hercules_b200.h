@@ -91,7 +91,11 @@ typedef struct hc_params {
     int    is_ri_var;
     double ri_str, ri_end;
     int    precision;
-    int    reserved[7];
+    /* tile shapes, 0 = automatic (the autotuner in hercules_b200/autotune.py
+     * writes these): [0] x-FFT rows per block, [1] y-FFT lines per block,
+     * [2] momentum-RHS levels per block, [3] column-solve threads per block */
+    int    tile[4];
+    int    reserved[3];
 } hc_params;
 
 /*
@@ -170,6 +174,16 @@ int hc_last_step_ms(hc_handle* h, double* ms);
 
 /* Number of kernel launches the last hc_step issued. */
 int hc_last_launch_count(hc_handle* h, long long* n);
+
+/* Optional per-launch timing: with profiling on, hc_step brackets every kernel
+ * launch with a CUDA-event pair on the handle's stream and sums the elapsed
+ * times per kernel. No counterpart in the reference (it prints cpu_time only,
+ * src/module_io.f90:72-75). */
+int hc_set_profiling(hc_handle* h, int enable);
+
+/* Per-kernel totals since profiling was enabled: names in 32-byte slots. */
+int hc_kernel_profile(hc_handle* h, int max, char* names, double* total_ms,
+                      long long* launches, int* count);
 
 int hc_destroy(hc_handle* h);
 

@@ -303,9 +303,30 @@ static cplx kx_pois(or_state* s, int l, double h2, cplx w1, double L)
     return -sq(2.0 * PI / L * l);
 }
 
+/* The builders evaluate kx, ky inside their k,j,i loops; the values depend on
+ * the mode only, so they are evaluated once per i and once per j here. */
+typedef struct { cplx* x; cplx* y; } symtab;
+static symtab sym_tables(or_state* s, int pois, double dif)
+{
+    symtab t;
+    t.x = (cplx*)malloc(sizeof(cplx) * (size_t)(s->nx + 1));
+    t.y = (cplx*)malloc(sizeof(cplx) * (size_t)(s->ny + 1));
+    for (int i = 1; i <= s->nx; ++i) {
+        int l = lmap(i, s->nx);
+        t.x[i] = pois ? kx_pois(s, l, s->dx2, s->wx1, s->prm.lx) : kx_helm(s, l, dif, s->dx2, s->wx1, s->prm.lx);
+    }
+    for (int j = 1; j <= s->ny; ++j) {
+        int m = lmap(j, s->ny);
+        t.y[j] = pois ? kx_pois(s, m, s->dy2, s->wy1, s->prm.ly) : kx_helm(s, m, dif, s->dy2, s->wy1, s->prm.ly);
+    }
+    return t;
+}
+static void sym_free(symtab t) { free(t.x); free(t.y); }
+
 /* get_p_eqn_coeff (src/module_poisson_solver.f90:32-122) */
 static void get_p_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
 {
+    symtab tb = sym_tables(s, 1, 0.0);
     for (int k = 1; k <= s->nka; ++k) { aa[k] = 0.0; cc[k] = 0.0; }
     memset(bb, 0, sizeof(cplx) * (size_t)s->nx * s->ny * s->nka);
     for (int k = s->kstr3; k <= s->kend3; ++k) {
@@ -313,20 +334,20 @@ static void get_p_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
         cc[k] = 1.0 / s->dz[k] / s->dz_t[k];
         for (int j = 1; j <= s->ny; ++j)
             for (int i = 1; i <= s->nx; ++i) {
-                int l = lmap(i, s->nx), m = lmap(j, s->ny);
-                cplx kx = kx_pois(s, l, s->dx2, s->wx1, s->prm.lx);
-                cplx ky = kx_pois(s, m, s->dy2, s->wy1, s->prm.ly);
+                cplx kx = tb.x[i], ky = tb.y[j];
                 C(bb, i, j, k) = kx + ky - aa[k] - cc[k];
                 if (k == s->kstr3) { C(bb, i, j, k) = C(bb, i, j, k) + aa[k]; aa[k] = 0.0; }
                 if (k == s->kend3) { C(bb, i, j, k) = C(bb, i, j, k) + cc[k]; cc[k] = 0.0; }
             }
     }
+    sym_free(tb);
 }
 
 /* get_u_eqn_coeff (src/module_poisson_solver.f90:181-282) */
 static void get_u_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
 {
     double dt = s->prm.dt, nu = s->prm.nu;
+    symtab tb = sym_tables(s, 0, nu);
     for (int k = 1; k <= s->nka; ++k) { aa[k] = 0.0; cc[k] = 0.0; }
     memset(bb, 0, sizeof(cplx) * (size_t)s->nx * s->ny * s->nka);
     for (int k = s->kstr3; k <= s->kend3; ++k) {
@@ -334,9 +355,7 @@ static void get_u_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
         cc[k] = -0.5 * dt * nu / s->dz[k] / s->dz_t[k];
         for (int j = 1; j <= s->ny; ++j)
             for (int i = 1; i <= s->nx; ++i) {
-                int l = lmap(i, s->nx), m = lmap(j, s->ny);
-                cplx kx = kx_helm(s, l, nu, s->dx2, s->wx1, s->prm.lx);
-                cplx ky = kx_helm(s, m, nu, s->dy2, s->wy1, s->prm.ly);
+                cplx kx = tb.x[i], ky = tb.y[j];
                 C(bb, i, j, k) = -kx - ky - aa[k] - cc[k];
                 if (k == s->kstr3) { C(bb, i, j, k) = C(bb, i, j, k) - aa[k]; aa[k] = 0.0; }
                 if (k == s->kend3) {
@@ -345,12 +364,14 @@ static void get_u_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
                 }
             }
     }
+    sym_free(tb);
 }
 
 /* get_w_eqn_coeff (src/module_poisson_solver.f90:287-374) */
 static void get_w_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
 {
     double dt = s->prm.dt, nu = s->prm.nu;
+    symtab tb = sym_tables(s, 0, nu);
     for (int k = 1; k <= s->nka; ++k) { aa[k] = 0.0; cc[k] = 0.0; }
     memset(bb, 0, sizeof(cplx) * (size_t)s->nx * s->ny * s->nka);
     for (int k = s->kstr3; k <= s->kend3 - 1; ++k) {
@@ -358,20 +379,20 @@ static void get_w_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
         cc[k] = -0.5 * dt * nu / s->dz[k + 1] / s->dz_t[k];
         for (int j = 1; j <= s->ny; ++j)
             for (int i = 1; i <= s->nx; ++i) {
-                int l = lmap(i, s->nx), m = lmap(j, s->ny);
-                cplx kx = kx_helm(s, l, nu, s->dx2, s->wx1, s->prm.lx);
-                cplx ky = kx_helm(s, m, nu, s->dy2, s->wy1, s->prm.ly);
+                cplx kx = tb.x[i], ky = tb.y[j];
                 C(bb, i, j, k) = -kx - ky - aa[k] - cc[k];
                 if (k == s->kstr3) aa[k] = 0.0;
                 if (k == s->kend3 - 1) cc[k] = 0.0;
             }
     }
+    sym_free(tb);
 }
 
 /* get_t_eqn_coeff (src/module_poisson_solver.f90:379-477) */
 static void get_t_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
 {
     double dt = s->prm.dt, al = s->prm.alpha;
+    symtab tb = sym_tables(s, 0, al);
     for (int k = 1; k <= s->nka; ++k) { aa[k] = 0.0; cc[k] = 0.0; }
     memset(bb, 0, sizeof(cplx) * (size_t)s->nx * s->ny * s->nka);
     for (int k = s->kstr3; k <= s->kend3; ++k) {
@@ -379,14 +400,13 @@ static void get_t_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
         cc[k] = -0.5 * dt * al / s->dz[k] / s->dz_t[k];
         for (int j = 1; j <= s->ny; ++j)
             for (int i = 1; i <= s->nx; ++i) {
-                int l = lmap(i, s->nx), m = lmap(j, s->ny);
-                cplx kx = kx_helm(s, l, al, s->dx2, s->wx1, s->prm.lx);
-                cplx ky = kx_helm(s, m, al, s->dy2, s->wy1, s->prm.ly);
+                cplx kx = tb.x[i], ky = tb.y[j];
                 C(bb, i, j, k) = -kx - ky - aa[k] - cc[k];
                 if (k == s->kstr3) { C(bb, i, j, k) = C(bb, i, j, k) - aa[k]; aa[k] = 0.0; }
                 if (k == s->kend3) { C(bb, i, j, k) = C(bb, i, j, k) - cc[k]; cc[k] = 0.0; }
             }
     }
+    sym_free(tb);
 }
 
 /* ------------------------------------------------------------------------ */
