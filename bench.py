@@ -32,6 +32,8 @@ WORKLOADS = {
     "channel_fd4_512x384x256": (512, 384, 256),
     "channel_fd4_256x256x128": (256, 256, 128),
     "channel_fd4_96x64x64": (96, 64, 64),
+    # profiling size: production nz with a few GB on the device
+    "channel_fd4_256x192x256": (256, 192, 256),
 }
 DEFAULT_WORKLOAD = "channel_fd4_512x384x256"
 # CPU samples of the same physics, sized for 10-30 s of host work

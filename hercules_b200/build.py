@@ -7,7 +7,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SO = os.path.join(HERE, "libhercules_b200.so")
-SRC = os.path.join(HERE, "csrc", "hc_api.cu")
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("hc_api.cu",)]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
@@ -28,7 +28,7 @@ def needs_build() -> bool:
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     if force or needs_build():
-        cmd = [NVCC] + FLAGS + (extra or []) + ["-o", SO, SRC]
+        cmd = [NVCC] + FLAGS + (extra or []) + ["-o", SO] + SRCS
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

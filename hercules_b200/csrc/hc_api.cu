@@ -21,6 +21,7 @@
 #include "hc_fft.cuh"
 #include "hc_column.cuh"
 #include "hc_rhs_tiled.cuh"
+#include "hc_column_warp.cuh"
 
 // ---------------------------------------------------------------------------
 // small device kernels for the scalar state
@@ -213,7 +214,7 @@ struct hc_handle {
     double2* twbuf;
     FftPlan px, py;
     double2* wpack;
-    int rows_x, tl_y, col_threads;
+    int rows_x, tl_y, col_threads, col_warp;
     size_t smem_x, smem_y;
     double dpx_coef;
     cudaEvent_t e0, e1;
@@ -340,8 +341,8 @@ static int build_tables(hc_handle* h)
     size_t o_hx = put(nxh), o_hy = put(ny), o_hxt = put(nxh), o_hyt = put(ny), o_px = put(nxh), o_py = put(ny);
     size_t o_dx = put(2 * nxh), o_dy = put(2 * ny), o_gx = put(2 * nxh), o_gy = put(2 * ny);
     size_t o_lx = put(nxh), o_ly = put(ny);
-    size_t o_k[16];
-    for (int q = 0; q < 16; ++q) o_k[q] = put(nz);
+    size_t o_k[19];
+    for (int q = 0; q < 19; ++q) o_k[q] = put(nz);
     auto lsig = [](int idx, int n) { return idx < n / 2 ? idx : idx - n; };
     for (int l = 0; l < nxh; ++l) {
         buf[o_hx + l] = helm_sym(cds, l, nx, dx2, dt, nu, p.lx);
@@ -387,6 +388,9 @@ static int build_tables(hc_handle* h)
     double* ap = &buf[o_k[8]]; double* cp = &buf[o_k[9]]; double* dgp = &buf[o_k[10]]; double* d0p = &buf[o_k[11]];
     double* at = &buf[o_k[12]]; double* ct = &buf[o_k[13]]; double* dgt = &buf[o_k[14]]; double* d0t = &buf[o_k[15]];
     for (int k = 0; k < nz; ++k) {
+        buf[o_k[16] + k] = 1.0 / dz(k);
+        buf[o_k[17] + k] = 1.0 / dzt(k);
+        buf[o_k[18] + k] = 1.0 / dzb(k);
         // u, v (get_u_eqn_coeff :198-278)
         double a0 = -0.5 * dt * nu / dz(k) / dzb(k), c0 = -0.5 * dt * nu / dz(k) / dzt(k);
         au[k] = k == 0 ? 0.0 : a0;
@@ -432,6 +436,7 @@ static int build_tables(hc_handle* h)
     c.aw = b + o_k[4]; c.cw = b + o_k[5]; c.dgw = b + o_k[6]; c.d0w = b + o_k[7];
     c.ap = b + o_k[8]; c.cp = b + o_k[9]; c.dgp = b + o_k[10]; c.d0p = b + o_k[11];
     c.at = b + o_k[12]; c.ct = b + o_k[13]; c.dgt = b + o_k[14]; c.d0t = b + o_k[15];
+    c.rdz = b + o_k[16]; c.rdzt = b + o_k[17]; c.rdzb = b + o_k[18];
     return HC_OK;
 }
 
@@ -459,12 +464,13 @@ static int build_fft(hc_handle* h)
     h->py.tw = h->twbuf + nxh;
     h->wpack = h->twbuf + nxh + ny;
     const size_t c2 = 2 * h->rsz;     // bytes of one complex
-    h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : 2048 / nxh;
+    h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : (h->rsz == sizeof(double) ? 1024 : 2048) / nxh;
     if (h->rows_x < 1) h->rows_x = 1; if (h->rows_x > 64) h->rows_x = 64;
     h->smem_x = 2 * (size_t)h->rows_x * nxh * c2;
-    h->col_threads = h->p.tile[3] > 0 ? h->p.tile[3] : 128;
+    h->col_threads = h->p.tile[3] > 1 ? h->p.tile[3] : 128;
+    h->col_warp = h->p.tile[3] != 1 && h->p.nz <= 32 * 8;
     if (h->col_threads < 32 || h->col_threads > 256 || (h->col_threads & 31)) return HC_ERR_PARAM;
-    h->tl_y = h->p.tile[1] > 0 ? h->p.tile[1] : 2048 / ny;
+    h->tl_y = h->p.tile[1] > 0 ? h->p.tile[1] : 1536 / ny;
     if (h->tl_y < 1) h->tl_y = 1; if (h->tl_y > 32) h->tl_y = 32; if (h->tl_y > nxh) h->tl_y = nxh;
     h->smem_y = 2 * (size_t)h->tl_y * (ny + 1) * c2;
     if (h->smem_x > 200 * 1024 || h->smem_y > 200 * 1024) return HC_ERR_UNSUPPORTED;
@@ -584,6 +590,63 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base
     return HC_OK;
 }
 
+// Column solves: one warp per wavenumber pair while nz <= 256 (rows per lane
+// K = ceil(nz/32)), else (or when tile[3] asks for it) one thread per pair.
+template <typename R, int K> static int col_fd_k(hc_handle* h, const ColArgs<R>& ca)
+{
+    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
+    k_column_fd_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(ca);
+    CKL();
+    return HC_OK;
+}
+template <typename R> static int launch_column_fd(hc_handle* h, const ColArgs<R>& ca)
+{
+    const int K = (h->p.nz + 31) / 32;
+    if (h->col_warp) {
+        switch (K) {
+        case 1: return col_fd_k<R, 1>(h, ca);
+        case 2: return col_fd_k<R, 2>(h, ca);
+        case 3: return col_fd_k<R, 3>(h, ca);
+        case 4: return col_fd_k<R, 4>(h, ca);
+        case 5: return col_fd_k<R, 5>(h, ca);
+        case 6: return col_fd_k<R, 6>(h, ca);
+        case 7: return col_fd_k<R, 7>(h, ca);
+        case 8: return col_fd_k<R, 8>(h, ca);
+        default: break;
+        }
+    }
+    k_column_fd<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ca);
+    CKL();
+    return HC_OK;
+}
+template <typename R, int K> static int col_t_k(hc_handle* h, const ColTArgs<R>& ct)
+{
+    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
+    k_column_t_warp<R, K><<<nb, CW_WARPS * 32, 0, h->st>>>(ct);
+    CKL();
+    return HC_OK;
+}
+template <typename R> static int launch_column_t(hc_handle* h, const ColTArgs<R>& ct)
+{
+    const int K = (h->p.nz + 31) / 32;
+    if (h->col_warp) {
+        switch (K) {
+        case 1: return col_t_k<R, 1>(h, ct);
+        case 2: return col_t_k<R, 2>(h, ct);
+        case 3: return col_t_k<R, 3>(h, ct);
+        case 4: return col_t_k<R, 4>(h, ct);
+        case 5: return col_t_k<R, 5>(h, ct);
+        case 6: return col_t_k<R, 6>(h, ct);
+        case 7: return col_t_k<R, 7>(h, ct);
+        case 8: return col_t_k<R, 8>(h, ct);
+        default: break;
+        }
+    }
+    k_column_t<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ct);
+    CKL();
+    return HC_OK;
+}
+
 template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
 {
     typedef typename V2<R>::T T2;
@@ -618,6 +681,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
         int kc = p.tile[2] > 0 ? p.tile[2] : (int)((long long)bx * by * p.nz / want);
         if (p.tile[2] <= 0) { if (kc < 4) kc = 4; if (kc > 32) kc = 32; }
         if (kc < 1) kc = 1;
+        if (kc > RT_KMAX) kc = RT_KMAX;
         if (kc > p.nz) kc = p.nz;
         m.kchunk = kc;
         dim3 gr(bx, by, (p.nz + kc - 1) / kc);
@@ -648,8 +712,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     }
     ca.halt = halt;
     prof_begin(h, K_COLUMN);
-    k_column_fd<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ca);
-    CKL();
+    rc = launch_column_fd<R>(h, ca);
+    if (rc) return rc;
 
     R* outs[4] = {(R*)h->fld[F_U], (R*)h->fld[F_V], (R*)h->fld[F_W], (R*)h->fld[F_P]};
     const int add[4] = {0, 0, 0, 1};
@@ -678,8 +742,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
             ct.bct1 = -2.0 * cc_t_zend * p.ttop;
         }
         prof_begin(h, K_COLUMN_T);
-        k_column_t<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ct);
-        CKL();
+        rc = launch_column_t<R>(h, ct);
+        if (rc) return rc;
         R* tout[1] = {(R*)h->fld[F_T]};
         const int add0[1] = {0};
         rc = fft_inverse<R>(h, S, tout, add0, 1);

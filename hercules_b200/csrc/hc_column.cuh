@@ -38,6 +38,8 @@ struct ColCoef {
     const double* aw; const double* cw; const double* dgw; const double* d0w;
     const double* ap; const double* cp; const double* dgp; const double* d0p;
     const double* at; const double* ct; const double* dgt; const double* d0t;
+    // per k reciprocals of dz, dz_t, dz_b
+    const double* rdz; const double* rdzt; const double* rdzb;
 };
 
 struct ColScratch {

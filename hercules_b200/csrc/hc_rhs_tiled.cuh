@@ -37,9 +37,11 @@ template <typename R> struct RhsTArgs {
     int with_t;
 };
 
+#define RT_KMAX 64
 template <typename R> __host__ size_t rhs_tiled_smem(int with_t)
 {
-    return sizeof(R) * ((size_t)(9 + 2 + (with_t ? 2 : 0)) * RT_P4 + (size_t)RT_NFLUX * RT_P2);
+    return sizeof(R) * ((size_t)(9 + 2 + (with_t ? 2 : 0)) * RT_P4 + (size_t)RT_NFLUX * RT_P2) +
+           sizeof(R) * 6 * (RT_KMAX + 1);
 }
 
 #define RT_NLD ((RT_P4 + 255) / 256)
@@ -75,6 +77,39 @@ __device__ __forceinline__ void rt_load_plane(R* dst, const R* src, const Geo& g
     }
 }
 
+// Register-staged variant used to overlap the next level's loads with the
+// current level's arithmetic: fetch issues the loads, put stores to SMEM.
+template <typename R>
+__device__ __forceinline__ void rt_fetch(R* v, const R* src, const Geo& g, const int* off, int lvl, int kind,
+                                         R um, R tbot, R ttop, int closed)
+{
+    const int nz = g.nz;
+    int sl = lvl;
+    R sgn = R(1), add = R(0);
+    if (lvl >= nz) {
+        sl = nz - 1;
+        if (kind == 0) { if (closed) { sgn = R(-1); add = -R(2) * um; } }
+        else if (kind == 1) { if (closed) sgn = R(-1); }
+        else if (kind == 2) { sl = nz - 2; sgn = R(-1); }
+        else if (kind == 4) { sgn = R(-1); add = R(2) * ttop; }
+    }
+    const R* base = src + (long long)sl * g.nxy;
+#pragma unroll
+    for (int r = 0; r < RT_NLD; ++r) {
+        const int e = threadIdx.x + 256 * r;
+        v[r] = (e < RT_P4) ? sgn * __ldg(base + off[r]) + add : R(0);
+    }
+}
+template <typename R>
+__device__ __forceinline__ void rt_put(R* dst, const R* v)
+{
+#pragma unroll
+    for (int r = 0; r < RT_NLD; ++r) {
+        const int e = threadIdx.x + 256 * r;
+        if (e < RT_P4) dst[e] = v[r];
+    }
+}
+
 template <typename R, int CDS>
 __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
 {
@@ -94,6 +129,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
     R* F_B = FX + 5 * RT_P2;     // uhy * vhx
     R* F_CZ = FX + 6 * RT_P2;    // uhz * whx
     R* F_EZ = FX + 7 * RT_P2;    // vhz * why
+    R* ZM = FX + RT_NFLUX * RT_P2;   // per level of the chunk: 1/dz, 1/dz_t, 1/dz_b, l_t, 1/dz(k+1)
 
     const Geo& g = a.g;
     const int nz = g.nz;
@@ -118,6 +154,14 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
     const R h16 = R(0.0625);
 
     auto slot3 = [](int lvl) { return (lvl + 3) % 3; };
+    for (int q = threadIdx.x; q < ke - kb; q += blockDim.x) {
+        const int k = kb + q;
+        ZM[q] = R(1) / (R)ldz(g.z.dz, k);
+        ZM[(RT_KMAX + 1) + q] = R(1) / (R)ldz(g.z.dz_t, k);
+        ZM[2 * (RT_KMAX + 1) + q] = R(1) / (R)ldz(g.z.dz_b, k);
+        ZM[3 * (RT_KMAX + 1) + q] = (R)ldz(g.z.l_t, k);
+        ZM[4 * (RT_KMAX + 1) + q] = R(1) / (R)ldz(g.z.dz, k + 1);
+    }
     int off[RT_NLD];
 #pragma unroll
     for (int r = 0; r < RT_NLD; ++r) {
@@ -162,11 +206,28 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
     }
 
     for (int k = kb; k < ke; ++k) {
+        const bool more = k + 1 < ke;
+        R nu_[RT_NLD], nv_[RT_NLD], nw_[RT_NLD], np_[RT_NLD], nt_[RT_NLD];
+        if (more) {
+            const int L = k + 2;
+            rt_fetch<R>(nu_, a.f.u, g, off, L, 0, um, tbot, ttop, closed);
+            rt_fetch<R>(nv_, a.f.v, g, off, L, 1, um, tbot, ttop, closed);
+            rt_fetch<R>(nw_, a.f.w, g, off, L, 2, um, tbot, ttop, closed);
+            rt_fetch<R>(np_, a.f.p, g, off, L, 3, um, tbot, ttop, closed);
+            if (a.with_t) rt_fetch<R>(nt_, a.f.t, g, off, L, 4, um, tbot, ttop, closed);
+        }
+        const long long id = ((long long)k * g.ny + yj) * g.nx + xi;
+        R f0u = R(0), f0v = R(0), f0w = R(0);
+        if (active) {
+            f0u = a.ff[id];
+            f0v = a.gg[id];
+            if (k < nz - 1) f0w = a.hh[id];
+        }
         const R* um1 = SU + slot3(k - 1) * RT_P4; const R* u0 = SU + slot3(k) * RT_P4; const R* up1 = SU + slot3(k + 1) * RT_P4;
         const R* vm1 = SV + slot3(k - 1) * RT_P4; const R* v0 = SV + slot3(k) * RT_P4; const R* vp1 = SV + slot3(k + 1) * RT_P4;
         const R* wm1 = SW + slot3(k - 1) * RT_P4; const R* w0 = SW + slot3(k) * RT_P4; const R* wp1 = SW + slot3(k + 1) * RT_P4;
         const R* p0 = SP + (k & 1) * RT_P4; const R* pp1 = SP + ((k + 1) & 1) * RT_P4;
-        const R lt = (R)ldz(g.z.l_t, k);
+        const R lt = ZM[3 * (RT_KMAX + 1) + (k - kb)];
         const bool wface = k < nz - 1;   // whx, why vanish on the top wall level
         // ---- level-k products on the 2-point halo
         for (int e = threadIdx.x; e < RT_P2; e += blockDim.x) {
@@ -200,9 +261,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
         __syncthreads();
 
         if (active) {
-            const long long id = ((long long)k * g.ny + yj) * g.nx + xi;
-            const R dz = (R)ldz(g.z.dz, k), dzt = (R)ldz(g.z.dz_t, k), dzb = (R)ldz(g.z.dz_b, k);
-            const R rdz = R(1) / dz, rdzt = R(1) / dzt, rdzb = R(1) / dzb;
+            const R rdz = ZM[k - kb], rdzt = ZM[(RT_KMAX + 1) + (k - kb)], rdzb = ZM[2 * (RT_KMAX + 1) + (k - kb)];
             const int f = fc0;
             // ---------------- U ----------------
             {
@@ -232,9 +291,8 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
                 R fu;
                 if (a.ph.dp_opt == 3) fu = -uux - uvy - uwz - um * ux + fc * (R(0.5) * (F_VHX[f] + F_VHX[f - RT_W2]) - (R)a.ph.vg);
                 else fu = -uux - uvy - uwz + dpx - um * ux;
-                const R f0 = a.ff[id];
                 a.ff[id] = fu;
-                a.qu[id] = uc + dt * (rka * fu + rkb * f0) + cdif * (uxx + uyy + uzz) - rkc * dt * dpdx;
+                a.qu[id] = uc + dt * (rka * fu + rkb * f0u) + cdif * (uxx + uyy + uzz) - rkc * dt * dpdx;
                 if (a.uhx_s) a.uhx_s[id] = F_UHX[f];
             }
             // ---------------- V ----------------
@@ -267,9 +325,8 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
                 R fv;
                 if (a.ph.dp_opt == 3) fv = -vux - vvy - vwz - um * vx + fc * ((R)a.ph.ug - R(0.5) * (F_UHY[f] + F_UHY[f - 1]) - um);
                 else fv = -vux - vvy - vwz - um * vx;
-                const R g0 = a.gg[id];
                 a.gg[id] = fv;
-                a.qv[id] = vc + dt * (rka * fv + rkb * g0) + cdif * (vxx + vyy + vzz) - rkc * dt * dpdy;
+                a.qv[id] = vc + dt * (rka * fv + rkb * f0v) + cdif * (vxx + vyy + vzz) - rkc * dt * dpdy;
                 if (a.vhy_s) a.vhy_s[id] = F_VHY[f];
             }
             // ---------------- W (k <= nz-2) ----------------
@@ -292,7 +349,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
                 R a1 = R(0.5) * (wc + wp); a1 = a1 * a1;
                 R a2 = R(0.5) * (wc + wm); a2 = a2 * a2;
                 const R wwz = (a1 - a2) * rdzt;
-                const R rdzp = R(1) / (R)ldz(g.z.dz, k + 1);
+                const R rdzp = ZM[4 * (RT_KMAX + 1) + (k - kb)];
                 const R wzz = ((wp - wc) * rdzp - (wc - wm) * rdz) * rdzt;
                 R fw = -wux - wvy - wwz - um * wx;
                 if (a.ph.isscalar == 1) {
@@ -300,20 +357,21 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
                     fw = fw + got * ((R(1) - lt) * t0[rc] + lt * tp1[rc] - (R)a.ph.t_ref);
                 }
                 const R dpdz = (pp1[rc] - p0[rc]) * rdzt;
-                const R h0 = a.hh[id];
                 a.hh[id] = fw;
-                a.qw[id] = wc + dt * (rka * fw + rkb * h0) + cdif * (wxx + wyy + wzz) - rkc * dt * dpdz;
+                a.qw[id] = wc + dt * (rka * fw + rkb * f0w) + cdif * (wxx + wyy + wzz) - rkc * dt * dpdz;
             }
         }
-        if (k + 1 >= ke) break;
+        if (!more) break;
         __syncthreads();
         // advance the window: level k+2 replaces k-1 (u, v, w) and k (p, t)
-        const int L = k + 2;
-        rt_load_plane<R>(SU + slot3(L) * RT_P4, a.f.u, g, off, L, 0, um, tbot, ttop, closed);
-        rt_load_plane<R>(SV + slot3(L) * RT_P4, a.f.v, g, off, L, 1, um, tbot, ttop, closed);
-        rt_load_plane<R>(SW + slot3(L) * RT_P4, a.f.w, g, off, L, 2, um, tbot, ttop, closed);
-        rt_load_plane<R>(SP + (L & 1) * RT_P4, a.f.p, g, off, L, 3, um, tbot, ttop, closed);
-        if (a.with_t) rt_load_plane<R>(ST + (L & 1) * RT_P4, a.f.t, g, off, L, 4, um, tbot, ttop, closed);
+        {
+            const int L = k + 2;
+            rt_put<R>(SU + slot3(L) * RT_P4, nu_);
+            rt_put<R>(SV + slot3(L) * RT_P4, nv_);
+            rt_put<R>(SW + slot3(L) * RT_P4, nw_);
+            rt_put<R>(SP + (L & 1) * RT_P4, np_);
+            if (a.with_t) rt_put<R>(ST + (L & 1) * RT_P4, nt_);
+        }
         __syncthreads();
     }
 }
