@@ -30,7 +30,7 @@ HC_ERRORS = {0: "ok", -1: "bad argument", -2: "parameter check failed", -3: "CUD
 ABI_SYMBOLS = ["hc_create", "hc_set_grid", "hc_get_grid", "hc_upload", "hc_download",
                "hc_initialize", "hc_step", "hc_get_scalars", "hc_upload_dev", "hc_download_dev",
                "hc_last_step_ms", "hc_last_launch_count", "hc_set_profiling", "hc_kernel_profile",
-               "hc_destroy", "hc_error_string"]
+               "hc_divergence_noalloc", "hc_destroy", "hc_error_string"]
 
 
 class HerculesError(RuntimeError):
@@ -65,6 +65,8 @@ def load_library(path: str = LIB_PATH):
     L.hc_last_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.hc_set_profiling.argtypes = [vp, ip]
     L.hc_kernel_profile.argtypes = [vp, ip, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ip)]
+    L.hc_divergence_noalloc.argtypes = [ctypes.POINTER(HcParams), ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.hc_destroy.argtypes = [vp]
     L.hc_error_string.argtypes = [ip]
     L.hc_error_string.restype = ctypes.c_char_p

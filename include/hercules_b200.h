@@ -185,6 +185,22 @@ int hc_set_profiling(hc_handle* h, int enable);
 int hc_kernel_profile(hc_handle* h, int max, char* names, double* total_ms,
                       long long* launches, int* count);
 
+/* Divergence check of caller-owned device fields that allocates nothing. No
+ * counterpart in the reference. It is for hosts that own all device memory and
+ * let no library call cudaMalloc (for instance a Fortran code whose device arrays
+ * come from its own arena or OpenACC data regions): u, v, w are the caller's
+ * interior-only (nx,ny,nz) arrays of the storage type of p->precision, dz is the
+ * host copy of the nz+4 vertical spacings, out_dev is 3 doubles in device memory
+ * receiving {mean |div|, signed div at the largest |div|, NaN flag} exactly as
+ * hc_step's divergence diagnostic computes them. Scratch lives in one fixed
+ * array per device (about 61 KB, held until exit): nz <= 4096 and
+ * nx*ny*nz < 2^31, else HC_ERR_SIZE. The first call on a device looks up that
+ * array's address; make it before any stream capture. Calls share the array, so
+ * calls that overlap on the GPU race with each other. `stream` is a
+ * cudaStream_t (NULL for the default stream); the call does not synchronise. */
+int hc_divergence_noalloc(const hc_params* p, const double* dz, const void* u,
+                          const void* v, const void* w, double* out_dev, void* stream);
+
 int hc_destroy(hc_handle* h);
 
 const char* hc_error_string(int code);
