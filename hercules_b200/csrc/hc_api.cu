@@ -18,7 +18,7 @@
 #include "../../include/hercules_b200.h"
 #include "hc_common.cuh"
 #include "hc_fd.cuh"
-#include "hc_fft.cuh"
+#include "hc_fft_t.cuh"
 #include "hc_column.cuh"
 #include "hc_rhs_tiled.cuh"
 #include "hc_column_warp.cuh"
@@ -212,6 +212,8 @@ struct hc_handle {
     hc_diag* diag_dev;
     int diag_cap;
     double2* twbuf;
+    void* twt;               // the same tables in the storage precision (FP64: twbuf)
+    int fft_tx, fft_ty;      // 1: the compile-time-length kernels serve x / y
     FftPlan px, py;
     double2* wpack;
     int rows_x, tl_y, col_threads, col_warp;
@@ -450,6 +452,79 @@ static int upload_zgrid(hc_handle* h)
     return HC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// compile-time-length FFT kernels (hc_fft_t.cuh): lengths with a specialisation
+// ---------------------------------------------------------------------------
+#define HC_FFT_T_RMAX 16
+#define HC_FFT_T_LENGTHS(X) X(8) X(12) X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) \
+    X(192) X(256) X(320) X(384) X(512)
+
+static bool fft_t_length_ok(int n)
+{
+    switch (n) {
+#define HC_LEN_CASE(N) case N: return true;
+    HC_FFT_T_LENGTHS(HC_LEN_CASE)
+#undef HC_LEN_CASE
+    }
+    return false;
+}
+
+// op 0: raise the shared-memory limit of the kernels this handle uses;
+// op 1: x forward, 2: x inverse, 3: y forward, 4: y inverse
+template <typename R, int N> static int fft_t_op(hc_handle* h, int op, const void* args, dim3 grid)
+{
+    constexpr int RM = HC_FFT_T_RMAX;
+    constexpr size_t sx = fft_t_smem<R, N, FxLines<N>::v>();
+    constexpr size_t sy = fft_t_smem<R, N, HC_FFT_TL>();
+    static_assert(FPlan<N, RM>::valid, "length must be 2^a 3^b 5^c");
+    if (op == 0) {
+        if (N == h->g.nxh && h->fft_tx) {
+            CK(cudaFuncSetAttribute(k_fft_x_r2c_t<R, N, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx));
+            CK(cudaFuncSetAttribute(k_fft_x_c2r_t<R, N, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx));
+        }
+        if (N == h->g.ny && h->fft_ty) {
+            CK(cudaFuncSetAttribute(k_fft_y_t<R, N, -1, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
+            CK(cudaFuncSetAttribute(k_fft_y_t<R, N, 1, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
+        }
+        return HC_OK;
+    }
+    if (op == 1) k_fft_x_r2c_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
+    else if (op == 2) k_fft_x_c2r_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
+    else if (op == 3) k_fft_y_t<R, N, -1, RM><<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
+    else k_fft_y_t<R, N, 1, RM><<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
+    return HC_OK;
+}
+
+template <typename R> static int fft_t_dispatch(hc_handle* h, int n, int op, const void* args, dim3 grid)
+{
+    switch (n) {
+#define HC_LEN_CASE(N) case N: return fft_t_op<R, N>(h, op, args, grid);
+    HC_FFT_T_LENGTHS(HC_LEN_CASE)
+#undef HC_LEN_CASE
+    }
+    return HC_ERR_UNSUPPORTED;
+}
+
+template <typename R> static int fft_t_setup(hc_handle* h)
+{
+    int rc = HC_OK;
+    if (h->fft_tx) rc = fft_t_dispatch<R>(h, h->g.nxh, 0, nullptr, dim3());
+    if (rc == HC_OK && h->fft_ty && !(h->fft_tx && h->g.ny == h->g.nxh))
+        rc = fft_t_dispatch<R>(h, h->g.ny, 0, nullptr, dim3());
+    return rc;
+}
+
+template <typename R> static long long fft_t_xblocks(int n, long long nrows)
+{
+    long long lines = 1;
+    switch (n) {
+#define HC_LEN_CASE(N) case N: lines = FxLines<N>::v; break;
+    HC_FFT_T_LENGTHS(HC_LEN_CASE)
+#undef HC_LEN_CASE
+    }
+    return (nrows + lines - 1) / lines;
+}
+
 static int build_fft(hc_handle* h)
 {
     const int nx = h->p.nx, ny = h->p.ny, nxh = nx / 2;
@@ -463,6 +538,21 @@ static int build_fft(hc_handle* h)
     h->px.tw = h->twbuf;
     h->py.tw = h->twbuf + nxh;
     h->wpack = h->twbuf + nxh + ny;
+    if (h->rsz == sizeof(double)) {
+        h->twt = h->twbuf;
+    } else {
+        std::vector<float2> tf(tw.size());
+        for (size_t e = 0; e < tw.size(); ++e) tf[e] = make_float2((float)tw[e].x, (float)tw[e].y);
+        CK(cudaMalloc(&h->twt, tf.size() * sizeof(float2)));
+        CK(cudaMemcpy(h->twt, tf.data(), tf.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    // explicit tile sizes (tile[0], tile[1]) select the runtime-length kernels
+    h->fft_tx = h->p.tile[0] == 0 && fft_t_length_ok(nxh);
+    h->fft_ty = h->p.tile[1] == 0 && fft_t_length_ok(ny);
+    if (h->fft_tx || h->fft_ty) {
+        int rc = h->rsz == sizeof(double) ? fft_t_setup<double>(h) : fft_t_setup<float>(h);
+        if (rc != HC_OK) return rc;
+    }
     const size_t c2 = 2 * h->rsz;     // bytes of one complex
     h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : (h->rsz == sizeof(double) ? 1024 : 2048) / nxh;
     if (h->rows_x < 1) h->rows_x = 1; if (h->rows_x > 64) h->rows_x = 64;
@@ -505,10 +595,29 @@ template <typename R> static Acc<R> make_acc(hc_handle* h)
     return a;
 }
 
+template <typename R> static const typename V2<R>::T* fft_tw(hc_handle* h, int which)
+{
+    const typename V2<R>::T* t = (const typename V2<R>::T*)h->twt;
+    return which == 0 ? t : (which == 1 ? t + h->g.nxh : t + h->g.nxh + h->g.ny);
+}
+
+// x then y forward transform of nf physical fields into half spectra
 template <typename R> static int fft_forward(hc_handle* h, const R* const* in, typename V2<R>::T* const* out, int nf)
 {
     typedef typename V2<R>::T T2;
     const int* halt = &h->sc->nan_flag;
+    if (nf < 1 || nf > HC_FFT_MAXF) return HC_ERR_ARG;
+    if (h->fft_tx) {
+        FxArgs<R> a;
+        memset(&a, 0, sizeof(a));
+        for (int f = 0; f < nf; ++f) { a.in[f] = in[f]; a.out[f] = out[f]; }
+        a.nrows = (long long)h->g.ny * h->g.nz;
+        a.tw = fft_tw<R>(h, 0); a.wp = fft_tw<R>(h, 2); a.scale = (R)(1.0 / h->p.nx); a.halt = halt;
+        prof_begin(h, K_FFT_X_FWD);
+        int rc = fft_t_dispatch<R>(h, h->g.nxh, 1, &a, dim3((unsigned)fft_t_xblocks<R>(h->g.nxh, a.nrows), nf, 1));
+        if (rc) return rc;
+        CKL();
+    } else {
     FftXArgs<R> ax;
     memset(&ax, 0, sizeof(ax));
     for (int f = 0; f < nf; ++f) { ax.in[f] = in[f]; ax.out[f] = out[f]; }
@@ -518,6 +627,18 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     prof_begin(h, K_FFT_X_FWD);
     k_fft_x_r2c<R><<<gx, 256, h->smem_x, h->st>>>(ax);
     CKL();
+    }
+    if (h->fft_ty) {
+        FyArgs<R> a;
+        memset(&a, 0, sizeof(a));
+        for (int f = 0; f < nf; ++f) a.dst[f] = out[f];
+        a.nxh = h->g.nxh; a.tw = fft_tw<R>(h, 1); a.scale = (R)(1.0 / h->p.ny); a.halt = halt;
+        prof_begin(h, K_FFT_Y_FWD);
+        int rc = fft_t_dispatch<R>(h, h->g.ny, 3, &a, dim3((h->g.nxh + HC_FFT_TL - 1) / HC_FFT_TL, h->g.nz, nf));
+        if (rc) return rc;
+        CKL();
+        return HC_OK;
+    }
     FftYArgs<R> ay;
     memset(&ay, 0, sizeof(ay));
     for (int f = 0; f < nf; ++f) ay.data[f] = out[f];
@@ -530,9 +651,22 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     return HC_OK;
 }
 
+// y then x inverse transform of nf half spectra (in place in y) into physical
+// fields, stored or (add[f] = 1) added
 template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* const* in, R* const* out, const int* add, int nf)
 {
     const int* halt = &h->sc->nan_flag;
+    if (nf < 1 || nf > HC_FFT_MAXF) return HC_ERR_ARG;
+    if (h->fft_ty) {
+        FyArgs<R> a;
+        memset(&a, 0, sizeof(a));
+        for (int f = 0; f < nf; ++f) a.dst[f] = in[f];
+        a.nxh = h->g.nxh; a.tw = fft_tw<R>(h, 1); a.scale = (R)1; a.halt = halt;
+        prof_begin(h, K_FFT_Y_INV);
+        int rc = fft_t_dispatch<R>(h, h->g.ny, 4, &a, dim3((h->g.nxh + HC_FFT_TL - 1) / HC_FFT_TL, h->g.nz, nf));
+        if (rc) return rc;
+        CKL();
+    } else {
     FftYArgs<R> ay;
     memset(&ay, 0, sizeof(ay));
     for (int f = 0; f < nf; ++f) ay.data[f] = in[f];
@@ -541,6 +675,19 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
     prof_begin(h, K_FFT_Y_INV);
     k_fft_y<R, 1><<<gy, 256, h->smem_y, h->st>>>(ay);
     CKL();
+    }
+    if (h->fft_tx) {
+        FxArgs<R> a;
+        memset(&a, 0, sizeof(a));
+        for (int f = 0; f < nf; ++f) { a.in[f] = in[f]; a.out[f] = out[f]; a.add[f] = add[f]; }
+        a.nrows = (long long)h->g.ny * h->g.nz;
+        a.tw = fft_tw<R>(h, 0); a.wp = fft_tw<R>(h, 2); a.scale = (R)1; a.halt = halt;
+        prof_begin(h, K_FFT_X_INV);
+        int rc = fft_t_dispatch<R>(h, h->g.nxh, 2, &a, dim3((unsigned)fft_t_xblocks<R>(h->g.nxh, a.nrows), nf, 1));
+        if (rc) return rc;
+        CKL();
+        return HC_OK;
+    }
     FftXInvArgs<R> ax;
     memset(&ax, 0, sizeof(ax));
     for (int f = 0; f < nf; ++f) { ax.in[f] = in[f]; ax.out[f] = out[f]; ax.add[f] = add[f]; }
@@ -811,6 +958,7 @@ static void free_all(hc_handle* h)
     if (h->part_st) cudaFree(h->part_st);
     if (h->sc) cudaFree(h->sc);
     if (h->diag_dev) cudaFree(h->diag_dev);
+    if (h->twt && h->twt != (void*)h->twbuf) cudaFree(h->twt);
     if (h->twbuf) cudaFree(h->twbuf);
     for (size_t q = 0; q < h->ev_pool.size(); ++q) cudaEventDestroy(h->ev_pool[q]);
     if (h->e0) cudaEventDestroy(h->e0);
@@ -839,7 +987,7 @@ int hc_create(const hc_params* p, hc_handle** out)
     for (int q = 0; q < 4; ++q) h->spec[q] = nullptr;
     for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
-    h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
+    h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
     h->diag_cap = 0; h->last_ms = 0.0; h->launches = 0; h->initialized = 0;
     h->prof = 0; h->cur_cat = 0; h->ev_used = 0;
     for (int q = 0; q < K_NCAT; ++q) { h->cat_ms[q] = 0.0; h->cat_n[q] = 0; }

@@ -27,6 +27,22 @@ __device__ __forceinline__ double2 shfl_dn2(double2 v, int s)
     return make_double2(__shfl_down_sync(0xffffffffu, v.x, s), __shfl_down_sync(0xffffffffu, v.y, s));
 }
 
+// Reciprocal by Newton-Raphson iteration on f(y) = 1/y - x, i.e.
+// y <- y + y (1 - x y), seeded with the single-precision reciprocal. Each step
+// doubles the number of correct bits (about 23 -> 46 -> 92), so two steps reach
+// FP64 round-off. The pivots of the diagonally dominant column systems stay far
+// inside the FP32 range; anything outside it (and NaN) takes the IEEE division.
+__device__ __forceinline__ double rcp_nr(double x)
+{
+    const double ax = fabs(x);
+    if (!(ax > 1e-30 && ax < 1e30)) return 1.0 / x;
+    double y = (double)__frcp_rn((float)x);
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
 // Solve sum_j A(r,j) x_j = d_r for NR right-hand sides. coef(r, a, b, c) gives row
 // r's sub-diagonal, diagonal and super-diagonal (identity rows past the end).
 template <int K, int NR, typename CF>
@@ -37,7 +53,7 @@ __device__ __forceinline__ void warp_partition_solve(const CF& coef, double2 (&d
     if (K >= 2) {
         double a0, b0, c0;
         coef(r0, a0, b0, c0);
-        ib[0] = 1.0 / b0;
+        ib[0] = rcp_nr(b0);
         vv[0] = -a0;
         ww[0] = (K == 2) ? -c0 : 0.0;
         double cprev = c0;
@@ -46,7 +62,7 @@ __device__ __forceinline__ void warp_partition_solve(const CF& coef, double2 (&d
             double ai, bi, ci;
             coef(r0 + i, ai, bi, ci);
             const double mlt = ai * ib[i - 1];
-            ib[i] = 1.0 / (bi - mlt * cprev);
+            ib[i] = rcp_nr(bi - mlt * cprev);
 #pragma unroll
             for (int q = 0; q < NR; ++q) d[q][i] = zsub(d[q][i], zscale(d[q][i - 1], mlt));
             vv[i] = -mlt * vv[i - 1];
@@ -98,7 +114,7 @@ __device__ __forceinline__ void warp_partition_solve(const CF& coef, double2 (&d
         const bool lo = ln < s, hi = ln + s > 31;
         if (lo) { Am = 0.0; Bm = 1.0; Cm = 0.0; }
         if (hi) { Ap = 0.0; Bp = 1.0; Cp = 0.0; }
-        const double k1 = A / Bm, k2 = C / Bp;
+        const double k1 = A * rcp_nr(Bm), k2 = C * rcp_nr(Bp);
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
             double2 Dm = shfl_up2(D[q], s), Dp = shfl_dn2(D[q], s);
@@ -109,7 +125,7 @@ __device__ __forceinline__ void warp_partition_solve(const CF& coef, double2 (&d
         const double nA = -Am * k1, nC = -Cp * k2, nB = B - Cm * k1 - Ap * k2;
         A = nA; B = nB; C = nC;
     }
-    const double iB = 1.0 / B;
+    const double iB = rcp_nr(B);
 #pragma unroll
     for (int q = 0; q < NR; ++q) {
         const double2 y = zscale(D[q], iB);
@@ -127,7 +143,7 @@ __device__ __forceinline__ void warp_partition_solve(const CF& coef, double2 (&d
 template <int K> __host__ size_t column_warp_smem() { return (size_t)CW_WARPS * 3 * K * 32 * sizeof(double2); }
 
 template <typename R, int K>
-__global__ void __launch_bounds__(CW_WARPS * 32) k_column_fd_warp(ColArgs<R> a)
+__global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_fd_warp(ColArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
@@ -149,13 +165,6 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_column_fd_warp(ColArgs<R> a)
     const double* dgp = is00 ? a.c.d0p : a.c.dgp;
     const int r0 = ln * K;
 
-    // all inputs are read up front so their latency overlaps
-    double2 dw[1][K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-        const int r = r0 + i;
-        dw[0][i] = r < nz - 1 ? ld2<R>(a.qw, (long long)r * ncol + c) : make_double2(0, 0);
-    }
     // ---- u*, v*: one matrix, two right-hand sides
     {
         double2 d[2][K];
@@ -186,6 +195,12 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_column_fd_warp(ColArgs<R> a)
     }
     // ---- w*: rows 0..nz-2 (the top-wall row is an identity row with zero source)
     {
+        double2 dw[1][K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            dw[0][i] = r < nz - 1 ? ld2<R>(a.qw, (long long)r * ncol + c) : make_double2(0, 0);
+        }
         auto cf = [&](int r, double& aa, double& bb, double& cc) {
             if (r < nz - 1) {
                 aa = rk * __ldg(a.c.aw + r);

@@ -126,7 +126,7 @@ __device__ typename V2<R>::T* stockham(typename V2<R>::T* A, typename V2<R>::T* 
     return src;
 }
 
-#define HC_FFT_MAXF 4
+#define HC_FFT_MAXF 16
 
 // ---------------------------------------------------------------------------
 // x direction, forward: real rows -> nx/2 modes, divided by nx
@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r(FftXInvArgs<R> a)
 // y direction, in place on the half spectrum [k][m][l]
 // ---------------------------------------------------------------------------
 template <typename R> struct FftYArgs {
+    const typename V2<R>::T* src[HC_FFT_MAXF];   // null: transform data in place
     typename V2<R>::T* data[HC_FFT_MAXF];
     int nxh, ny, tl;
     FftPlan pl;             // length ny
@@ -254,12 +255,13 @@ __global__ void __launch_bounds__(256) k_fft_y(FftYArgs<R> a)
     const int l0 = blockIdx.x * tl;
     const long long k = blockIdx.y;
     T2* d = a.data[blockIdx.z] + k * (long long)ny * a.nxh;
+    const T2* sd = a.src[blockIdx.z] ? a.src[blockIdx.z] + k * (long long)ny * a.nxh : d;
     const int nyq = ny / 2;
     for (int idx = threadIdx.x; idx < tl * ny; idx += blockDim.x) {
         const int lt = idx % tl, m = idx / tl;
         const int l = l0 + lt;
         T2 v; v.x = R(0); v.y = R(0);
-        if (l < a.nxh && !(S > 0 && m == nyq)) v = d[(long long)m * a.nxh + l];
+        if (l < a.nxh && !(S > 0 && m == nyq)) v = sd[(long long)m * a.nxh + l];
         A[lt * ls + m] = v;
     }
     __syncthreads();
