@@ -22,6 +22,7 @@
 #include "hc_column.cuh"
 #include "hc_rhs_tiled.cuh"
 #include "hc_column_warp.cuh"
+#include "hc_spec.cuh"
 
 // ---------------------------------------------------------------------------
 // small device kernels for the scalar state
@@ -67,7 +68,7 @@ struct FinalArgs {
     int step_base;
     int write_diag;
     int cds;
-    double cfl_prev_dummy;
+    int set_ubar;             // 0: keep the bulk velocity (spectral set-up)
 };
 
 __device__ double block_sum_fixed(double v, double* sh)
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinalArgs a)
         s->div_max[q] = dmax[q];
         if (fabs(dmax[q]) > fabs(s->div_hist)) s->div_hist = dmax[q];
     }
-    if (a.dp_opt == 2) s->ubar = ub / a.lz / a.nx / a.ny;
+    if (a.dp_opt == 2 && a.set_ubar) s->ubar = ub / a.lz / a.nx / a.ny;
     s->cfl = cf;
     if (nan) s->nan_flag = 1;
     if (a.write_diag) {
@@ -185,10 +186,16 @@ enum { F_U, F_V, F_W, F_P, F_T, F_FF, F_GG, F_HH, F_SS, F_QU, F_QV, F_QW, F_UHX,
 
 // kernel categories for the optional per-launch CUDA-event profile
 enum { K_BEGIN, K_RHS_MOM, K_FFT_X_FWD, K_FFT_Y_FWD, K_COLUMN, K_FFT_Y_INV, K_FFT_X_INV,
-       K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_NCAT };
+       K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_SPEC_PROD, K_SPEC_ASM, K_SPEC_AUX, K_NCAT };
 static const char* K_NAMES[K_NCAT] = {"substep_begin", "rhs_momentum", "fft_x_r2c", "fft_y_fwd", "column_fd",
                                       "fft_y_inv", "fft_x_c2r", "rhs_temperature", "column_t", "div_check",
-                                      "stats", "finalize"};
+                                      "stats", "finalize", "spec_products", "spec_assemble", "spec_aux"};
+
+// spectral-path buffers (cds = 3), each n values of the storage type: the half
+// spectra of the state and histories, phi, the divergence, the assembled
+// right-hand sides and work fields (physical products / their spectra)
+enum { SP_U, SP_V, SP_W, SP_P, SP_T, SP_FF, SP_GG, SP_HH, SP_SS, SP_PHI, SP_DIV, SP_QU, SP_QV, SP_QW, SP_W0,
+       NSP = SP_W0 + 14 };
 
 struct hc_handle {
     hc_params p;
@@ -199,6 +206,9 @@ struct hc_handle {
     size_t rsz;              // bytes of the storage type
     void* fld[NFLD];
     void* spec[4];
+    void* sp[NSP];           // cds = 3 only
+    double* dsig;            // cds = 3, isdamp = 1: sigma per level (0 below the layer)
+    double* dmean;           // [5][nz] plane means of the damped levels
     double* mean[11];
     double* zbuf;            // 5*(nz+4)
     double* coef;
@@ -358,12 +368,17 @@ static int build_tables(hc_handle* h)
         buf[o_py + mm] = pois_sym(cds, m, ny, dy2, p.ly);
     }
     // divergence / gradient / second-derivative symbols of the staggered FD operators
-    auto fill_ops = [&](int idx, int n, double hh, size_t od, size_t og, size_t ol, int sgn_idx) {
+    auto fill_ops = [&](int idx, int n, double hh, double L, size_t od, size_t og, size_t ol, int sgn_idx) {
         const int l = sgn_idx;
         const double th = 2.0 * HC_PI * l / n;
         const double c1 = cos(th), s1 = sin(th), c2 = cos(2.0 * th), s2 = sin(2.0 * th);
         double dre, dim, gre, gim, lap;
-        if (cds == 1) {
+        if (cds == 3) {
+            // dev_fft_linear_cmplx (src/module_spectral.f90:1274-1340): i 2 pi l / L and
+            // -(2 pi l / L)^2, zero on the Nyquist mode
+            const double kk = (2 * l == -n) ? 0.0 : 2.0 * HC_PI / L * l;
+            dre = 0.0; dim = kk; gre = 0.0; gim = kk; lap = -kk * kk;
+        } else if (cds == 1) {
             dre = (1.0 - c1) / hh; dim = s1 / hh;
             gre = (c1 - 1.0) / hh; gim = s1 / hh;
             lap = (2.0 * c1 - 2.0) / (hh * hh);
@@ -376,8 +391,8 @@ static int build_tables(hc_handle* h)
         buf[og + 2 * idx] = gre; buf[og + 2 * idx + 1] = gim;
         buf[ol + idx] = lap;
     };
-    for (int l = 0; l < nxh; ++l) fill_ops(l, nx, dx, o_dx, o_gx, o_lx, l);
-    for (int mm = 0; mm < ny; ++mm) fill_ops(mm, ny, dy, o_dy, o_gy, o_ly, lsig(mm, ny));
+    for (int l = 0; l < nxh; ++l) fill_ops(l, nx, dx, p.lx, o_dx, o_gx, o_lx, l);
+    for (int mm = 0; mm < ny; ++mm) fill_ops(mm, ny, dy, p.ly, o_dy, o_gy, o_ly, lsig(mm, ny));
     // per-k Thomas coefficients (interior level kk = Fortran k-3)
     const std::vector<double>& DZ = h->zhost[0];
     const std::vector<double>& DZT = h->zhost[1];
@@ -651,16 +666,18 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     return HC_OK;
 }
 
-// y then x inverse transform of nf half spectra (in place in y) into physical
-// fields, stored or (add[f] = 1) added
-template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* const* in, R* const* out, const int* add, int nf)
+// y then x inverse transform of nf half spectra into physical fields, stored or
+// (add[f] = 1) added. The y pass runs in place on in[f], or reads ysrc[f] and
+// writes in[f] (which then serves as scratch) when ysrc is given.
+template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* const* in, R* const* out, const int* add, int nf,
+                                             const typename V2<R>::T* const* ysrc = nullptr)
 {
     const int* halt = &h->sc->nan_flag;
     if (nf < 1 || nf > HC_FFT_MAXF) return HC_ERR_ARG;
     if (h->fft_ty) {
         FyArgs<R> a;
         memset(&a, 0, sizeof(a));
-        for (int f = 0; f < nf; ++f) a.dst[f] = in[f];
+        for (int f = 0; f < nf; ++f) { a.dst[f] = in[f]; a.src[f] = ysrc ? ysrc[f] : nullptr; }
         a.nxh = h->g.nxh; a.tw = fft_tw<R>(h, 1); a.scale = (R)1; a.halt = halt;
         prof_begin(h, K_FFT_Y_INV);
         int rc = fft_t_dispatch<R>(h, h->g.ny, 4, &a, dim3((h->g.nxh + HC_FFT_TL - 1) / HC_FFT_TL, h->g.nz, nf));
@@ -669,7 +686,7 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
     } else {
     FftYArgs<R> ay;
     memset(&ay, 0, sizeof(ay));
-    for (int f = 0; f < nf; ++f) ay.data[f] = in[f];
+    for (int f = 0; f < nf; ++f) { ay.data[f] = in[f]; ay.src[f] = ysrc ? ysrc[f] : nullptr; }
     ay.nxh = h->g.nxh; ay.ny = h->g.ny; ay.tl = h->tl_y; ay.pl = h->py; ay.scale = 1.0; ay.halt = halt;
     dim3 gy((h->g.nxh + ay.tl - 1) / ay.tl, h->g.nz, nf);
     prof_begin(h, K_FFT_Y_INV);
@@ -722,7 +739,7 @@ template <typename R> static int launch_stats(hc_handle* h, int accumulate)
     return HC_OK;
 }
 
-static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base)
+static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base, int set_ubar = 1)
 {
     FinalArgs f;
     memset(&f, 0, sizeof(f));
@@ -731,6 +748,7 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base
     f.nx = h->p.nx; f.ny = h->p.ny; f.nz = h->p.nz; f.lz = h->p.lz;
     f.dp_opt = h->p.dp_opt; f.diag = h->diag_dev; f.step_base = step_base; f.write_diag = write_diag;
     f.cds = h->p.cds;
+    f.set_ubar = set_ubar;
     prof_begin(h, K_FINAL);
     k_finalize<<<1, 256, 0, h->st>>>(f);
     CKL();
@@ -880,6 +898,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
         if (rc) return rc;
         ColTArgs<R> ct;
         ct.qt = S[0]; ct.c = h->cc; ct.s = h->cs; ct.g = h->g; ct.rk_c = rk_c; ct.halt = halt;
+        ct.out = S[0]; ct.ltr = 0; ct.mtr = 0;
         {
             const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
             const int ks = 2, ke = p.nz + 1;
@@ -918,11 +937,267 @@ template <typename R, int CDS> static int step_fd(hc_handle* h, int step_base)
     return launch_finalize(h, nsub, 1, step_base);
 }
 
+// ---------------------------------------------------------------------------
+// pseudo-spectral sub-step (cds = 3), time_advancement_sp
+// (src/module_navier_stokes.f90:371-517)
+// ---------------------------------------------------------------------------
+static int spec_kchunk(const hc_handle* h, long long columns)
+{
+    // enough blocks for about 8 per SM, chunks of 4..32 levels
+    const long long blocks = (columns + 255) / 256;
+    long long kc = blocks * h->p.nz / (8LL * 148);
+    if (kc < 4) kc = 4;
+    if (kc > 32) kc = 32;
+    if (kc > h->p.nz) kc = h->p.nz;
+    return (int)kc;
+}
+
+template <typename R> static DampTab spec_damp_tab(hc_handle* h)
+{
+    DampTab d;
+    d.sig = h->p.isdamp == 1 ? h->dsig : nullptr;
+    d.mean = h->dmean;
+    return d;
+}
+
+template <typename R, int K> static int col_sp_k(hc_handle* h, const SpColArgs<R>& a)
+{
+    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
+    k_column_sp_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(a);
+    CKL();
+    return HC_OK;
+}
+template <typename R> static int launch_column_sp(hc_handle* h, const SpColArgs<R>& a)
+{
+    switch ((h->p.nz + 31) / 32) {
+    case 1: return col_sp_k<R, 1>(h, a);
+    case 2: return col_sp_k<R, 2>(h, a);
+    case 3: return col_sp_k<R, 3>(h, a);
+    case 4: return col_sp_k<R, 4>(h, a);
+    case 5: return col_sp_k<R, 5>(h, a);
+    case 6: return col_sp_k<R, 6>(h, a);
+    case 7: return col_sp_k<R, 7>(h, a);
+    case 8: return col_sp_k<R, 8>(h, a);
+    default: break;
+    }
+    return HC_ERR_UNSUPPORTED;
+}
+
+template <typename R> static int substep_sp(hc_handle* h, int sub)
+{
+    typedef typename V2<R>::T T2;
+    const hc_params& p = h->p;
+    const Geo& g = h->g;
+    const int* halt = &h->sc->nan_flag;
+    double rk_a, rk_b, rk_c;
+    if (p.dts == 2) { rk_a = RKC1[sub]; rk_b = RKC2[sub]; rk_c = RKC3[sub]; }
+    else { rk_a = 1.5; rk_b = -0.5; rk_c = 1.0; }
+    T2* S[NSP];
+    R* Q[NSP];
+    for (int q = 0; q < NSP; ++q) { S[q] = (T2*)h->sp[q]; Q[q] = (R*)h->sp[q]; }
+    const double tpx = 2.0 * HC_PI / p.lx, tpy = 2.0 * HC_PI / p.ly;
+    const DampTab dtab = spec_damp_tab<R>(h);
+    const int ltr = (int)(p.nx / 3.0), mtr = (int)(p.ny / 3.0);
+    int rc;
+
+    ScalarArgs sa;
+    sa.sc = h->sc; sa.sub = sub; sa.dt = p.dt; sa.dp_opt = p.dp_opt; sa.dpx_coef = h->dpx_coef; sa.um = p.u_mrf;
+    sa.is_ri_var = p.is_ri_var; sa.ri_str = p.ri_str; sa.ri_end = p.ri_end; sa.imax = p.imax;
+    prof_begin(h, K_BEGIN);
+    k_substep_begin<<<1, 1, 0, h->st>>>(sa);
+    CKL();
+
+    // rayleigh_damping_spec on u, v, w, p, t: plane means of the damped levels
+    if (p.isdamp == 1) {
+        DampArgs<R> da;
+        const int fs[5] = {SP_U, SP_V, SP_W, SP_P, SP_T};
+        for (int f = 0; f < 5; ++f) da.f[f] = S[fs[f]];
+        da.mean = h->dmean; da.g = g; da.kd = p.nz - 1 - p.nzdamp; da.halt = halt;
+        prof_begin(h, K_SPEC_AUX);
+        k_spec_damp_mean<R><<<dim3(p.nzdamp + 1, 5), 256, 0, h->st>>>(da);
+        CKL();
+    }
+    // skew-symmetric form: physical images of the horizontal derivatives
+    if (p.issk == 1) {
+        DerivArgs<R> dv;
+        dv.s[0] = S[SP_U]; dv.s[1] = S[SP_V]; dv.s[2] = S[SP_W];
+        for (int f = 0; f < 6; ++f) dv.out[f] = S[SP_W0 + 8 + f];
+        dv.dt = dtab; dv.g = g; dv.tpx = tpx; dv.tpy = tpy; dv.halt = halt;
+        prof_begin(h, K_SPEC_AUX);
+        k_spec_deriv<R><<<RED_BLOCKS, 256, 0, h->st>>>(dv);
+        CKL();
+        T2* din[6];
+        R* dout[6];
+        const int add0[6] = {0, 0, 0, 0, 0, 0};
+        for (int f = 0; f < 6; ++f) { din[f] = S[SP_W0 + 8 + f]; dout[f] = Q[SP_W0 + 8 + f]; }
+        if ((rc = fft_inverse<R>(h, din, dout, add0, 6))) return rc;
+    }
+    // physical products, then one batched forward transform
+    {
+        ProdArgs<R> pa;
+        pa.u = (const R*)h->fld[F_U]; pa.v = (const R*)h->fld[F_V]; pa.w = (const R*)h->fld[F_W]; pa.t = (const R*)h->fld[F_T];
+        for (int f = 0; f < 6; ++f) pa.d[f] = p.issk == 1 ? Q[SP_W0 + 8 + f] : nullptr;
+        for (int f = 0; f < 8; ++f) pa.out[f] = Q[SP_W0 + f];
+        pa.g = g; pa.sc = h->sc;
+        pa.um = p.u_mrf; pa.fc = p.fc; pa.ug = p.ug; pa.vg = p.vg; pa.t_ref = p.t_ref; pa.tbot = p.tbot; pa.ttop = p.ttop;
+        pa.inv_coe = 1.0 / (p.issk == 1 ? 0.5 : 1.0);
+        pa.closed = p.ochannel == 0; pa.dp3 = p.dp_opt == 3; pa.scalar = p.isscalar == 1; pa.skew = p.issk == 1;
+        pa.kchunk = spec_kchunk(h, g.nxy); pa.halt = halt;
+        prof_begin(h, K_SPEC_PROD);
+        k_spec_products<R><<<dim3((unsigned)((g.nxy + 255) / 256), (p.nz + pa.kchunk - 1) / pa.kchunk), 256, 0, h->st>>>(pa);
+        CKL();
+        const R* fin[8];
+        T2* fout[8];
+        for (int f = 0; f < 8; ++f) { fin[f] = Q[SP_W0 + f]; fout[f] = S[SP_W0 + f]; }
+        if ((rc = fft_forward<R>(h, fin, fout, 8))) return rc;
+    }
+    // right-hand sides and new histories, mode by mode
+    {
+        AsmArgs<R> aa;
+        aa.su = S[SP_U]; aa.sv = S[SP_V]; aa.sw = S[SP_W]; aa.sp = S[SP_P];
+        for (int f = 0; f < 8; ++f) aa.F[f] = S[SP_W0 + f];
+        aa.ff = S[SP_FF]; aa.gg = S[SP_GG]; aa.hh = S[SP_HH];
+        aa.qu = S[SP_QU]; aa.qv = S[SP_QV]; aa.qw = S[SP_QW];
+        aa.dt = dtab; aa.g = g; aa.tpx = tpx; aa.tpy = tpy;
+        aa.rk_a = rk_a; aa.rk_b = rk_b; aa.rk_c = rk_c; aa.dtime = p.dt; aa.nu = p.nu; aa.um = p.u_mrf;
+        aa.coe = p.issk == 1 ? 0.5 : 1.0;
+        aa.closed = p.ochannel == 0; aa.kchunk = spec_kchunk(h, g.ncol); aa.halt = halt;
+        prof_begin(h, K_SPEC_ASM);
+        k_spec_assemble<R><<<dim3((unsigned)((g.ncol + 255) / 256), (p.nz + aa.kchunk - 1) / aa.kchunk), 256, 0, h->st>>>(aa);
+        CKL();
+    }
+    // solves, projection, pressure update, truncation, divergence spectrum
+    {
+        SpColArgs<R> ca;
+        memset(&ca, 0, sizeof(ca));
+        ca.b.qu = S[SP_QU]; ca.b.qv = S[SP_QV]; ca.b.qw = S[SP_QW]; ca.b.psi = nullptr;
+        ca.b.c = h->cc; ca.b.s = h->cs; ca.b.g = g;
+        ca.b.rk_c = rk_c; ca.b.dt = p.dt; ca.b.nu = p.nu;
+        const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
+        const int ks = 2, ke = p.nz + 1;
+        ca.b.bcu0 = 2.0 * (-0.5 * rk_c * p.dt * p.nu / DZ[ks] / DZB[ks]) * p.u_mrf;
+        ca.b.bcu1 = p.ochannel == 0 ? 2.0 * (-0.5 * rk_c * p.dt * p.nu / DZ[ke] / DZT[ke]) * p.u_mrf : 0.0;
+        ca.b.halt = halt;
+        ca.su = S[SP_U]; ca.sv = S[SP_V]; ca.sw = S[SP_W]; ca.sp = S[SP_P]; ca.phi = S[SP_PHI]; ca.div = S[SP_DIV];
+        ca.dt = dtab; ca.ltr = ltr; ca.mtr = mtr;
+        prof_begin(h, K_COLUMN);
+        if ((rc = launch_column_sp<R>(h, ca))) return rc;
+    }
+    // physical u, v, w and the divergence image (y out of place into work fields)
+    {
+        const T2* ys[4] = {S[SP_U], S[SP_V], S[SP_W], S[SP_DIV]};
+        T2* scr[4] = {S[SP_W0], S[SP_W0 + 1], S[SP_W0 + 2], S[SP_W0 + 3]};
+        R* outs[4] = {(R*)h->fld[F_U], (R*)h->fld[F_V], (R*)h->fld[F_W], Q[SP_W0 + 3]};
+        const int add0[4] = {0, 0, 0, 0};
+        if ((rc = fft_inverse<R>(h, scr, outs, add0, 4, ys))) return rc;
+    }
+    if (p.isscalar == 1) {
+        ProdTArgs<R> pt;
+        pt.u = (const R*)h->fld[F_U]; pt.v = (const R*)h->fld[F_V]; pt.w = (const R*)h->fld[F_W]; pt.t = (const R*)h->fld[F_T];
+        for (int f = 0; f < 3; ++f) pt.out[f] = Q[SP_W0 + 4 + f];
+        pt.g = g; pt.tbot = p.tbot; pt.ttop = p.ttop; pt.kchunk = spec_kchunk(h, g.nxy); pt.halt = halt;
+        prof_begin(h, K_SPEC_PROD);
+        k_spec_products_t<R><<<dim3((unsigned)((g.nxy + 255) / 256), (p.nz + pt.kchunk - 1) / pt.kchunk), 256, 0, h->st>>>(pt);
+        CKL();
+        const R* fin[3] = {Q[SP_W0 + 4], Q[SP_W0 + 5], Q[SP_W0 + 6]};
+        T2* fout[3] = {S[SP_W0 + 4], S[SP_W0 + 5], S[SP_W0 + 6]};
+        if ((rc = fft_forward<R>(h, fin, fout, 3))) return rc;
+        AsmTArgs<R> at;
+        at.st = S[SP_T];
+        for (int f = 0; f < 3; ++f) at.F[f] = S[SP_W0 + 4 + f];
+        at.ss = S[SP_SS]; at.qt = S[SP_QU];
+        at.dt = dtab; at.g = g; at.tpx = tpx; at.tpy = tpy;
+        at.rk_a = rk_a; at.rk_b = rk_b; at.rk_c = rk_c; at.dtime = p.dt; at.alpha = p.alpha; at.um = p.u_mrf;
+        at.tbot = p.tbot; at.ttop = p.ttop; at.kchunk = spec_kchunk(h, g.ncol); at.halt = halt;
+        prof_begin(h, K_SPEC_ASM);
+        k_spec_assemble_t<R><<<dim3((unsigned)((g.ncol + 255) / 256), (p.nz + at.kchunk - 1) / at.kchunk), 256, 0, h->st>>>(at);
+        CKL();
+        ColTArgs<R> ct;
+        ct.qt = S[SP_QU]; ct.out = S[SP_T]; ct.ltr = ltr; ct.mtr = mtr;
+        ct.c = h->cc; ct.s = h->cs; ct.g = g; ct.rk_c = rk_c; ct.halt = halt;
+        const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
+        const int ks = 2, ke = p.nz + 1;
+        ct.bct0 = -2.0 * (-0.5 * rk_c * p.dt * p.alpha / DZ[ks] / DZB[ks]) * p.tbot;
+        ct.bct1 = -2.0 * (-0.5 * rk_c * p.dt * p.alpha / DZ[ke] / DZT[ke]) * p.ttop;
+        prof_begin(h, K_COLUMN_T);
+        if ((rc = launch_column_t<R>(h, ct))) return rc;
+        const T2* ys[1] = {S[SP_T]};
+        T2* scr[1] = {S[SP_W0]};
+        R* tout[1] = {(R*)h->fld[F_T]};
+        const int add0[1] = {0};
+        if ((rc = fft_inverse<R>(h, scr, tout, add0, 1, ys))) return rc;
+    }
+    FieldsIn<R> fi;
+    fi.u = (const R*)h->fld[F_U]; fi.v = (const R*)h->fld[F_V]; fi.w = (const R*)h->fld[F_W];
+    fi.p = nullptr; fi.t = nullptr;
+    prof_begin(h, K_DIV);
+    k_spec_div_reduce<R><<<(unsigned)h->nbd, 256, 0, h->st>>>(Q[SP_W0 + 3], fi, g.n, h->part_div + (long long)sub * h->nbd * 3);
+    CKL();
+    return HC_OK;
+}
+
+template <typename R> static int step_sp(hc_handle* h, int step_base)
+{
+    const int nsub = h->p.dts == 2 ? 3 : 1;
+    for (int sub = 0; sub < nsub; ++sub) {
+        int rc = substep_sp<R>(h, sub);
+        if (rc) return rc;
+    }
+    int rc = launch_stats<R>(h, 1);
+    if (rc) return rc;
+    return launch_finalize(h, nsub, 1, step_base);
+}
+
+// set-up of the spectral state (src/module_navier_stokes.f90:61-129 with
+// real_2_cmplx, spectral_truncation and cmplx_2_real of src/module_spectral.f90):
+// spectra of u, v, w, p, t and the histories, truncation of the state spectra,
+// and the truncated physical images.
+template <typename R> static int init_sp(hc_handle* h)
+{
+    typedef typename V2<R>::T T2;
+    const int fin_ids[9] = {F_U, F_V, F_W, F_P, F_T, F_FF, F_GG, F_HH, F_SS};
+    const R* in[9];
+    T2* out[9];
+    for (int f = 0; f < 9; ++f) { in[f] = (const R*)h->fld[fin_ids[f]]; out[f] = (T2*)h->sp[SP_U + f]; }
+    int rc = fft_forward<R>(h, in, out, 9);
+    if (rc) return rc;
+    TruncArgs<R> ta;
+    for (int f = 0; f < 5; ++f) ta.f[f] = (T2*)h->sp[SP_U + f];
+    ta.nf = 5; ta.g = h->g; ta.ltr = (int)(h->p.nx / 3.0); ta.mtr = (int)(h->p.ny / 3.0);
+    prof_begin(h, K_SPEC_AUX);
+    k_spec_truncate<R><<<RED_BLOCKS, 256, 0, h->st>>>(ta);
+    CKL();
+    const T2* ys[5];
+    T2* scr[5];
+    R* phys[5];
+    const int add0[5] = {0, 0, 0, 0, 0};
+    for (int f = 0; f < 5; ++f) {
+        ys[f] = (const T2*)h->sp[SP_U + f];
+        scr[f] = (T2*)h->sp[SP_W0 + f];
+        phys[f] = (R*)h->fld[fin_ids[f]];
+    }
+    return fft_inverse<R>(h, scr, phys, add0, 5, ys);
+}
+
+// Physical image of a spectral-only quantity (p, phi, ff..ss) in work field 0.
+template <typename R> static int spec_image(hc_handle* h, int sp_id, void** out)
+{
+    typedef typename V2<R>::T T2;
+    const T2* ys[1] = {(const T2*)h->sp[sp_id]};
+    T2* scr[1] = {(T2*)h->sp[SP_W0]};
+    R* phys[1] = {(R*)h->sp[SP_W0]};
+    const int add0[1] = {0};
+    int rc = fft_inverse<R>(h, scr, phys, add0, 1, ys);
+    if (rc) return rc;
+    *out = h->sp[SP_W0];
+    return HC_OK;
+}
+
 template <typename R> static int step_dispatch(hc_handle* h, int step_base)
 {
     if (h->p.cds == 1) return step_fd<R, 1>(h, step_base);
     if (h->p.cds == 2) return step_fd<R, 2>(h, step_base);
-    return HC_ERR_UNSUPPORTED;
+    return step_sp<R>(h, step_base);
 }
 
 // ---------------------------------------------------------------------------
@@ -950,6 +1225,9 @@ static void free_all(hc_handle* h)
 {
     for (int q = 0; q < NFLD; ++q) if (h->fld[q]) cudaFree(h->fld[q]);
     for (int q = 0; q < 4; ++q) if (h->spec[q]) cudaFree(h->spec[q]);
+    for (int q = 0; q < NSP; ++q) if (h->sp[q]) cudaFree(h->sp[q]);
+    if (h->dsig) cudaFree(h->dsig);
+    if (h->dmean) cudaFree(h->dmean);
     for (int q = 0; q < 11; ++q) if (h->mean[q]) cudaFree(h->mean[q]);
     if (h->zbuf) cudaFree(h->zbuf);
     if (h->coef) cudaFree(h->coef);
@@ -977,14 +1255,18 @@ int hc_create(const hc_params* p, hc_handle** out)
     if (p->isscalar != 0 && p->isscalar != 1) return HC_ERR_PARAM;
     if (p->dp_opt < 1 || p->dp_opt > 3) return HC_ERR_PARAM;
     if (p->precision != HC_PREC_FP64 && p->precision != HC_PREC_MIXED) return HC_ERR_PARAM;
-    if (p->cds == 3) return HC_ERR_UNSUPPORTED;
-    if (p->isdamp == 1) return HC_ERR_UNSUPPORTED;
+    if (p->isdamp == 1 && (p->nzdamp < 1 || p->nzdamp > p->nz - 1)) return HC_ERR_PARAM;
+    if (p->isdamp == 1 && p->cds != 3) return HC_ERR_UNSUPPORTED;
+    // the spectral column kernel keeps a whole column in one warp (nz <= 256)
+    if (p->cds == 3 && p->nz > 256) return HC_ERR_UNSUPPORTED;
 
     hc_handle* h = new hc_handle();
     memset((void*)&h->p, 0, sizeof(h->p));
     h->p = *p;
     for (int q = 0; q < NFLD; ++q) h->fld[q] = nullptr;
     for (int q = 0; q < 4; ++q) h->spec[q] = nullptr;
+    for (int q = 0; q < NSP; ++q) h->sp[q] = nullptr;
+    h->dsig = nullptr; h->dmean = nullptr;
     for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
@@ -1020,6 +1302,26 @@ int hc_create(const hc_params* p, hc_handle** out)
         for (int q = 0; q < 11; ++q) {
             if (cudaMalloc(&h->mean[q], n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
             if (cudaMemset(h->mean[q], 0, n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        }
+        if (p->cds == 3) {
+            const int nsp = SP_W0 + (p->issk == 1 ? 14 : 8);
+            for (int q = 0; q < nsp; ++q) {
+                if (cudaMalloc(&h->sp[q], n * h->rsz) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+                if (cudaMemset(h->sp[q], 0, n * h->rsz) != cudaSuccess) FAIL(HC_ERR_CUDA);
+            }
+            if (cudaMalloc(&h->dmean, 5 * p->nz * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+            if (cudaMemset(h->dmean, 0, 5 * p->nz * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+            if (p->isdamp == 1) {
+                // sigma of rayleigh_damping_spec (src/module_spectral.f90:1345-1391) per level
+                std::vector<double> sig(p->nz, 0.0);
+                const int nzd = p->nzdamp;
+                for (int kk = p->nz - 1 - nzd; kk < p->nz; ++kk) {
+                    const double zd = (kk - (p->nz - 1) + nzd) * 1.0 / nzd;
+                    sig[kk] = p->cdamp * 0.5 * (1.0 - cos(HC_PI * zd));
+                }
+                if (cudaMalloc(&h->dsig, p->nz * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+                if (cudaMemcpy(h->dsig, sig.data(), p->nz * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) FAIL(HC_ERR_CUDA);
+            }
         }
         const long long cz = g.ncol * g.nz;
         if (cudaMalloc(&h->scratch, cz * (3 * sizeof(double) + 4 * sizeof(double2))) != cudaSuccess) FAIL(HC_ERR_NOMEM);
@@ -1113,6 +1415,7 @@ static void* field_dev(hc_handle* h, int id, int* is_mean)
 int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, int ghost)
 {
     if (!h || !host || ghost < 0 || ld1 < h->p.nx + 2 * ghost || ld2 < h->p.ny + 2 * ghost) return HC_ERR_ARG;
+    if (h->p.cds == 3 && h->initialized) return HC_ERR_STATE;
     int is_mean;
     void* d = field_dev(h, field_id, &is_mean);
     if (!d) return HC_ERR_ARG;
@@ -1132,13 +1435,46 @@ int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, 
     return HC_OK;
 }
 
+// On the spectral path p, phi and the histories live as spectra only (after
+// hc_initialize); their physical images are produced on request.
+static int spec_source(hc_handle* h, int field_id)
+{
+    if (h->p.cds != 3) return -1;
+    if (field_id == HC_FIELD_PHI) return SP_PHI;
+    if (!h->initialized) return -1;
+    switch (field_id) {
+    case HC_FIELD_P: return SP_P;
+    case HC_FIELD_FF: return SP_FF;
+    case HC_FIELD_GG: return SP_GG;
+    case HC_FIELD_HH: return SP_HH;
+    case HC_FIELD_SS: return SP_SS;
+    default: break;
+    }
+    return -1;
+}
+
+static void* download_source(hc_handle* h, int field_id, int* is_mean, int* rc)
+{
+    *rc = HC_OK;
+    const int sid = spec_source(h, field_id);
+    if (sid >= 0) {
+        *is_mean = 0;
+        void* d = nullptr;
+        *rc = h->rsz == sizeof(float) ? spec_image<float>(h, sid, &d) : spec_image<double>(h, sid, &d);
+        return *rc ? nullptr : d;
+    }
+    if (field_id == HC_FIELD_PHI) { *rc = HC_ERR_UNSUPPORTED; return nullptr; }
+    void* d = field_dev(h, field_id, is_mean);
+    if (!d) *rc = HC_ERR_ARG;
+    return d;
+}
+
 int hc_download(hc_handle* h, int field_id, double* host, int ld1, int ld2, int ghost)
 {
     if (!h || !host || ghost < 0 || ld1 < h->p.nx + 2 * ghost || ld2 < h->p.ny + 2 * ghost) return HC_ERR_ARG;
-    if (field_id == HC_FIELD_PHI) return HC_ERR_UNSUPPORTED;
-    int is_mean;
-    void* d = field_dev(h, field_id, &is_mean);
-    if (!d) return HC_ERR_ARG;
+    int is_mean, rc;
+    void* d = download_source(h, field_id, &is_mean, &rc);
+    if (!d) return rc;
     CK(cudaStreamSynchronize(h->st));
     const int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
     const long long n = (long long)nx * ny * nz;
@@ -1159,6 +1495,7 @@ int hc_download(hc_handle* h, int field_id, double* host, int ld1, int ld2, int 
 int hc_upload_dev(hc_handle* h, int field_id, const void* dev)
 {
     if (!h || !dev) return HC_ERR_ARG;
+    if (h->p.cds == 3 && h->initialized) return HC_ERR_STATE;
     int is_mean;
     void* d = field_dev(h, field_id, &is_mean);
     if (!d) return HC_ERR_ARG;
@@ -1171,9 +1508,9 @@ int hc_upload_dev(hc_handle* h, int field_id, const void* dev)
 int hc_download_dev(hc_handle* h, int field_id, void* dev)
 {
     if (!h || !dev) return HC_ERR_ARG;
-    int is_mean;
-    void* d = field_dev(h, field_id, &is_mean);
-    if (!d) return HC_ERR_ARG;
+    int is_mean, rc;
+    void* d = download_source(h, field_id, &is_mean, &rc);
+    if (!d) return rc;
     const size_t bytes = h->g.n * (is_mean ? sizeof(double) : h->rsz);
     CK(cudaMemcpyAsync(dev, d, bytes, cudaMemcpyDeviceToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
@@ -1196,6 +1533,17 @@ int hc_initialize(hc_handle* h)
     if (rc) return rc;
     rc = launch_finalize(h, 0, 0, 0);
     if (rc) return rc;
+    if (p.cds == 3) {
+        // the bulk velocity above is that of the fields as given; the spectral
+        // set-up then truncates them, and the first step's CFL sees the truncated ones
+        rc = h->rsz == sizeof(float) ? init_sp<float>(h) : init_sp<double>(h);
+        if (rc) return rc;
+        CK(cudaMemsetAsync((char*)h->fld[F_W] + (size_t)(p.nz - 1) * h->g.nxy * h->rsz, 0, h->g.nxy * h->rsz, h->st));
+        rc = h->rsz == sizeof(float) ? launch_stats<float>(h, 0) : launch_stats<double>(h, 0);
+        if (rc) return rc;
+        rc = launch_finalize(h, 0, 0, 0, 0);
+        if (rc) return rc;
+    }
     CK(cudaStreamSynchronize(h->st));
     h->initialized = 1;
     return HC_OK;

@@ -242,8 +242,19 @@ template <typename R> struct ColTArgs {
     Geo g;
     double rk_c;
     double bct0, bct1;       // (0,0)-mode Dirichlet source corrections (tbnd)
+    typename V2<R>::T* out;  // solution (may equal qt)
+    int ltr, mtr;            // > 0: spectral truncation, modes |l| >= ltr or |m| >= mtr set to 0
     const int* halt;
 };
+
+// 2/3-rule truncation test (spectral_truncation, src/module_spectral.f90:1222-1268)
+// for half-spectrum column (l, m); m in FFT order.
+__device__ __forceinline__ bool spec_truncated(int l, int m, int ny, int ltr, int mtr)
+{
+    if (ltr <= 0) return false;
+    const int ms = m < ny / 2 ? m : m - ny;
+    return l >= ltr || ms >= mtr || ms <= -mtr;
+}
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_column_t(ColTArgs<R> a)
@@ -278,6 +289,7 @@ __global__ void __launch_bounds__(256) k_column_t(ColTArgs<R> a)
         b_p = b; s_p = s;
     }
     double2 x = make_double2(0, 0);
+    const bool tr = spec_truncated(l, m, a.g.ny, a.ltr, a.mtr);
     for (int k = nz - 1; k >= 0; --k) {
         const long long id = (long long)k * ncol + c;
         const double b = a.s.bu[id];
@@ -287,6 +299,6 @@ __global__ void __launch_bounds__(256) k_column_t(ColTArgs<R> a)
             const double cc = rk * __ldg(a.c.ct + k);
             x = make_double2((s.x - cc * x.x) / b, (s.y - cc * x.y) / b);
         }
-        st2<R>(a.qt, id, x);
+        st2<R>(a.out, id, tr ? make_double2(0, 0) : x);
     }
 }

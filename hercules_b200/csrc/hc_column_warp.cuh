@@ -313,9 +313,10 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_column_t_warp(ColTArgs<R> a)
         } else { aa = 0.0; bb = 1.0; cc = 0.0; }
     };
     warp_partition_solve<K, 1>(cf, d, ln);
+    const bool tr = spec_truncated(l, m, a.g.ny, a.ltr, a.mtr);
 #pragma unroll
     for (int i = 0; i < K; ++i) {
         const int r = r0 + i;
-        if (r < nz) st2<R>(a.qt, (long long)r * ncol + c, d[0][i]);
+        if (r < nz) st2<R>(a.out, (long long)r * ncol + c, tr ? make_double2(0, 0) : d[0][i]);
     }
 }

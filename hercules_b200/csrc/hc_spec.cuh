@@ -1,0 +1,688 @@
+// hc_spec.cuh -- kernels of the pseudo-spectral time step (cds = 3).
+//
+// The reference (time_advancement_sp, src/module_navier_stokes.f90:371-517, with
+// the operators of src/module_spectral.f90) keeps u, v, w, p, t and the
+// explicit-term histories ff, gg, hh, ss as 2-D spectra per level and takes
+// every horizontal derivative by multiplying with i k. This engine keeps the
+// same state as half spectra [k][m][l] (l < nx/2) and restructures the work:
+//   * every physical-space product of get_momentum_cnvdiff_spec (:35-504) is
+//     formed in one pass (k_spec_products) and the eight resulting fields go
+//     through one batched forward FFT; the skew-symmetric terms (issk = 1) are
+//     added into the same fields, which FFT linearity allows;
+//   * the terms the reference forms in physical space from u, v, w, p and phi
+//     with linear z-stencils (d2/dz2, dp/dz, dw/dz, dphi/dz) are applied to the
+//     spectra directly, with the ghost values of update_boundary_uvw/p/t
+//     (src/module_boundary.f90:33-196) carried over to the modes (a constant
+//     ghost offset lands on the (0,0) mode only);
+//   * Rayleigh damping (rayleigh_damping_spec, src/module_spectral.f90:1345-1391)
+//     is applied on the fly from a per-level table (sigma, plane mean), so the
+//     undamped spectra stay available for the terms the reference takes from
+//     the (undamped) physical fields;
+//   * the solves, the divergence source, the projection, the pressure update,
+//     the 2/3-rule truncation and the divergence diagnostic are fused into one
+//     warp-per-column kernel (k_column_sp_warp).
+// All arithmetic of the spectral operators is FP64; spectra are stored in the
+// storage precision.
+#pragma once
+#include "hc_column_warp.cuh"
+#include "hc_fd.cuh"
+
+// x / y wavenumber of half-spectrum column (l, m); the y Nyquist row (m = ny/2)
+// is zeroed by every dev_fft_* operator and forward transform of the reference.
+struct SpecWave {
+    double kx, ky;    // 2 pi l / lx, 2 pi m' / ly (0 on the Nyquist row)
+    double zp;        // 0 on the Nyquist row, else 1
+    bool is00;
+};
+__device__ __forceinline__ SpecWave spec_wave(long long c, const Geo& g, double tpx, double tpy)
+{
+    SpecWave s;
+    const int l = (int)(c % g.nxh), m = (int)(c / g.nxh);
+    const int ms = m < g.ny / 2 ? m : m - g.ny;
+    const bool nyq = (m == g.ny / 2);
+    s.kx = nyq ? 0.0 : tpx * l;
+    s.ky = nyq ? 0.0 : tpy * ms;
+    s.zp = nyq ? 0.0 : 1.0;
+    s.is00 = (c == 0);
+    return s;
+}
+__device__ __forceinline__ double2 mul_i(double2 a, double k) { return make_double2(-k * a.y, k * a.x); }   // i k a
+__device__ __forceinline__ double2 zfma(double2 acc, double2 a, double s) { return make_double2(acc.x + s * a.x, acc.y + s * a.y); }
+
+// damped value of a mode: c - sigma (c - mean), the mean being real
+__device__ __forceinline__ double2 damp_mode(double2 c, double sig, double mall)
+{
+    return make_double2(c.x - sig * (c.x - mall), c.y - sig * c.y);
+}
+
+// ---------------------------------------------------------------------------
+// plane means of the damped levels (rayleigh_damping_spec :1345-1391): the real
+// part of the sum over the full spectrum, i.e. the l = 0 column once and every
+// l > 0 mode twice (its conjugate partner is not stored), divided by nx ny.
+// grid (levels, fields), 256 threads; fixed reduction order.
+// ---------------------------------------------------------------------------
+template <typename R> struct DampArgs {
+    const typename V2<R>::T* f[5];   // S_u, S_v, S_w, S_p, S_t
+    double* mean;                    // [5][nz], written for k >= kd
+    Geo g;
+    int kd;
+    const int* halt;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_damp_mean(DampArgs<R> a)
+{
+    __shared__ double sh[8];
+    if (a.halt && *a.halt) return;
+    const int k = a.kd + blockIdx.x, f = blockIdx.y;
+    const long long ncol = a.g.ncol;
+    const typename V2<R>::T* s = a.f[f] + (long long)k * ncol;
+    double sm = 0.0;
+    for (long long c = threadIdx.x; c < ncol; c += blockDim.x) {
+        const double re = (double)s[c].x;
+        sm += (c % a.g.nxh == 0) ? re : 2.0 * re;
+    }
+    sm = warp_sum(sm);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        a.mean[f * a.g.nz + k] = t / (double)a.g.nx / (double)a.g.ny;
+    }
+}
+
+// per-level damping of field f: (sigma, mean); sigma = 0 below the layer
+struct DampTab {
+    const double* sig;     // [nz] (null: no damping)
+    const double* mean;    // [5][nz]
+    __device__ __forceinline__ double2 at(double2 c, int f, int k, int nz) const
+    {
+        if (!sig) return c;
+        const double s = __ldg(sig + k);
+        return s == 0.0 ? c : damp_mode(c, s, mean[f * nz + k]);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// spectra of the horizontal derivatives of the damped u, v, w for the skew-
+// symmetric terms (issk = 1): i kx D_u, i ky D_u, i kx D_v, i ky D_v, i kx D_w,
+// i ky D_w (dev_fft_linear_cmplx :1274-1340, Nyquist row zeroed)
+// ---------------------------------------------------------------------------
+template <typename R> struct DerivArgs {
+    const typename V2<R>::T* s[3];   // S_u, S_v, S_w
+    typename V2<R>::T* out[6];
+    DampTab dt;
+    Geo g;
+    double tpx, tpy;
+    const int* halt;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_deriv(DerivArgs<R> a)
+{
+    if (a.halt && *a.halt) return;
+    const long long ncol = a.g.ncol, n = ncol * a.g.nz;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < n; id += (long long)gridDim.x * blockDim.x) {
+        const long long c = id % ncol;
+        const int k = (int)(id / ncol);
+        const SpecWave w = spec_wave(c, a.g, a.tpx, a.tpy);
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            const double2 d = a.dt.at(ld2<R>(a.s[f], id), f, k, a.g.nz);
+            st2<R>(a.out[2 * f], id, mul_i(d, w.kx));
+            st2<R>(a.out[2 * f + 1], id, mul_i(d, w.ky));
+        }
+    }
+}
+
+// spectral_truncation (src/module_spectral.f90:1222-1268) of nf spectra
+template <typename R> struct TruncArgs {
+    typename V2<R>::T* f[5];
+    int nf;
+    Geo g;
+    int ltr, mtr;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_truncate(TruncArgs<R> a)
+{
+    const long long ncol = a.g.ncol, n = ncol * a.g.nz;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < n; id += (long long)gridDim.x * blockDim.x) {
+        const long long c = id % ncol;
+        if (!spec_truncated((int)(c % a.g.nxh), (int)(c / a.g.nxh), a.g.ny, a.ltr, a.mtr)) continue;
+        for (int f = 0; f < a.nf; ++f) st2<R>(a.f[f], id, make_double2(0, 0));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// physical-space products of get_momentum_cnvdiff_spec (:35-504), one thread per
+// (i, j), marching over a chunk of levels with the z neighbours in registers:
+//   P0 = u u, P1 = u v, P2 = v v                       (dev_fft_nonlinear_cmplx)
+//   P3 = u_t w, P4 = v_t w    (u_t = l_t u(k+1) + (1 - l_t) u(k), the w equation)
+//   P5..P7 = the per-equation physical terms that are transformed without a
+//   derivative: pressure drive / Coriolis / buoyancy divided by coe_sk, minus
+//   the vertical flux divergence, minus (issk = 1) the three skew-symmetric
+//   products, whose spectra the reference subtracts with the same factor coe_sk.
+// Ghost values follow update_boundary_uvw / update_boundary_t.
+// ---------------------------------------------------------------------------
+template <typename R> struct ProdArgs {
+    const R* u; const R* v; const R* w; const R* t;
+    const R* d[6];          // issk: du/dx, du/dy, dv/dx, dv/dy, dw/dx, dw/dy (physical), else null
+    R* out[8];
+    Geo g;
+    const DevScalars* sc;
+    double um, fc, ug, vg, t_ref, tbot, ttop, inv_coe;
+    int closed, dp3, scalar, skew, kchunk;
+    const int* halt;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_products(ProdArgs<R> a)
+{
+    if (a.halt && *a.halt) return;
+    const Geo& g = a.g;
+    const long long ij = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= g.nxy) return;
+    const int nz = g.nz;
+    const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    const long long nxy = g.nxy;
+    const double um = a.um;
+    auto U = [&](int k) -> double {
+        if (k < 0) return -(double)a.u[ij] - 2.0 * um;
+        if (k >= nz) return a.closed ? -(double)a.u[(long long)(nz - 1) * nxy + ij] - 2.0 * um : (double)a.u[(long long)(nz - 1) * nxy + ij];
+        return (double)a.u[(long long)k * nxy + ij];
+    };
+    auto V = [&](int k) -> double {
+        if (k < 0) return -(double)a.v[ij];
+        if (k >= nz) return a.closed ? -(double)a.v[(long long)(nz - 1) * nxy + ij] : (double)a.v[(long long)(nz - 1) * nxy + ij];
+        return (double)a.v[(long long)k * nxy + ij];
+    };
+    auto W = [&](int k) -> double {
+        if (k < 0) return 0.0;
+        if (k >= nz) return -(double)a.w[(long long)(nz - 2) * nxy + ij];
+        return (double)a.w[(long long)k * nxy + ij];
+    };
+    auto T = [&](int k) -> double {
+        if (!a.scalar) return 0.0;
+        if (k < 0) return 2.0 * a.tbot - (double)a.t[ij];
+        if (k >= nz) return 2.0 * a.ttop - (double)a.t[(long long)(nz - 1) * nxy + ij];
+        return (double)a.t[(long long)k * nxy + ij];
+    };
+    const double dpx = a.sc->dpx_drive, got = a.sc->got, ic = a.inv_coe;
+    double um_ = U(k0 - 1), uk = U(k0), vm = V(k0 - 1), vk = V(k0), wm = W(k0 - 1), wk = W(k0), tk = T(k0);
+    for (int k = k0; k < k1; ++k) {
+        const double up = U(k + 1), vp = V(k + 1), wp = W(k + 1), tp = T(k + 1);
+        const double lt = ldz(g.z.l_t, k), lb = ldz(g.z.l_b, k);
+        const double rdz = 1.0 / ldz(g.z.dz, k), rdzt = 1.0 / ldz(g.z.dz_t, k);
+        const long long q = (long long)k * nxy + ij;
+        const double a1u = up * lt + uk * (1.0 - lt), a2u = um_ * lb + uk * (1.0 - lb);
+        const double a1v = vp * lt + vk * (1.0 - lt), a2v = vm * lb + vk * (1.0 - lb);
+        double cu = ic * (a.dp3 ? a.fc * (vk - a.vg) : dpx) - (a1u * wk - a2u * wm) * rdz;
+        double cv = ic * (a.dp3 ? a.fc * (a.ug - uk - um) : 0.0) - (a1v * wk - a2v * wm) * rdz;
+        const double hp = 0.5 * (wk + wp), hm = 0.5 * (wk + wm);
+        const double tmpw = (hp * hp - hm * hm) * rdzt;
+        double cw = a.scalar ? ic * (got * ((1.0 - lt) * tk + lt * tp - a.t_ref)) - tmpw : -tmpw;
+        if (a.skew) {
+            const double wc = 0.5 * (wk + wm);
+            cu -= uk * (double)a.d[0][q] + vk * (double)a.d[1][q] + (a1u - a2u) * rdz * wc;
+            cv -= uk * (double)a.d[2][q] + vk * (double)a.d[3][q] + (a1v - a2v) * rdz * wc;
+            cw -= a1u * (double)a.d[4][q] + a1v * (double)a.d[5][q] + wk * ((hp - hm) * rdzt);
+        }
+        a.out[0][q] = (R)(uk * uk);
+        a.out[1][q] = (R)(uk * vk);
+        a.out[2][q] = (R)(vk * vk);
+        a.out[3][q] = (R)(a1u * wk);
+        a.out[4][q] = (R)(a1v * wk);
+        a.out[5][q] = (R)cu;
+        a.out[6][q] = (R)cv;
+        a.out[7][q] = (R)cw;
+        um_ = uk; uk = up; vm = vk; vk = vp; wm = wk; wk = wp; tk = tp;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Right-hand sides and new explicit-term histories of the momentum equations,
+// mode by mode (get_momentum_cnvdiff_spec :35-504). One thread per column
+// (l, m), marching over a chunk of levels with the z neighbours in registers.
+// With D_x the damped and S_x the undamped spectrum, ad = rk_c dt nu / 2:
+//   q_u = D_u - ad (kx^2 + ky^2) D_u + ad Lz S_u - rk_c dt i kx D_p + rk_b dt ff
+//   ff' = -u_mrf i kx D_u - coe (i kx F[uu] + i ky F[uv]) + coe F[P5]
+//   q_u += rk_a dt ff'
+// and alike for v (gg) and w (hh, with -rk_c dt d/dz S_p and the staggered
+// operator Lzw). Lz / Lzw / d/dz act on the modes with the ghost values the
+// reference's boundary routines give the physical fields.
+// ---------------------------------------------------------------------------
+template <typename R> struct AsmArgs {
+    const typename V2<R>::T* su; const typename V2<R>::T* sv; const typename V2<R>::T* sw; const typename V2<R>::T* sp;
+    const typename V2<R>::T* F[8];    // spectra of P0..P7
+    typename V2<R>::T* ff; typename V2<R>::T* gg; typename V2<R>::T* hh;   // in: old, out: new
+    typename V2<R>::T* qu; typename V2<R>::T* qv; typename V2<R>::T* qw;
+    DampTab dt;
+    Geo g;
+    double tpx, tpy;
+    double rk_a, rk_b, rk_c, dtime, nu, um, coe;
+    int closed, kchunk;
+    const int* halt;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_assemble(AsmArgs<R> a)
+{
+    typedef typename V2<R>::T T2;
+    if (a.halt && *a.halt) return;
+    const Geo& g = a.g;
+    const long long ncol = g.ncol;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncol) return;
+    const int nz = g.nz;
+    const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    const SpecWave wv = spec_wave(c, g, a.tpx, a.tpy);
+    const double o00 = wv.is00 ? -2.0 * a.um : 0.0;     // u ghost offset, (0,0) mode only
+    auto ld = [&](const T2* f, int k) { return ld2<R>(f, (long long)k * ncol + c); };
+    auto SU = [&](int k) -> double2 {
+        if (k < 0) { double2 s = ld(a.su, 0); return make_double2(-s.x + o00, -s.y); }
+        if (k >= nz) {
+            double2 s = ld(a.su, nz - 1);
+            return a.closed ? make_double2(-s.x + o00, -s.y) : s;
+        }
+        return ld(a.su, k);
+    };
+    auto SV = [&](int k) -> double2 {
+        if (k < 0) { double2 s = ld(a.sv, 0); return make_double2(-s.x, -s.y); }
+        if (k >= nz) { double2 s = ld(a.sv, nz - 1); return a.closed ? make_double2(-s.x, -s.y) : s; }
+        return ld(a.sv, k);
+    };
+    // w as the physical field sees it: 0 below the bottom wall and on the top wall
+    auto SW = [&](int k) -> double2 {
+        if (k < 0 || k == nz - 1) return make_double2(0, 0);
+        if (k >= nz) { double2 s = ld(a.sw, nz - 2); return make_double2(-s.x, -s.y); }
+        return ld(a.sw, k);
+    };
+    auto SP = [&](int k) -> double2 { return ld(a.sp, k < 0 ? 0 : (k >= nz ? nz - 1 : k)); };
+    const double ad = a.rk_c * 0.5 * a.dtime * a.nu, cdt = a.rk_c * a.dtime;
+    const double bdt = a.rk_b * a.dtime, adt = a.rk_a * a.dtime, coe = a.coe;
+    const double k2 = wv.kx * wv.kx + wv.ky * wv.ky;
+    double2 um_ = SU(k0 - 1), uk = SU(k0), vm = SV(k0 - 1), vk = SV(k0), wm = SW(k0 - 1), wk = SW(k0);
+    double2 pk = SP(k0);
+    for (int k = k0; k < k1; ++k) {
+        const double2 up = SU(k + 1), vp = SV(k + 1), wp = SW(k + 1), pp = SP(k + 1);
+        const long long id = (long long)k * ncol + c;
+        const double rdz = 1.0 / ldz(g.z.dz, k), rdzt = 1.0 / ldz(g.z.dz_t, k), rdzb = 1.0 / ldz(g.z.dz_b, k);
+        const double rdz1 = 1.0 / ldz(g.z.dz, k + 1);
+        const double2 Du = a.dt.at(uk, 0, k, nz);
+        const double2 Dv = a.dt.at(vk, 1, k, nz);
+        const double2 Dw = a.dt.at(ld(a.sw, k), 2, k, nz);
+        const double2 Dp = a.dt.at(pk, 3, k, nz);
+        const double2 Fuu = ld(a.F[0], k), Fuv = ld(a.F[1], k), Fvv = ld(a.F[2], k), Futw = ld(a.F[3], k);
+        const double2 Fvtw = ld(a.F[4], k), Fcu = ld(a.F[5], k), Fcv = ld(a.F[6], k), Fcw = ld(a.F[7], k);
+        // vertical operators (zero on the Nyquist row, as the forward FFT leaves them)
+        const double zs = wv.zp;
+        const double2 lzu = make_double2(zs * (((up.x - uk.x) * rdzt - (uk.x - um_.x) * rdzb) * rdz),
+                                         zs * (((up.y - uk.y) * rdzt - (uk.y - um_.y) * rdzb) * rdz));
+        const double2 lzv = make_double2(zs * (((vp.x - vk.x) * rdzt - (vk.x - vm.x) * rdzb) * rdz),
+                                         zs * (((vp.y - vk.y) * rdzt - (vk.y - vm.y) * rdzb) * rdz));
+        const double2 lzw = make_double2(zs * (((wp.x - wk.x) * rdz1 - (wk.x - wm.x) * rdz) * rdzt),
+                                         zs * (((wp.y - wk.y) * rdz1 - (wk.y - wm.y) * rdz) * rdzt));
+        const double2 dpz = make_double2(zs * (pp.x - pk.x) * rdzt, zs * (pp.y - pk.y) * rdzt);
+        // u
+        double2 q = zfma(zfma(Du, Du, -ad * k2), lzu, ad);
+        q = zfma(q, mul_i(Dp, wv.kx), -cdt);
+        q = zfma(q, ld(a.ff, k), bdt);
+        double2 h = make_double2(0, 0);
+        h = zfma(h, mul_i(Du, wv.kx), -a.um);
+        h = zfma(h, mul_i(Fuu, wv.kx), -coe);
+        h = zfma(h, mul_i(Fuv, wv.ky), -coe);
+        h = zfma(h, Fcu, coe);
+        st2<R>(a.ff, id, h);
+        st2<R>(a.qu, id, zfma(q, h, adt));
+        // v
+        q = zfma(zfma(Dv, Dv, -ad * k2), lzv, ad);
+        q = zfma(q, mul_i(Dp, wv.ky), -cdt);
+        q = zfma(q, ld(a.gg, k), bdt);
+        h = make_double2(0, 0);
+        h = zfma(h, mul_i(Dv, wv.kx), -a.um);
+        h = zfma(h, mul_i(Fuv, wv.kx), -coe);
+        h = zfma(h, mul_i(Fvv, wv.ky), -coe);
+        h = zfma(h, Fcv, coe);
+        st2<R>(a.gg, id, h);
+        st2<R>(a.qv, id, zfma(q, h, adt));
+        // w
+        q = zfma(zfma(Dw, Dw, -ad * k2), lzw, ad);
+        q = zfma(q, dpz, -cdt);
+        q = zfma(q, ld(a.hh, k), bdt);
+        h = make_double2(0, 0);
+        h = zfma(h, mul_i(Dw, wv.kx), -a.um);
+        h = zfma(h, mul_i(Futw, wv.kx), -coe);
+        h = zfma(h, mul_i(Fvtw, wv.ky), -coe);
+        h = zfma(h, Fcw, coe);
+        st2<R>(a.hh, id, h);
+        st2<R>(a.qw, id, zfma(q, h, adt));
+        um_ = uk; uk = up; vm = vk; vk = vp; wm = wk; wk = wp; pk = pp;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// temperature (get_temperature_cnvdiff_spec :509-595): products u t, t v and the
+// vertical flux divergence d(t w)/dz with the new u, v, w and the old t
+// ---------------------------------------------------------------------------
+template <typename R> struct ProdTArgs {
+    const R* u; const R* v; const R* w; const R* t;
+    R* out[3];
+    Geo g;
+    double tbot, ttop;
+    int kchunk;
+    const int* halt;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_products_t(ProdTArgs<R> a)
+{
+    if (a.halt && *a.halt) return;
+    const Geo& g = a.g;
+    const long long ij = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= g.nxy) return;
+    const int nz = g.nz;
+    const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    const long long nxy = g.nxy;
+    auto T = [&](int k) -> double {
+        if (k < 0) return 2.0 * a.tbot - (double)a.t[ij];
+        if (k >= nz) return 2.0 * a.ttop - (double)a.t[(long long)(nz - 1) * nxy + ij];
+        return (double)a.t[(long long)k * nxy + ij];
+    };
+    double tm = T(k0 - 1), tk = T(k0);
+    double wm = k0 > 0 ? (double)a.w[(long long)(k0 - 1) * nxy + ij] : 0.0;
+    for (int k = k0; k < k1; ++k) {
+        const double tp = T(k + 1);
+        const long long q = (long long)k * nxy + ij;
+        const double uk = (double)a.u[q], vk = (double)a.v[q], wk = (double)a.w[q];
+        const double lt = ldz(g.z.l_t, k), lb = ldz(g.z.l_b, k);
+        const double a1 = tp * lt + tk * (1.0 - lt), a2 = tm * lb + tk * (1.0 - lb);
+        a.out[0][q] = (R)(uk * tk);
+        a.out[1][q] = (R)(tk * vk);
+        a.out[2][q] = (R)((a1 * wk - a2 * wm) / ldz(g.z.dz, k));
+        tm = tk; tk = tp; wm = wk;
+    }
+}
+
+template <typename R> struct AsmTArgs {
+    const typename V2<R>::T* st;
+    const typename V2<R>::T* F[3];
+    typename V2<R>::T* ss;     // in: old, out: new
+    typename V2<R>::T* qt;
+    DampTab dt;
+    Geo g;
+    double tpx, tpy;
+    double rk_a, rk_b, rk_c, dtime, alpha, um, tbot, ttop;
+    int kchunk;
+    const int* halt;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_assemble_t(AsmTArgs<R> a)
+{
+    typedef typename V2<R>::T T2;
+    if (a.halt && *a.halt) return;
+    const Geo& g = a.g;
+    const long long ncol = g.ncol;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncol) return;
+    const int nz = g.nz;
+    const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    const SpecWave wv = spec_wave(c, g, a.tpx, a.tpy);
+    auto ld = [&](const T2* f, int k) { return ld2<R>(f, (long long)k * ncol + c); };
+    auto ST = [&](int k) -> double2 {
+        if (k < 0) { double2 s = ld(a.st, 0); return make_double2(-s.x + (wv.is00 ? 2.0 * a.tbot : 0.0), -s.y); }
+        if (k >= nz) { double2 s = ld(a.st, nz - 1); return make_double2(-s.x + (wv.is00 ? 2.0 * a.ttop : 0.0), -s.y); }
+        return ld(a.st, k);
+    };
+    const double at = a.rk_c * 0.5 * a.dtime * a.alpha;
+    const double bdt = a.rk_b * a.dtime, adt = a.rk_a * a.dtime;
+    const double k2 = wv.kx * wv.kx + wv.ky * wv.ky;
+    double2 tm = ST(k0 - 1), tk = ST(k0);
+    for (int k = k0; k < k1; ++k) {
+        const double2 tp = ST(k + 1);
+        const long long id = (long long)k * ncol + c;
+        const double rdz = 1.0 / ldz(g.z.dz, k), rdzt = 1.0 / ldz(g.z.dz_t, k), rdzb = 1.0 / ldz(g.z.dz_b, k);
+        const double2 Dt = a.dt.at(tk, 4, k, nz);
+        const double zs = wv.zp;
+        const double2 lzt = make_double2(zs * (((tp.x - tk.x) * rdzt - (tk.x - tm.x) * rdzb) * rdz),
+                                         zs * (((tp.y - tk.y) * rdzt - (tk.y - tm.y) * rdzb) * rdz));
+        double2 q = zfma(zfma(Dt, Dt, -at * k2), lzt, at);
+        q = zfma(q, ld(a.ss, k), bdt);
+        double2 h = make_double2(0, 0);
+        h = zfma(h, mul_i(Dt, wv.kx), -a.um);
+        h = zfma(h, mul_i(ld(a.F[0], k), wv.kx), -1.0);
+        h = zfma(h, mul_i(ld(a.F[1], k), wv.ky), -1.0);
+        h = zfma(h, ld(a.F[2], k), -1.0);
+        st2<R>(a.ss, id, h);
+        st2<R>(a.qt, id, zfma(q, h, adt));
+        tm = tk; tk = tp;
+    }
+}
+
+// screen_div_error_spec (src/module_spectral.f90:899-1007) on the physical image
+// of the divergence spectrum: per block sum |div|, the div of largest magnitude
+// and a NaN flag over u, v, w (same partial layout as k_div_check).
+template <typename R>
+__global__ void __launch_bounds__(256) k_spec_div_reduce(const R* div, FieldsIn<R> f, long long n, double* part)
+{
+    __shared__ double s_sum[8], s_max[8];
+    __shared__ int s_nan;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_nan = 0;
+    __syncthreads();
+    double sm = 0.0, mx = 0.0;
+    int nan = 0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + tid; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const double d = (double)div[q];
+        const double uc = (double)f.u[q], vc = (double)f.v[q], wc = (double)f.w[q];
+        if (uc != uc || vc != vc || wc != wc || d != d) { nan = 1; continue; }
+        sm += fabs(d);
+        mx = absmax_pick(mx, d);
+    }
+    if (nan) s_nan = 1;
+    sm = warp_sum(sm);
+    mx = warp_absmax(mx);
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) { s_sum[wid] = sm; s_max[wid] = mx; }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        sm = lane < nw ? s_sum[lane] : 0.0;
+        mx = lane < nw ? s_max[lane] : 0.0;
+        sm = warp_sum(sm);
+        mx = warp_absmax(mx);
+        if (lane == 0) {
+            part[3 * blockIdx.x + 0] = sm;
+            part[3 * blockIdx.x + 1] = mx;
+            part[3 * blockIdx.x + 2] = s_nan ? 1.0 : 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused wall-normal part of one spectral sub-step, one warp per column (l, m)
+// (rows per lane K = ceil(nz/32)), in the order of time_advancement_sp
+// (src/module_navier_stokes.f90:371-517):
+//   u*, v*, w* Helmholtz solves (poisson_solver_fft_spec :602-746, ubnd and
+//   zstagger as the finite-difference path); the phi source get_div_spec/dt
+//   (:752-795) with the delnull pin; the phi Poisson solve; the pressure update
+//   p = D_p + phi - rk_c dt nu/2 lap(phi) (calculate_new_p_spec :854-894); the
+//   projection (calculate_uvw_spec :801-849); the 2/3-rule truncation of u, v,
+//   w, p; and the divergence spectrum of the final fields for the diagnostic.
+// phi is stored untruncated (the reference's physical phi is its image).
+// ---------------------------------------------------------------------------
+template <typename R> struct SpColArgs {
+    ColArgs<R> b;                    // qu, qv, qw: assembled right-hand sides (read only)
+    typename V2<R>::T* su; typename V2<R>::T* sv; typename V2<R>::T* sw; typename V2<R>::T* sp;
+    typename V2<R>::T* phi; typename V2<R>::T* div;
+    DampTab dt;
+    int ltr, mtr;
+};
+
+template <typename R> __device__ __forceinline__ double2 round_to(double2 v)
+{
+    return make_double2((double)(R)v.x, (double)(R)v.y);
+}
+
+template <typename R, int K>
+__global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_sp_warp(SpColArgs<R> A)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const ColArgs<R>& a = A.b;
+    if (a.halt && *a.halt) return;
+    const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const long long ncol = a.g.ncol;
+    const long long c = (long long)blockIdx.x * CW_WARPS + wp;
+    if (c >= ncol) return;                       // uniform per warp
+    double2* SU = reinterpret_cast<double2*>(smem_raw) + (size_t)wp * 3 * K * 32;
+    double2* SV = SU + K * 32;
+    double2* SW = SV + K * 32;
+    const int nz = a.g.nz;
+    const int l = (int)(c % a.g.nxh), m = (int)(c / a.g.nxh);
+    const bool is00 = (c == 0), nyq = (m == a.g.ny / 2);
+    const double rk = a.rk_c, dt = a.dt;
+    const double lam = __ldg(a.c.hx + l) + __ldg(a.c.hy + m);
+    const double lamp = __ldg(a.c.px + l) + __ldg(a.c.py + m);
+    const double* dgu = is00 ? a.c.d0u : a.c.dgu;
+    const double* dgw = is00 ? a.c.d0w : a.c.dgw;
+    const double* dgp = is00 ? a.c.d0p : a.c.dgp;
+    const int r0 = ln * K;
+    // ---- u*, v*: one matrix, two right-hand sides
+    {
+        double2 d[2][K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            if (r < nz) {
+                const long long id = (long long)r * ncol + c;
+                d[0][i] = ld2<R>(a.qu, id);
+                d[1][i] = ld2<R>(a.qv, id);
+                if (is00 && r == 0) d[0][i].x += a.bcu0;
+                if (is00 && r == nz - 1) d[0][i].x += a.bcu1;
+            } else {
+                d[0][i] = make_double2(0, 0);
+                d[1][i] = make_double2(0, 0);
+            }
+        }
+        auto cf = [&](int r, double& aa, double& bb, double& cc) {
+            if (r < nz) {
+                aa = rk * __ldg(a.c.au + r);
+                cc = rk * __ldg(a.c.cu + r);
+                bb = 1.0 + rk * (-lam + __ldg(dgu + r));
+            } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+        };
+        warp_partition_solve<K, 2>(cf, d, ln);
+#pragma unroll
+        for (int i = 0; i < K; ++i) { SU[i * 32 + ln] = d[0][i]; SV[i * 32 + ln] = d[1][i]; }
+    }
+    // ---- w*: rows 0..nz-2 (the top-wall row is an identity row with zero source)
+    {
+        double2 dw[1][K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            dw[0][i] = r < nz - 1 ? ld2<R>(a.qw, (long long)r * ncol + c) : make_double2(0, 0);
+        }
+        auto cf = [&](int r, double& aa, double& bb, double& cc) {
+            if (r < nz - 1) {
+                aa = rk * __ldg(a.c.aw + r);
+                cc = rk * __ldg(a.c.cw + r);
+                bb = 1.0 + rk * (-lam + __ldg(dgw + r));
+            } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+        };
+        warp_partition_solve<K, 1>(cf, dw, ln);
+#pragma unroll
+        for (int i = 0; i < K; ++i) SW[i * 32 + ln] = dw[0][i];
+    }
+    __syncwarp();
+    // ---- phi: source (i kx u* + i ky v* + dw*/dz) / dt, zero on the Nyquist row
+    const double2 DX = __ldg(a.c.dx + l), DY = __ldg(a.c.dy + m);
+    const double rdt = 1.0 / dt;
+    double2 ph[1][K];
+    {
+        const double2 wlast = SW[(K - 1) * 32 + ln];
+        double2 wprev0 = shfl_up2(wlast, 1);
+        if (ln == 0) wprev0 = make_double2(0, 0);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            if (r < nz && !nyq) {
+                const double2 us = SU[i * 32 + ln], vs = SV[i * 32 + ln], ws = SW[i * 32 + ln];
+                const double2 wm = i > 0 ? SW[(i - 1) * 32 + ln] : wprev0;
+                const double rdz = __ldg(a.c.rdz + r);
+                double2 dv = zadd(zmul(DX, us), zmul(DY, vs));
+                dv = zadd(dv, make_double2((ws.x - wm.x) * rdz, (ws.y - wm.y) * rdz));
+                ph[0][i] = make_double2(dv.x * rdt, dv.y * rdt);
+                if (is00 && r == 0) ph[0][i] = make_double2(0, 0);
+            } else {
+                ph[0][i] = make_double2(0, 0);
+            }
+        }
+        auto cf = [&](int r, double& aa, double& bb, double& cc) {
+            if (r < nz) {
+                aa = rk * __ldg(a.c.ap + r);
+                cc = (is00 && r == 0) ? 0.0 : rk * __ldg(a.c.cp + r);
+                bb = rk * (lamp + __ldg(dgp + r));
+            } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+        };
+        warp_partition_solve<K, 1>(cf, ph, ln);
+    }
+    // ---- pressure update, projection, truncation
+    const bool tr = spec_truncated(l, m, a.g.ny, A.ltr, A.mtr);
+    {
+        const double2 GX = __ldg(a.c.gx + l), GY = __ldg(a.c.gy + m);
+        const double lxy = __ldg(a.c.lx + l) + __ldg(a.c.ly + m);
+        const double cpr = rk * dt, cps = rk * 0.5 * dt * a.nu;
+        double2 nxt0 = shfl_dn2(ph[0][0], 1);
+        double2 prv0 = shfl_up2(ph[0][K - 1], 1);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            if (r >= nz) continue;
+            const long long id = (long long)r * ncol + c;
+            const double2 pc = ph[0][i];
+            const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
+            const double2 pd = (r == 0) ? pc : (i > 0 ? ph[0][i - 1] : prv0);
+            const double2 us = SU[i * 32 + ln], vs = SV[i * 32 + ln], ws = SW[i * 32 + ln];
+            const double rdzt = __ldg(a.c.rdzt + r), rdzb = __ldg(a.c.rdzb + r), rdz = __ldg(a.c.rdz + r);
+            double2 fu = zsub(us, zscale(zmul(GX, pc), cpr));
+            double2 fv = zsub(vs, zscale(zmul(GY, pc), cpr));
+            double2 fw = r <= nz - 2 ? make_double2(ws.x - cpr * (pu.x - pc.x) * rdzt, ws.y - cpr * (pu.y - pc.y) * rdzt)
+                                     : make_double2(0, 0);
+            double2 lz;
+            lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
+            lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
+            const double2 psi = make_double2(pc.x - cps * (lxy * pc.x + lz.x), pc.y - cps * (lxy * pc.y + lz.y));
+            double2 fp = zadd(A.dt.at(ld2<R>(A.sp, id), 3, r, nz), psi);
+            if (tr) { fu = make_double2(0, 0); fv = fu; fw = fu; fp = fu; }
+            st2<R>(A.phi, id, pc);
+            st2<R>(A.su, id, fu);
+            st2<R>(A.sv, id, fv);
+            st2<R>(A.sw, id, fw);
+            st2<R>(A.sp, id, fp);
+            SU[i * 32 + ln] = round_to<R>(fu);
+            SV[i * 32 + ln] = round_to<R>(fv);
+            SW[i * 32 + ln] = round_to<R>(fw);
+        }
+    }
+    __syncwarp();
+    // ---- divergence spectrum of the stored fields (the physical w is 0 below
+    //      the bottom wall and on the top wall)
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const int r = r0 + i;
+        if (r >= nz) continue;
+        const long long id = (long long)r * ncol + c;
+        double2 dv = make_double2(0, 0);
+        if (!nyq) {
+            const double2 fu = SU[i * 32 + ln], fv = SV[i * 32 + ln], fw = SW[i * 32 + ln];
+            const double2 fwm = r == 0 ? make_double2(0, 0) : (i > 0 ? SW[(i - 1) * 32 + ln] : SW[(K - 1) * 32 + ln - 1]);
+            const double rdz = __ldg(a.c.rdz + r);
+            dv = zadd(zmul(DX, fu), zmul(DY, fv));
+            dv = zadd(dv, make_double2((fw.x - fwm.x) * rdz, (fw.y - fwm.y) * rdz));
+        }
+        st2<R>(A.div, id, dv);
+    }
+}
