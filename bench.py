@@ -34,6 +34,9 @@ WORKLOADS = {
     "channel_fd4_96x64x64": (96, 64, 64),
     # profiling size: production nz with a few GB on the device
     "channel_fd4_256x192x256": (256, 192, 256),
+    # stratified open channel, pseudo-spectral horizontal derivatives (cds=3, issk=1)
+    "open_spectral_256x256x128": (256, 256, 128),
+    "open_spectral_128x128x128": (128, 128, 128),
 }
 DEFAULT_WORKLOAD = "channel_fd4_512x384x256"
 # CPU samples of the same physics, sized for 10-30 s of host work
@@ -50,7 +53,25 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="run one precision only (profiling); the headline needs both")
     return ap.parse_args()
+
+
+def is_spectral(workload: str) -> bool:
+    return workload.startswith("open_spectral")
+
+
+def make_case(workload: str, prec: int):
+    """Parameters and seeded initial fields of a workload."""
+    from hercules_b200 import inputs
+    from hercules_b200.params import config_channel_fd, config_open_channel_spectral
+    nx, ny, nz = WORKLOADS[workload]
+    if is_spectral(workload):
+        p = config_open_channel_spectral(nx, ny, nz, got=0.1, precision=prec)
+        return p, inputs.loglaw_stratified(p, seed=10)
+    p = config_channel_fd(nx, ny, nz, precision=prec)
+    return p, inputs.poiseuille_noise(p, seed=3)
 
 
 def dist_env():
@@ -124,17 +145,35 @@ def peaks():
         return 6650.0, "fallback"
 
 
-# algorithmic words per grid point per launch of each kernel (FD path, neutral);
-# physical fields and half spectra both count one word per point
-ALG_WORDS = {"rhs_momentum": 13, "fft_x_r2c": 6, "fft_y_fwd": 6, "column_fd": 7, "fft_y_inv": 8,
-             "fft_x_c2r": 9, "div_check": 3}
+# Algorithmic words per grid point per RK sub-step of each kernel category
+# (physical fields and half spectra both count one word per point; every input
+# read once, every output written once).
+ALG_WORDS_SUB = {
+    # FD path, neutral: RHS reads u,v,w,p,ff,gg,hh, writes qu,qv,qw,ff,gg,hh; the
+    # column kernel reads 3 spectra, writes u,v,w,psi; the x inverse also reads p (+=)
+    "fd": {"rhs_momentum": 13, "fft_x_r2c": 6, "fft_y_fwd": 6, "column_fd": 7, "fft_y_inv": 8,
+           "fft_x_c2r": 9, "div_check": 3},
+    # spectral path (issk=1, scalar): products read u,v,w,t + 6 derivative images,
+    # write 8 (+ 7 for T); assembly reads 4 spectra, 8 product spectra, 3 histories,
+    # writes 3 histories + 3 RHS (+ 7 for T); the column kernel reads 3 RHS + p,
+    # writes u,v,w,p,phi,div; transforms: 6 derivative + 4 state + 1 T inverse,
+    # 8 + 3 forward, each pass reads and writes every field
+    "sp": {"spec_products": 25, "fft_x_r2c": 22, "fft_y_fwd": 22, "spec_assemble": 28, "column_fd": 10,
+           "column_t": 2, "fft_y_inv": 22, "fft_x_c2r": 22, "div_check": 4, "spec_aux": 9},
+}
 
 
-def alg_bytes(kernel: str, npts: int, wbytes: int) -> float:
+# DRAM bytes (read + write) of one launch of the dominant kernel, from an ncu
+# capture (profiles/); filled in per workload once measured
+TRAFFIC = {}
+
+
+def alg_bytes_step(kernel: str, npts: int, wbytes: int, kind: str, nsub: int = 3) -> float:
+    """Algorithmic bytes of one time step in one kernel category."""
     if kernel == "stats":
-        # reads u, v, w, t, uhx, vhy in the storage type; 11 FP64 accumulators RMW
-        return npts * (6 * wbytes + 22 * 8)
-    return ALG_WORDS.get(kernel, 0) * npts * wbytes
+        # reads u, v, w, t (+ uhx, vhy on the FD path) in the storage type; 11 FP64 accumulators RMW
+        return npts * ((6 if kind == "fd" else 4) * wbytes + 22 * 8)
+    return ALG_WORDS_SUB[kind].get(kernel, 0) * nsub * npts * wbytes
 
 
 def run_gpu(args, ws, rank):
@@ -165,10 +204,11 @@ def run_gpu(args, ws, rank):
 
     results = {}
     chans = {}
-    for prec in (PREC_FP64, PREC_MIXED):
-        p = config_channel_fd(nx, ny, nz, precision=prec)
+    precs = {"both": (PREC_FP64, PREC_MIXED), "fp64": (PREC_FP64,), "mixed": (PREC_MIXED,)}[args.precision]
+    for prec in precs:
+        p, fields = make_case(args.workload, prec)
         c = engine.Channel(p)
-        c.load(inputs.poiseuille_noise(p, seed=3))
+        c.load(fields)
         c.initialize()
         rc = c.step_nodiag(args.warmup)
         assert rc == 0, rc
@@ -184,6 +224,10 @@ def run_gpu(args, ws, rank):
                          "value": ws * npts * args.steps / (ms * 1e-3), "clocks": clk.summary()}
         chans[prec] = c
 
+    if len(precs) == 1:
+        for c in chans.values():
+            c.close()
+        return results, None, {}, None
     # mixed-vs-FP64 error after the same warmup+steps from the same seed
     err = {}
     for f in ("u", "v", "w"):
@@ -194,29 +238,30 @@ def run_gpu(args, ws, rank):
     pf = chans[PREC_FP64].download("p")
     err["p"] = float(np.max(np.abs((pm - pm.mean()) - (pf - pf.mean()))) / np.max(np.abs(pf - pf.mean())))
 
-    # per-kernel CUDA-event profile of 2 steps of the headline (mixed) run
+    # per-kernel CUDA-event profile of 2 steps of each run
     kern = {}
+    kind = "sp" if is_spectral(args.workload) else "fd"
+    nprof = 2
     for prec, tag in ((PREC_MIXED, "mixed"), (PREC_FP64, "fp64")):
         c = chans[prec]
         c.set_profiling(True)
-        c.step_nodiag(2)
+        c.step_nodiag(nprof)
         prof = c.kernel_profile()
         c.set_profiling(False)
         wb = 4 if prec == PREC_MIXED else 8
         kern[tag] = {}
         for k, v in prof.items():
             avg = v["total_ms"] / max(v["launches"], 1)
-            b = alg_bytes(k, npts, wb)
-            kern[tag][k] = {"launches": v["launches"], "avg_ms": avg,
-                            "alg_gbs": (b / (avg * 1e-3) / 1e9) if b and avg > 0 else None}
+            b = alg_bytes_step(k, npts, wb, kind) * nprof
+            kern[tag][k] = {"launches": v["launches"], "avg_ms": avg, "total_ms": v["total_ms"],
+                            "alg_gbs": (b / (v["total_ms"] * 1e-3) / 1e9) if b and v["total_ms"] > 0 else None}
     for c in chans.values():
         c.close()
 
     # end-to-end through the public API with host buffers (mixed)
     e2e = None
     if not args.no_e2e:
-        p = config_channel_fd(nx, ny, nz, precision=PREC_MIXED)
-        host = inputs.poiseuille_noise(p, seed=3)
+        p, host = make_case(args.workload, PREC_MIXED)
         host = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in host.items()}
         barrier()
         t0 = time.perf_counter()
@@ -226,6 +271,7 @@ def run_gpu(args, ws, rank):
         for _ in range(args.steps):
             c.step(1)
         outs = {f: c.download(f) for f in ("u", "v", "w", "p", "t")}
+        outs = None
         barrier()
         t1 = time.perf_counter()
         c.close()
@@ -274,9 +320,15 @@ def main():
     base = {"metric": "gridpoint-steps/s mixed vs FP64 at stated err (1 B200)", "unit": "gridpoint-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded Poiseuille + 10% uniform noise)"}
-    cfg = {"workload": args.workload, "grid": [nx, ny, nz], "physics": "neutral closed channel, FD4 horizontal, "
-           "FD2 vertical, RK3, dp_opt=2, nu=1/2800, dt=1e-3, zstretch=1", "parallelism": f"replicas x{args.gpus}",
-           "l2": "working set larger than L2 (one FP64 field 403 MB, FP32 201 MB)"}
+    if is_spectral(args.workload):
+        physics = ("stably stratified open channel, pseudo-spectral horizontal (2/3 rule, skew form), FD2 vertical, "
+                   "RK3, dp_opt=1, nu=1/180, Pr=0.71, Ri_b=0.1, Dirichlet T, dt=1e-3")
+        base["data"] = "synthetic (seeded log-law + 5% Gaussian noise, linear T + 1% noise)"
+    else:
+        physics = "neutral closed channel, FD4 horizontal, FD2 vertical, RK3, dp_opt=2, nu=1/2800, dt=1e-3, zstretch=1"
+    fb = nx * ny * nz * 8
+    cfg = {"workload": args.workload, "grid": [nx, ny, nz], "physics": physics, "parallelism": f"replicas x{args.gpus}",
+           "l2": f"working set larger than L2 (one FP64 field {fb / 1e6:.0f} MB, FP32 {fb / 2e6:.0f} MB)"}
 
     if args.impl == "reference":
         if rank != 0:
@@ -301,16 +353,35 @@ def main():
     if rank != 0:
         return
     from hercules_b200.params import PREC_FP64, PREC_MIXED
+    if args.precision != "both":
+        # one precision only (profiling runs): no headline, no error or e2e legs
+        r = next(iter(results.values()))
+        line = dict(base)
+        line.update({"value": r["value"], "ms_per_step": r["ms_per_step"], "precision": args.precision,
+                     "config": cfg, "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
+                     "note": "single-precision profiling run, not a headline line"})
+        print(json.dumps(line), flush=True)
+        return
     mixed, fp64 = results[PREC_MIXED], results[PREC_FP64]
     # dominant kernel of the headline run and its roofline
     km = kern["mixed"]
-    dom = max((k for k in km if ALG_WORDS.get(k) or k == "stats"), key=lambda k: km[k]["avg_ms"] * km[k]["launches"])
+    kind = "sp" if is_spectral(args.workload) else "fd"
+    dom = max((k for k in km if km[k]["alg_gbs"]), key=lambda k: km[k]["total_ms"])
     ach = km[dom]["alg_gbs"]
+    npts = nx * ny * nz
     roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
-            "frac": ach / hbm if ach else None, "peak_kind": peak_kind, "traffic": None,
-            "alg_bytes_per_launch": alg_bytes(dom, nx * ny * nz, 4),
-            "step_frac_of_hbm": 580.0 * mixed["value"] / args.gpus / (hbm * 1e9),
-            "step_frac_fp64": 1048.0 * fp64["value"] / args.gpus / (hbm * 1e9)}
+            "frac": ach / hbm if ach else None, "peak_kind": peak_kind, "traffic": TRAFFIC.get((args.workload, dom)),
+            "alg_bytes_per_launch": alg_bytes_step(dom, npts, 4, kind) / max(km[dom]["launches"] / 2, 1)}
+    # whole-step HBM fraction with the fixed per-point accounting of an ideally
+    # fused step: FD neutral RK3 131 words (117 field words + 14 FP64 mean words);
+    # spectral scalar RK3 3*49 field words + 4 stats reads + 22 FP64 mean words
+    if kind == "fd":
+        step_b = {PREC_FP64: 1048.0, PREC_MIXED: 117 * 4 + 14 * 8.0}
+    else:
+        step_b = {PREC_FP64: (3 * 49 + 4) * 8 + 22 * 8.0, PREC_MIXED: (3 * 49 + 4) * 4 + 22 * 8.0}
+    roof["step_bytes_per_point"] = {"mixed": step_b[PREC_MIXED], "fp64": step_b[PREC_FP64]}
+    roof["step_frac_of_hbm"] = step_b[PREC_MIXED] * mixed["value"] / args.gpus / (hbm * 1e9)
+    roof["step_frac_fp64"] = step_b[PREC_FP64] * fp64["value"] / args.gpus / (hbm * 1e9)
     cpu = None
     if not args.no_cpu_baseline and args.gpus == 1:
         rate, el = cpu_oracle_rate(CPU_SAMPLE_GRID, 1)

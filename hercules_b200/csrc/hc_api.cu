@@ -588,6 +588,11 @@ template <typename R> static int set_smem_attrs()
     CK(cudaFuncSetAttribute(k_fft_x_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(k_fft_y<R, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(k_fft_y<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<4>()));
+    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<5>()));
+    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<6>()));
+    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<7>()));
+    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<8>()));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     return HC_OK;
@@ -759,8 +764,14 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base
 // K = ceil(nz/32)), else (or when tile[3] asks for it) one thread per pair.
 template <typename R, int K> static int col_fd_k(hc_handle* h, const ColArgs<R>& ca)
 {
-    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
-    k_column_fd_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(ca);
+    if (h->p.tile[3] == 2) {      // per-warp variant without the coalescing tiles
+        const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
+        k_column_fd_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(ca);
+        CKL();
+        return HC_OK;
+    }
+    const unsigned nb = (unsigned)((h->g.ncol + CT_COLS - 1) / CT_COLS);
+    k_column_fd_tile<R, K><<<nb, CT_COLS * 32, column_tile_smem<K>(), h->st>>>(ca);
     CKL();
     return HC_OK;
 }
