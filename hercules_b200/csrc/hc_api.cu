@@ -56,8 +56,9 @@ __global__ void k_substep_begin(ScalarArgs a)
 
 struct FinalArgs {
     DevScalars* sc;
-    const double* part_div;   // [3][nbd][3]
-    long long nbd;
+    const double* part_div;   // [3][stride][3]
+    long long stride;
+    long long nbq[3];         // partial blocks written for each sub-step
     int nsub;
     const double* part_st;    // [nbs][2]
     long long nbs;
@@ -122,9 +123,9 @@ __global__ void __launch_bounds__(256) k_finalize(FinalArgs a)
     double davg[3] = {0, 0, 0}, dmax[3] = {0, 0, 0};
     int nan = 0;
     for (int q = 0; q < a.nsub; ++q) {
-        const double* p = a.part_div + (long long)q * a.nbd * 3;
+        const double* p = a.part_div + (long long)q * a.stride * 3;
         double sm = 0.0, mx = 0.0, nn = 0.0;
-        for (long long b = tid; b < a.nbd; b += blockDim.x) {
+        for (long long b = tid; b < a.nbq[q]; b += blockDim.x) {
             sm += p[3 * b];
             mx = absmax_pick(mx, p[3 * b + 1]);
             nn = fmax(nn, p[3 * b + 2]);
@@ -218,6 +219,9 @@ struct hc_handle {
     double* part_div;
     double* part_st;
     long long nbd, nbs, stx, sty;
+    long long pd_stride;     // partial slots per sub-step (max over the writers)
+    dim3 rhs_grid;           // FD momentum RHS grid and its level chunk
+    int rhs_kc;
     DevScalars* sc;
     hc_diag* diag_dev;
     int diag_cap;
@@ -748,7 +752,12 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base
 {
     FinalArgs f;
     memset(&f, 0, sizeof(f));
-    f.sc = h->sc; f.part_div = h->part_div; f.nbd = h->nbd; f.nsub = nsub;
+    f.sc = h->sc; f.part_div = h->part_div; f.stride = h->pd_stride; f.nsub = nsub;
+    // FD RK3: the checks of sub-steps 1 and 2 run inside the next sub-step's RHS
+    const long long nrhs = (long long)h->rhs_grid.x * h->rhs_grid.y * h->rhs_grid.z;
+    // FD: sub-steps before the last are checked inside the next sub-step's RHS
+    for (int q = 0; q < 3; ++q)
+        f.nbq[q] = (h->p.cds != 3 && q < nsub - 1) ? nrhs : h->nbd;
     f.part_st = h->part_st; f.nbs = h->nbs;
     f.nx = h->p.nx; f.ny = h->p.ny; f.nz = h->p.nz; f.lz = h->p.lz;
     f.dp_opt = h->p.dp_opt; f.diag = h->diag_dev; f.step_base = step_base; f.write_diag = write_diag;
@@ -850,21 +859,12 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     m.uhx_s = last ? (R*)h->fld[F_UHX] : nullptr; m.vhy_s = last ? (R*)h->fld[F_VHY] : nullptr;
     m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph; m.sc = h->sc;
     m.with_t = p.isscalar == 1;
-    {
-        const int bx = (h->g.nx + RT_TX - 1) / RT_TX, by = (h->g.ny + RT_TY - 1) / RT_TY;
-        // enough blocks for ~4 per SM, chunks of 4..32 levels
-        long long want = 4LL * 148;
-        int kc = p.tile[2] > 0 ? p.tile[2] : (int)((long long)bx * by * p.nz / want);
-        if (p.tile[2] <= 0) { if (kc < 4) kc = 4; if (kc > 32) kc = 32; }
-        if (kc < 1) kc = 1;
-        if (kc > RT_KMAX) kc = RT_KMAX;
-        if (kc > p.nz) kc = p.nz;
-        m.kchunk = kc;
-        dim3 gr(bx, by, (p.nz + kc - 1) / kc);
-        prof_begin(h, K_RHS_MOM);
-        k_rhs_momentum_tiled<R, CDS><<<gr, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
-        CKL();
-    }
+    // the divergence check of the previous sub-step rides along (slot sub-1)
+    m.part_div = sub > 0 ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
+    m.kchunk = h->rhs_kc;
+    prof_begin(h, K_RHS_MOM);
+    k_rhs_momentum_tiled<R, CDS><<<h->rhs_grid, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
+    CKL();
 
     T2* S[4] = {(T2*)h->spec[0], (T2*)h->spec[1], (T2*)h->spec[2], (T2*)h->spec[3]};
     const R* qin[3] = {(const R*)h->fld[F_QU], (const R*)h->fld[F_QV], (const R*)h->fld[F_QW]};
@@ -930,8 +930,11 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     FieldsIn<R> fi;
     fi.u = (const R*)h->fld[F_U]; fi.v = (const R*)h->fld[F_V]; fi.w = (const R*)h->fld[F_W];
     fi.p = (const R*)h->fld[F_P]; fi.t = (const R*)h->fld[F_T];
+    // the divergence check of this sub-step runs inside the next sub-step's RHS;
+    // the last one has its own pass
+    if (!last) return HC_OK;
     prof_begin(h, K_DIV);
-    k_div_check<R, CDS><<<(unsigned)h->nbd, 256, 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->nbd * 3);
+    k_div_check<R, CDS><<<(unsigned)h->nbd, 256, 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->pd_stride * 3);
     CKL();
     return HC_OK;
 }
@@ -1142,7 +1145,7 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
     fi.u = (const R*)h->fld[F_U]; fi.v = (const R*)h->fld[F_V]; fi.w = (const R*)h->fld[F_W];
     fi.p = nullptr; fi.t = nullptr;
     prof_begin(h, K_DIV);
-    k_spec_div_reduce<R><<<(unsigned)h->nbd, 256, 0, h->st>>>(Q[SP_W0 + 3], fi, g.n, h->part_div + (long long)sub * h->nbd * 3);
+    k_spec_div_reduce<R><<<(unsigned)h->nbd, 256, 0, h->st>>>(Q[SP_W0 + 3], fi, g.n, h->part_div + (long long)sub * h->pd_stride * 3);
     CKL();
     return HC_OK;
 }
@@ -1346,13 +1349,28 @@ int hc_create(const hc_params* p, hc_handle** out)
         if (rc != HC_OK) goto fail;
         h->nbd = (g.n + 255) / 256;
         if (h->nbd > RED_BLOCKS) h->nbd = RED_BLOCKS;
+        {
+            // momentum RHS tiles: enough blocks for ~4 per SM, chunks of 4..32 levels
+            const int bx = (g.nx + RT_TX - 1) / RT_TX, by = (g.ny + RT_TY - 1) / RT_TY;
+            int kc = p->tile[2] > 0 ? p->tile[2] : (int)((long long)bx * by * p->nz / (4LL * 148));
+            if (p->tile[2] <= 0) { if (kc < 4) kc = 4; if (kc > 32) kc = 32; }
+            if (kc < 1) kc = 1;
+            if (kc > RT_KMAX) kc = RT_KMAX;
+            if (kc > p->nz) kc = p->nz;
+            h->rhs_kc = kc;
+            h->rhs_grid = dim3(bx, by, (p->nz + kc - 1) / kc);
+        }
         h->stx = (g.nxy + 255) / 256;
         h->sty = (2 * RED_BLOCKS) / h->stx;
         if (h->sty < 1) h->sty = 1;
         if (h->sty > p->nz) h->sty = p->nz;
         h->nbs = h->stx * h->sty;
-        if (cudaMalloc(&h->part_div, 3 * h->nbd * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
-        if (cudaMemset(h->part_div, 0, 3 * h->nbd * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        h->pd_stride = h->nbd;
+        if (h->nbs > h->pd_stride) h->pd_stride = h->nbs;
+        if ((long long)h->rhs_grid.x * h->rhs_grid.y * h->rhs_grid.z > h->pd_stride)
+            h->pd_stride = (long long)h->rhs_grid.x * h->rhs_grid.y * h->rhs_grid.z;
+        if (cudaMalloc(&h->part_div, 3 * h->pd_stride * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+        if (cudaMemset(h->part_div, 0, 3 * h->pd_stride * 3 * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
         if (cudaMalloc(&h->part_st, 2 * h->nbs * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
         if (cudaMalloc(&h->sc, sizeof(DevScalars)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
         DevScalars s0;

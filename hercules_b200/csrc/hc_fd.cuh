@@ -333,6 +333,26 @@ __device__ __forceinline__ double warp_max(double v)
 // the grid size only: the sums are deterministic from run to run.
 #define RED_BLOCKS 1184
 
+// Divergence of the staggered fields at one point (get_p_eqn_src without the
+// 1/dt, src/module_poisson_solver.f90:127-176; screen_div_error,
+// src/module_io.f90:85-206). Every kernel that reports the divergence diagnostic
+// goes through this one expression, so they agree bit for bit.
+//   ux[0..3] = u(i+1), u(i), u(i-1), u(i-2); vy[0..3] likewise in j; w0, wm = w(k), w(k-1)
+template <int CDS>
+__device__ __forceinline__ double fd_div_point(const double* ux, const double* vy, double w0, double wm, double dx,
+                                               double dy, double dzk)
+{
+    double dudx, dvdy;
+    if (CDS == 1) {
+        dudx = (ux[1] - ux[2]) * (1.0 / dx);
+        dvdy = (vy[1] - vy[2]) * (1.0 / dy);
+    } else {
+        dudx = (-ux[0] + 27.0 * ux[1] - 27.0 * ux[2] + ux[3]) * (1.0 / (24.0 * dx));
+        dvdy = (-vy[0] + 27.0 * vy[1] - 27.0 * vy[2] + vy[3]) * (1.0 / (24.0 * dy));
+    }
+    return dudx + dvdy + (w0 - wm) / dzk;
+}
+
 __device__ __forceinline__ void decode_pt(long long q, const Geo& g, int& i, int& j, int& k)
 {
     i = (int)(q % g.nx);
@@ -351,25 +371,21 @@ __global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double*
     const int tid = threadIdx.x;
     if (tid == 0) s_nan = 0;
     __syncthreads();
-    const double r24dx = 1.0 / (24.0 * g.dx), r24dy = 1.0 / (24.0 * g.dy), rdx = 1.0 / g.dx, rdy = 1.0 / g.dy;
     double sm = 0.0, mx = 0.0;
     int nan = 0;
     for (long long q = (long long)blockIdx.x * blockDim.x + tid; q < g.n; q += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         decode_pt(q, g, i, j, k);
-        double dudx, dvdy;
         const double uc = (double)f.u[q], vc = (double)f.v[q], wc = (double)f.w[q];
-        if (CDS == 1) {
-            dudx = (uc - (double)ldf(f.u, g, i - 1, j, k)) * rdx;
-            dvdy = (vc - (double)ldf(f.v, g, i, j - 1, k)) * rdy;
-        } else {
-            dudx = (-(double)ldf(f.u, g, i + 1, j, k) + 27.0 * uc - 27.0 * (double)ldf(f.u, g, i - 1, j, k) +
-                    (double)ldf(f.u, g, i - 2, j, k)) * r24dx;
-            dvdy = (-(double)ldf(f.v, g, i, j + 1, k) + 27.0 * vc - 27.0 * (double)ldf(f.v, g, i, j - 1, k) +
-                    (double)ldf(f.v, g, i, j - 2, k)) * r24dy;
+        double ux[4], vy[4];
+        ux[1] = uc; vy[1] = vc;
+        ux[2] = (double)ldf(f.u, g, i - 1, j, k); vy[2] = (double)ldf(f.v, g, i, j - 1, k);
+        if (CDS == 2) {
+            ux[0] = (double)ldf(f.u, g, i + 1, j, k); ux[3] = (double)ldf(f.u, g, i - 2, j, k);
+            vy[0] = (double)ldf(f.v, g, i, j + 1, k); vy[3] = (double)ldf(f.v, g, i, j - 2, k);
         }
         const double wm = k > 0 ? (double)f.w[q - g.nxy] : 0.0;
-        const double d = dudx + dvdy + (wc - wm) / ldz(g.z.dz, k);
+        const double d = fd_div_point<CDS>(ux, vy, wc, wm, g.dx, g.dy, ldz(g.z.dz, k));
         if (uc != uc || vc != vc || wc != wc || d != d) { nan = 1; continue; }
         sm += fabs(d);
         mx = absmax_pick(mx, d);

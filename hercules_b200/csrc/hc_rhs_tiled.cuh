@@ -35,6 +35,10 @@ template <typename R> struct RhsTArgs {
     const DevScalars* sc;
     int kchunk;
     int with_t;
+    // divergence check of the incoming u, v, w (screen_div_error of the previous
+    // sub-step, src/module_io.f90:85-206), per block: sum |div|, signed div of
+    // largest magnitude, NaN flag; null when not wanted
+    double* part_div;
 };
 
 #define RT_KMAX 64
@@ -205,6 +209,8 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
         ez_prev = vhz * why;
     }
 
+    double dv_sum = 0.0, dv_max = 0.0;
+    int dv_nan = 0;
     for (int k = kb; k < ke; ++k) {
         const bool more = k + 1 < ke;
         R nu_[RT_NLD], nv_[RT_NLD], nw_[RT_NLD], np_[RT_NLD], nt_[RT_NLD];
@@ -260,6 +266,15 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
         }
         __syncthreads();
 
+        if (active && a.part_div) {
+            // FP64 divergence of the stored fields, as k_div_check computes it
+            const double uc = (double)u0[rc], vc = (double)v0[rc], wc = (double)w0[rc];
+            double ux[4] = {(double)u0[rc + 1], uc, (double)u0[rc - 1], (double)u0[rc - 2]};
+            double vy[4] = {(double)v0[rc + RT_W4], vc, (double)v0[rc - RT_W4], (double)v0[rc - 2 * RT_W4]};
+            const double d = fd_div_point<CDS>(ux, vy, wc, k > 0 ? (double)wm1[rc] : 0.0, g.dx, g.dy, ldz(g.z.dz, k));
+            if (uc != uc || vc != vc || wc != wc || d != d) dv_nan = 1;
+            else { dv_sum += fabs(d); dv_max = absmax_pick(dv_max, d); }
+        }
         if (active) {
             const R rdz = ZM[k - kb], rdzt = ZM[(RT_KMAX + 1) + (k - kb)], rdzb = ZM[2 * (RT_KMAX + 1) + (k - kb)];
             const int f = fc0;
@@ -373,5 +388,30 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
             if (a.with_t) rt_put<R>(ST + (L & 1) * RT_P4, nt_);
         }
         __syncthreads();
+    }
+    if (a.part_div) {
+        __shared__ double s_sum[8], s_max[8];
+        __shared__ int s_nan;
+        __syncthreads();
+        if (threadIdx.x == 0) s_nan = 0;
+        __syncthreads();
+        if (dv_nan) s_nan = 1;
+        dv_sum = warp_sum(dv_sum);
+        dv_max = warp_absmax(dv_max);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) { s_sum[wid] = dv_sum; s_max[wid] = dv_max; }
+        __syncthreads();
+        if (wid == 0) {
+            dv_sum = lane < 8 ? s_sum[lane] : 0.0;
+            dv_max = lane < 8 ? s_max[lane] : 0.0;
+            dv_sum = warp_sum(dv_sum);
+            dv_max = warp_absmax(dv_max);
+            if (lane == 0) {
+                const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+                a.part_div[3 * b + 0] = dv_sum;
+                a.part_div[3 * b + 1] = dv_max;
+                a.part_div[3 * b + 2] = s_nan ? 1.0 : 0.0;
+            }
+        }
     }
 }
