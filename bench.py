@@ -159,7 +159,7 @@ ALG_WORDS_SUB = {
     # writes u,v,w,p,phi,div; transforms: 6 derivative + 4 state + 1 T inverse,
     # 8 + 3 forward, each pass reads and writes every field
     "sp": {"spec_products": 25, "fft_x_r2c": 22, "fft_y_fwd": 22, "spec_assemble": 28, "column_fd": 10,
-           "column_t": 2, "fft_y_inv": 22, "fft_x_c2r": 22, "div_check": 4, "spec_aux": 9},
+           "column_t": 2, "fft_y_inv": 22, "fft_x_c2r": 22, "div_check": 4, "aux": 9},
 }
 
 

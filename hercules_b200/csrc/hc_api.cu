@@ -190,7 +190,7 @@ enum { K_BEGIN, K_RHS_MOM, K_FFT_X_FWD, K_FFT_Y_FWD, K_COLUMN, K_FFT_Y_INV, K_FF
        K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_SPEC_PROD, K_SPEC_ASM, K_SPEC_AUX, K_NCAT };
 static const char* K_NAMES[K_NCAT] = {"substep_begin", "rhs_momentum", "fft_x_r2c", "fft_y_fwd", "column_fd",
                                       "fft_y_inv", "fft_x_c2r", "rhs_temperature", "column_t", "div_check",
-                                      "stats", "finalize", "spec_products", "spec_assemble", "spec_aux"};
+                                      "stats", "finalize", "spec_products", "spec_assemble", "aux"};
 
 // spectral-path buffers (cds = 3), each n values of the storage type: the half
 // spectra of the state and histories, phi, the divergence, the assembled
@@ -210,6 +210,8 @@ struct hc_handle {
     void* sp[NSP];           // cds = 3 only
     double* dsig;            // cds = 3, isdamp = 1: sigma per level (0 below the layer)
     double* dmean;           // [5][nz] plane means of the damped levels
+    void* dstale;            // FD, isdamp = 1: undamped copies of u, v, w, p, t on the damped levels
+    int div_in_rhs;          // FD without damping: sub-step checks ride in the next RHS
     double* mean[11];
     double* zbuf;            // 5*(nz+4)
     double* coef;
@@ -616,6 +618,8 @@ template <typename R> static Acc<R> make_acc(hc_handle* h)
     a.g = h->g;
     a.um = (R)h->p.u_mrf; a.tbot = (R)h->p.tbot; a.ttop = (R)h->p.ttop;
     a.closed = h->p.ochannel == 0;
+    a.su = a.sv = a.sw = a.sp = a.st = nullptr;
+    a.kd = h->p.nz;
     return a;
 }
 
@@ -757,7 +761,7 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base
     const long long nrhs = (long long)h->rhs_grid.x * h->rhs_grid.y * h->rhs_grid.z;
     // FD: sub-steps before the last are checked inside the next sub-step's RHS
     for (int q = 0; q < 3; ++q)
-        f.nbq[q] = (h->p.cds != 3 && q < nsub - 1) ? nrhs : h->nbd;
+        f.nbq[q] = (h->div_in_rhs && q < nsub - 1) ? nrhs : h->nbd;
     f.part_st = h->part_st; f.nbs = h->nbs;
     f.nx = h->p.nx; f.ny = h->p.ny; f.nz = h->p.nz; f.lz = h->p.lz;
     f.dp_opt = h->p.dp_opt; f.diag = h->diag_dev; f.step_base = step_base; f.write_diag = write_diag;
@@ -849,6 +853,35 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     k_substep_begin<<<1, 1, 0, h->st>>>(sa);
     CKL();
 
+    // Rayleigh damping of the top layer (isdamp = 1), undamped copies kept for
+    // the ghost reads of this sub-step's right-hand sides
+    Acc<R> acc = make_acc<R>(h);
+    if (p.isdamp == 1) {
+        const int kd = p.nz - 1 - p.nzdamp;
+        const long long lv = (long long)(p.nzdamp + 1) * h->g.nxy;
+        FdDampArgs<R> da;
+        const int fids[5] = {F_U, F_V, F_W, F_P, F_T};
+        for (int f = 0; f < 5; ++f) { da.f[f] = (R*)h->fld[fids[f]]; da.stale[f] = (R*)h->dstale + f * lv; }
+        da.mean = h->dmean; da.sig = h->dsig; da.g = h->g; da.kd = kd;
+        prof_begin(h, K_SPEC_AUX);
+        k_fd_damp_mean<R><<<dim3(p.nzdamp + 1, 5), 256, 0, h->st>>>(da);
+        CKL();
+        prof_begin(h, K_SPEC_AUX);
+        k_fd_damp_apply<R><<<RED_BLOCKS, 256, 0, h->st>>>(da);
+        CKL();
+        acc.su = da.stale[0]; acc.sv = da.stale[1]; acc.sw = da.stale[2]; acc.sp = da.stale[3]; acc.st = da.stale[4];
+        acc.kd = kd;
+        // per-point RHS with the reference's ghost semantics of the damped layer
+        MomArgs<R> mm;
+        mm.a = acc;
+        mm.ff = (R*)h->fld[F_FF]; mm.gg = (R*)h->fld[F_GG]; mm.hh = (R*)h->fld[F_HH];
+        mm.qu = (R*)h->fld[F_QU]; mm.qv = (R*)h->fld[F_QV]; mm.qw = (R*)h->fld[F_QW];
+        mm.uhx_s = last ? (R*)h->fld[F_UHX] : nullptr; mm.vhy_s = last ? (R*)h->fld[F_VHY] : nullptr;
+        mm.rk_a = rk_a; mm.rk_b = rk_b; mm.rk_c = rk_c; mm.ph = h->ph; mm.sc = h->sc;
+        prof_begin(h, K_RHS_MOM);
+        k_rhs_momentum<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(mm);
+        CKL();
+    } else {
     // momentum RHS (SMEM-tiled, marching in k)
     RhsTArgs<R> m;
     m.f.u = (const R*)h->fld[F_U]; m.f.v = (const R*)h->fld[F_V]; m.f.w = (const R*)h->fld[F_W];
@@ -860,11 +893,12 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph; m.sc = h->sc;
     m.with_t = p.isscalar == 1;
     // the divergence check of the previous sub-step rides along (slot sub-1)
-    m.part_div = sub > 0 ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
+    m.part_div = (sub > 0 && h->div_in_rhs) ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
     m.kchunk = h->rhs_kc;
     prof_begin(h, K_RHS_MOM);
     k_rhs_momentum_tiled<R, CDS><<<h->rhs_grid, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
     CKL();
+    }
 
     T2* S[4] = {(T2*)h->spec[0], (T2*)h->spec[1], (T2*)h->spec[2], (T2*)h->spec[3]};
     const R* qin[3] = {(const R*)h->fld[F_QU], (const R*)h->fld[F_QV], (const R*)h->fld[F_QW]};
@@ -899,6 +933,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     if (p.isscalar == 1) {
         TempArgs<R> ta;
         ta.a = make_acc<R>(h);
+        if (p.isdamp == 1) { ta.a.st = acc.st; ta.a.kd = acc.kd; }   // t keeps its undamped ghosts
         ta.ss = (R*)h->fld[F_SS]; ta.qt = (R*)h->fld[F_QU];
         ta.rk_a = rk_a; ta.rk_b = rk_b; ta.rk_c = rk_c; ta.ph = h->ph;
         prof_begin(h, K_RHS_T);
@@ -930,9 +965,9 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     FieldsIn<R> fi;
     fi.u = (const R*)h->fld[F_U]; fi.v = (const R*)h->fld[F_V]; fi.w = (const R*)h->fld[F_W];
     fi.p = (const R*)h->fld[F_P]; fi.t = (const R*)h->fld[F_T];
-    // the divergence check of this sub-step runs inside the next sub-step's RHS;
-    // the last one has its own pass
-    if (!last) return HC_OK;
+    // the divergence check of this sub-step runs inside the next sub-step's RHS
+    // (without damping, which changes the fields first); the last one has its own pass
+    if (!last && h->div_in_rhs) return HC_OK;
     prof_begin(h, K_DIV);
     k_div_check<R, CDS><<<(unsigned)h->nbd, 256, 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->pd_stride * 3);
     CKL();
@@ -1241,6 +1276,7 @@ static void free_all(hc_handle* h)
     for (int q = 0; q < 4; ++q) if (h->spec[q]) cudaFree(h->spec[q]);
     for (int q = 0; q < NSP; ++q) if (h->sp[q]) cudaFree(h->sp[q]);
     if (h->dsig) cudaFree(h->dsig);
+    if (h->dstale) cudaFree(h->dstale);
     if (h->dmean) cudaFree(h->dmean);
     for (int q = 0; q < 11; ++q) if (h->mean[q]) cudaFree(h->mean[q]);
     if (h->zbuf) cudaFree(h->zbuf);
@@ -1270,7 +1306,6 @@ int hc_create(const hc_params* p, hc_handle** out)
     if (p->dp_opt < 1 || p->dp_opt > 3) return HC_ERR_PARAM;
     if (p->precision != HC_PREC_FP64 && p->precision != HC_PREC_MIXED) return HC_ERR_PARAM;
     if (p->isdamp == 1 && (p->nzdamp < 1 || p->nzdamp > p->nz - 1)) return HC_ERR_PARAM;
-    if (p->isdamp == 1 && p->cds != 3) return HC_ERR_UNSUPPORTED;
     // the spectral column kernel keeps a whole column in one warp (nz <= 256)
     if (p->cds == 3 && p->nz > 256) return HC_ERR_UNSUPPORTED;
 
@@ -1280,7 +1315,7 @@ int hc_create(const hc_params* p, hc_handle** out)
     for (int q = 0; q < NFLD; ++q) h->fld[q] = nullptr;
     for (int q = 0; q < 4; ++q) h->spec[q] = nullptr;
     for (int q = 0; q < NSP; ++q) h->sp[q] = nullptr;
-    h->dsig = nullptr; h->dmean = nullptr;
+    h->dsig = nullptr; h->dmean = nullptr; h->dstale = nullptr; h->div_in_rhs = 0;
     for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
@@ -1323,20 +1358,28 @@ int hc_create(const hc_params* p, hc_handle** out)
                 if (cudaMalloc(&h->sp[q], n * h->rsz) != cudaSuccess) FAIL(HC_ERR_NOMEM);
                 if (cudaMemset(h->sp[q], 0, n * h->rsz) != cudaSuccess) FAIL(HC_ERR_CUDA);
             }
+        }
+        if (p->cds == 3 || p->isdamp == 1) {
             if (cudaMalloc(&h->dmean, 5 * p->nz * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
             if (cudaMemset(h->dmean, 0, 5 * p->nz * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
-            if (p->isdamp == 1) {
-                // sigma of rayleigh_damping_spec (src/module_spectral.f90:1345-1391) per level
-                std::vector<double> sig(p->nz, 0.0);
-                const int nzd = p->nzdamp;
-                for (int kk = p->nz - 1 - nzd; kk < p->nz; ++kk) {
-                    const double zd = (kk - (p->nz - 1) + nzd) * 1.0 / nzd;
-                    sig[kk] = p->cdamp * 0.5 * (1.0 - cos(HC_PI * zd));
-                }
-                if (cudaMalloc(&h->dsig, p->nz * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
-                if (cudaMemcpy(h->dsig, sig.data(), p->nz * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) FAIL(HC_ERR_CUDA);
+        }
+        if (p->isdamp == 1) {
+            // sigma of rayleigh_damping / rayleigh_damping_spec (src/module_tools.f90:705-749,
+            // src/module_spectral.f90:1345-1391) per level
+            std::vector<double> sig(p->nz, 0.0);
+            const int nzd = p->nzdamp;
+            for (int kk = p->nz - 1 - nzd; kk < p->nz; ++kk) {
+                const double zd = (kk - (p->nz - 1) + nzd) * 1.0 / nzd;
+                sig[kk] = p->cdamp * 0.5 * (1.0 - cos(HC_PI * zd));
+            }
+            if (cudaMalloc(&h->dsig, p->nz * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+            if (cudaMemcpy(h->dsig, sig.data(), p->nz * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) FAIL(HC_ERR_CUDA);
+            if (p->cds != 3) {
+                const size_t sb = (size_t)5 * (nzd + 1) * g.nxy * h->rsz;
+                if (cudaMalloc(&h->dstale, sb) != cudaSuccess) FAIL(HC_ERR_NOMEM);
             }
         }
+        h->div_in_rhs = p->cds != 3 && p->isdamp != 1;
         const long long cz = g.ncol * g.nz;
         if (cudaMalloc(&h->scratch, cz * (3 * sizeof(double) + 4 * sizeof(double2))) != cudaSuccess) FAIL(HC_ERR_NOMEM);
         h->cs.bu = h->scratch; h->cs.bw = h->scratch + cz; h->cs.bp = h->scratch + 2 * cz;

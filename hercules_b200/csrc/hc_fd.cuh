@@ -18,74 +18,107 @@ template <typename R> __device__ __forceinline__ R ldf(const R* f, const Geo& g,
 }
 
 // ---- z ghost cells on load (update_boundary_uvw/p/t, src/module_boundary.f90:33-196) ----
+//
+// Rayleigh damping (FD path) changes the interior of the top levels kd..nz-1 at
+// the start of a sub-step but, in the reference, leaves every ghost cell as the
+// previous boundary update wrote it (rayleigh_damping, src/module_tools.f90:
+// 705-749, touches istr3..iend3 x jstr3..jend3 only). A value read outside the
+// domain (a periodic neighbour or a z ghost) therefore still holds the undamped
+// field. With the pre-damping copies s* of those levels set, every such read is
+// served from the copy; interpolants are evaluated at the wrapped point, as the
+// reference's interpolant ghosts are periodic copies of interior values.
 template <typename R> struct Acc {
     FieldsIn<R> f;
     Geo g;
     R um, tbot, ttop;
     int closed;   // ochannel == 0
+    // pre-damping copies of levels kd..nz-1 ([k-kd][j][i]); null: no damping
+    const R* su; const R* sv; const R* sw; const R* sp; const R* st;
+    int kd;
 
+    // value of field f at (i, j, k) with k inside [0, nz): the current value
+    // inside the domain, the undamped one across the periodic boundary
+    __device__ __forceinline__ R raw(const R* fp, const R* sp_, int i, int j, int k) const {
+        if (sp_ && k >= kd && !((unsigned)i < (unsigned)g.nx && (unsigned)j < (unsigned)g.ny))
+            return __ldg(sp_ + ((long long)(k - kd) * g.ny + wrapi(j, g.ny)) * g.nx + wrapi(i, g.nx));
+        return ldf(fp, g, i, j, k);
+    }
+    // source value of a z ghost (always the undamped field when damped)
+    __device__ __forceinline__ R gsrc(const R* fp, const R* sp_, int i, int j, int k) const {
+        if (sp_ && k >= kd) return __ldg(sp_ + ((long long)(k - kd) * g.ny + wrapi(j, g.ny)) * g.nx + wrapi(i, g.nx));
+        return ldf(fp, g, i, j, k);
+    }
     __device__ __forceinline__ R U(int i, int j, int k) const {
-        if (k < 0) return -ldf(f.u, g, i, j, 0) - R(2) * um;
-        if (k >= g.nz) return closed ? -ldf(f.u, g, i, j, g.nz - 1) - R(2) * um : ldf(f.u, g, i, j, g.nz - 1);
-        return ldf(f.u, g, i, j, k);
+        if (k < 0) return -gsrc(f.u, su, i, j, 0) - R(2) * um;
+        if (k >= g.nz) return closed ? -gsrc(f.u, su, i, j, g.nz - 1) - R(2) * um : gsrc(f.u, su, i, j, g.nz - 1);
+        return raw(f.u, su, i, j, k);
     }
     __device__ __forceinline__ R V(int i, int j, int k) const {
-        if (k < 0) return -ldf(f.v, g, i, j, 0);
-        if (k >= g.nz) return closed ? -ldf(f.v, g, i, j, g.nz - 1) : ldf(f.v, g, i, j, g.nz - 1);
-        return ldf(f.v, g, i, j, k);
+        if (k < 0) return -gsrc(f.v, sv, i, j, 0);
+        if (k >= g.nz) return closed ? -gsrc(f.v, sv, i, j, g.nz - 1) : gsrc(f.v, sv, i, j, g.nz - 1);
+        return raw(f.v, sv, i, j, k);
     }
     __device__ __forceinline__ R W(int i, int j, int k) const {
         if (k < 0) return R(0);
-        if (k >= g.nz) return -ldf(f.w, g, i, j, g.nz - 2);
-        return ldf(f.w, g, i, j, k);          // level nz-1 is the top wall, stored as 0
+        if (k >= g.nz) return -gsrc(f.w, sw, i, j, g.nz - 2);
+        return raw(f.w, sw, i, j, k);          // level nz-1 is the top wall, stored as 0
     }
     __device__ __forceinline__ R P(int i, int j, int k) const {
-        k = k < 0 ? 0 : (k >= g.nz ? g.nz - 1 : k);
-        return ldf(f.p, g, i, j, k);
+        if (k < 0) return gsrc(f.p, sp, i, j, 0);
+        if (k >= g.nz) return gsrc(f.p, sp, i, j, g.nz - 1);
+        return raw(f.p, sp, i, j, k);
     }
     __device__ __forceinline__ R T(int i, int j, int k) const {
-        if (k < 0) return R(2) * tbot - ldf(f.t, g, i, j, 0);
-        if (k >= g.nz) return R(2) * ttop - ldf(f.t, g, i, j, g.nz - 1);
-        return ldf(f.t, g, i, j, k);
+        if (k < 0) return R(2) * tbot - gsrc(f.t, st, i, j, 0);
+        if (k >= g.nz) return R(2) * ttop - gsrc(f.t, st, i, j, g.nz - 1);
+        return raw(f.t, st, i, j, k);
     }
     __device__ __forceinline__ R lt(int k) const { return (R)ldz(g.z.l_t, k); }
 
     // ---- mid-point interpolants (get_interp_fields_uvwhxyz, src/module_tools.f90:410-468) ----
     template <int CDS> __device__ __forceinline__ R uhx(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (CDS == 1) return R(0.5) * (U(i, j, k) + U(i - 1, j, k));
         return (-U(i + 1, j, k) + R(9) * U(i, j, k) + R(9) * U(i - 1, j, k) - U(i - 2, j, k)) * R(0.0625);
     }
     template <int CDS> __device__ __forceinline__ R uhy(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (CDS == 1) return R(0.5) * (U(i, j + 1, k) + U(i, j, k));
         return (-U(i, j + 2, k) + R(9) * U(i, j + 1, k) + R(9) * U(i, j, k) - U(i, j - 1, k)) * R(0.0625);
     }
     template <int CDS> __device__ __forceinline__ R vhx(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (CDS == 1) return R(0.5) * (V(i + 1, j, k) + V(i, j, k));
         return (-V(i + 2, j, k) + R(9) * V(i + 1, j, k) + R(9) * V(i, j, k) - V(i - 1, j, k)) * R(0.0625);
     }
     template <int CDS> __device__ __forceinline__ R vhy(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (CDS == 1) return R(0.5) * (V(i, j, k) + V(i, j - 1, k));
         return (-V(i, j + 1, k) + R(9) * V(i, j, k) + R(9) * V(i, j - 1, k) - V(i, j - 2, k)) * R(0.0625);
     }
     // whx/why: 0 on the wall ghost below and on the top wall (update_boundary_uvwhxyz :232-235, :281-282)
     template <int CDS> __device__ __forceinline__ R whx(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (k < 0 || k >= g.nz - 1) return R(0);
         if (CDS == 1) return R(0.5) * (W(i + 1, j, k) + W(i, j, k));
         return (-W(i + 2, j, k) + R(9) * W(i + 1, j, k) + R(9) * W(i, j, k) - W(i - 1, j, k)) * R(0.0625);
     }
     template <int CDS> __device__ __forceinline__ R why(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (k < 0 || k >= g.nz - 1) return R(0);
         if (CDS == 1) return R(0.5) * (W(i, j + 1, k) + W(i, j, k));
         return (-W(i, j + 2, k) + R(9) * W(i, j + 1, k) + R(9) * W(i, j, k) - W(i, j - 1, k)) * R(0.0625);
     }
     // uhz/vhz: linear in z; wall value below, wall (closed) or surface value (open) on top
     __device__ __forceinline__ R uhz(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (k < 0) return -um;
         if (k >= g.nz - 1) return closed ? -um : U(i, j, g.nz - 1);
         R l = lt(k);
         return U(i, j, k + 1) * l + U(i, j, k) * (R(1) - l);
     }
     __device__ __forceinline__ R vhz(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (k < 0) return R(0);
         if (k >= g.nz - 1) return closed ? R(0) : V(i, j, g.nz - 1);
         R l = lt(k);
@@ -93,14 +126,17 @@ template <typename R> struct Acc {
     }
     // temperature interpolants (get_interp_fields_thxyz :473-512, update_boundary_thxyz :311-355)
     template <int CDS> __device__ __forceinline__ R thx(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (CDS == 1) return R(0.5) * (T(i + 1, j, k) + T(i, j, k));
         return (-T(i + 2, j, k) + R(9) * T(i + 1, j, k) + R(9) * T(i, j, k) - T(i - 1, j, k)) * R(0.0625);
     }
     template <int CDS> __device__ __forceinline__ R thy(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (CDS == 1) return R(0.5) * (T(i, j + 1, k) + T(i, j, k));
         return (-T(i, j + 2, k) + R(9) * T(i, j + 1, k) + R(9) * T(i, j, k) - T(i, j - 1, k)) * R(0.0625);
     }
     __device__ __forceinline__ R thz(int i, int j, int k) const {
+        i = wrapi(i, g.nx); j = wrapi(j, g.ny);
         if (k < 0) return tbot;
         if (k >= g.nz - 1) return ttop;
         R l = lt(k);
@@ -479,5 +515,54 @@ __global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
             s.part[2 * b + 0] = ub;
             s.part[2 * b + 1] = cfl;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// rayleigh_damping (src/module_tools.f90:705-749) of u, v, w, p, t on levels
+// kd..nz-1: x -= sigma(k) (x - <x>_plane). The plane means come first (fixed
+// reduction order), then one pass keeps the undamped values of those levels
+// (the reference's ghost cells still hold them, see Acc) and damps the fields.
+// ---------------------------------------------------------------------------
+template <typename R> struct FdDampArgs {
+    R* f[5];
+    R* stale[5];          // [k-kd][j][i]
+    double* mean;         // [5][nz]
+    const double* sig;    // [nz], 0 below the layer
+    Geo g;
+    int kd;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_fd_damp_mean(FdDampArgs<R> a)
+{
+    __shared__ double sh[8];
+    const int k = a.kd + blockIdx.x, f = blockIdx.y;
+    const R* src = a.f[f] + (long long)k * a.g.nxy;
+    double sm = 0.0;
+    for (long long q = threadIdx.x; q < a.g.nxy; q += blockDim.x) sm += (double)src[q];
+    sm = warp_sum(sm);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        a.mean[f * a.g.nz + k] = t / (double)a.g.nx / (double)a.g.ny;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_fd_damp_apply(FdDampArgs<R> a)
+{
+    const long long per = (long long)(a.g.nz - a.kd) * a.g.nxy;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < 5 * per; q += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(q / per);
+        const long long r = q - f * per;
+        const int k = a.kd + (int)(r / a.g.nxy);
+        R* x = a.f[f] + (long long)a.kd * a.g.nxy + r;
+        const double v = (double)*x;
+        a.stale[f][r] = (R)v;
+        const double sg = __ldg(a.sig + k);
+        *x = (R)(v - sg * (v - a.mean[f * a.g.nz + k]));
     }
 }

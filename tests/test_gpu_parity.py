@@ -33,6 +33,12 @@ CASES = {
     "fd4_umrf_scalar": small(u_mrf=0.4, isscalar=1, got=0.3, tbot=0.5, ttop=-0.25),
     "fd4_open_umrf_rivar": small(ochannel=1, u_mrf=-0.2, isscalar=1, is_ri_var=1, ri_str=0.1, ri_end=2.0, imax=20),
     "fd4_nonsquare_radix": small(nx=48, ny=40, nz=9),
+    # Rayleigh damping: the undamped ghost cells of the reference (rayleigh_damping
+    # touches the interior only) must be reproduced at the periodic seams
+    "fd4_open_damp_scalar": small(ochannel=1, isscalar=1, got=0.3, tbot=-1.0, ttop=0.0,
+                                  isdamp=1, nzdamp=6, cdamp=0.7),
+    "fd2_closed_damp_full_depth": small(cds=1, isdamp=1, nzdamp=16, cdamp=1.0, isscalar=1, got=0.2),
+    "fd4_ab2_damp_umrf": small(dts=1, u_mrf=0.3, isdamp=1, nzdamp=3, cdamp=0.5),
 }
 
 
@@ -82,7 +88,7 @@ def test_config1_full_size_fp64_10_steps(oracle_lib, engine):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["fd4_closed_dp2", "fd4_open_scalar"])
+@pytest.mark.parametrize("name", ["fd4_closed_dp2", "fd4_open_scalar", "fd4_open_damp_scalar"])
 def test_fd_mixed_precision_10_steps(name, oracle_lib, engine):
     p = CASES[name].replace(precision=PREC_MIXED)
     fields = inputs.small_random(p, seed=3)
