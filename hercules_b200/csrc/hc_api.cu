@@ -65,8 +65,8 @@ struct FinalArgs {
     double inv_n;             // 1/(nx ny nz) as the reference's sequential division
     double nx, ny, nz, lz;
     int dp_opt;
-    hc_diag* diag;            // diag[step - step_base]
-    int step_base;
+    hc_diag* diag;            // ring of diag_cap records, slot (step - 1) % diag_cap
+    int diag_cap;
     int write_diag;
     int cds;
     int set_ubar;             // 0: keep the bulk velocity (spectral set-up)
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinalArgs a)
     s->cfl = cf;
     if (nan) s->nan_flag = 1;
     if (a.write_diag) {
-        hc_diag* d = a.diag + (s->step - a.step_base);
+        hc_diag* d = a.diag + (s->step - 1) % a.diag_cap;
         d->time_sim = s->time_sim;
         d->cfl = cfl_start;
         d->div_avg = davg[a.nsub - 1];
@@ -212,6 +212,12 @@ struct hc_handle {
     double* dmean;           // [5][nz] plane means of the damped levels
     void* dstale;            // FD, isdamp = 1: undamped copies of u, v, w, p, t on the damped levels
     int div_in_rhs;          // FD without damping: sub-step checks ride in the next RHS
+    void* bf[3];             // body force (storage type), allocated by hc_set_body_force
+    int has_bf;
+    // CUDA graph of one step (hc_set_graph): captured on first use, replayed per step
+    int use_graph;
+    cudaGraphExec_t gexec;
+    long long graph_launches;
     double* mean[11];
     double* zbuf;            // 5*(nz+4)
     double* coef;
@@ -752,7 +758,7 @@ template <typename R> static int launch_stats(hc_handle* h, int accumulate)
     return HC_OK;
 }
 
-static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base, int set_ubar = 1)
+static int launch_finalize(hc_handle* h, int nsub, int write_diag, int set_ubar = 1)
 {
     FinalArgs f;
     memset(&f, 0, sizeof(f));
@@ -764,7 +770,7 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int step_base
         f.nbq[q] = (h->div_in_rhs && q < nsub - 1) ? nrhs : h->nbd;
     f.part_st = h->part_st; f.nbs = h->nbs;
     f.nx = h->p.nx; f.ny = h->p.ny; f.nz = h->p.nz; f.lz = h->p.lz;
-    f.dp_opt = h->p.dp_opt; f.diag = h->diag_dev; f.step_base = step_base; f.write_diag = write_diag;
+    f.dp_opt = h->p.dp_opt; f.diag = h->diag_dev; f.diag_cap = h->diag_cap; f.write_diag = write_diag;
     f.cds = h->p.cds;
     f.set_ubar = set_ubar;
     prof_begin(h, K_FINAL);
@@ -878,6 +884,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
         mm.qu = (R*)h->fld[F_QU]; mm.qv = (R*)h->fld[F_QV]; mm.qw = (R*)h->fld[F_QW];
         mm.uhx_s = last ? (R*)h->fld[F_UHX] : nullptr; mm.vhy_s = last ? (R*)h->fld[F_VHY] : nullptr;
         mm.rk_a = rk_a; mm.rk_b = rk_b; mm.rk_c = rk_c; mm.ph = h->ph; mm.sc = h->sc;
+        mm.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
+        mm.bfy = (const R*)h->bf[1]; mm.bfz = (const R*)h->bf[2];
         prof_begin(h, K_RHS_MOM);
         k_rhs_momentum<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(mm);
         CKL();
@@ -895,6 +903,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     // the divergence check of the previous sub-step rides along (slot sub-1)
     m.part_div = (sub > 0 && h->div_in_rhs) ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
     m.kchunk = h->rhs_kc;
+    m.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
+    m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
     prof_begin(h, K_RHS_MOM);
     k_rhs_momentum_tiled<R, CDS><<<h->rhs_grid, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
     CKL();
@@ -974,7 +984,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     return HC_OK;
 }
 
-template <typename R, int CDS> static int step_fd(hc_handle* h, int step_base)
+template <typename R, int CDS> static int step_fd(hc_handle* h)
 {
     const int nsub = h->p.dts == 2 ? 3 : 1;
     for (int sub = 0; sub < nsub; ++sub) {
@@ -983,7 +993,7 @@ template <typename R, int CDS> static int step_fd(hc_handle* h, int step_base)
     }
     int rc = launch_stats<R>(h, 1);
     if (rc) return rc;
-    return launch_finalize(h, nsub, 1, step_base);
+    return launch_finalize(h, nsub, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -1087,6 +1097,7 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         pa.u = (const R*)h->fld[F_U]; pa.v = (const R*)h->fld[F_V]; pa.w = (const R*)h->fld[F_W]; pa.t = (const R*)h->fld[F_T];
         for (int f = 0; f < 6; ++f) pa.d[f] = p.issk == 1 ? Q[SP_W0 + 8 + f] : nullptr;
         for (int f = 0; f < 8; ++f) pa.out[f] = Q[SP_W0 + f];
+        for (int f = 0; f < 3; ++f) pa.bf[f] = h->has_bf ? (const R*)h->bf[f] : nullptr;
         pa.g = g; pa.sc = h->sc;
         pa.um = p.u_mrf; pa.fc = p.fc; pa.ug = p.ug; pa.vg = p.vg; pa.t_ref = p.t_ref; pa.tbot = p.tbot; pa.ttop = p.ttop;
         pa.inv_coe = 1.0 / (p.issk == 1 ? 0.5 : 1.0);
@@ -1185,7 +1196,7 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
     return HC_OK;
 }
 
-template <typename R> static int step_sp(hc_handle* h, int step_base)
+template <typename R> static int step_sp(hc_handle* h)
 {
     const int nsub = h->p.dts == 2 ? 3 : 1;
     for (int sub = 0; sub < nsub; ++sub) {
@@ -1194,7 +1205,7 @@ template <typename R> static int step_sp(hc_handle* h, int step_base)
     }
     int rc = launch_stats<R>(h, 1);
     if (rc) return rc;
-    return launch_finalize(h, nsub, 1, step_base);
+    return launch_finalize(h, nsub, 1);
 }
 
 // set-up of the spectral state (src/module_navier_stokes.f90:61-129 with
@@ -1242,11 +1253,11 @@ template <typename R> static int spec_image(hc_handle* h, int sp_id, void** out)
     return HC_OK;
 }
 
-template <typename R> static int step_dispatch(hc_handle* h, int step_base)
+template <typename R> static int step_dispatch(hc_handle* h)
 {
-    if (h->p.cds == 1) return step_fd<R, 1>(h, step_base);
-    if (h->p.cds == 2) return step_fd<R, 2>(h, step_base);
-    return step_sp<R>(h, step_base);
+    if (h->p.cds == 1) return step_fd<R, 1>(h);
+    if (h->p.cds == 2) return step_fd<R, 2>(h);
+    return step_sp<R>(h);
 }
 
 // ---------------------------------------------------------------------------
@@ -1270,13 +1281,47 @@ const char* hc_error_string(int code)
     return "unknown error";
 }
 
+static void graph_drop(hc_handle* h)
+{
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    h->gexec = nullptr;
+}
+
+// Capture one full step (all sub-steps, statistics, finaliser) of this handle
+// into an executable graph. Every kernel argument of a step is the same from
+// step to step (the step counter and the diagnostics slot live on the device),
+// so the graph stays valid until a buffer it refers to changes.
+static int graph_build(hc_handle* h)
+{
+    if (h->gexec) return HC_OK;
+    const long long l0 = h->launches;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int rc = h->rsz == sizeof(float) ? step_dispatch<float>(h) : step_dispatch<double>(h);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->st, &g);
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        h->launches = l0;
+        return rc ? rc : HC_ERR_CUDA;
+    }
+    h->graph_launches = h->launches - l0;
+    h->launches = l0;
+    e = cudaGraphInstantiate(&h->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { h->gexec = nullptr; return HC_ERR_CUDA; }
+    return HC_OK;
+}
+
 static void free_all(hc_handle* h)
 {
+    graph_drop(h);
     for (int q = 0; q < NFLD; ++q) if (h->fld[q]) cudaFree(h->fld[q]);
     for (int q = 0; q < 4; ++q) if (h->spec[q]) cudaFree(h->spec[q]);
     for (int q = 0; q < NSP; ++q) if (h->sp[q]) cudaFree(h->sp[q]);
     if (h->dsig) cudaFree(h->dsig);
     if (h->dstale) cudaFree(h->dstale);
+    for (int q = 0; q < 3; ++q) if (h->bf[q]) cudaFree(h->bf[q]);
     if (h->dmean) cudaFree(h->dmean);
     for (int q = 0; q < 11; ++q) if (h->mean[q]) cudaFree(h->mean[q]);
     if (h->zbuf) cudaFree(h->zbuf);
@@ -1316,6 +1361,8 @@ int hc_create(const hc_params* p, hc_handle** out)
     for (int q = 0; q < 4; ++q) h->spec[q] = nullptr;
     for (int q = 0; q < NSP; ++q) h->sp[q] = nullptr;
     h->dsig = nullptr; h->dmean = nullptr; h->dstale = nullptr; h->div_in_rhs = 0;
+    h->bf[0] = h->bf[1] = h->bf[2] = nullptr; h->has_bf = 0;
+    h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0;
     for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
@@ -1451,6 +1498,7 @@ int hc_set_grid(hc_handle* h, const double* dz, const double* l_t, const double*
     for (int q = 0; q < 5; ++q) h->zhost[q].assign(src[q], src[q] + nka);
     int rc = upload_zgrid(h);
     if (rc) return rc;
+    graph_drop(h);
     cudaFree(h->coef);
     h->coef = nullptr;
     return build_tables(h);
@@ -1564,6 +1612,29 @@ int hc_download(hc_handle* h, int field_id, double* host, int ld1, int ld2, int 
     return HC_OK;
 }
 
+int hc_set_body_force(hc_handle* h, const double* fx, const double* fy, const double* fz)
+{
+    if (!h) return HC_ERR_ARG;
+    graph_drop(h);
+    if (!fx && !fy && !fz) { h->has_bf = 0; return HC_OK; }
+    const long long n = h->g.n;
+    const double* src[3] = {fx, fy, fz};
+    for (int q = 0; q < 3; ++q) {
+        if (!h->bf[q]) CK(cudaMalloc(&h->bf[q], n * h->rsz));
+        CK(cudaStreamSynchronize(h->st));
+        if (!src[q]) { CK(cudaMemset(h->bf[q], 0, n * h->rsz)); continue; }
+        if (h->rsz == sizeof(double)) {
+            CK(cudaMemcpy(h->bf[q], src[q], n * sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> tf(n);
+            for (long long i = 0; i < n; ++i) tf[i] = (float)src[q][i];
+            CK(cudaMemcpy(h->bf[q], tf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+        }
+    }
+    h->has_bf = 1;
+    return HC_OK;
+}
+
 int hc_upload_dev(hc_handle* h, int field_id, const void* dev)
 {
     if (!h || !dev) return HC_ERR_ARG;
@@ -1603,7 +1674,7 @@ int hc_initialize(hc_handle* h)
     // calculate_ubar (dp_opt=2) and the CFL of the initial fields
     int rc = h->rsz == sizeof(float) ? launch_stats<float>(h, 0) : launch_stats<double>(h, 0);
     if (rc) return rc;
-    rc = launch_finalize(h, 0, 0, 0);
+    rc = launch_finalize(h, 0, 0, 1);   // sets ubar of the fields as given
     if (rc) return rc;
     if (p.cds == 3) {
         // the bulk velocity above is that of the fields as given; the spectral
@@ -1613,7 +1684,7 @@ int hc_initialize(hc_handle* h)
         CK(cudaMemsetAsync((char*)h->fld[F_W] + (size_t)(p.nz - 1) * h->g.nxy * h->rsz, 0, h->g.nxy * h->rsz, h->st));
         rc = h->rsz == sizeof(float) ? launch_stats<float>(h, 0) : launch_stats<double>(h, 0);
         if (rc) return rc;
-        rc = launch_finalize(h, 0, 0, 0, 0);
+        rc = launch_finalize(h, 0, 0, 0);   // CFL only, keeps that ubar
         if (rc) return rc;
     }
     CK(cudaStreamSynchronize(h->st));
@@ -1636,12 +1707,26 @@ int hc_step(hc_handle* h, int nsteps, hc_diag* out)
     while (done < nsteps) {
         const int chunk = (nsteps - done) < h->diag_cap ? (nsteps - done) : h->diag_cap;
         const int base = s.step + done + 1;
+        const bool graph = h->use_graph && !h->prof;
+        if (graph && (rc = graph_build(h))) return rc;
         for (int q = 0; q < chunk; ++q) {
-            rc = h->rsz == sizeof(float) ? step_dispatch<float>(h, base) : step_dispatch<double>(h, base);
+            if (graph) {
+                CK(cudaGraphLaunch(h->gexec, h->st));
+                h->launches += h->graph_launches;
+                continue;
+            }
+            rc = h->rsz == sizeof(float) ? step_dispatch<float>(h) : step_dispatch<double>(h);
             if (rc) return rc;
             if (h->prof && h->ev_used > 4096) { rc = prof_collect(h); if (rc) return rc; }
         }
-        if (out) CK(cudaMemcpyAsync(out + done, h->diag_dev, chunk * sizeof(hc_diag), cudaMemcpyDeviceToHost, h->st));
+        if (out) {
+            // the finaliser writes step n into slot (n - 1) % diag_cap
+            const int s0 = (base - 1) % h->diag_cap;
+            const int n1 = chunk < h->diag_cap - s0 ? chunk : h->diag_cap - s0;
+            CK(cudaMemcpyAsync(out + done, h->diag_dev + s0, n1 * sizeof(hc_diag), cudaMemcpyDeviceToHost, h->st));
+            if (chunk > n1)
+                CK(cudaMemcpyAsync(out + done + n1, h->diag_dev, (chunk - n1) * sizeof(hc_diag), cudaMemcpyDeviceToHost, h->st));
+        }
         done += chunk;
     }
     CK(cudaEventRecord(h->e1, h->st));
@@ -1691,6 +1776,131 @@ int hc_set_profiling(hc_handle* h, int enable)
     h->prof = enable ? 1 : 0;
     for (int q = 0; q < K_NCAT; ++q) { h->cat_ms[q] = 0.0; h->cat_n[q] = 0; }
     h->ev_used = 0;
+    return HC_OK;
+}
+
+int hc_set_graph(hc_handle* h, int enable)
+{
+    if (!h) return HC_ERR_ARG;
+    h->use_graph = enable ? 1 : 0;
+    if (!enable) graph_drop(h);
+    return HC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ensemble: independent channels advanced together, one graph per step with a
+// branch per member (the members' own streams, forked from and joined into the
+// ensemble stream), so small members run concurrently
+// ---------------------------------------------------------------------------
+struct hc_ensemble {
+    std::vector<hc_handle*> m;
+    cudaStream_t st;
+    cudaEvent_t e0, e1, fork;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t gexec;
+    long long launches_per_step;
+    double last_ms;
+};
+
+static void ensemble_free(hc_ensemble* e)
+{
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    for (size_t q = 0; q < e->join.size(); ++q) if (e->join[q]) cudaEventDestroy(e->join[q]);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->e0) cudaEventDestroy(e->e0);
+    if (e->e1) cudaEventDestroy(e->e1);
+    if (e->st) cudaStreamDestroy(e->st);
+    delete e;
+}
+
+int hc_ensemble_create(hc_handle* const* members, int n, hc_ensemble** out)
+{
+    if (!members || n < 1 || !out) return HC_ERR_ARG;
+    *out = nullptr;
+    for (int q = 0; q < n; ++q) {
+        if (!members[q]) return HC_ERR_ARG;
+        if (!members[q]->initialized) return HC_ERR_STATE;
+        if (members[q]->dev != members[0]->dev) return HC_ERR_ARG;
+        for (int r = 0; r < q; ++r) if (members[r] == members[q]) return HC_ERR_ARG;
+    }
+    hc_ensemble* e = new hc_ensemble();
+    e->st = nullptr; e->e0 = e->e1 = e->fork = nullptr; e->gexec = nullptr; e->launches_per_step = 0; e->last_ms = 0.0;
+    e->m.assign(members, members + n);
+    e->join.assign(n, nullptr);
+    int rc = HC_OK;
+    cudaGraph_t g = nullptr;
+    long long total = 0;
+    if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&e->e0) != cudaSuccess || cudaEventCreate(&e->e1) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
+    for (int q = 0; q < n; ++q)
+        if (cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
+    if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
+    cudaEventRecord(e->fork, e->st);
+    for (int q = 0; q < n && rc == HC_OK; ++q) {
+        hc_handle* h = e->m[q];
+        const int prof = h->prof;
+        h->prof = 0;
+        const long long l0 = h->launches;
+        cudaStreamWaitEvent(h->st, e->fork, 0);
+        rc = h->rsz == sizeof(float) ? step_dispatch<float>(h) : step_dispatch<double>(h);
+        total += h->launches - l0;
+        h->launches = l0;
+        h->prof = prof;
+        cudaEventRecord(e->join[q], h->st);
+        cudaStreamWaitEvent(e->st, e->join[q], 0);
+    }
+    {
+        cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+        if (rc == HC_OK && ce != cudaSuccess) rc = HC_ERR_CUDA;
+    }
+    if (rc != HC_OK) { if (g) cudaGraphDestroy(g); cudaGetLastError(); goto fail; }
+    if (cudaGraphInstantiate(&e->gexec, g, 0) != cudaSuccess) { cudaGraphDestroy(g); e->gexec = nullptr; rc = HC_ERR_CUDA; goto fail; }
+    cudaGraphDestroy(g);
+    e->launches_per_step = total;
+    *out = e;
+    return HC_OK;
+fail:
+    ensemble_free(e);
+    return rc;
+}
+
+int hc_ensemble_step(hc_ensemble* e, int nsteps)
+{
+    if (!e || nsteps < 0) return HC_ERR_ARG;
+    for (size_t q = 0; q < e->m.size(); ++q) {
+        DevScalars s;
+        CK(cudaMemcpy(&s, e->m[q]->sc, sizeof(s), cudaMemcpyDeviceToHost));
+        if (s.nan_flag) return HC_ERR_NAN;
+    }
+    CK(cudaEventRecord(e->e0, e->st));
+    for (int n = 0; n < nsteps; ++n) CK(cudaGraphLaunch(e->gexec, e->st));
+    CK(cudaEventRecord(e->e1, e->st));
+    CK(cudaEventSynchronize(e->e1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, e->e0, e->e1));
+    e->last_ms = ms;
+    for (size_t q = 0; q < e->m.size(); ++q) {
+        DevScalars s;
+        CK(cudaMemcpy(&s, e->m[q]->sc, sizeof(s), cudaMemcpyDeviceToHost));
+        if (s.nan_flag) return HC_ERR_NAN;
+    }
+    return HC_OK;
+}
+
+int hc_ensemble_last_ms(hc_ensemble* e, double* ms, long long* launches_per_step)
+{
+    if (!e) return HC_ERR_ARG;
+    if (ms) *ms = e->last_ms;
+    if (launches_per_step) *launches_per_step = e->launches_per_step;
+    return HC_OK;
+}
+
+int hc_ensemble_destroy(hc_ensemble* e)
+{
+    if (!e) return HC_ERR_ARG;
+    cudaStreamSynchronize(e->st);
+    ensemble_free(e);
     return HC_OK;
 }
 

@@ -152,6 +152,7 @@ template <typename R> struct MomArgs {
     double rk_a, rk_b, rk_c;
     Phys ph;
     const DevScalars* sc;
+    const R* bfx; const R* bfy; const R* bfz;   // body force (null: none)
 };
 
 // get_momentum_cnvdiff (src/module_cnvdiff.f90:35-374)
@@ -206,6 +207,7 @@ __global__ void __launch_bounds__(256) k_rhs_momentum(MomArgs<R> m)
             f = -uux - uvy - uwz - um * ux + fc * (R(0.5) * (A.template vhx<CDS>(i, j, k) + A.template vhx<CDS>(i, j - 1, k)) - (R)m.ph.vg);
         else
             f = -uux - uvy - uwz + dpx - um * ux;
+        if (m.bfx) f += m.bfx[id];
         R f0 = m.ff[id];
         m.ff[id] = f;
         m.qu[id] = uc + dt * (rka * f + rkb * f0) + cdif * (uxx + uyy + uzz) - rkc * dt * dpdx;
@@ -244,6 +246,7 @@ __global__ void __launch_bounds__(256) k_rhs_momentum(MomArgs<R> m)
             f = -vux - vvy - vwz - um * vx + fc * ((R)m.ph.ug - R(0.5) * (A.template uhy<CDS>(i, j, k) + A.template uhy<CDS>(i - 1, j, k)) - um);
         else
             f = -vux - vvy - vwz - um * vx;
+        if (m.bfx) f += m.bfy[id];
         R f0 = m.gg[id];
         m.gg[id] = f;
         m.qv[id] = vc + dt * (rka * f + rkb * f0) + cdif * (vxx + vyy + vzz) - rkc * dt * dpdy;
@@ -282,6 +285,7 @@ __global__ void __launch_bounds__(256) k_rhs_momentum(MomArgs<R> m)
             f = f + (R)m.sc->got * ((R(1) - l) * A.T(i, j, k) + l * A.T(i, j, k + 1) - (R)m.ph.t_ref);
         }
         R dpdz = (A.P(i, j, k + 1) - A.P(i, j, k)) / dzt;
+        if (m.bfx) f += m.bfz[id];
         R f0 = m.hh[id];
         m.hh[id] = f;
         m.qw[id] = wc + dt * (rka * f + rkb * f0) + cdif * (wxx + wyy + wzz) - rkc * dt * dpdz;

@@ -39,6 +39,7 @@ template <typename R> struct RhsTArgs {
     // sub-step, src/module_io.f90:85-206), per block: sum |div|, signed div of
     // largest magnitude, NaN flag; null when not wanted
     double* part_div;
+    const R* bfx; const R* bfy; const R* bfz;   // body force added to ff, gg, hh (null: none)
 };
 
 #define RT_KMAX 64
@@ -306,6 +307,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
                 R fu;
                 if (a.ph.dp_opt == 3) fu = -uux - uvy - uwz - um * ux + fc * (R(0.5) * (F_VHX[f] + F_VHX[f - RT_W2]) - (R)a.ph.vg);
                 else fu = -uux - uvy - uwz + dpx - um * ux;
+                if (a.bfx) fu += a.bfx[id];
                 a.ff[id] = fu;
                 a.qu[id] = uc + dt * (rka * fu + rkb * f0u) + cdif * (uxx + uyy + uzz) - rkc * dt * dpdx;
                 if (a.uhx_s) a.uhx_s[id] = F_UHX[f];
@@ -340,6 +342,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
                 R fv;
                 if (a.ph.dp_opt == 3) fv = -vux - vvy - vwz - um * vx + fc * ((R)a.ph.ug - R(0.5) * (F_UHY[f] + F_UHY[f - 1]) - um);
                 else fv = -vux - vvy - vwz - um * vx;
+                if (a.bfx) fv += a.bfy[id];
                 a.gg[id] = fv;
                 a.qv[id] = vc + dt * (rka * fv + rkb * f0v) + cdif * (vxx + vyy + vzz) - rkc * dt * dpdy;
                 if (a.vhy_s) a.vhy_s[id] = F_VHY[f];
@@ -372,6 +375,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
                     fw = fw + got * ((R(1) - lt) * t0[rc] + lt * tp1[rc] - (R)a.ph.t_ref);
                 }
                 const R dpdz = (pp1[rc] - p0[rc]) * rdzt;
+                if (a.bfx) fw += a.bfz[id];
                 a.hh[id] = fw;
                 a.qw[id] = wc + dt * (rka * fw + rkb * f0w) + cdif * (wxx + wyy + wzz) - rkc * dt * dpdz;
             }

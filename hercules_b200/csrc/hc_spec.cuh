@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(256) k_spec_truncate(TruncArgs<R> a)
 template <typename R> struct ProdArgs {
     const R* u; const R* v; const R* w; const R* t;
     const R* d[6];          // issk: du/dx, du/dy, dv/dx, dv/dy, dw/dx, dw/dy (physical), else null
+    const R* bf[3];         // body force (null: none); enters the histories with factor 1
     R* out[8];
     Geo g;
     const DevScalars* sc;
@@ -234,6 +235,11 @@ __global__ void __launch_bounds__(256) k_spec_products(ProdArgs<R> a)
         a.out[2][q] = (R)(vk * vk);
         a.out[3][q] = (R)(a1u * wk);
         a.out[4][q] = (R)(a1v * wk);
+        if (a.bf[0]) {
+            cu += ic * (double)a.bf[0][q];
+            cv += ic * (double)a.bf[1][q];
+            cw += ic * (double)a.bf[2][q];
+        }
         a.out[5][q] = (R)cu;
         a.out[6][q] = (R)cv;
         a.out[7][q] = (R)cw;

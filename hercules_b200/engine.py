@@ -30,7 +30,8 @@ HC_ERRORS = {0: "ok", -1: "bad argument", -2: "parameter check failed", -3: "CUD
 ABI_SYMBOLS = ["hc_create", "hc_set_grid", "hc_get_grid", "hc_upload", "hc_download",
                "hc_initialize", "hc_step", "hc_get_scalars", "hc_upload_dev", "hc_download_dev",
                "hc_last_step_ms", "hc_last_launch_count", "hc_set_profiling", "hc_kernel_profile",
-               "hc_divergence_noalloc", "hc_destroy", "hc_error_string"]
+               "hc_divergence_noalloc", "hc_set_body_force", "hc_set_graph", "hc_ensemble_create",
+               "hc_ensemble_step", "hc_ensemble_last_ms", "hc_ensemble_destroy", "hc_destroy", "hc_error_string"]
 
 
 class HerculesError(RuntimeError):
@@ -67,6 +68,12 @@ def load_library(path: str = LIB_PATH):
     L.hc_kernel_profile.argtypes = [vp, ip, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ip)]
     L.hc_divergence_noalloc.argtypes = [ctypes.POINTER(HcParams), ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.hc_set_body_force.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.hc_set_graph.argtypes = [vp, ip]
+    L.hc_ensemble_create.argtypes = [ctypes.POINTER(vp), ip, ctypes.POINTER(vp)]
+    L.hc_ensemble_step.argtypes = [vp, ip]
+    L.hc_ensemble_last_ms.argtypes = [vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_longlong)]
+    L.hc_ensemble_destroy.argtypes = [vp]
     L.hc_destroy.argtypes = [vp]
     L.hc_error_string.argtypes = [ip]
     L.hc_error_string.restype = ctypes.c_char_p
@@ -140,6 +147,20 @@ class Channel:
     def download_dev(self, name: str, ptr: int) -> None:
         _check(self._L.hc_download_dev(self.h, FIELD_IDS[name], ctypes.c_void_p(ptr)), "hc_download_dev")
 
+    def set_graph(self, enable: bool = True) -> None:
+        """Replay each step from a captured CUDA graph (saves launch cost)."""
+        _check(self._L.hc_set_graph(self.h, 1 if enable else 0), "hc_set_graph")
+
+    def set_body_force(self, fx=None, fy=None, fz=None) -> None:
+        """Body force (nz, ny, nx) added to ff, gg, hh; None components are zero,
+        all None removes it. No counterpart in the reference."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (fx, fy, fz)]
+        for a in arrs:
+            if a is not None and a.shape != self._shape(0):
+                raise ValueError(f"body force shape {a.shape} != {self._shape(0)}")
+        ptrs = [None if a is None else ctypes.c_void_p(a.ctypes.data) for a in arrs]
+        _check(self._L.hc_set_body_force(self.h, *ptrs), "hc_set_body_force")
+
     # ---- time stepping -------------------------------------------------
     def initialize(self) -> None:
         _check(self._L.hc_initialize(self.h), "hc_initialize")
@@ -207,3 +228,44 @@ class Channel:
     @property
     def mixed(self) -> bool:
         return self.p.precision == PREC_MIXED
+
+
+class Ensemble:
+    """Independent channels advanced together through one CUDA graph per step
+    (a branch per member). The channels stay owned by the caller; step them only
+    through the ensemble while it exists."""
+
+    def __init__(self, channels):
+        self._L = load_library()
+        self.channels = list(channels)
+        arr = (ctypes.c_void_p * len(self.channels))(*[c.h for c in self.channels])
+        h = ctypes.c_void_p()
+        _check(self._L.hc_ensemble_create(arr, len(self.channels), ctypes.byref(h)), "hc_ensemble_create")
+        self.h = h
+
+    def step(self, n: int = 1) -> None:
+        _check(self._L.hc_ensemble_step(self.h, int(n)), "hc_ensemble_step")
+
+    @property
+    def last_ms(self) -> float:
+        ms = ctypes.c_double()
+        self._L.hc_ensemble_last_ms(self.h, ctypes.byref(ms), None)
+        return ms.value
+
+    @property
+    def launches_per_step(self) -> int:
+        n = ctypes.c_longlong()
+        self._L.hc_ensemble_last_ms(self.h, None, ctypes.byref(n))
+        return n.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._L.hc_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -73,3 +73,61 @@ def small_random(p: Params, seed: int = 0, amp: float = 0.1):
             out[k] = amp * g.uniform(-1, 1, shape)
         out["hh"][-1] = 0.0
     return out
+
+
+def gaussian_body_force(p: Params, seed: int = 4, ell: float = 1.0, amp: float = 0.01):
+    """Seeded smooth body force (fx, fy, fz) for the hc_set_body_force term: white
+    noise filtered to a power spectrum proportional to exp(-k^2 ell^2 / 2), with
+    the horizontal filter applied by FFT (periodic) and the wall-normal one as a
+    Gaussian kernel over the cell centres of the stretched grid; scaled to RMS amp.
+    fz vanishes on the top-wall level, where w is not advanced."""
+    g = _rng(seed)
+    zc = mesh(p)["zc"]
+    shape = (p.nz, p.ny, p.nx)
+    kx = 2 * np.pi * np.fft.fftfreq(p.nx, p.lx / p.nx)
+    ky = 2 * np.pi * np.fft.fftfreq(p.ny, p.ly / p.ny)
+    hfilt = np.exp(-(ky[:, None] ** 2 + kx[None, :] ** 2) * ell ** 2 / 4.0)
+    dz = zc[:, None] - zc[None, :]
+    zker = np.exp(-dz ** 2 / (ell ** 2))
+    zker /= zker.sum(axis=1, keepdims=True)
+    out = []
+    for _ in range(3):
+        x = g.standard_normal(shape)
+        x = np.real(np.fft.ifft2(np.fft.fft2(x, axes=(1, 2)) * hfilt[None], axes=(1, 2)))
+        x = np.tensordot(zker, x, axes=(1, 0))
+        x *= amp / max(np.sqrt(np.mean(x ** 2)), 1e-300)
+        out.append(x)
+    out[2][-1] = 0.0
+    return tuple(out)
+
+
+ENSEMBLE_GRIDS = ((32, 32, 33), (48, 32, 49), (64, 48, 65), (96, 64, 65))
+
+
+def ensemble_members(n: int = 64, seed: int = 1000, precision: int = 0):
+    """Seeded ensemble of independent closed channels: grid drawn uniformly from
+    ENSEMBLE_GRIDS, Re_tau ~ U[100, 300] (nu = 1/Re_tau, constant pressure drive
+    dp_opt=1), Richardson number ~ U[0, 1], Pr = 0.71, stable stratification
+    (t: 0 at the bottom wall, 1 at the top), laminar Poiseuille plus 10% uniform
+    noise. Member q uses seed + q. Returns a list of (Params, fields)."""
+    from .params import config_channel_fd
+    out = []
+    for q in range(n):
+        g = _rng(seed + q)
+        nx, ny, nz = ENSEMBLE_GRIDS[int(g.integers(len(ENSEMBLE_GRIDS)))]
+        re_tau = float(g.uniform(100.0, 300.0))
+        ri = float(g.uniform(0.0, 1.0))
+        nu = 1.0 / re_tau
+        p = config_channel_fd(nx, ny, nz, precision=precision).replace(
+            dp_opt=1, nu=nu, alpha=nu / 0.71, isscalar=1, got=ri, tbot=0.0, ttop=1.0, dt=2e-4, imax=500)
+        zc = mesh(p)["zc"]
+        shape = (p.nz, p.ny, p.nx)
+        ul = zc * (p.lz - zc) / (2.0 * nu)
+        amp = 0.1 * float(ul.max())
+        u = ul[:, None, None] + amp * g.uniform(-1, 1, shape)
+        v = amp * g.uniform(-1, 1, shape)
+        w = amp * g.uniform(-1, 1, shape)
+        w[-1] = 0.0
+        t = (zc / p.lz)[:, None, None] + 0.01 * g.uniform(-1, 1, shape)
+        out.append((p, {"u": u, "v": v, "w": w, "p": np.zeros(shape), "t": t}))
+    return out

@@ -201,6 +201,32 @@ int hc_kernel_profile(hc_handle* h, int max, char* names, double* total_ms,
 int hc_divergence_noalloc(const hc_params* p, const double* dz, const void* u,
                           const void* v, const void* w, double* out_dev, void* stream);
 
+/* Body force, no counterpart in the reference: fx, fy, fz are interior-only
+ * (nx,ny,nz) Fortran-order host arrays added to the explicit momentum terms ff,
+ * gg, hh every sub-step (the FD right-hand side; on the spectral path through
+ * their spectra). A NULL component is zero; all three NULL remove the force. */
+int hc_set_body_force(hc_handle* h, const double* fx, const double* fy, const double* fz);
+
+/* Advance hc_step through a CUDA graph of one whole step, captured on the first
+ * call after enabling and replayed once per step (no counterpart in the
+ * reference). Saves the per-kernel launch cost, which dominates small grids.
+ * Ignored while profiling is on; hc_set_grid and hc_set_body_force drop the graph
+ * (it is captured again on the next step). */
+int hc_set_graph(hc_handle* h, int enable);
+
+/* Ensemble of independent channels (no counterpart in the reference): one CUDA
+ * graph per step holds a branch per member, each member's kernels on its own
+ * stream, so small members run side by side. Members stay owned by the caller,
+ * must be initialized, on one device, distinct, and not stepped on their own
+ * while the ensemble lives. hc_ensemble_step advances every member nsteps steps
+ * (their diagnostics ring on the device as in hc_step; read scalars with
+ * hc_get_scalars) and returns HC_ERR_NAN if any member has seen a NaN. */
+typedef struct hc_ensemble hc_ensemble;
+int hc_ensemble_create(hc_handle* const* members, int n, hc_ensemble** out);
+int hc_ensemble_step(hc_ensemble* e, int nsteps);
+int hc_ensemble_last_ms(hc_ensemble* e, double* ms, long long* launches_per_step);
+int hc_ensemble_destroy(hc_ensemble* e);
+
 int hc_destroy(hc_handle* h);
 
 const char* hc_error_string(int code);

@@ -129,6 +129,7 @@ struct or_state {
     double *ff, *gg, *hh, *ss, *ff0, *gg0, *hh0, *ss0, *qu, *qv, *qw;
     double *uhx, *uhy, *uhz, *vhx, *vhy, *vhz, *whx, *why, *thx, *thy, *thz;
     double *mean[11];
+    double *bfx, *bfy, *bfz;                    /* body force (NULL: none), not in the reference */
     double *aa, *cc;                            /* (nx,ny,nka) */
     cplx *bb;
     double *aa_u, *cc_u, *aa_w, *cc_w, *aa_p, *cc_p, *aa_t, *cc_t;
@@ -683,6 +684,7 @@ static void get_momentum_cnvdiff(or_state* s)
                     F(s->ff, i, j, k) = -uux - uvy - uwz - um * ux + fc * (0.5 * (F(vhx, i, j, k) + F(vhx, i, j - 1, k)) - vg);
                 else
                     F(s->ff, i, j, k) = -uux - uvy - uwz + dpx_drive - um * ux;
+                if (s->bfx) F(s->ff, i, j, k) += F(s->bfx, i, j, k);
                 if (cds == 1) dpdx = (F(p, i + 1, j, k) - F(p, i, j, k)) / dx;
                 else if (cds == 2) dpdx = (-F(p, i + 2, j, k) + 27.0 * F(p, i + 1, j, k) - 27.0 * F(p, i, j, k) + F(p, i - 1, j, k)) / 24.0 / dx;
                 F(s->qu, i, j, k) = F(u, i, j, k) + dt * (rk_a * F(s->ff, i, j, k) + rk_b * F(s->ff0, i, j, k)) +
@@ -717,6 +719,7 @@ static void get_momentum_cnvdiff(or_state* s)
                     F(s->gg, i, j, k) = -vux - vvy - vwz - um * vx + fc * (ug - 0.5 * (F(uhy, i, j, k) + F(uhy, i - 1, j, k)) - um);
                 else
                     F(s->gg, i, j, k) = -vux - vvy - vwz - um * vx;
+                if (s->bfx) F(s->gg, i, j, k) += F(s->bfy, i, j, k);
                 if (cds == 1) dpdy = (F(p, i, j + 1, k) - F(p, i, j, k)) / dy;
                 else if (cds == 2) dpdy = (-F(p, i, j + 2, k) + 27.0 * F(p, i, j + 1, k) - 27.0 * F(p, i, j, k) + F(p, i, j - 1, k)) / 24.0 / dy;
                 F(s->qv, i, j, k) = F(v, i, j, k) + dt * (rk_a * F(s->gg, i, j, k) + rk_b * F(s->gg0, i, j, k)) +
@@ -753,6 +756,7 @@ static void get_momentum_cnvdiff(or_state* s)
                     F(s->hh, i, j, k) = -wux - wvy - wwz - um * wx + got * ((1.0 - l_t[k]) * F(t, i, j, k) + l_t[k] * F(t, i, j, k + 1) - t_ref);
                 else
                     F(s->hh, i, j, k) = -wux - wvy - wwz - um * wx;
+                if (s->bfx) F(s->hh, i, j, k) += F(s->bfz, i, j, k);
                 double dpdz = (F(p, i, j, k + 1) - F(p, i, j, k)) / dz_t[k];
                 F(s->qw, i, j, k) = F(w, i, j, k) + dt * (rk_a * F(s->hh, i, j, k) + rk_b * F(s->hh0, i, j, k)) +
                                     rk_c * 0.5 * dt * nu * (wxx + wyy + wzz) - rk_c * dt * dpdz;
@@ -1240,6 +1244,7 @@ static void get_momentum_cnvdiff_spec(or_state* s)
         }
         mpi_2d_fft(s, cv, -1); cadd(s, s->c_ff, cv, -coe_sk);
     }
+    if (s->bfx) { real_2_cmplx(s, s->bfx, cv); cadd(s, s->c_ff, cv, 1.0); }
     cadd(s, s->c_qu, s->c_ff, rk_a * dt);
 
     /* ---- V ---- */
@@ -1281,6 +1286,7 @@ static void get_momentum_cnvdiff_spec(or_state* s)
         }
         mpi_2d_fft(s, cv, -1); cadd(s, s->c_gg, cv, -coe_sk);
     }
+    if (s->bfx) { real_2_cmplx(s, s->bfy, cv); cadd(s, s->c_gg, cv, 1.0); }
     cadd(s, s->c_qv, s->c_gg, rk_a * dt);
 
     /* ---- W ---- */
@@ -1332,6 +1338,7 @@ static void get_momentum_cnvdiff_spec(or_state* s)
         }
         mpi_2d_fft(s, cv, -1); cadd(s, s->c_hh, cv, -coe_sk);
     }
+    if (s->bfx) { real_2_cmplx(s, s->bfz, cv); cadd(s, s->c_hh, cv, 1.0); }
     cadd(s, s->c_qw, s->c_hh, rk_a * dt);
 }
 
@@ -1560,9 +1567,32 @@ void or_destroy(or_state* s)
     cplx* cl[] = {s->bb, s->bb_u, s->bb_w, s->bb_p, s->bb_t, s->c_src, s->c_var, s->c_u, s->c_v, s->c_w, s->c_p,
                   s->c_phi, s->c_t, s->c_qu, s->c_qv, s->c_qw, s->c_ff, s->c_gg, s->c_hh, s->c_ss};
     for (size_t q = 0; q < sizeof(cl) / sizeof(cl[0]); ++q) free(cl[q]);
+    free(s->bfx); free(s->bfy); free(s->bfz);
     plan_free(&s->px);
     plan_free(&s->py);
     free(s);
+}
+
+/* Body force (no reference counterpart): a field added to ff, gg, hh of the
+ * momentum equations (the FD right-hand side and the spectral histories alike).
+ * NULL for all three removes it; a NULL component is zero. */
+int or_set_body_force(or_state* s, const double* fx, const double* fy, const double* fz)
+{
+    free(s->bfx); free(s->bfy); free(s->bfz);
+    s->bfx = s->bfy = s->bfz = NULL;
+    if (!fx && !fy && !fz) return 0;
+    size_t nf = (size_t)s->nia * s->nja * s->nka;
+    double** dst[3] = {&s->bfx, &s->bfy, &s->bfz};
+    const double* src[3] = {fx, fy, fz};
+    for (int c = 0; c < 3; ++c) {
+        *dst[c] = (double*)calloc(nf, sizeof(double));
+        if (!src[c]) continue;
+        size_t q = 0;
+        for (int k = 1; k <= s->nz; ++k)
+            for (int j = 1; j <= s->ny; ++j)
+                for (int i = 1; i <= s->nx; ++i) F(*dst[c], i + 2, j + 2, k + 2) = src[c][q++];
+    }
+    return 0;
 }
 
 int or_get_grid(or_state* s, double* dz, double* l_t, double* l_b, double* dz_t, double* dz_b)

@@ -30,6 +30,7 @@ int       or_get_field(or_state* s, int id, double* interior);
 int       or_initialize(or_state* s);
 int       or_step(or_state* s, int nsteps, hc_diag* diag);
 void      or_set_threads(int n);
+int       or_set_body_force(or_state* s, const double* fx, const double* fy, const double* fz);
 
 /* unit-level entry points used by the known-answer tests */
 int or_fft2d(int nx, int ny, int nz, double* c_interleaved, int direction);

@@ -44,6 +44,7 @@ def lib():
         L.or_fft2d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
         L.or_helmholtz_u.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
         L.or_set_threads.argtypes = [ctypes.c_int]
+        L.or_set_body_force.argtypes = [ctypes.c_void_p] * 4
         _lib = L
     return _lib
 
@@ -98,6 +99,13 @@ class Oracle:
     def load(self, fields: dict) -> None:
         for k, v in fields.items():
             self.set(k, v)
+
+    def set_body_force(self, fx=None, fy=None, fz=None) -> None:
+        """Body force added to ff, gg, hh (None: zero component; all None: off)."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (fx, fy, fz)]
+        self._bf = arrs        # keep alive for the call
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        assert lib().or_set_body_force(self.h, *ptrs) == 0
 
     def initialize(self) -> None:
         assert lib().or_initialize(self.h) == 0

@@ -125,3 +125,34 @@ def test_nan_is_reported_not_fatal(oracle_lib, engine):
     c2.initialize()
     d = c2.step(1)
     assert d[0]["nan_flag"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["fd4_ekman", "fd2_open_scalar", "fd4_open_damp_scalar"])
+def test_fd_body_force_parity(name, oracle_lib, engine):
+    """The body-force term (no reference counterpart) against the oracle's."""
+    p = CASES[name]
+    fields = inputs.small_random(p, seed=9)
+    bf = inputs.gaussian_body_force(p, seed=4, amp=0.05)
+    o = oracle_lib.Oracle(p)
+    o.load(fields)
+    o.set_body_force(*bf)
+    o.initialize()
+    rc, od = o.step(10)
+    assert rc == 0
+    c = engine.Channel(p)
+    c.load(fields)
+    c.set_body_force(*bf)
+    c.initialize()
+    c.step(10)
+    for f in ["u", "v", "w", "p", "ff", "gg", "hh"]:
+        e = rel_err(c.download(f), o.get(f))
+        assert e <= FP64_TOL, f"{name}: field {f} rel err {e:.3e}"
+    # the force changes the flow
+    o2 = oracle_lib.Oracle(p)
+    o2.load(fields)
+    o2.initialize()
+    o2.step(10)
+    assert rel_err(o2.get("u"), o.get("u")) > 1e-6
+    c.close()
+

@@ -120,3 +120,27 @@ def test_spectral_upload_after_initialize_is_refused(engine):
         c.load({"u": f["u"]})
     assert ei.value.code == -6
     c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["sp_open_scalar_skew", "sp_open_damp_skew_ekman"])
+def test_spectral_body_force_parity(name, oracle_lib, engine):
+    p = SP_CASES[name]
+    fields = _fields(p, 9)
+    bf = inputs.gaussian_body_force(p, seed=4, amp=0.05)
+    o = oracle_lib.Oracle(p)
+    o.load(fields)
+    o.set_body_force(*bf)
+    o.initialize()
+    rc, od = o.step(10)
+    assert rc == 0
+    c = engine.Channel(p)
+    c.load(fields)
+    c.set_body_force(*bf)
+    c.initialize()
+    c.step(10)
+    for f in ["u", "v", "w", "p", "ff", "gg", "hh"]:
+        e = rel_err(c.download(f), o.get(f))
+        assert e <= FP64_TOL, f"{name}: field {f} rel err {e:.3e}"
+    c.close()
+
