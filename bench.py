@@ -37,6 +37,9 @@ WORKLOADS = {
     # stratified open channel, pseudo-spectral horizontal derivatives (cds=3, issk=1)
     "open_spectral_256x256x128": (256, 256, 128),
     "open_spectral_128x128x128": (128, 128, 128),
+    # 64 independent stratified closed channels of uneven grids, one CUDA graph per
+    # step (grids from {32x32x33, 48x32x49, 64x48x65, 96x64x65}; size = total points)
+    "ensemble64": (0, 0, 0),
 }
 DEFAULT_WORKLOAD = "channel_fd4_512x384x256"
 # CPU samples of the same physics, sized for 10-30 s of host work
@@ -55,6 +58,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="run one precision only (profiling); the headline needs both")
+    ap.add_argument("--graph", action="store_true", help="replay each step from a captured CUDA graph")
     return ap.parse_args()
 
 
@@ -210,6 +214,8 @@ def run_gpu(args, ws, rank):
         c = engine.Channel(p)
         c.load(fields)
         c.initialize()
+        if args.graph:
+            c.set_graph(True)
         rc = c.step_nodiag(args.warmup)
         assert rc == 0, rc
         barrier()
@@ -291,6 +297,38 @@ def run_gpu(args, ws, rank):
     return results, err, kern, e2e
 
 
+def run_ensemble(args):
+    """All members of the seeded ensemble advanced through one graph per step,
+    FP64 and mixed; value = total gridpoint-steps / device time."""
+    import numpy as np
+    import torch
+    from hercules_b200 import engine, inputs
+    from hercules_b200.params import PREC_FP64, PREC_MIXED
+    torch.cuda.set_device(0)
+    out = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        cases = inputs.ensemble_members(n=64, seed=1000, precision=prec)
+        chans = []
+        for p, fields in cases:
+            c = engine.Channel(p)
+            c.load(fields)
+            c.initialize()
+            chans.append(c)
+        npts = sum(p.nx * p.ny * p.nz for p, _ in cases)
+        e = engine.Ensemble(chans)
+        e.step(args.warmup)
+        clk = Clocks(0)
+        with clk:
+            e.step(args.steps)
+        ms = e.last_ms
+        out[prec] = {"value": npts * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps, "npts": npts,
+                     "launches": e.launches_per_step * args.steps, "clocks": clk.summary()}
+        e.close()
+        for c in chans:
+            c.close()
+    return out
+
+
 def cpu_oracle_rate(grid, steps, warm=1):
     """Time the CPU restatement of the reference step (OpenMP, all host cores)."""
     from oracle import oracle as O
@@ -349,6 +387,24 @@ def main():
         print(json.dumps(line), flush=True)
         return
 
+    if args.workload == "ensemble64":
+        if ws > 1:
+            raise SystemExit("the ensemble workload runs on one GPU per process; launch replicas instead")
+        r = run_ensemble(args)
+        from hercules_b200.params import PREC_FP64, PREC_MIXED
+        line = dict(base)
+        line["data"] = "synthetic (64 seeded perturbed-Poiseuille members, Re_tau~U[100,300], Ri~U[0,1])"
+        line.update({"value": r[PREC_MIXED]["value"], "ms_per_step": r[PREC_MIXED]["ms_per_step"],
+                     "dtype": "f32 fields/FFT + f64 Thomas",
+                     "config": {"workload": "ensemble64", "members": 64, "total_points": r[PREC_MIXED]["npts"],
+                                "physics": "stratified closed channels, FD4, RK3, dp_opt=1, one CUDA graph per step",
+                                "parallelism": "one GPU, members as concurrent graph branches"},
+                     "fp64": {"value": r[PREC_FP64]["value"], "ms_per_step": r[PREC_FP64]["ms_per_step"]},
+                     "mixed_speedup_vs_fp64": r[PREC_FP64]["ms_per_step"] / r[PREC_MIXED]["ms_per_step"],
+                     "gpu_launches": int(r[PREC_MIXED]["launches"]), "clocks": r[PREC_MIXED]["clocks"],
+                     "roofline": None, "cpu_baseline": None, "e2e": None})
+        print(json.dumps(line), flush=True)
+        return
     results, err, kern, e2e = run_gpu(args, ws, rank)
     if rank != 0:
         return
