@@ -501,8 +501,8 @@ static bool fft_t_length_ok(int n)
 template <typename R, int N> static int fft_t_op(hc_handle* h, int op, const void* args, dim3 grid)
 {
     constexpr int RM = HC_FFT_T_RMAX;
-    constexpr size_t sx = fft_t_smem<R, N, FxLines<N>::v>();
-    constexpr size_t sy = fft_t_smem<R, N, HC_FFT_TL>();
+    constexpr size_t sx = fft_x_smem<R, N, RM>();
+    constexpr size_t sy = fft_y_smem<R, N, RM>();
     static_assert(FPlan<N, RM>::valid, "length must be 2^a 3^b 5^c");
     if (op == 0) {
         if (N == h->g.nxh && h->fft_tx) {
@@ -539,6 +539,17 @@ template <typename R> static int fft_t_setup(hc_handle* h)
     if (rc == HC_OK && h->fft_ty && !(h->fft_tx && h->g.ny == h->g.nxh))
         rc = fft_t_dispatch<R>(h, h->g.ny, 0, nullptr, dim3());
     return rc;
+}
+
+// y tile width (columns l per block) of the length-n kernel
+static int fft_t_ytl(int n)
+{
+    switch (n) {
+#define HC_LEN_CASE(N) case N: return FyLines<N>::v;
+    HC_FFT_T_LENGTHS(HC_LEN_CASE)
+#undef HC_LEN_CASE
+    }
+    return 1;
 }
 
 template <typename R> static long long fft_t_xblocks(int n, long long nrows)
@@ -668,7 +679,7 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
         for (int f = 0; f < nf; ++f) a.dst[f] = out[f];
         a.nxh = h->g.nxh; a.tw = fft_tw<R>(h, 1); a.scale = (R)(1.0 / h->p.ny); a.halt = halt;
         prof_begin(h, K_FFT_Y_FWD);
-        int rc = fft_t_dispatch<R>(h, h->g.ny, 3, &a, dim3((h->g.nxh + HC_FFT_TL - 1) / HC_FFT_TL, h->g.nz, nf));
+        int rc = fft_t_dispatch<R>(h, h->g.ny, 3, &a, dim3((h->g.nxh + fft_t_ytl(h->g.ny) - 1) / fft_t_ytl(h->g.ny), h->g.nz, nf));
         if (rc) return rc;
         CKL();
         return HC_OK;
@@ -699,7 +710,7 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
         for (int f = 0; f < nf; ++f) { a.dst[f] = in[f]; a.src[f] = ysrc ? ysrc[f] : nullptr; }
         a.nxh = h->g.nxh; a.tw = fft_tw<R>(h, 1); a.scale = (R)1; a.halt = halt;
         prof_begin(h, K_FFT_Y_INV);
-        int rc = fft_t_dispatch<R>(h, h->g.ny, 4, &a, dim3((h->g.nxh + HC_FFT_TL - 1) / HC_FFT_TL, h->g.nz, nf));
+        int rc = fft_t_dispatch<R>(h, h->g.ny, 4, &a, dim3((h->g.nxh + fft_t_ytl(h->g.ny) - 1) / fft_t_ytl(h->g.ny), h->g.nz, nf));
         if (rc) return rc;
         CKL();
     } else {

@@ -25,21 +25,31 @@ __host__ __device__ constexpr int fft_pow2_exp(int n) { return (n % 2 == 0) ? 1 
 __host__ __device__ constexpr int fft_exp_of(int n, int q) { return (n % q == 0) ? 1 + fft_exp_of(n / q, q) : 0; }
 __host__ __device__ constexpr int fft_log2(int r) { return r <= 1 ? 0 : 1 + fft_log2(r / 2); }
 
+// Passes: the power-of-two part in passes of at most RMAX points, as evenly as
+// possible; one factor 3 folded with 8 or 4 of them into a radix-24 / radix-12
+// pass (so 384 = 16 x 24 and 192 = 8 x 24 take two passes); remaining factors
+// 3 and 5 as radix-3 / radix-5 passes.
 template <int N, int RMAX> struct FPlan {
-    static constexpr int e2 = fft_pow2_exp(N);
+    static constexpr int e2all = fft_pow2_exp(N);
     static constexpr int e3 = fft_exp_of(N, 3);
     static constexpr int e5 = fft_exp_of(N, 5);
+    static constexpr int fold = e3 >= 1 ? (e2all >= 3 ? 3 : (e2all >= 2 ? 2 : 0)) : 0;   // 2^fold folded with a 3
+    static constexpr int e2 = e2all - fold;
     static constexpr int bits = fft_log2(RMAX);
     static constexpr int q2 = (e2 + bits - 1) / bits;            // power-of-two passes
-    static constexpr int npass = q2 + e3 + e5;
-    static constexpr bool valid = (N == (1 << e2) * (e3 == 0 ? 1 : (e3 == 1 ? 3 : (e3 == 2 ? 9 : 27))) *
+    static constexpr int qd = q2 > 0 ? q2 : 1;                   // divisor guard when there is no 2^k pass
+    static constexpr int nfold = fold ? 1 : 0;
+    static constexpr int npass = q2 + nfold + (e3 - nfold) + e5;
+    static constexpr bool valid = (N == (1 << e2all) * (e3 == 0 ? 1 : (e3 == 1 ? 3 : (e3 == 2 ? 9 : 27))) *
                                            (e5 == 0 ? 1 : (e5 == 1 ? 5 : 25)));
     __host__ __device__ static constexpr int rad(int p)
     {
-        return p < q2 ? (1 << (e2 / q2 + (p < e2 % q2 ? 1 : 0))) : (p < q2 + e3 ? 3 : 5);
+        return p < q2 ? (1 << (e2 / qd + (p < e2 % qd ? 1 : 0)))
+                      : (p < q2 + nfold ? (3 << fold) : (p < q2 + e3 ? 3 : 5));
     }
     // product of the radices of passes 0..p-1 (the Stockham span Ns of pass p)
     __host__ __device__ static constexpr int span(int p) { return p == 0 ? 1 : span(p - 1) * rad(p - 1); }
+    __host__ __device__ static constexpr int maxrad(int p = 0) { return p >= npass ? 1 : (rad(p) > maxrad(p + 1) ? rad(p) : maxrad(p + 1)); }
 };
 
 // padded shared-memory slot of element e of a line: one spare slot per G elements
@@ -51,28 +61,37 @@ template <typename R> struct FPad { static constexpr int G = sizeof(R) == 8 ? 8 
 // ----------------------------------------------------------------------------
 // butterflies with compile-time radix
 // ----------------------------------------------------------------------------
-// cos(2 pi e / 16) and sin(2 pi e / 16), e taken mod 16
-__host__ __device__ constexpr double cos16(int e)
+// cos(2 pi e / 48) on the quarter wave e in [0, 12] (angles k x 7.5 degrees),
+// exact values from sqrt(2), sqrt(3), sqrt(6) and half-angle identities
+__host__ __device__ constexpr double cosq48(int e)
 {
-    return (e & 15) == 0 ? 1.0 : (e & 15) == 1 ? 0.92387953251128675613 : (e & 15) == 2 ? 0.70710678118654752440
-         : (e & 15) == 3 ? 0.38268343236508977173 : (e & 15) == 4 ? 0.0 : (e & 15) == 5 ? -0.38268343236508977173
-         : (e & 15) == 6 ? -0.70710678118654752440 : (e & 15) == 7 ? -0.92387953251128675613 : (e & 15) == 8 ? -1.0
-         : (e & 15) == 9 ? -0.92387953251128675613 : (e & 15) == 10 ? -0.70710678118654752440
-         : (e & 15) == 11 ? -0.38268343236508977173 : (e & 15) == 12 ? 0.0 : (e & 15) == 13 ? 0.38268343236508977173
-         : (e & 15) == 14 ? 0.70710678118654752440 : 0.92387953251128675613;
+    return e == 0 ? 1.0 : e == 1 ? 0.991444861373810411145 : e == 2 ? 0.965925826289068286750
+         : e == 3 ? 0.923879532511286756128 : e == 4 ? 0.866025403784438646764 : e == 5 ? 0.793353340291235164580
+         : e == 6 ? 0.707106781186547524401 : e == 7 ? 0.608761429008720639416 : e == 8 ? 0.5
+         : e == 9 ? 0.382683432365089771728 : e == 10 ? 0.258819045102520762349 : e == 11 ? 0.130526192220051591548
+         : 0.0;
 }
-__host__ __device__ constexpr double sin16(int e) { return cos16(e - 4); }
+// cos and sin of 2 pi e / 48 for any e (reduced by quarter-wave symmetry)
+__host__ __device__ constexpr double cos48(int e)
+{
+    return ((e % 48) + 48) % 48 <= 12 ? cosq48(((e % 48) + 48) % 48)
+         : ((e % 48) + 48) % 48 <= 24 ? -cosq48(24 - ((e % 48) + 48) % 48)
+         : ((e % 48) + 48) % 48 <= 36 ? -cosq48(((e % 48) + 48) % 48 - 24)
+         : cosq48(48 - ((e % 48) + 48) % 48);
+}
+__host__ __device__ constexpr double sin48(int e) { return cos48(e - 12); }
 
-// v * exp(S 2 pi i E / M) for M in {4, 8, 16}; E compile-time
+// v * exp(S 2 pi i E / M) for M dividing 48 (4, 8, 12, 16, 24); E compile-time
 template <int M, int E, int S, typename T2> __device__ __forceinline__ T2 twc(T2 v)
 {
-    constexpr int e = (E * (16 / M)) & 15;
+    static_assert(48 % M == 0, "constant twiddles cover divisors of 48");
+    constexpr int e = (E * (48 / M)) % 48;
     typedef decltype(v.x) R;
     if (e == 0) return v;
-    if (e == 8) { T2 r; r.x = -v.x; r.y = -v.y; return r; }
-    if (e == 4) return mul_si<S>(v);                 // exp(S i pi/2) = S i
-    if (e == 12) return mul_si<-S>(v);
-    const R c = (R)cos16(e), s = (R)(S * sin16(e));
+    if (e == 24) { T2 r; r.x = -v.x; r.y = -v.y; return r; }
+    if (e == 12) return mul_si<S>(v);                // exp(S i pi/2) = S i
+    if (e == 36) return mul_si<-S>(v);
+    const R c = (R)cos48(e), s = (R)(S * sin48(e));
     T2 r; r.x = v.x * c - v.y * s; r.y = v.x * s + v.y * c; return r;
 }
 
@@ -137,32 +156,46 @@ template <int S, typename T2> struct Dft<8, S, T2> {
 template <int S, typename T2> struct Dft<16, S, T2> {
     static __device__ __forceinline__ void run(T2* v) { dft_split<4, 4, S>(v); }
 };
+template <int S, typename T2> struct Dft<12, S, T2> {
+    static __device__ __forceinline__ void run(T2* v) { dft_split<4, 3, S>(v); }
+};
+template <int S, typename T2> struct Dft<24, S, T2> {
+    static __device__ __forceinline__ void run(T2* v) { dft_split<8, 3, S>(v); }
+};
 
 // ----------------------------------------------------------------------------
-// Stockham passes over LINES lines of length N held in shared memory
+// Stockham passes over LINES lines of length N
 // ----------------------------------------------------------------------------
-// One pass of radix RAD with span NS: item j of a line reads s[j + r N/RAD],
-// r < RAD, multiplies by w^{r k N/(NS RAD)} (k = j mod NS), transforms, and
-// writes d[(j/NS) NS RAD + k + r NS].
-template <typename R, int N, int S, int RAD, int NS, int LINES, int NT>
-__device__ __forceinline__ void stock_pass(const typename V2<R>::T* __restrict__ src, typename V2<R>::T* __restrict__ dst,
-                                           const typename V2<R>::T* __restrict__ tw)
+// One pass of radix RAD with span NS: item j of a line reads element j + r N/RAD
+// (r < RAD), multiplies by w^{r k N/(NS RAD)} (k = j mod NS), transforms, and
+// writes element (j/NS) NS RAD + k + r NS. The first pass's reads and the last
+// pass's writes walk consecutive elements with consecutive items, so those two
+// passes read and write global memory directly; only the passes in between go
+// through shared memory. SRC::ld(line, e) and DST::st(line, e, v) are the
+// element accessors; LMINOR maps consecutive threads to consecutive lines
+// (y direction, whose lines are the strided columns) instead of consecutive
+// elements of one line (x direction).
+template <typename T2, int LS, int G> struct SmemIO {
+    T2* b;
+    __device__ __forceinline__ T2 ld(int line, int e) const { return b[line * LS + fpi<G>(e)]; }
+    __device__ __forceinline__ void st(int line, int e, T2 v) const { b[line * LS + fpi<G>(e)] = v; }
+};
+
+template <typename R, int N, int S, int RAD, int NS, int LINES, int NT, bool LMINOR, class SRC, class DST>
+__device__ __forceinline__ void stock_pass(const SRC& src, const DST& dst, const typename V2<R>::T* __restrict__ tw)
 {
     typedef typename V2<R>::T T2;
-    constexpr int G = FPad<R>::G;
-    constexpr int LS = FLine<N, G>::stride;
     constexpr int NR = N / RAD;
     constexpr int TS = N / (NS * RAD);
     for (int it = threadIdx.x; it < LINES * NR; it += NT) {
-        const int line = it / NR;
-        const int j = it - line * NR;
+        int line, j;
+        if (LMINOR) { j = it / LINES; line = it - j * LINES; }
+        else { line = it / NR; j = it - line * NR; }
         const int k = NS == 1 ? 0 : j % NS;
-        const T2* s = src + line * LS;
-        T2* d = dst + line * LS;
         T2 v[RAD];
 #pragma unroll
         for (int r = 0; r < RAD; ++r) {
-            T2 x = s[fpi<G>(j + r * NR)];
+            T2 x = src.ld(line, j + r * NR);
             if (NS > 1 && r > 0) {
                 T2 w = __ldg(tw + r * k * TS);
                 if (S > 0) w.y = -w.y;
@@ -173,24 +206,39 @@ __device__ __forceinline__ void stock_pass(const typename V2<R>::T* __restrict__
         Dft<RAD, S, T2>::run(v);
         const int base = (j / NS) * NS * RAD + k;
 #pragma unroll
-        for (int r = 0; r < RAD; ++r) d[fpi<G>(base + r * NS)] = v[r];
+        for (int r = 0; r < RAD; ++r) dst.st(line, base + r * NS, v[r]);
     }
 }
 
-// Runs passes P..npass-1 and returns the buffer holding the transform.
-template <typename R, int N, int S, int RMAX, int LINES, int NT, int P>
-__device__ __forceinline__ typename V2<R>::T* run_passes(typename V2<R>::T* src, typename V2<R>::T* dst,
-                                                         const typename V2<R>::T* tw)
+// Passes P..npass-1. Pass P reads SRC; passes after the first read shared
+// buffer A (ping-pong with B); the last pass writes DST. Every pass but the last
+// ends with a barrier.
+template <typename R, int N, int S, int RMAX, int LINES, int NT, bool LMINOR, int P, class SRC, class DST>
+__device__ __forceinline__ void run_passes(const SRC& src, const DST& dst, typename V2<R>::T* A, typename V2<R>::T* B,
+                                           const typename V2<R>::T* tw)
 {
     typedef FPlan<N, RMAX> PL;
-    if constexpr (P >= PL::npass) {
-        return src;
+    typedef typename V2<R>::T T2;
+    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride;
+    if constexpr (P == PL::npass - 1) {
+        stock_pass<R, N, S, PL::rad(P), PL::span(P), LINES, NT, LMINOR>(src, dst, tw);
     } else {
-        stock_pass<R, N, S, PL::rad(P), PL::span(P), LINES, NT>(src, dst, tw);
+        const SmemIO<T2, LS, G> out{A};
+        stock_pass<R, N, S, PL::rad(P), PL::span(P), LINES, NT, LMINOR>(src, out, tw);
         __syncthreads();
-        return run_passes<R, N, S, RMAX, LINES, NT, P + 1>(dst, src, tw);
+        const SmemIO<T2, LS, G> in{A};
+        run_passes<R, N, S, RMAX, LINES, NT, LMINOR, P + 1>(in, dst, B, A, tw);
     }
 }
+
+// Shared line buffers per kernel. y: one between two passes, two (ping-pong)
+// from three passes on, one staging buffer for an in-place single pass. x: the
+// split step's buffer plus at most one more, reused in turn by the passes.
+template <int N, int RMAX> struct FBufs {
+    static constexpr int np = FPlan<N, RMAX>::npass;
+    static constexpr int y = np >= 3 ? 2 : 1;
+    static constexpr int x = np >= 2 ? 2 : 1;
+};
 
 // ----------------------------------------------------------------------------
 // kernel arguments
@@ -215,16 +263,64 @@ template <typename R> struct FyArgs {
     const int* halt;
 };
 
-// lines per block: about 2048 complex values per block, at least one line
+// x: about 2048 complex values per block (at least one line)
 template <int N> struct FxLines { static constexpr int v = N >= 2048 ? 1 : 2048 / N; };
-// y tiles: 8 columns (128-byte runs of FP64, 64-byte runs of FP32)
-#define HC_FFT_TL 8
+// y: 16 columns per tile (128-byte row segments in FP32, 256 in FP64); 8 below 64 points
+template <int N> struct FyLines { static constexpr int v = N >= 64 ? 16 : 8; };
 #define HC_FFT_NT 256
 
-template <typename R, int N, int LINES> __host__ __device__ constexpr size_t fft_t_smem()
+template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_x_smem()
 {
-    return 2 * (size_t)LINES * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
+    return (size_t)FBufs<N, RMAX>::x * FxLines<N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
 }
+template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_y_smem()
+{
+    return (size_t)FBufs<N, RMAX>::y * FyLines<N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
+}
+
+// ---- global accessors -------------------------------------------------------
+template <typename T2, int N> struct XRowsIn {       // rows row0.., zero past the last
+    const T2* in; int nr;
+    __device__ __forceinline__ T2 ld(int line, int e) const
+    {
+        if (line < nr) return in[(long long)line * N + e];
+        T2 z; z.x = 0; z.y = 0; return z;
+    }
+};
+template <typename T2, int N> struct XRowsOut {      // c2r result, stored or added
+    T2* out; int nr; int add;
+    __device__ __forceinline__ void st(int line, int e, T2 v) const
+    {
+        if (line >= nr) return;
+        T2* p = out + (long long)line * N + e;
+        if (add) { const T2 o = *p; v.x += o.x; v.y += o.y; }
+        *p = v;
+    }
+};
+template <typename T2, int N, int S> struct YColsIn {   // column l0+line of one plane
+    const T2* s; int l0, nxh;
+    __device__ __forceinline__ T2 ld(int line, int e) const
+    {
+        const int l = l0 + line;
+        T2 z; z.x = 0; z.y = 0;
+        if (l >= nxh || (S > 0 && e == N / 2)) return z;   // inverse: Nyquist zeroed before
+        return s[(long long)e * nxh + l];
+    }
+};
+template <typename R, int N, int S> struct YColsOut {
+    typedef typename V2<R>::T T2;
+    T2* d; int l0, nxh; R sc;
+    __device__ __forceinline__ void st(int line, int e, T2 v) const
+    {
+        const int l = l0 + line;
+        if (l >= nxh) return;
+        if (S < 0) {                                       // forward: 1/ny, Nyquist zeroed after
+            v.x *= sc; v.y *= sc;
+            if (e == N / 2) { v.x = 0; v.y = 0; }
+        }
+        d[(long long)e * nxh + l] = v;
+    }
+};
 
 // ----------------------------------------------------------------------------
 // x direction, forward: real rows -> nx/2 modes, divided by nx
@@ -236,18 +332,20 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_r2c_t(FxArgs<R> a)
     constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, L = FxLines<N>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
+    // pass q (not the last) writes A for even q, B for odd q; the last pass lands
+    // in the buffer it does not read, where the split step finds it
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* B = A + L * LS;
+    T2* B = A + (FBufs<N, RMAX>::x >= 2 ? L * LS : 0);
     const int f = blockIdx.y;
     const long long row0 = (long long)blockIdx.x * L;
     const int nr = (int)min((long long)L, a.nrows - row0);
-    const T2* in = reinterpret_cast<const T2*>(a.in[f]) + row0 * N;
-    for (int idx = threadIdx.x; idx < L * N; idx += HC_FFT_NT) {
-        const int line = idx / N, l = idx - line * N;
-        A[line * LS + fpi<G>(l)] = idx < nr * N ? in[idx] : mk2<R>(R(0), R(0));
-    }
+    const XRowsIn<T2, N> src{reinterpret_cast<const T2*>(a.in[f]) + row0 * N, nr};
+    // the last pass lands in the shared buffer the split step reads
+    constexpr int np = FPlan<N, RMAX>::npass;
+    T2* Z = (np % 2 == 1) ? A : B;
+    const SmemIO<T2, LS, G> zout{Z};
+    run_passes<R, N, -1, RMAX, L, HC_FFT_NT, false, 0>(src, zout, A, B, a.tw);
     __syncthreads();
-    T2* Z = run_passes<R, N, -1, RMAX, L, HC_FFT_NT, 0>(A, B, a.tw);
     T2* out = reinterpret_cast<T2*>(a.out[f]) + row0 * N;
     const R sc = a.scale;
     for (int idx = threadIdx.x; idx < nr * N; idx += HC_FFT_NT) {
@@ -272,77 +370,93 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
     constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, L = FxLines<N>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
-    T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* B = A + L * LS;
+    // the pre-split lines Zs feed pass 0; later passes alternate A and Zs
+    T2* Zs = reinterpret_cast<T2*>(smem_raw);
+    T2* A = Zs + (FBufs<N, RMAX>::x >= 2 ? L * LS : 0);
+    T2* B = Zs;
     const int f = blockIdx.y;
     const long long row0 = (long long)blockIdx.x * L;
     const int nr = (int)min((long long)L, a.nrows - row0);
     const T2* in = reinterpret_cast<const T2*>(a.in[f]) + row0 * N;
-    for (int idx = threadIdx.x; idx < L * N; idx += HC_FFT_NT) {
-        const int line = idx / N, l = idx - line * N;
-        A[line * LS + fpi<G>(l)] = idx < nr * N ? in[idx] : mk2<R>(R(0), R(0));
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < L * N; idx += HC_FFT_NT) {
-        const int line = idx / N, l = idx - line * N;
-        const T2 x = A[line * LS + fpi<G>(l)];
-        T2 xn = mk2<R>(R(0), R(0));
-        if (l != 0) { xn = A[line * LS + fpi<G>(N - l)]; xn.y = -xn.y; }
-        T2 wc = __ldg(a.wp + l);
+    // pre-split straight from global: Z(l) = (X(l) + conj X(N-l)) + i conj(W_l) (X(l) - conj X(N-l));
+    // the partner of l = 0 is the x Nyquist mode (zero, not stored). FP32: one
+    // thread per pair (l, N-l), so every mode is read once.
+    auto zsplit = [&](T2 a0, T2 b0, int ll) {               // a0 = X(ll), b0 = X(N-ll)
+        T2 bc = b0; bc.y = -bc.y;
+        T2 wc = __ldg(a.wp + ll);
         wc.y = -wc.y;
-        const T2 s = cadd2(x, xn);
-        const T2 d = cmulc(wc, csub2(x, xn));
-        B[line * LS + fpi<G>(l)] = mk2<R>(s.x - d.y, s.y + d.x);     // s + i d
+        const T2 s = cadd2(a0, bc);
+        const T2 d = cmulc(wc, csub2(a0, bc));
+        return mk2<R>(s.x - d.y, s.y + d.x);                   // s + i d
+    };
+    if constexpr (sizeof(R) == 8) {
+        // FP64: one thread per mode, the partner read again (measured faster here)
+        for (int idx = threadIdx.x; idx < L * N; idx += HC_FFT_NT) {
+            const int line = idx / N, l = idx - line * N;
+            T2 x = mk2<R>(R(0), R(0)), y = x;
+            if (line < nr) {
+                x = in[(long long)line * N + l];
+                if (l != 0) y = in[(long long)line * N + N - l];
+            }
+            Zs[line * LS + fpi<G>(l)] = zsplit(x, y, l);
+        }
+        __syncthreads();
+        const SmemIO<T2, LS, G> src64{Zs};
+        const XRowsOut<T2, N> dst64{reinterpret_cast<T2*>(a.out[f]) + row0 * N, nr, a.add[f]};
+        run_passes<R, N, 1, RMAX, L, HC_FFT_NT, false, 0>(src64, dst64, A, B, a.tw);
+        return;
+    }
+    constexpr int NP = N / 2 + 1;
+    for (int idx = threadIdx.x; idx < L * NP; idx += HC_FFT_NT) {
+        const int line = idx / NP, l = idx - line * NP;
+        T2 x = mk2<R>(R(0), R(0)), y = x;
+        if (line < nr) {
+            x = in[(long long)line * N + l];
+            if (l != 0) y = in[(long long)line * N + N - l];
+        }
+        Zs[line * LS + fpi<G>(l)] = zsplit(x, y, l);
+        if (l != 0 && 2 * l != N) Zs[line * LS + fpi<G>(N - l)] = zsplit(y, x, N - l);
     }
     __syncthreads();
-    T2* Z = run_passes<R, N, 1, RMAX, L, HC_FFT_NT, 0>(B, A, a.tw);
-    T2* out = reinterpret_cast<T2*>(a.out[f]) + row0 * N;
-    const int add = a.add[f];
-    for (int idx = threadIdx.x; idx < nr * N; idx += HC_FFT_NT) {
-        const int line = idx / N, l = idx - line * N;
-        T2 v = Z[line * LS + fpi<G>(l)];
-        if (add) { const T2 o = out[idx]; v.x += o.x; v.y += o.y; }
-        out[idx] = v;
-    }
+    const SmemIO<T2, LS, G> src{Zs};
+    const XRowsOut<T2, N> dst{reinterpret_cast<T2*>(a.out[f]) + row0 * N, nr, a.add[f]};
+    run_passes<R, N, 1, RMAX, L, HC_FFT_NT, false, 0>(src, dst, A, B, a.tw);
 }
 
 // ----------------------------------------------------------------------------
-// y direction on the half spectrum [k][m][l]: tiles of HC_FFT_TL columns l of one
-// plane k; grid (ceil(nxh/TL), nz, fields)
+// y direction on the half spectrum [k][m][l]: tiles of FyLines<N> columns l of
+// one plane k; grid (ceil(nxh/TL), nz, fields)
 // ----------------------------------------------------------------------------
 template <typename R, int N, int S, int RMAX>
 __global__ void __launch_bounds__(HC_FFT_NT) k_fft_y_t(FyArgs<R> a)
 {
     typedef typename V2<R>::T T2;
-    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, TL = HC_FFT_TL, NYQ = N / 2;
+    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, TL = FyLines<N>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* B = A + TL * LS;
-    const int nxh = a.nxh;
+    T2* B = A + (FBufs<N, RMAX>::y >= 2 ? TL * LS : 0);
     const int l0 = blockIdx.x * TL;
-    const long long plane = (long long)blockIdx.y * N * nxh;
+    const long long plane = (long long)blockIdx.y * N * a.nxh;
     T2* d = a.dst[blockIdx.z] + plane;
     const T2* s = a.src[blockIdx.z] ? a.src[blockIdx.z] + plane : d;
-    for (int idx = threadIdx.x; idx < TL * N; idx += HC_FFT_NT) {
-        const int lt = idx % TL, m = idx / TL;
-        const int l = l0 + lt;
-        T2 v = mk2<R>(R(0), R(0));
-        if (l < nxh && !(S > 0 && m == NYQ)) v = s[(long long)m * nxh + l];
-        A[lt * LS + fpi<G>(m)] = v;
-    }
-    __syncthreads();
-    T2* Z = run_passes<R, N, S, RMAX, TL, HC_FFT_NT, 0>(A, B, a.tw);
-    const R sc = a.scale;
-    for (int idx = threadIdx.x; idx < TL * N; idx += HC_FFT_NT) {
-        const int lt = idx % TL, m = idx / TL;
-        const int l = l0 + lt;
-        if (l >= nxh) continue;
-        T2 v = Z[lt * LS + fpi<G>(m)];
-        if (S < 0) {
-            v.x *= sc; v.y *= sc;
-            if (m == NYQ) v = mk2<R>(R(0), R(0));
+    const YColsIn<T2, N, S> src{s, l0, a.nxh};
+    const YColsOut<R, N, S> dst{d, l0, a.nxh, a.scale};
+    if constexpr (FPlan<N, RMAX>::npass == 1) {
+        // one pass: in place is safe only through a barrier between reads and writes
+        if (s == d) {
+            constexpr int LSz = FLine<N, G>::stride;
+            const SmemIO<T2, LSz, G> stage{A};
+            for (int idx = threadIdx.x; idx < TL * N; idx += HC_FFT_NT) {
+                const int m = idx / TL, lt = idx - m * TL;
+                stage.st(lt, m, src.ld(lt, m));
+            }
+            __syncthreads();
+            stock_pass<R, N, S, FPlan<N, RMAX>::rad(0), 1, TL, HC_FFT_NT, true>(stage, dst, a.tw);
+            return;
         }
-        d[(long long)m * nxh + l] = v;
     }
+    // in place (s == d) with two or more passes: the first pass reads every
+    // element of the tile before its barrier, and only the last pass writes it
+    run_passes<R, N, S, RMAX, TL, HC_FFT_NT, true, 0>(src, dst, A, B, a.tw);
 }
