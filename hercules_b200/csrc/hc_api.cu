@@ -611,6 +611,18 @@ template <typename R> static int set_smem_attrs()
     CK(cudaFuncSetAttribute(k_fft_x_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(k_fft_y<R, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(k_fft_y<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    {
+        // the largest tile (K = 8) bounds every instantiation
+        const int sm = (int)column_tile_smem_r<8>(sizeof(typename V2<R>::T));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    }
     CK(cudaFuncSetAttribute(k_column_fd_tile<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<4>()));
     CK(cudaFuncSetAttribute(k_column_fd_tile<R, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<5>()));
     CK(cudaFuncSetAttribute(k_column_fd_tile<R, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<6>()));
@@ -801,7 +813,7 @@ template <typename R, int K> static int col_fd_k(hc_handle* h, const ColArgs<R>&
         return HC_OK;
     }
     const unsigned nb = (unsigned)((h->g.ncol + CT_COLS - 1) / CT_COLS);
-    k_column_fd_tile<R, K><<<nb, CT_COLS * 32, column_tile_smem<K>(), h->st>>>(ca);
+    k_column_fd_tile_r<R, K><<<nb, CT_COLS * 32, column_tile_smem_r<K>(sizeof(typename V2<R>::T)), h->st>>>(ca);
     CKL();
     return HC_OK;
 }

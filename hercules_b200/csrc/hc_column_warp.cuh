@@ -516,3 +516,324 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile(ColArgs<R> a
     __syncthreads();
     ct_store<R, K>(a.psi, TU, c0, ncol, nz);
 }
+
+// ---------------------------------------------------------------------------
+// The partition + PCR solve on a chosen arithmetic type T (float or double):
+// the mixed-precision column kernel runs its Helmholtz solves in FP32 and keeps
+// the Poisson solve and the (0,0) mean mode in FP64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float rcp_t(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_t(double x) { return rcp_nr(x); }
+
+template <typename T> __device__ __forceinline__ typename V2<T>::T t2sub(typename V2<T>::T a, typename V2<T>::T b)
+{
+    return mk2<T>(a.x - b.x, a.y - b.y);
+}
+template <typename T> __device__ __forceinline__ typename V2<T>::T t2axpy(typename V2<T>::T a, typename V2<T>::T b, T s)
+{
+    return mk2<T>(a.x - s * b.x, a.y - s * b.y);           // a - s b
+}
+template <typename T> __device__ __forceinline__ typename V2<T>::T t2scale(typename V2<T>::T a, T s)
+{
+    return mk2<T>(a.x * s, a.y * s);
+}
+template <typename T> __device__ __forceinline__ typename V2<T>::T t2shfl_up(typename V2<T>::T v, int s)
+{
+    return mk2<T>(__shfl_up_sync(0xffffffffu, v.x, s), __shfl_up_sync(0xffffffffu, v.y, s));
+}
+template <typename T> __device__ __forceinline__ typename V2<T>::T t2shfl_dn(typename V2<T>::T v, int s)
+{
+    return mk2<T>(__shfl_down_sync(0xffffffffu, v.x, s), __shfl_down_sync(0xffffffffu, v.y, s));
+}
+
+template <typename T, int K, int NR, typename CF>
+__device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename V2<T>::T (&d)[NR][K], int ln)
+{
+    typedef typename V2<T>::T T2;
+    const int r0 = ln * K;
+    T vv[K], ww[K], ib[K];
+    if (K >= 2) {
+        T a0, b0, c0;
+        coef(r0, a0, b0, c0);
+        ib[0] = rcp_t(b0);
+        vv[0] = -a0;
+        ww[0] = (K == 2) ? -c0 : T(0);
+        T cprev = c0;
+#pragma unroll
+        for (int i = 1; i <= K - 2; ++i) {
+            T ai, bi, ci;
+            coef(r0 + i, ai, bi, ci);
+            const T mlt = ai * ib[i - 1];
+            ib[i] = rcp_t(bi - mlt * cprev);
+#pragma unroll
+            for (int q = 0; q < NR; ++q) d[q][i] = t2axpy<T>(d[q][i], d[q][i - 1], mlt);
+            vv[i] = -mlt * vv[i - 1];
+            ww[i] = (i == K - 2 ? -ci : T(0)) - mlt * ww[i - 1];
+            cprev = ci;
+        }
+#pragma unroll
+        for (int q = 0; q < NR; ++q) d[q][K - 2] = t2scale<T>(d[q][K - 2], ib[K - 2]);
+        vv[K - 2] *= ib[K - 2];
+        ww[K - 2] *= ib[K - 2];
+#pragma unroll
+        for (int i = K - 3; i >= 0; --i) {
+            T ai, bi, ci;
+            coef(r0 + i, ai, bi, ci);
+#pragma unroll
+            for (int q = 0; q < NR; ++q) d[q][i] = t2scale<T>(t2axpy<T>(d[q][i], d[q][i + 1], ci), ib[i]);
+            vv[i] = (vv[i] - ci * vv[i + 1]) * ib[i];
+            ww[i] = (ww[i] - ci * ww[i + 1]) * ib[i];
+        }
+    }
+    T aK, bK, cK;
+    coef(r0 + K - 1, aK, bK, cK);
+    const T xm_v = K >= 2 ? vv[K - 2] : T(1);
+    const T xm_w = K >= 2 ? ww[K - 2] : T(0);
+    const T f_v = K >= 2 ? vv[0] : T(0);
+    const T f_w = K >= 2 ? ww[0] : T(1);
+    const T nf_v = __shfl_down_sync(0xffffffffu, f_v, 1);
+    const T nf_w = __shfl_down_sync(0xffffffffu, f_w, 1);
+    T A = aK * xm_v;
+    T B = aK * xm_w + bK + cK * nf_v;
+    T C = cK * nf_w;
+    T2 D[NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+        const T2 z = mk2<T>(T(0), T(0));
+        const T2 xm_g = K >= 2 ? d[q][K - 2 < 0 ? 0 : K - 2] : z;
+        const T2 f_g = K >= 2 ? d[q][0] : z;
+        const T2 nf_g = t2shfl_dn<T>(f_g, 1);
+        D[q] = t2axpy<T>(t2axpy<T>(d[q][K - 1], xm_g, aK), nf_g, cK);
+    }
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        T Am = __shfl_up_sync(0xffffffffu, A, s), Bm = __shfl_up_sync(0xffffffffu, B, s);
+        T Cm = __shfl_up_sync(0xffffffffu, C, s);
+        T Ap = __shfl_down_sync(0xffffffffu, A, s), Bp = __shfl_down_sync(0xffffffffu, B, s);
+        T Cp = __shfl_down_sync(0xffffffffu, C, s);
+        const bool lo = ln < s, hi = ln + s > 31;
+        if (lo) { Am = T(0); Bm = T(1); Cm = T(0); }
+        if (hi) { Ap = T(0); Bp = T(1); Cp = T(0); }
+        const T k1 = A * rcp_t(Bm), k2 = C * rcp_t(Bp);
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            T2 Dm = t2shfl_up<T>(D[q], s), Dp = t2shfl_dn<T>(D[q], s);
+            if (lo) Dm = mk2<T>(T(0), T(0));
+            if (hi) Dp = mk2<T>(T(0), T(0));
+            D[q] = t2axpy<T>(t2axpy<T>(D[q], Dm, k1), Dp, k2);
+        }
+        const T nA = -Am * k1, nC = -Cp * k2, nB = B - Cm * k1 - Ap * k2;
+        A = nA; B = nB; C = nC;
+    }
+    const T iB = rcp_t(B);
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+        const T2 y = t2scale<T>(D[q], iB);
+        T2 yp = t2shfl_up<T>(y, 1);
+        if (ln == 0) yp = mk2<T>(T(0), T(0));
+#pragma unroll
+        for (int i = 0; i < K - 1; ++i)
+            d[q][i] = mk2<T>(d[q][i].x + vv[i] * yp.x + ww[i] * y.x, d[q][i].y + vv[i] * yp.y + ww[i] * y.y);
+        d[q][K - 1] = y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_column_fd_tile with the tiles in the storage type and the Helmholtz solves
+// in the storage precision: in the mixed-precision mode the u, v, w solves run
+// in FP32 (the (0,0) mean mode, with its forcing, and the phi Poisson solve stay
+// FP64); in FP64 mode it computes exactly what k_column_fd_tile computes.
+// ---------------------------------------------------------------------------
+template <int K> __host__ size_t column_tile_smem_r(size_t elem) { return (size_t)3 * CT_COLS * ct_stride<K>() * elem; }
+
+template <typename R, int K>
+__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R> a)
+{
+    typedef typename V2<R>::T TT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (a.halt && *a.halt) return;
+    const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const long long ncol = a.g.ncol;
+    const long long c0 = (long long)blockIdx.x * CT_COLS;
+    const long long c = c0 + wp;
+    const bool active = c < ncol;
+    const int nz = a.g.nz;
+    constexpr int STR = ct_stride<K>();
+    TT* TU = reinterpret_cast<TT*>(smem_raw);
+    TT* TV = TU + CT_COLS * STR;
+    TT* TW = TV + CT_COLS * STR;
+    auto load = [&](const TT* __restrict__ q, TT* T, int nrows) {
+        for (int idx = threadIdx.x; idx < nrows * CT_COLS; idx += blockDim.x) {
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            const long long cc = c0 + cb;
+            T[cb * STR + (r % K) * 32 + r / K] = cc < ncol ? q[(long long)r * ncol + cc] : mk2<R>(R(0), R(0));
+        }
+    };
+    auto store = [&](TT* __restrict__ q, const TT* T, int nrows) {
+        for (int idx = threadIdx.x; idx < nrows * CT_COLS; idx += blockDim.x) {
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            const long long cc = c0 + cb;
+            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * 32 + r / K];
+        }
+    };
+    load(a.qu, TU, nz);
+    load(a.qv, TV, nz);
+    load(a.qw, TW, nz - 1);
+    __syncthreads();
+    TT* SU = TU + wp * STR;
+    TT* SV = TV + wp * STR;
+    TT* SW = TW + wp * STR;
+    const int l = (int)(c % a.g.nxh), m = (int)(c / a.g.nxh);
+    const bool is00 = (c == 0);
+    const double rk = a.rk_c, dt = a.dt;
+    const int r0 = ln * K;
+    double2 ph[1][K];
+    if (active) {
+        const double lam = __ldg(a.c.hx + l) + __ldg(a.c.hy + m);
+        const double lamp = __ldg(a.c.px + l) + __ldg(a.c.py + m);
+        const double* dgp = is00 ? a.c.d0p : a.c.dgp;
+        // ---- u*, v* (one matrix, two right-hand sides) and w*, in the type T
+        auto helmholtz = [&](auto tag) {
+            typedef decltype(tag) T;
+            typedef typename V2<T>::T T2;
+            const double* dgu = is00 ? a.c.d0u : a.c.dgu;
+            const double* dgw = is00 ? a.c.d0w : a.c.dgw;
+            {
+                T2 d[2][K];
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    const int r = r0 + i;
+                    if (r < nz) {
+                        const TT xu = SU[i * 32 + ln], xv = SV[i * 32 + ln];
+                        double ux = (double)xu.x;
+                        if (is00 && r == 0) ux += a.bcu0;
+                        if (is00 && r == nz - 1) ux += a.bcu1;
+                        d[0][i] = mk2<T>((T)ux, (T)xu.y);
+                        d[1][i] = mk2<T>((T)xv.x, (T)xv.y);
+                    } else {
+                        d[0][i] = mk2<T>(T(0), T(0));
+                        d[1][i] = mk2<T>(T(0), T(0));
+                    }
+                }
+                auto cf = [&](int r, T& aa, T& bb, T& cc) {
+                    if (r < nz) {
+                        aa = (T)(rk * __ldg(a.c.au + r));
+                        cc = (T)(rk * __ldg(a.c.cu + r));
+                        bb = (T)(1.0 + rk * (-lam + __ldg(dgu + r)));
+                    } else { aa = T(0); bb = T(1); cc = T(0); }
+                };
+                warp_partition_solve_t<T, K, 2>(cf, d, ln);
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    SU[i * 32 + ln] = mk2<R>((R)d[0][i].x, (R)d[0][i].y);
+                    SV[i * 32 + ln] = mk2<R>((R)d[1][i].x, (R)d[1][i].y);
+                }
+            }
+            {
+                T2 dw[1][K];
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    const TT x = SW[i * 32 + ln];
+                    dw[0][i] = r0 + i < nz - 1 ? mk2<T>((T)x.x, (T)x.y) : mk2<T>(T(0), T(0));
+                }
+                auto cf = [&](int r, T& aa, T& bb, T& cc) {
+                    if (r < nz - 1) {
+                        aa = (T)(rk * __ldg(a.c.aw + r));
+                        cc = (T)(rk * __ldg(a.c.cw + r));
+                        bb = (T)(1.0 + rk * (-lam + __ldg(dgw + r)));
+                    } else { aa = T(0); bb = T(1); cc = T(0); }
+                };
+                warp_partition_solve_t<T, K, 1>(cf, dw, ln);
+#pragma unroll
+                for (int i = 0; i < K; ++i) SW[i * 32 + ln] = mk2<R>((R)dw[0][i].x, (R)dw[0][i].y);
+            }
+        };
+        if (is00) helmholtz(double(0)); else helmholtz(R(0));
+        __syncwarp();
+        // ---- phi: source div(u*)/dt, Poisson with the null-space pin on (0,0), FP64
+        const double2 DX = __ldg(a.c.dx + l), DY = __ldg(a.c.dy + m);
+        const double rdt = 1.0 / dt;
+        {
+            auto ldt = [&](const TT* S, int idx) { const TT x = S[idx]; return make_double2((double)x.x, (double)x.y); };
+            const double2 wlast = ldt(SW, (K - 1) * 32 + ln);
+            double2 wprev0 = shfl_up2(wlast, 1);
+            if (ln == 0) wprev0 = make_double2(0, 0);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                if (r < nz) {
+                    const double2 us = ldt(SU, i * 32 + ln), vs = ldt(SV, i * 32 + ln), ws = ldt(SW, i * 32 + ln);
+                    const double2 wm = i > 0 ? ldt(SW, (i - 1) * 32 + ln) : wprev0;
+                    const double rdz = __ldg(a.c.rdz + r);
+                    double2 div = zadd(zmul(DX, us), zmul(DY, vs));
+                    div = zadd(div, make_double2((ws.x - wm.x) * rdz, (ws.y - wm.y) * rdz));
+                    ph[0][i] = make_double2(div.x * rdt, div.y * rdt);
+                    if (is00 && r == 0) ph[0][i] = make_double2(0, 0);
+                } else {
+                    ph[0][i] = make_double2(0, 0);
+                }
+            }
+            auto cf = [&](int r, double& aa, double& bb, double& cc) {
+                if (r < nz) {
+                    aa = rk * __ldg(a.c.ap + r);
+                    cc = (is00 && r == 0) ? 0.0 : rk * __ldg(a.c.cp + r);
+                    bb = rk * (lamp + __ldg(dgp + r));
+                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+            };
+            warp_partition_solve<K, 1>(cf, ph, ln);
+        }
+        // ---- projection of u*, v*, w* in place in the tiles
+        {
+            const double2 GX = __ldg(a.c.gx + l), GY = __ldg(a.c.gy + m);
+            const double cpr = rk * dt;
+            const double2 nxt0 = shfl_dn2(ph[0][0], 1);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                if (r >= nz) continue;
+                const double2 pc = ph[0][i];
+                const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
+                const TT us = SU[i * 32 + ln], vs = SV[i * 32 + ln], ws = SW[i * 32 + ln];
+                const double rdzt = __ldg(a.c.rdzt + r);
+                const double2 gu = zmul(GX, pc), gv = zmul(GY, pc);
+                SU[i * 32 + ln] = mk2<R>((R)((double)us.x - cpr * gu.x), (R)((double)us.y - cpr * gu.y));
+                SV[i * 32 + ln] = mk2<R>((R)((double)vs.x - cpr * gv.x), (R)((double)vs.y - cpr * gv.y));
+                SW[i * 32 + ln] = r <= nz - 2 ? mk2<R>((R)((double)ws.x - cpr * (pu.x - pc.x) * rdzt),
+                                                       (R)((double)ws.y - cpr * (pu.y - pc.y) * rdzt))
+                                              : mk2<R>(R(0), R(0));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < K; ++i) ph[0][i] = make_double2(0, 0);
+    }
+    __syncthreads();
+    store(a.qu, TU, nz);
+    store(a.qv, TV, nz);
+    store(a.qw, TW, nz);
+    __syncthreads();
+    // ---- psi = phi - rk_c dt nu/2 lap(phi), staged through the u tile
+    {
+        const double2 nxt0 = shfl_dn2(ph[0][0], 1);
+        const double2 prv0 = shfl_up2(ph[0][K - 1], 1);
+        if (active) {
+            const double lxy = __ldg(a.c.lx + l) + __ldg(a.c.ly + m);
+            const double cps = rk * 0.5 * dt * a.nu;
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                if (r >= nz) continue;
+                const double2 pc = ph[0][i];
+                const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
+                const double2 pd = (r == 0) ? pc : (i > 0 ? ph[0][i - 1] : prv0);
+                const double rdzt = __ldg(a.c.rdzt + r), rdzb = __ldg(a.c.rdzb + r), rdz = __ldg(a.c.rdz + r);
+                double2 lz;
+                lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
+                lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
+                SU[i * 32 + ln] = mk2<R>((R)(pc.x - cps * (lxy * pc.x + lz.x)), (R)(pc.y - cps * (lxy * pc.y + lz.y)));
+            }
+        }
+    }
+    __syncthreads();
+    store(a.psi, TU, nz);
+}
