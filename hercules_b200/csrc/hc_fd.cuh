@@ -476,31 +476,44 @@ __global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
     const int k0 = blockIdx.y * kc, k1 = min(g.nz, k0 + kc);
     double ub = 0.0, cfl = 0.0;
     if (ij < g.nxy) {
+        // the fields are never written here and the accumulators never read as
+        // fields, so the loads of consecutive levels may overlap
+        const R* __restrict__ fu = s.f.u; const R* __restrict__ fv = s.f.v;
+        const R* __restrict__ fw = s.f.w; const R* __restrict__ ft = s.f.t;
+        const R* __restrict__ fux = s.uhx_s; const R* __restrict__ fvy = s.vhy_s;
+        double* __restrict__ m0 = s.mean[0]; double* __restrict__ m1 = s.mean[1];
+        double* __restrict__ m2 = s.mean[2]; double* __restrict__ m3 = s.mean[3];
+        double* __restrict__ m4 = s.mean[4]; double* __restrict__ m5 = s.mean[5];
+        double* __restrict__ m6 = s.mean[6]; double* __restrict__ m7 = s.mean[7];
+        double* __restrict__ m8 = s.mean[8]; double* __restrict__ m9 = s.mean[9];
+        double* __restrict__ m10 = s.mean[10];
+        const double um = s.um;
+        double wm = k0 > 0 ? (double)fw[(long long)(k0 - 1) * g.nxy + ij] : 0.0;
+#pragma unroll 2
         for (int k = k0; k < k1; ++k) {
             const long long q = (long long)k * g.nxy + ij;
-            const double u = (double)s.f.u[q], v = (double)s.f.v[q], w = (double)s.f.w[q];
+            const double u = (double)fu[q], v = (double)fv[q], w = (double)fw[q];
             const double dzk = ldz(g.z.dz, k);
             ub += u * dzk;
             cfl = fmax(cfl, s.dt * fabs(u) * rdx + s.dt * fabs(v) * rdy + s.dt * fabs(w) / dzk);
             if (s.accumulate) {
-                const double t = (double)s.f.t[q];
-                const double wm = k > 0 ? (double)s.f.w[q - g.nxy] : 0.0;
+                const double t = (double)ft[q];
                 const double wc = 0.5 * (w + wm);
-                const double ux = s.uhx_s ? (double)s.uhx_s[q] : u;
-                const double vy = s.vhy_s ? (double)s.vhy_s[q] : v;
-                const double um = s.um;
-                s.mean[4][q] += (u + um) * (u + um);
-                s.mean[5][q] += v * v;
-                s.mean[6][q] += w * w;
-                s.mean[7][q] += wc * (ux + um);
-                s.mean[8][q] += wc * vy;
-                s.mean[9][q] += t * t;
-                s.mean[10][q] += t * 0.5 * (w + wm);
-                s.mean[0][q] += u + um;
-                s.mean[1][q] += v;
-                s.mean[2][q] += w;
-                s.mean[3][q] += t;
+                const double ux = fux ? (double)fux[q] : u;
+                const double vy = fvy ? (double)fvy[q] : v;
+                m4[q] += (u + um) * (u + um);
+                m5[q] += v * v;
+                m6[q] += w * w;
+                m7[q] += wc * (ux + um);
+                m8[q] += wc * vy;
+                m9[q] += t * t;
+                m10[q] += t * 0.5 * (w + wm);
+                m0[q] += u + um;
+                m1[q] += v;
+                m2[q] += w;
+                m3[q] += t;
             }
+            wm = w;
         }
     }
     ub = warp_sum(ub);

@@ -406,16 +406,28 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
         run_passes<R, N, 1, RMAX, L, HC_FFT_NT, false, 0>(src64, dst64, A, B, a.tw);
         return;
     }
+    // all of a thread's pairs are loaded before any is used, so the loads overlap
     constexpr int NP = N / 2 + 1;
-    for (int idx = threadIdx.x; idx < L * NP; idx += HC_FFT_NT) {
+    constexpr int ROUNDS = (L * NP + HC_FFT_NT - 1) / HC_FFT_NT;
+    T2 xs[ROUNDS], ys[ROUNDS];
+#pragma unroll
+    for (int q = 0; q < ROUNDS; ++q) {
+        const int idx = threadIdx.x + q * HC_FFT_NT;
         const int line = idx / NP, l = idx - line * NP;
-        T2 x = mk2<R>(R(0), R(0)), y = x;
-        if (line < nr) {
-            x = in[(long long)line * N + l];
-            if (l != 0) y = in[(long long)line * N + N - l];
+        xs[q] = mk2<R>(R(0), R(0));
+        ys[q] = xs[q];
+        if (idx < L * NP && line < nr) {
+            xs[q] = in[(long long)line * N + l];
+            if (l != 0) ys[q] = in[(long long)line * N + N - l];
         }
-        Zs[line * LS + fpi<G>(l)] = zsplit(x, y, l);
-        if (l != 0 && 2 * l != N) Zs[line * LS + fpi<G>(N - l)] = zsplit(y, x, N - l);
+    }
+#pragma unroll
+    for (int q = 0; q < ROUNDS; ++q) {
+        const int idx = threadIdx.x + q * HC_FFT_NT;
+        if (idx >= L * NP) break;
+        const int line = idx / NP, l = idx - line * NP;
+        Zs[line * LS + fpi<G>(l)] = zsplit(xs[q], ys[q], l);
+        if (l != 0 && 2 * l != N) Zs[line * LS + fpi<G>(N - l)] = zsplit(ys[q], xs[q], N - l);
     }
     __syncthreads();
     const SmemIO<T2, LS, G> src{Zs};
