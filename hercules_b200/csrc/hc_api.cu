@@ -23,6 +23,7 @@
 #include "hc_rhs_tiled.cuh"
 #include "hc_column_warp.cuh"
 #include "hc_spec.cuh"
+#include "hc_adjoint.cuh"
 
 // ---------------------------------------------------------------------------
 // small device kernels for the scalar state
@@ -214,6 +215,15 @@ struct hc_handle {
     int div_in_rhs;          // FD without damping: sub-step checks ride in the next RHS
     void* bf[3];             // body force (storage type), allocated by hc_set_body_force
     int has_bf;
+    // discrete adjoint (hc_adjoint): one allocation for checkpoints, tape and adjoint fields
+    double* adj_buf;
+    size_t adj_bytes;
+    DevScalars* adj_sc;      // scalar state at each checkpoint and at the end
+    int adj_nsc;
+    double adj_ms[2];        // forward pass, reverse sweep (recomputation included)
+    int adj_nsteps, adj_ckpt, adj_nseg, adj_seglen;
+    int adj_ready;           // 1: checkpoints of the last hc_adjoint_forward are valid
+    long long adj_launches[2];
     // CUDA graph of one step (hc_set_graph): captured on first use, replayed per step
     int use_graph;
     cudaGraphExec_t gexec;
@@ -1283,6 +1293,186 @@ template <typename R> static int step_dispatch(hc_handle* h)
     return step_sp<R>(h);
 }
 
+
+// ---------------------------------------------------------------------------
+// discrete adjoint of the FD step (hc_adjoint)
+// ---------------------------------------------------------------------------
+struct AdjBufs {
+    double* lam[4];      // adjoint of u, v, w, p at the current point of the sweep
+    double* lh[3];       // adjoint of the histories ff, gg, hh
+    double* lq[3];       // lambda_q of the current sub-step (physical)
+    double* lbf[3];      // body-force gradient
+    double* ckpt;        // checkpoint c: 7 fields (u, v, w, p, ff, gg, hh) at ckpt + 7 c n
+    double* tape;        // sub-step t of a segment: its start state u, v, w, p at tape + 4 t n
+    double* fin;         // the final state, 7 fields
+};
+
+static const int ADJ_STATE[7] = {F_U, F_V, F_W, F_P, F_FF, F_GG, F_HH};
+
+template <int K> static int col_adj_k(hc_handle* h, const ColAdjArgs& a)
+{
+    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
+    k_column_fd_adj<K><<<nb, CW_WARPS * 32, 0, h->st>>>(a);
+    CKL();
+    return HC_OK;
+}
+static int launch_column_adj(hc_handle* h, const ColAdjArgs& a)
+{
+    switch ((h->p.nz + 31) / 32) {
+    case 1: return col_adj_k<1>(h, a);
+    case 2: return col_adj_k<2>(h, a);
+    case 3: return col_adj_k<3>(h, a);
+    case 4: return col_adj_k<4>(h, a);
+    case 5: return col_adj_k<5>(h, a);
+    case 6: return col_adj_k<6>(h, a);
+    case 7: return col_adj_k<7>(h, a);
+    case 8: return col_adj_k<8>(h, a);
+    default: return HC_ERR_UNSUPPORTED;
+    }
+}
+
+// Adjoint of one FD sub-step: on entry b.lam / b.lh hold the adjoints of the
+// sub-step's outputs, on return those of its inputs (the state st[] it started from).
+template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* const* st, AdjBufs& b)
+{
+    const hc_params& p = h->p;
+    double rk_a, rk_b, rk_c;
+    if (p.dts == 2) { rk_a = RKC1[sub]; rk_b = RKC2[sub]; rk_c = RKC3[sub]; }
+    else { rk_a = 1.5; rk_b = -0.5; rk_c = 1.0; }
+    double2* S[4] = {(double2*)h->spec[0], (double2*)h->spec[1], (double2*)h->spec[2], (double2*)h->spec[3]};
+    // M^T = iFFT . C^H . FFT applied to the adjoints of (u', v', w', psi = p' - p)
+    const double* lin[4] = {b.lam[0], b.lam[1], b.lam[2], b.lam[3]};
+    int rc = fft_forward<double>(h, lin, S, 4);
+    if (rc) return rc;
+    ColAdjArgs ca;
+    ca.au = S[0]; ca.av = S[1]; ca.aw = S[2]; ca.apsi = S[3];
+    ca.c = h->cc; ca.g = h->g; ca.rk_c = rk_c; ca.dt = p.dt; ca.nu = p.nu;
+    prof_begin(h, K_COLUMN);
+    rc = launch_column_adj(h, ca);
+    if (rc) return rc;
+    double* lq[3] = {b.lq[0], b.lq[1], b.lq[2]};
+    const int add0[3] = {0, 0, 0};
+    rc = fft_inverse<double>(h, S, lq, add0, 3);
+    if (rc) return rc;
+    // adjoint of the right-hand side: lambda_u, v, w restart from zero, lambda_p
+    // keeps lambda_p' (p' = p + psi) and gains the pressure-gradient terms
+    const size_t fb = (size_t)h->g.n * sizeof(double);
+    for (int f = 0; f < 3; ++f) CK(cudaMemsetAsync(b.lam[f], 0, fb, h->st));
+    AdjRhsArgs m;
+    m.a = make_acc<double>(h);
+    m.a.f.u = st[0]; m.a.f.v = st[1]; m.a.f.w = st[2]; m.a.f.p = st[3];
+    for (int f = 0; f < 3; ++f) { m.lq[f] = b.lq[f]; m.lf_out[f] = b.lh[f]; m.lf_prev[f] = b.lh[f]; m.lbf[f] = b.lbf[f]; }
+    m.out.u = b.lam[0]; m.out.v = b.lam[1]; m.out.w = b.lam[2]; m.out.p = b.lam[3];
+    m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph;
+    prof_begin(h, K_RHS_MOM);
+    k_rhs_momentum_adj<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
+    CKL();
+    return HC_OK;
+}
+
+static int adj_copy_state(hc_handle* h, double* dst, int nf, int to_fields)
+{
+    const size_t fb = (size_t)h->g.n * sizeof(double);
+    for (int f = 0; f < nf; ++f) {
+        double* a = dst + (size_t)f * h->g.n;
+        void* fld = h->fld[ADJ_STATE[f]];
+        if (to_fields) CK(cudaMemcpyAsync(fld, a, fb, cudaMemcpyDeviceToDevice, h->st));
+        else CK(cudaMemcpyAsync(a, fld, fb, cudaMemcpyDeviceToDevice, h->st));
+    }
+    return HC_OK;
+}
+
+// Buffers of the adjoint inside the handle's allocation (layout fixed by
+// hc_adjoint_forward: nseg checkpoints, a tape of one segment's sub-steps).
+static AdjBufs adj_bufs(hc_handle* h)
+{
+    const long long n = h->g.n;
+    AdjBufs b;
+    double* q = h->adj_buf;
+    for (int f = 0; f < 4; ++f) { b.lam[f] = q; q += n; }
+    for (int f = 0; f < 3; ++f) { b.lh[f] = q; q += n; }
+    for (int f = 0; f < 3; ++f) { b.lq[f] = q; q += n; }
+    for (int f = 0; f < 3; ++f) { b.lbf[f] = q; q += n; }
+    b.ckpt = q; q += (size_t)7 * h->adj_nseg * n;
+    b.tape = q; q += (size_t)4 * h->adj_seglen * (h->p.dts == 2 ? 3 : 1) * n;
+    b.fin = q;
+    return b;
+}
+
+// Forward pass with a checkpoint every ckpt steps: the state and scalars at
+// steps 0, ckpt, 2 ckpt, ... and at the end. The steps are plain steps (the
+// handle's statistics and diagnostics advance as in hc_step).
+template <int CDS> static int adjoint_forward(hc_handle* h, AdjBufs& b)
+{
+    const int nsteps = h->adj_nsteps, ckpt = h->adj_ckpt, nseg = h->adj_nseg;
+    const long long n = h->g.n;
+    int rc;
+    h->launches = 0;
+    CK(cudaEventRecord(h->e0, h->st));
+    for (int s = 0; s < nsteps; ++s) {
+        if (s % ckpt == 0) {
+            rc = adj_copy_state(h, b.ckpt + (size_t)(s / ckpt) * 7 * n, 7, 0);
+            if (rc) return rc;
+            CK(cudaMemcpyAsync(h->adj_sc + s / ckpt, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
+        }
+        rc = step_fd<double, CDS>(h);
+        if (rc) return rc;
+    }
+    rc = adj_copy_state(h, b.fin, 7, 0);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->adj_sc + nseg, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaEventRecord(h->e1, h->st));
+    CK(cudaEventSynchronize(h->e1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, h->e0, h->e1));
+    h->adj_ms[0] = ms;
+    h->adj_launches[0] = h->launches;
+    return HC_OK;
+}
+
+// Reverse sweep: per segment, last first, recompute the start state of each of
+// its sub-steps from the checkpoint, then run the sub-step adjoints backwards.
+// Ends with the final state and scalars of the forward pass restored.
+template <int CDS> static int adjoint_reverse(hc_handle* h, AdjBufs& b)
+{
+    const int nsteps = h->adj_nsteps, ckpt = h->adj_ckpt, nseg = h->adj_nseg;
+    const int nsub = h->p.dts == 2 ? 3 : 1;
+    const long long n = h->g.n;
+    int rc;
+    h->launches = 0;
+    CK(cudaEventRecord(h->e0, h->st));
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        rc = adj_copy_state(h, b.ckpt + (size_t)seg * 7 * n, 7, 1);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(h->sc, h->adj_sc + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
+        const int s0 = seg * ckpt, s1 = (s0 + ckpt < nsteps ? s0 + ckpt : nsteps);
+        int t = 0;
+        for (int s = s0; s < s1; ++s)
+            for (int sub = 0; sub < nsub; ++sub, ++t) {
+                rc = adj_copy_state(h, b.tape + (size_t)t * 4 * n, 4, 0);
+                if (rc) return rc;
+                rc = substep_fd<double, CDS>(h, sub);
+                if (rc) return rc;
+            }
+        for (--t; t >= 0; --t) {
+            const double* st[4];
+            for (int f = 0; f < 4; ++f) st[f] = b.tape + ((size_t)t * 4 + f) * n;
+            rc = adj_substep<CDS>(h, t % nsub, st, b);
+            if (rc) return rc;
+        }
+    }
+    rc = adj_copy_state(h, b.fin, 7, 1);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->sc, h->adj_sc + nseg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaEventRecord(h->e1, h->st));
+    CK(cudaEventSynchronize(h->e1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, h->e0, h->e1));
+    h->adj_ms[1] = ms;
+    h->adj_launches[1] = h->launches;
+    return HC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // C-ABI
 // ---------------------------------------------------------------------------
@@ -1345,6 +1535,8 @@ static void free_all(hc_handle* h)
     if (h->dsig) cudaFree(h->dsig);
     if (h->dstale) cudaFree(h->dstale);
     for (int q = 0; q < 3; ++q) if (h->bf[q]) cudaFree(h->bf[q]);
+    if (h->adj_buf) cudaFree(h->adj_buf);
+    if (h->adj_sc) cudaFree(h->adj_sc);
     if (h->dmean) cudaFree(h->dmean);
     for (int q = 0; q < 11; ++q) if (h->mean[q]) cudaFree(h->mean[q]);
     if (h->zbuf) cudaFree(h->zbuf);
@@ -1385,6 +1577,7 @@ int hc_create(const hc_params* p, hc_handle** out)
     for (int q = 0; q < NSP; ++q) h->sp[q] = nullptr;
     h->dsig = nullptr; h->dmean = nullptr; h->dstale = nullptr; h->div_in_rhs = 0;
     h->bf[0] = h->bf[1] = h->bf[2] = nullptr; h->has_bf = 0;
+    h->adj_buf = nullptr; h->adj_bytes = 0; h->adj_sc = nullptr; h->adj_nsc = 0;
     h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0;
     for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
@@ -1514,6 +1707,7 @@ int hc_destroy(hc_handle* h)
 
 int hc_set_grid(hc_handle* h, const double* dz, const double* l_t, const double* l_b, const double* dz_t, const double* dz_b)
 {
+    if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
     if (!h || !dz || !l_t || !l_b || !dz_t || !dz_b) return HC_ERR_ARG;
     if (h->initialized) return HC_ERR_STATE;
     const int nka = h->p.nz + 4;
@@ -1557,6 +1751,7 @@ static void* field_dev(hc_handle* h, int id, int* is_mean)
 
 int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, int ghost)
 {
+    if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
     if (!h || !host || ghost < 0 || ld1 < h->p.nx + 2 * ghost || ld2 < h->p.ny + 2 * ghost) return HC_ERR_ARG;
     if (h->p.cds == 3 && h->initialized) return HC_ERR_STATE;
     int is_mean;
@@ -1637,6 +1832,7 @@ int hc_download(hc_handle* h, int field_id, double* host, int ld1, int ld2, int 
 
 int hc_set_body_force(hc_handle* h, const double* fx, const double* fy, const double* fz)
 {
+    if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
     if (!h) return HC_ERR_ARG;
     graph_drop(h);
     if (!fx && !fy && !fz) { h->has_bf = 0; return HC_OK; }
@@ -1660,6 +1856,7 @@ int hc_set_body_force(hc_handle* h, const double* fx, const double* fy, const do
 
 int hc_upload_dev(hc_handle* h, int field_id, const void* dev)
 {
+    if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
     if (!h || !dev) return HC_ERR_ARG;
     if (h->p.cds == 3 && h->initialized) return HC_ERR_STATE;
     int is_mean;
@@ -1685,6 +1882,7 @@ int hc_download_dev(hc_handle* h, int field_id, void* dev)
 
 int hc_initialize(hc_handle* h)
 {
+    if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
     if (!h) return HC_ERR_ARG;
     const hc_params& p = h->p;
     // update_boundary_uvw sets w = 0 on the top wall before the loop (src/module_navier_stokes.f90:127)
@@ -1717,6 +1915,7 @@ int hc_initialize(hc_handle* h)
 
 int hc_step(hc_handle* h, int nsteps, hc_diag* out)
 {
+    if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
     if (!h || nsteps < 0) return HC_ERR_ARG;
     if (!h->initialized) return HC_ERR_STATE;
     DevScalars s;
@@ -1924,6 +2123,105 @@ int hc_ensemble_destroy(hc_ensemble* e)
     if (!e) return HC_ERR_ARG;
     cudaStreamSynchronize(e->st);
     ensemble_free(e);
+    return HC_OK;
+}
+
+int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
+{
+    if (!h || nsteps < 1 || ckpt < 1) return HC_ERR_ARG;
+    if (!h->initialized) return HC_ERR_STATE;
+    const hc_params& p = h->p;
+    if (h->rsz != sizeof(double) || (p.cds != 1 && p.cds != 2) || (p.dp_opt != 1 && p.dp_opt != 3) ||
+        p.isscalar != 0 || p.isdamp != 0 || p.nz > 256)
+        return HC_ERR_UNSUPPORTED;
+    h->adj_ready = 0;
+    DevScalars s0;
+    CK(cudaMemcpy(&s0, h->sc, sizeof(s0), cudaMemcpyDeviceToHost));
+    if (s0.nan_flag) return HC_ERR_NAN;
+    graph_drop(h);
+    const long long n = h->g.n;
+    const int nsub = p.dts == 2 ? 3 : 1;
+    const int nseg = (nsteps + ckpt - 1) / ckpt;
+    const int seglen = ckpt < nsteps ? ckpt : nsteps;
+    // 13 adjoint fields, 7 per checkpoint, 4 per taped sub-step, 7 for the final state
+    const size_t nfield = 13 + (size_t)7 * nseg + (size_t)4 * seglen * nsub + 7;
+    const size_t bytes = nfield * (size_t)n * sizeof(double);
+    if (bytes > h->adj_bytes) {
+        if (h->adj_buf) cudaFree(h->adj_buf);
+        h->adj_buf = nullptr; h->adj_bytes = 0;
+        if (cudaMalloc((void**)&h->adj_buf, bytes) != cudaSuccess) { cudaGetLastError(); return HC_ERR_NOMEM; }
+        h->adj_bytes = bytes;
+    }
+    if (nseg + 1 > h->adj_nsc) {
+        if (h->adj_sc) cudaFree(h->adj_sc);
+        h->adj_sc = nullptr; h->adj_nsc = 0;
+        if (cudaMalloc((void**)&h->adj_sc, (nseg + 1) * sizeof(DevScalars)) != cudaSuccess) { cudaGetLastError(); return HC_ERR_NOMEM; }
+        h->adj_nsc = nseg + 1;
+    }
+    h->adj_nsteps = nsteps; h->adj_ckpt = ckpt; h->adj_nseg = nseg; h->adj_seglen = seglen;
+    AdjBufs b = adj_bufs(h);
+    const int prof = h->prof;
+    h->prof = 0;
+    int rc = p.cds == 1 ? adjoint_forward<1>(h, b) : adjoint_forward<2>(h, b);
+    h->prof = prof;
+    if (rc) return rc;
+    DevScalars s1;
+    CK(cudaMemcpy(&s1, h->sc, sizeof(s1), cudaMemcpyDeviceToHost));
+    if (s1.nan_flag) return HC_ERR_NAN;
+    h->adj_ready = 1;
+    return HC_OK;
+}
+
+int hc_adjoint_reverse(hc_handle* h, const double* lu, const double* lv, const double* lw, const double* lp,
+                       double* gu, double* gv, double* gw, double* gp, double* gbf)
+{
+    if (!h) return HC_ERR_ARG;
+    if (!h->adj_ready) return HC_ERR_STATE;
+    AdjBufs b = adj_bufs(h);
+    const long long n = h->g.n;
+    const size_t fb = (size_t)n * sizeof(double);
+    const double* seed[4] = {lu, lv, lw, lp};
+    for (int f = 0; f < 4; ++f) {
+        if (seed[f]) CK(cudaMemcpyAsync(b.lam[f], seed[f], fb, cudaMemcpyHostToDevice, h->st));
+        else CK(cudaMemsetAsync(b.lam[f], 0, fb, h->st));
+    }
+    for (int f = 0; f < 3; ++f) {
+        CK(cudaMemsetAsync(b.lh[f], 0, fb, h->st));
+        CK(cudaMemsetAsync(b.lbf[f], 0, fb, h->st));
+    }
+    const int prof = h->prof;
+    h->prof = 0;
+    int rc = h->p.cds == 1 ? adjoint_reverse<1>(h, b) : adjoint_reverse<2>(h, b);
+    h->prof = prof;
+    if (rc) { h->adj_ready = 0; return rc; }
+    double* out[4] = {gu, gv, gw, gp};
+    for (int f = 0; f < 4; ++f)
+        if (out[f]) CK(cudaMemcpyAsync(out[f], b.lam[f], fb, cudaMemcpyDeviceToHost, h->st));
+    if (gbf)
+        for (int f = 0; f < 3; ++f) CK(cudaMemcpyAsync(gbf + (size_t)f * n, b.lbf[f], fb, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    DevScalars s1;
+    CK(cudaMemcpy(&s1, h->sc, sizeof(s1), cudaMemcpyDeviceToHost));
+    if (s1.nan_flag) return HC_ERR_NAN;
+    return HC_OK;
+}
+
+int hc_adjoint(hc_handle* h, int nsteps, int ckpt, const double* lu, const double* lv, const double* lw, const double* lp,
+               double* gu, double* gv, double* gw, double* gp, double* gbf)
+{
+    int rc = hc_adjoint_forward(h, nsteps, ckpt);
+    if (rc) return rc;
+    return hc_adjoint_reverse(h, lu, lv, lw, lp, gu, gv, gw, gp, gbf);
+}
+
+int hc_adjoint_last_ms(hc_handle* h, double* forward_ms, double* reverse_ms, long long* forward_launches,
+                       long long* reverse_launches)
+{
+    if (!h) return HC_ERR_ARG;
+    if (forward_ms) *forward_ms = h->adj_ms[0];
+    if (reverse_ms) *reverse_ms = h->adj_ms[1];
+    if (forward_launches) *forward_launches = h->adj_launches[0];
+    if (reverse_launches) *reverse_launches = h->adj_launches[1];
     return HC_OK;
 }
 

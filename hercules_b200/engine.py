@@ -31,7 +31,8 @@ ABI_SYMBOLS = ["hc_create", "hc_set_grid", "hc_get_grid", "hc_upload", "hc_downl
                "hc_initialize", "hc_step", "hc_get_scalars", "hc_upload_dev", "hc_download_dev",
                "hc_last_step_ms", "hc_last_launch_count", "hc_set_profiling", "hc_kernel_profile",
                "hc_divergence_noalloc", "hc_set_body_force", "hc_set_graph", "hc_ensemble_create",
-               "hc_ensemble_step", "hc_ensemble_last_ms", "hc_ensemble_destroy", "hc_destroy", "hc_error_string"]
+               "hc_ensemble_step", "hc_ensemble_last_ms", "hc_ensemble_destroy", "hc_adjoint_forward",
+               "hc_adjoint_reverse", "hc_adjoint", "hc_adjoint_last_ms", "hc_destroy", "hc_error_string"]
 
 
 class HerculesError(RuntimeError):
@@ -74,6 +75,11 @@ def load_library(path: str = LIB_PATH):
     L.hc_ensemble_step.argtypes = [vp, ip]
     L.hc_ensemble_last_ms.argtypes = [vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_longlong)]
     L.hc_ensemble_destroy.argtypes = [vp]
+    L.hc_adjoint.argtypes = [vp, ip, ip] + [ctypes.c_void_p] * 9
+    L.hc_adjoint_forward.argtypes = [vp, ip, ip]
+    L.hc_adjoint_reverse.argtypes = [vp] + [ctypes.c_void_p] * 9
+    L.hc_adjoint_last_ms.argtypes = [vp, ctypes.POINTER(dp), ctypes.POINTER(dp),
+                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.hc_destroy.argtypes = [vp]
     L.hc_error_string.argtypes = [ip]
     L.hc_error_string.restype = ctypes.c_char_p
@@ -162,6 +168,50 @@ class Channel:
         _check(self._L.hc_set_body_force(self.h, *ptrs), "hc_set_body_force")
 
     # ---- time stepping -------------------------------------------------
+    def adjoint_forward(self, nsteps: int, ckpt: int = 10) -> None:
+        """Advance nsteps (as step() would), keeping a checkpoint every ckpt steps
+        for adjoint_reverse. No counterpart in the reference."""
+        _check(self._L.hc_adjoint_forward(self.h, nsteps, ckpt), "hc_adjoint_forward")
+
+    def adjoint_reverse(self, seeds: Dict[str, np.ndarray], body_force: bool = True) -> Dict[str, np.ndarray]:
+        """Gradient of J = sum over f in seeds of <seeds[f], f_N> (f in u, v, w, p;
+        the fields after the last adjoint_forward) with respect to the fields that
+        pass started from (keys "u", "v", "w", "p") and, with body_force, to the
+        body force ("fx", "fy", "fz")."""
+        shp = self._shape(0)
+        sd = []
+        for f in ("u", "v", "w", "p"):
+            a = seeds.get(f)
+            if a is not None:
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                if a.shape != shp:
+                    raise ValueError(f"seed {f}: shape {a.shape} != {shp}")
+            sd.append(a)
+        g = {f: np.zeros(shp) for f in ("u", "v", "w", "p")}
+        gbf = np.zeros((3,) + shp) if body_force else None
+        ptr = lambda a: None if a is None else ctypes.c_void_p(a.ctypes.data)
+        _check(self._L.hc_adjoint_reverse(self.h, *[ptr(a) for a in sd],
+                                          *[ptr(g[f]) for f in ("u", "v", "w", "p")], ptr(gbf)),
+               "hc_adjoint_reverse")
+        if body_force:
+            g.update(fx=gbf[0], fy=gbf[1], fz=gbf[2])
+        return g
+
+    def adjoint(self, nsteps: int, seeds: Dict[str, np.ndarray], ckpt: int = 10,
+                body_force: bool = True) -> Dict[str, np.ndarray]:
+        """adjoint_forward then adjoint_reverse."""
+        self.adjoint_forward(nsteps, ckpt)
+        return self.adjoint_reverse(seeds, body_force)
+
+    def adjoint_timing(self) -> dict:
+        """Device time (ms) and launches of the last adjoint(): forward pass and reverse sweep."""
+        f, r = ctypes.c_double(), ctypes.c_double()
+        lf, lr = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self._L.hc_adjoint_last_ms(self.h, ctypes.byref(f), ctypes.byref(r), ctypes.byref(lf),
+                                          ctypes.byref(lr)), "hc_adjoint_last_ms")
+        return {"forward_ms": f.value, "reverse_ms": r.value, "forward_launches": lf.value,
+                "reverse_launches": lr.value}
+
     def initialize(self) -> None:
         _check(self._L.hc_initialize(self.h), "hc_initialize")
 

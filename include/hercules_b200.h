@@ -227,6 +227,31 @@ int hc_ensemble_step(hc_ensemble* e, int nsteps);
 int hc_ensemble_last_ms(hc_ensemble* e, double* ms, long long* launches_per_step);
 int hc_ensemble_destroy(hc_ensemble* e);
 
+/* Discrete adjoint of FD steps (no counterpart in the reference), in two calls.
+ * hc_adjoint_forward advances the handle by nsteps like hc_step (same final
+ * fields, scalars and statistics), keeping a checkpoint of the state every ckpt
+ * steps. hc_adjoint_reverse then returns the gradient of
+ * J = <lu,u_N> + <lv,v_N> + <lw,w_N> + <lp,p_N> (the seeds, (nx,ny,nz) host
+ * arrays, NULL = 0) with respect to the state the forward pass started from
+ * (gu, gv, gw, gp) and to the body force (gbf: 3*nx*ny*nz, fx then fy then fz);
+ * any output may be NULL. It recomputes one segment of ckpt steps at a time
+ * from its checkpoint, leaves the handle in the forward pass's final state and
+ * may be called again with other seeds. Any call that changes the state
+ * (hc_step, hc_upload*, hc_initialize, hc_set_grid, hc_set_body_force)
+ * invalidates the checkpoints (HC_ERR_STATE). Built for FP64 storage, cds = 1
+ * or 2, dp_opt = 1 or 3, isscalar = 0, isdamp = 0, nz <= 256; else
+ * HC_ERR_UNSUPPORTED. With AB2 (dts = 1) the gradient with respect to the
+ * starting histories is not returned. hc_adjoint is the two calls in one. */
+int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt);
+int hc_adjoint_reverse(hc_handle* h, const double* lu, const double* lv, const double* lw, const double* lp,
+                       double* gu, double* gv, double* gw, double* gp, double* gbf);
+int hc_adjoint(hc_handle* h, int nsteps, int ckpt, const double* lu, const double* lv, const double* lw,
+               const double* lp, double* gu, double* gv, double* gw, double* gp, double* gbf);
+/* Device time and kernel launches of the last adjoint forward pass and reverse
+ * sweep (recomputation of the segments included). */
+int hc_adjoint_last_ms(hc_handle* h, double* forward_ms, double* reverse_ms, long long* forward_launches,
+                       long long* reverse_launches);
+
 int hc_destroy(hc_handle* h);
 
 const char* hc_error_string(int code);
