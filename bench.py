@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="run one precision only (profiling); the headline needs both")
     ap.add_argument("--graph", action="store_true", help="replay each step from a captured CUDA graph")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing leg")
     return ap.parse_args()
 
 
@@ -297,6 +298,52 @@ def run_gpu(args, ws, rank):
     return results, err, kern, e2e
 
 
+def run_adjoint(nsteps=50, ckpt=10):
+    """The adjoint workload: Ekman layer 64x64x65 FP64, gradient of the mean wall
+    shear stress at step 50 with respect to the starting velocity and a smooth
+    body force, a checkpoint every 10 steps. Device time of the plain forward
+    (hc_step, eager) against the checkpointed forward and the reverse sweep."""
+    import numpy as np
+    import torch
+    from hercules_b200 import adjoint, engine, inputs
+    from hercules_b200.params import config_ekman
+    torch.cuda.set_device(0)
+    p = config_ekman()
+    f0 = inputs.small_random(p, seed=21)
+    fields = {k: f0[k] for k in ("u", "v", "w")}
+    bf = inputs.gaussian_body_force(p, seed=22, ell=1.0, amp=0.01)
+    seeds = {"u": adjoint.wall_shear_seed(p)}
+
+    def fresh():
+        c = engine.Channel(p)
+        c.load(fields)
+        c.set_body_force(*bf)
+        c.initialize()
+        return c
+    c = fresh()
+    c.step_nodiag(nsteps)          # warm-up of the plain path
+    c.close()
+    c = fresh()
+    rc = c.step_nodiag(nsteps)
+    assert rc == 0, rc
+    fwd_ms, fwd_launch = c.last_ms, c.last_launches
+    c.close()
+    c = fresh()
+    c.adjoint(nsteps, seeds, ckpt=ckpt)    # warm-up (allocates the checkpoints)
+    c.close()
+    c = fresh()
+    g = c.adjoint(nsteps, seeds, ckpt=ckpt)
+    t = c.adjoint_timing()
+    c.close()
+    return {"workload": f"ekman {p.nx}x{p.ny}x{p.nz} FP64, mean wall shear at step {nsteps}, ckpt {ckpt}",
+            "forward_ms": fwd_ms, "forward_launches": fwd_launch,
+            "ckpt_forward_ms": t["forward_ms"], "reverse_ms": t["reverse_ms"],
+            "reverse_launches": t["reverse_launches"],
+            "reverse_over_forward": t["reverse_ms"] / fwd_ms,
+            "gradient_over_forward": (t["forward_ms"] + t["reverse_ms"]) / fwd_ms,
+            "grad_norm_u": float(np.sqrt(np.sum(g["u"] ** 2)))}
+
+
 def run_ensemble(args):
     """All members of the seeded ensemble advanced through one graph per step,
     FP64 and mixed; value = total gridpoint-steps / device time."""
@@ -438,6 +485,7 @@ def main():
     roof["step_bytes_per_point"] = {"mixed": step_b[PREC_MIXED], "fp64": step_b[PREC_FP64]}
     roof["step_frac_of_hbm"] = step_b[PREC_MIXED] * mixed["value"] / args.gpus / (hbm * 1e9)
     roof["step_frac_fp64"] = step_b[PREC_FP64] * fp64["value"] / args.gpus / (hbm * 1e9)
+    adj = None if args.no_adjoint or is_spectral(args.workload) else run_adjoint()
     cpu = None
     if not args.no_cpu_baseline and args.gpus == 1:
         rate, el = cpu_oracle_rate(CPU_SAMPLE_GRID, 1)
@@ -450,7 +498,7 @@ def main():
                  "mixed_speedup_vs_fp64": fp64["ms_per_step"] / mixed["ms_per_step"],
                  "err_vs_fp64": err, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                  "gpu_launches": int(mixed["launches"]), "clocks": mixed["clocks"], "clocks_fp64": fp64["clocks"],
-                 "kernels": kern})
+                 "adjoint": adj, "kernels": kern})
     print(json.dumps(line), flush=True)
 
 

@@ -13,127 +13,48 @@
 //   lambda_f  = dt rk_a lambda_q + lambda_f(out);  lambda_f_prev = dt rk_b lambda_q
 //   lambda_u  = lambda_q + c_d L^T lambda_q + (dF/du)^T lambda_f, and alike for v, w
 //   lambda_p  = lambda_p' - rk_c dt G^T lambda_q;     lambda_bodyforce += lambda_f
-// The nonlinear RHS is differentiated point by point in reverse mode: every
-// interpolant and difference of the forward expression passes its adjoint back
-// to the raw values it read, through the same periodic wrap and z ghost
-// relations (the ghost of a wall value folds back onto that value), accumulated
-// with FP64 atomics.
+// The nonlinear RHS is differentiated by transposed stencils in two gather
+// passes, without atomics (so the gradient is bitwise reproducible): first the
+// adjoint of every interpolant (uhx ... vhz) at its own point, gathered from the
+// equations whose differences read it, then the adjoint of every raw value,
+// gathered through the interpolation weights, the identity, the diffusion and
+// pressure-gradient stencils and the z ghost relations (the ghost of a wall
+// value folds back onto that value).
 #pragma once
 #include "hc_fd.cuh"
 #include "hc_column_warp.cuh"
-
-struct AdjFields {
-    double* u; double* v; double* w; double* p;       // adjoint accumulators (scatter targets)
-};
 
 struct AdjRhsArgs {
     Acc<double> a;                 // the forward state at the sub-step's start
     const double* lq[3];           // lambda_q (physical)
     const double* lf_out[3];       // adjoint of the new histories ff, gg, hh
-    double* lf_prev[3];            // out: adjoint of the old histories
+    double* lf_prev[3];            // out: adjoint of the old histories (not lf_out's buffers)
     double* lbf[3];                // body-force gradient, accumulated
-    AdjFields out;                 // lambda_u, v, w, p accumulated
+    double* ax[8];                 // adjoints of the interpolants uhx, uhy, vhx, vhy, whx, why, uhz, vhz
+    double* out[4];                // lambda_u, v, w (written), lambda_p (accumulated)
     double rk_a, rk_b, rk_c;
     Phys ph;
 };
 
-// ---- scatter helpers: adjoint of a raw read (wrap + ghost relation) ----------
-struct AdjScatter {
-    const Geo& g;
-    int closed;
-    AdjFields t;
-    __device__ __forceinline__ long long at(int i, int j, int k) const
-    {
-        return ((long long)k * g.ny + wrapi(j, g.ny)) * g.nx + wrapi(i, g.nx);
-    }
-    // U(k<0) = -U(0) - 2 u_mrf; U(k>=nz) = closed ? -U(nz-1) - 2 u_mrf : U(nz-1)
-    __device__ __forceinline__ void U(int i, int j, int k, double lam) const
-    {
-        if (lam == 0.0) return;
-        if (k < 0) { atomicAdd(t.u + at(i, j, 0), -lam); return; }
-        if (k >= g.nz) { atomicAdd(t.u + at(i, j, g.nz - 1), closed ? -lam : lam); return; }
-        atomicAdd(t.u + at(i, j, k), lam);
-    }
-    __device__ __forceinline__ void V(int i, int j, int k, double lam) const
-    {
-        if (lam == 0.0) return;
-        if (k < 0) { atomicAdd(t.v + at(i, j, 0), -lam); return; }
-        if (k >= g.nz) { atomicAdd(t.v + at(i, j, g.nz - 1), closed ? -lam : lam); return; }
-        atomicAdd(t.v + at(i, j, k), lam);
-    }
-    // W(k<0) = 0; W(k>=nz) = -W(nz-2)
-    __device__ __forceinline__ void W(int i, int j, int k, double lam) const
-    {
-        if (lam == 0.0 || k < 0) return;
-        if (k >= g.nz) { atomicAdd(t.w + at(i, j, g.nz - 2), -lam); return; }
-        atomicAdd(t.w + at(i, j, k), lam);
-    }
-    __device__ __forceinline__ void P(int i, int j, int k, double lam) const
-    {
-        if (lam == 0.0) return;
-        k = k < 0 ? 0 : (k >= g.nz ? g.nz - 1 : k);
-        atomicAdd(t.p + at(i, j, k), lam);
-    }
-    // interpolants (get_interp_fields_uvwhxyz with the ghosts of update_boundary_uvwhxyz)
-    template <int CDS> __device__ __forceinline__ void uhx(int i, int j, int k, double lam) const
-    {
-        if (CDS == 1) { U(i, j, k, 0.5 * lam); U(i - 1, j, k, 0.5 * lam); return; }
-        U(i + 1, j, k, -lam / 16); U(i, j, k, 9 * lam / 16); U(i - 1, j, k, 9 * lam / 16); U(i - 2, j, k, -lam / 16);
-    }
-    template <int CDS> __device__ __forceinline__ void uhy(int i, int j, int k, double lam) const
-    {
-        if (CDS == 1) { U(i, j + 1, k, 0.5 * lam); U(i, j, k, 0.5 * lam); return; }
-        U(i, j + 2, k, -lam / 16); U(i, j + 1, k, 9 * lam / 16); U(i, j, k, 9 * lam / 16); U(i, j - 1, k, -lam / 16);
-    }
-    template <int CDS> __device__ __forceinline__ void vhx(int i, int j, int k, double lam) const
-    {
-        if (CDS == 1) { V(i + 1, j, k, 0.5 * lam); V(i, j, k, 0.5 * lam); return; }
-        V(i + 2, j, k, -lam / 16); V(i + 1, j, k, 9 * lam / 16); V(i, j, k, 9 * lam / 16); V(i - 1, j, k, -lam / 16);
-    }
-    template <int CDS> __device__ __forceinline__ void vhy(int i, int j, int k, double lam) const
-    {
-        if (CDS == 1) { V(i, j, k, 0.5 * lam); V(i, j - 1, k, 0.5 * lam); return; }
-        V(i, j + 1, k, -lam / 16); V(i, j, k, 9 * lam / 16); V(i, j - 1, k, 9 * lam / 16); V(i, j - 2, k, -lam / 16);
-    }
-    template <int CDS> __device__ __forceinline__ void whx(int i, int j, int k, double lam) const
-    {
-        if (k < 0 || k >= g.nz - 1) return;
-        if (CDS == 1) { W(i + 1, j, k, 0.5 * lam); W(i, j, k, 0.5 * lam); return; }
-        W(i + 2, j, k, -lam / 16); W(i + 1, j, k, 9 * lam / 16); W(i, j, k, 9 * lam / 16); W(i - 1, j, k, -lam / 16);
-    }
-    template <int CDS> __device__ __forceinline__ void why(int i, int j, int k, double lam) const
-    {
-        if (k < 0 || k >= g.nz - 1) return;
-        if (CDS == 1) { W(i, j + 1, k, 0.5 * lam); W(i, j, k, 0.5 * lam); return; }
-        W(i, j + 2, k, -lam / 16); W(i, j + 1, k, 9 * lam / 16); W(i, j, k, 9 * lam / 16); W(i, j - 1, k, -lam / 16);
-    }
-    __device__ __forceinline__ void uhz(int i, int j, int k, double lam) const
-    {
-        if (k < 0) return;
-        if (k >= g.nz - 1) { if (!closed) U(i, j, g.nz - 1, lam); return; }
-        const double l = ldz(g.z.l_t, k);
-        U(i, j, k + 1, lam * l); U(i, j, k, lam * (1.0 - l));
-    }
-    __device__ __forceinline__ void vhz(int i, int j, int k, double lam) const
-    {
-        if (k < 0) return;
-        if (k >= g.nz - 1) { if (!closed) V(i, j, g.nz - 1, lam); return; }
-        const double l = ldz(g.z.l_t, k);
-        V(i, j, k + 1, lam * l); V(i, j, k, lam * (1.0 - l));
-    }
-};
-
-// staggered first difference D(f)(i) over the points i+2, i+1, i, i-1 (cds=2) or
-// i+1, i (cds=1) of the *flux position* index: coefficients and offsets
+// staggered first difference of the x/y fluxes: D(h)(i) = sum_q c(q) h(i + off(q)),
+// off = 2, 1, 0, -1 (cds=2, c = -1, 27, -27, 1 over 24) or 1, 0 (cds=1, c = 1, -1)
 template <int CDS> struct Dif {
     static constexpr int n = CDS == 1 ? 2 : 4;
-    __device__ static double c(int q) { return CDS == 1 ? (q == 0 ? 1.0 : -1.0) : (q == 0 ? -1.0 : q == 1 ? 27.0 : q == 2 ? -27.0 : 1.0); }
-    __device__ static double den() { return CDS == 1 ? 1.0 : 24.0; }
+    __device__ static int off(int q) { return CDS == 1 ? 1 - q : 2 - q; }
+    __device__ static double c(int q) { return CDS == 1 ? (q == 0 ? 1.0 : -1.0) : (q == 0 ? -1.0 : q == 1 ? 27.0 : q == 2 ? -27.0 : 1.0) / 24.0; }
 };
 
-// Reverse mode of k_rhs_momentum at one point (i, j, k).
+__device__ __forceinline__ long long adj_at(const Geo& g, int i, int j, int k)
+{
+    return ((long long)k * g.ny + wrapi(j, g.ny)) * g.nx + wrapi(i, g.nx);
+}
+
+// Pass 1, per point: the adjoint of every interpolant evaluated at this point,
+// gathered from the right-hand sides that read it (lambda_f = dt rk_a lambda_q +
+// lambda_f(out) at those points), and this point's history and body-force
+// adjoints. The interpolants are the forward ones (Acc, same wrap and ghosts).
 template <int CDS>
-__global__ void __launch_bounds__(256) k_rhs_momentum_adj(AdjRhsArgs m)
+__global__ void __launch_bounds__(256) k_rhs_adj_interp(AdjRhsArgs m)
 {
     const Acc<double>& A = m.a;
     const Geo& g = A.g;
@@ -142,164 +63,164 @@ __global__ void __launch_bounds__(256) k_rhs_momentum_adj(AdjRhsArgs m)
     const int k = blockIdx.z;
     if (i >= g.nx || j >= g.ny) return;
     const long long id = ((long long)k * g.ny + j) * g.nx + i;
-    const AdjScatter S{g, A.closed, m.out};
-    const double dx = g.dx, dy = g.dy, dx2 = g.dx2, dy2 = g.dy2;
-    const double dt = m.ph.dt, nu = m.ph.nu, um = A.um, fc = m.ph.fc;
-    const double dz = ldz(g.z.dz, k), dzt = ldz(g.z.dz_t, k), dzb = ldz(g.z.dz_b, k);
-    const double cdif = m.rk_c * 0.5 * dt * nu;
-    const double crp = m.rk_c * dt;
-    // offsets of the difference D(.) of the x/y fluxes: flux points i+2, i+1, i, i-1 (cds=2)
-    const int o2[4] = {2, 1, 0, -1}, o1[2] = {1, 0};
-    // ---------------- U ----------------
-    {
-        const double Lq = m.lq[0][id];
-        const double Lf = dt * m.rk_a * Lq + m.lf_out[0][id];
-        m.lf_prev[0][id] = dt * m.rk_b * Lq;
-        m.lbf[0][id] += Lf;
-        // uux = D_x(uhx^2) over uhx at i+2, i+1, i, i-1 (cds=1: i+1, i); f -= uux + um D_x(uhx)
-        for (int q = 0; q < Dif<CDS>::n; ++q) {
-            const int ii = i + (CDS == 1 ? o1[q] : o2[q]);
-            const double h = A.template uhx<CDS>(ii, j, k);
-            const double cq = Dif<CDS>::c(q) / (Dif<CDS>::den() * dx);
-            S.template uhx<CDS>(ii, j, k, -Lf * cq * (2.0 * h + um));
-        }
-        // uvy = D_y(uhy vhx) over j+1, j, j-1, j-2 (cds=1: j, j-1)
-        for (int q = 0; q < Dif<CDS>::n; ++q) {
-            const int jj = j + (CDS == 1 ? o1[q] - 1 : o2[q] - 1);
-            const double cq = Dif<CDS>::c(q) / (Dif<CDS>::den() * dy);
-            const double dB = -Lf * cq;
-            S.template uhy<CDS>(i, jj, k, dB * A.template vhx<CDS>(i, jj, k));
-            S.template vhx<CDS>(i, jj, k, dB * A.template uhy<CDS>(i, jj, k));
-        }
-        // uwz = (uhz whx(k) - uhz whx(k-1)) / dz
-        {
-            const double dC = -Lf / dz;
-            S.uhz(i, j, k, dC * A.template whx<CDS>(i, j, k));
-            S.template whx<CDS>(i, j, k, dC * A.uhz(i, j, k));
-            S.uhz(i, j, k - 1, -dC * A.template whx<CDS>(i, j, k - 1));
-            S.template whx<CDS>(i, j, k - 1, -dC * A.uhz(i, j, k - 1));
-        }
-        if (m.ph.dp_opt == 3) {      // fc (0.5 (vhx(j) + vhx(j-1)) - vg)
-            S.template vhx<CDS>(i, j, k, 0.5 * fc * Lf);
-            S.template vhx<CDS>(i, j - 1, k, 0.5 * fc * Lf);
-        }
-        // qu = u + ... + c_d (uxx + uyy + uzz) - rk_c dt dpdx
-        S.U(i, j, k, Lq);
-        if (CDS == 1) {
-            S.U(i + 1, j, k, cdif * Lq / dx2); S.U(i, j, k, -2.0 * cdif * Lq / dx2); S.U(i - 1, j, k, cdif * Lq / dx2);
-            S.U(i, j + 1, k, cdif * Lq / dy2); S.U(i, j, k, -2.0 * cdif * Lq / dy2); S.U(i, j - 1, k, cdif * Lq / dy2);
-            S.P(i + 1, j, k, -crp * Lq / dx); S.P(i, j, k, crp * Lq / dx);
+    const int nz = g.nz;
+    const double dta = m.ph.dt * m.rk_a, dtb = m.ph.dt * m.rk_b;
+    // lambda_f of component c at a point; zero where the component has no equation
+    auto Lf = [&](int c, int ii, int jj, int kk) -> double {
+        if (kk < 0 || kk >= nz || (c == 2 && kk > nz - 2)) return 0.0;
+        const long long q = adj_at(g, ii, jj, kk);
+        return dta * __ldg(m.lq[c] + q) + __ldg(m.lf_out[c] + q);
+    };
+    for (int c = 0; c < 3; ++c) {
+        if (c < 2 || k <= nz - 2) {
+            m.lf_prev[c][id] = dtb * m.lq[c][id];
+            m.lbf[c][id] += Lf(c, i, j, k);
         } else {
-            const double e[5] = {-1.0, 16.0, -30.0, 16.0, -1.0};
-            for (int q = 0; q < 5; ++q) {
-                S.U(i + 2 - q, j, k, cdif * Lq * e[q] / (12.0 * dx2));
-                S.U(i, j + 2 - q, k, cdif * Lq * e[q] / (12.0 * dy2));
-            }
-            const double c4[4] = {-1.0, 27.0, -27.0, 1.0};
-            for (int q = 0; q < 4; ++q) S.P(i + 2 - q, j, k, -crp * Lq * c4[q] / (24.0 * dx));
+            m.lf_prev[c][id] = m.lf_out[c][id];       // hh of the top-wall level is carried over
         }
-        S.U(i, j, k + 1, cdif * Lq / (dzt * dz));
-        S.U(i, j, k, -cdif * Lq * (1.0 / dzt + 1.0 / dzb) / dz);
-        S.U(i, j, k - 1, cdif * Lq / (dzb * dz));
     }
-    // ---------------- V ----------------
-    {
-        const double Lq = m.lq[1][id];
-        const double Lf = dt * m.rk_a * Lq + m.lf_out[1][id];
-        m.lf_prev[1][id] = dt * m.rk_b * Lq;
-        m.lbf[1][id] += Lf;
-        // vux = D_x(vhx uhy) over i+1, i, i-1, i-2 (cds=1: i, i-1); vx = D_x(vhx) likewise
-        for (int q = 0; q < Dif<CDS>::n; ++q) {
-            const int ii = i + (CDS == 1 ? o1[q] - 1 : o2[q] - 1);
-            const double cq = Dif<CDS>::c(q) / (Dif<CDS>::den() * dx);
-            const double dB = -Lf * cq;
-            S.template vhx<CDS>(ii, j, k, dB * (A.template uhy<CDS>(ii, j, k) + um));
-            S.template uhy<CDS>(ii, j, k, dB * A.template vhx<CDS>(ii, j, k));
-        }
-        // vvy = D_y(vhy^2) over j+2, j+1, j, j-1 (cds=1: j+1, j)
-        for (int q = 0; q < Dif<CDS>::n; ++q) {
-            const int jj = j + (CDS == 1 ? o1[q] : o2[q]);
-            const double h = A.template vhy<CDS>(i, jj, k);
-            const double cq = Dif<CDS>::c(q) / (Dif<CDS>::den() * dy);
-            S.template vhy<CDS>(i, jj, k, -Lf * cq * 2.0 * h);
-        }
-        {
-            const double dC = -Lf / dz;
-            S.vhz(i, j, k, dC * A.template why<CDS>(i, j, k));
-            S.template why<CDS>(i, j, k, dC * A.vhz(i, j, k));
-            S.vhz(i, j, k - 1, -dC * A.template why<CDS>(i, j, k - 1));
-            S.template why<CDS>(i, j, k - 1, -dC * A.vhz(i, j, k - 1));
-        }
-        if (m.ph.dp_opt == 3) {      // fc (ug - 0.5 (uhy(i) + uhy(i-1)) - um)
-            S.template uhy<CDS>(i, j, k, -0.5 * fc * Lf);
-            S.template uhy<CDS>(i - 1, j, k, -0.5 * fc * Lf);
-        }
-        S.V(i, j, k, Lq);
-        if (CDS == 1) {
-            S.V(i + 1, j, k, cdif * Lq / dx2); S.V(i, j, k, -2.0 * cdif * Lq / dx2); S.V(i - 1, j, k, cdif * Lq / dx2);
-            S.V(i, j + 1, k, cdif * Lq / dy2); S.V(i, j, k, -2.0 * cdif * Lq / dy2); S.V(i, j - 1, k, cdif * Lq / dy2);
-            S.P(i, j + 1, k, -crp * Lq / dy); S.P(i, j, k, crp * Lq / dy);
-        } else {
-            const double e[5] = {-1.0, 16.0, -30.0, 16.0, -1.0};
-            for (int q = 0; q < 5; ++q) {
-                S.V(i + 2 - q, j, k, cdif * Lq * e[q] / (12.0 * dx2));
-                S.V(i, j + 2 - q, k, cdif * Lq * e[q] / (12.0 * dy2));
-            }
-            const double c4[4] = {-1.0, 27.0, -27.0, 1.0};
-            for (int q = 0; q < 4; ++q) S.P(i, j + 2 - q, k, -crp * Lq * c4[q] / (24.0 * dy));
-        }
-        S.V(i, j, k + 1, cdif * Lq / (dzt * dz));
-        S.V(i, j, k, -cdif * Lq * (1.0 / dzt + 1.0 / dzb) / dz);
-        S.V(i, j, k - 1, cdif * Lq / (dzb * dz));
+    double sxu = 0, syu = 0, sxv = 0, syv = 0, sxw = 0, syw = 0;
+#pragma unroll
+    for (int q = 0; q < Dif<CDS>::n; ++q) {
+        const int o = Dif<CDS>::off(q);
+        const double cx = Dif<CDS>::c(q) / g.dx, cy = Dif<CDS>::c(q) / g.dy;
+        sxu += cx * Lf(0, i - o, j, k);          // uux: uhx(i) in the U equations at i - off
+        syu += cy * Lf(0, i, j - o + 1, k);      // uvy: uhy vhx(j) at j - off + 1
+        sxv += cx * Lf(1, i - o + 1, j, k);      // vux: vhx uhy(i) at i - off + 1
+        syv += cy * Lf(1, i, j - o, k);          // vvy: vhy(j) at j - off
+        sxw += cx * Lf(2, i - o + 1, j, k);      // wux: whx uhz(i)
+        syw += cy * Lf(2, i, j - o + 1, k);      // wvy: why vhz(j)
     }
-    // ---------------- W (k <= nz-2; the top-wall level passes its history through) ----------------
-    if (k <= g.nz - 2) {
-        const double Lq = m.lq[2][id];
-        const double Lf = dt * m.rk_a * Lq + m.lf_out[2][id];
-        m.lf_prev[2][id] = dt * m.rk_b * Lq;
-        m.lbf[2][id] += Lf;
-        // wux = D_x(whx uhz) over i+1, i, i-1, i-2 (cds=1: i, i-1); wx = D_x(whx)
-        for (int q = 0; q < Dif<CDS>::n; ++q) {
-            const int ii = i + (CDS == 1 ? o1[q] - 1 : o2[q] - 1);
-            const double cq = Dif<CDS>::c(q) / (Dif<CDS>::den() * dx);
-            const double dB = -Lf * cq;
-            S.template whx<CDS>(ii, j, k, dB * (A.uhz(ii, j, k) + um));
-            S.uhz(ii, j, k, dB * A.template whx<CDS>(ii, j, k));
-        }
-        // wvy = D_y(why vhz) over j+1, j, j-1, j-2 (cds=1: j, j-1)
-        for (int q = 0; q < Dif<CDS>::n; ++q) {
-            const int jj = j + (CDS == 1 ? o1[q] - 1 : o2[q] - 1);
-            const double cq = Dif<CDS>::c(q) / (Dif<CDS>::den() * dy);
-            const double dB = -Lf * cq;
-            S.template why<CDS>(i, jj, k, dB * A.vhz(i, jj, k));
-            S.vhz(i, jj, k, dB * A.template why<CDS>(i, jj, k));
-        }
-        // wwz = ((0.5 (w + w(k+1)))^2 - (0.5 (w + w(k-1)))^2) / dz_t
-        {
-            const double wc = A.W(i, j, k), wp = A.W(i, j, k + 1), wm = A.W(i, j, k - 1);
-            const double d1 = -Lf / dzt * 0.5 * (wc + wp), d2 = Lf / dzt * 0.5 * (wc + wm);
-            S.W(i, j, k, d1 + d2); S.W(i, j, k + 1, d1); S.W(i, j, k - 1, d2);
-        }
-        S.W(i, j, k, Lq);
-        if (CDS == 1) {
-            S.W(i + 1, j, k, cdif * Lq / dx2); S.W(i, j, k, -2.0 * cdif * Lq / dx2); S.W(i - 1, j, k, cdif * Lq / dx2);
-            S.W(i, j + 1, k, cdif * Lq / dy2); S.W(i, j, k, -2.0 * cdif * Lq / dy2); S.W(i, j - 1, k, cdif * Lq / dy2);
-        } else {
-            const double e[5] = {-1.0, 16.0, -30.0, 16.0, -1.0};
-            for (int q = 0; q < 5; ++q) {
-                S.W(i + 2 - q, j, k, cdif * Lq * e[q] / (12.0 * dx2));
-                S.W(i, j + 2 - q, k, cdif * Lq * e[q] / (12.0 * dy2));
-            }
-        }
-        const double dzp = ldz(g.z.dz, k + 1);
-        S.W(i, j, k + 1, cdif * Lq / (dzp * dzt));
-        S.W(i, j, k, -cdif * Lq * (1.0 / dzp + 1.0 / dz) / dzt);
-        S.W(i, j, k - 1, cdif * Lq / (dz * dzt));
-        S.P(i, j, k + 1, -crp * Lq / dzt);
-        S.P(i, j, k, crp * Lq / dzt);
+    const double um = A.um, fc = m.ph.fc;
+    const bool cor = m.ph.dp_opt == 3;
+    const double uhx = A.template uhx<CDS>(i, j, k), uhy = A.template uhy<CDS>(i, j, k);
+    const double vhx = A.template vhx<CDS>(i, j, k), vhy = A.template vhy<CDS>(i, j, k);
+    m.ax[0][id] = -(2.0 * uhx + um) * sxu;
+    m.ax[1][id] = -vhx * (syu + sxv) - (cor ? 0.5 * fc * (Lf(1, i, j, k) + Lf(1, i + 1, j, k)) : 0.0);
+    m.ax[2][id] = -uhy * syu - (uhy + um) * sxv + (cor ? 0.5 * fc * (Lf(0, i, j, k) + Lf(0, i, j + 1, k)) : 0.0);
+    m.ax[3][id] = -2.0 * vhy * syv;
+    if (k <= nz - 2) {
+        // uwz, vwz: the face k between levels k and k+1 enters both with 1/dz
+        const double zu = -Lf(0, i, j, k) / ldz(g.z.dz, k) + Lf(0, i, j, k + 1) / ldz(g.z.dz, k + 1);
+        const double zv = -Lf(1, i, j, k) / ldz(g.z.dz, k) + Lf(1, i, j, k + 1) / ldz(g.z.dz, k + 1);
+        const double uhz = A.uhz(i, j, k), vhz = A.vhz(i, j, k);
+        const double whx = A.template whx<CDS>(i, j, k), why = A.template why<CDS>(i, j, k);
+        m.ax[4][id] = uhz * zu - (uhz + um) * sxw;
+        m.ax[5][id] = vhz * zv - vhz * syw;
+        m.ax[6][id] = whx * zu - whx * sxw;
+        m.ax[7][id] = why * zv - why * syw;
     } else {
-        m.lf_prev[2][id] = m.lf_out[2][id];
+        m.ax[4][id] = 0.0; m.ax[5][id] = 0.0; m.ax[6][id] = 0.0; m.ax[7][id] = 0.0;
     }
+}
+
+// Pass 2, per point: lambda_u, v, w, p by the transposed stencils -- the
+// interpolant adjoints through the transposed interpolation weights, lambda_q
+// through the identity, the transposed diffusion (horizontal stencils are
+// symmetric; the wall ghosts of the z second difference fold back onto the
+// first and last levels) and the transposed pressure gradient, plus the w^2
+// flux of the w equation. lambda_p keeps its incoming value (p' = p + psi).
+template <int CDS>
+__global__ void __launch_bounds__(256) k_rhs_adj_gather(AdjRhsArgs m)
+{
+    const Acc<double>& A = m.a;
+    const Geo& g = A.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const long long id = ((long long)k * g.ny + j) * g.nx + i;
+    const int nz = g.nz;
+    const double dt = m.ph.dt, cdif = m.rk_c * 0.5 * dt * m.ph.nu, crp = m.rk_c * dt, dta = dt * m.rk_a;
+    auto X = [&](int f, int ii, int jj, int kk) -> double { return __ldg(m.ax[f] + adj_at(g, ii, jj, kk)); };
+    auto LQ = [&](int c, int ii, int jj, int kk) -> double {
+        if (kk < 0 || kk >= nz || (c == 2 && kk > nz - 2)) return 0.0;
+        return __ldg(m.lq[c] + adj_at(g, ii, jj, kk));
+    };
+    auto dz = [&](int kk) { return ldz(g.z.dz, kk); };
+    auto dzt = [&](int kk) { return ldz(g.z.dz_t, kk); };
+    auto dzb = [&](int kk) { return ldz(g.z.dz_b, kk); };
+    double lu, lv, lw, lp;
+    // ---- transposed interpolation weights
+    if (CDS == 1) {
+        lu = 0.5 * (X(0, i, j, k) + X(0, i + 1, j, k)) + 0.5 * (X(1, i, j - 1, k) + X(1, i, j, k));
+        lv = 0.5 * (X(2, i - 1, j, k) + X(2, i, j, k)) + 0.5 * (X(3, i, j, k) + X(3, i, j + 1, k));
+        lw = 0.5 * (X(4, i - 1, j, k) + X(4, i, j, k)) + 0.5 * (X(5, i, j - 1, k) + X(5, i, j, k));
+    } else {
+        lu = (-X(0, i - 1, j, k) + 9.0 * X(0, i, j, k) + 9.0 * X(0, i + 1, j, k) - X(0, i + 2, j, k)) * 0.0625 +
+             (-X(1, i, j - 2, k) + 9.0 * X(1, i, j - 1, k) + 9.0 * X(1, i, j, k) - X(1, i, j + 1, k)) * 0.0625;
+        lv = (-X(2, i - 2, j, k) + 9.0 * X(2, i - 1, j, k) + 9.0 * X(2, i, j, k) - X(2, i + 1, j, k)) * 0.0625 +
+             (-X(3, i, j - 1, k) + 9.0 * X(3, i, j, k) + 9.0 * X(3, i, j + 1, k) - X(3, i, j + 2, k)) * 0.0625;
+        lw = (-X(4, i - 2, j, k) + 9.0 * X(4, i - 1, j, k) + 9.0 * X(4, i, j, k) - X(4, i + 1, j, k)) * 0.0625 +
+             (-X(5, i, j - 2, k) + 9.0 * X(5, i, j - 1, k) + 9.0 * X(5, i, j, k) - X(5, i, j + 1, k)) * 0.0625;
+    }
+    if (k >= 1) {
+        const double l = ldz(g.z.l_t, k - 1);
+        lu += X(6, i, j, k - 1) * l;
+        lv += X(7, i, j, k - 1) * l;
+    }
+    if (k <= nz - 2) {
+        const double l = ldz(g.z.l_t, k);
+        lu += X(6, i, j, k) * (1.0 - l);
+        lv += X(7, i, j, k) * (1.0 - l);
+    }
+    // ---- identity, diffusion (transposed), pressure gradient (transposed)
+    double hq[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const double q0 = LQ(c, i, j, k);
+        double h;
+        if (CDS == 1) {
+            h = (LQ(c, i + 1, j, k) - 2.0 * q0 + LQ(c, i - 1, j, k)) / g.dx2 +
+                (LQ(c, i, j + 1, k) - 2.0 * q0 + LQ(c, i, j - 1, k)) / g.dy2;
+        } else {
+            h = (-LQ(c, i + 2, j, k) + 16.0 * LQ(c, i + 1, j, k) - 30.0 * q0 + 16.0 * LQ(c, i - 1, j, k) - LQ(c, i - 2, j, k)) / (12.0 * g.dx2) +
+                (-LQ(c, i, j + 2, k) + 16.0 * LQ(c, i, j + 1, k) - 30.0 * q0 + 16.0 * LQ(c, i, j - 1, k) - LQ(c, i, j - 2, k)) / (12.0 * g.dy2);
+        }
+        hq[c] = q0 + cdif * h;
+    }
+    const bool closed = A.closed;
+    {   // u, v: second difference over cell centres with the no-slip / free-slip ghosts
+        const double qu = LQ(0, i, j, k), qv = LQ(1, i, j, k);
+        double zu = -qu * (1.0 / dzt(k) + 1.0 / dzb(k)) / dz(k), zv = -qv * (1.0 / dzt(k) + 1.0 / dzb(k)) / dz(k);
+        if (k >= 1) { const double e = 1.0 / (dzt(k - 1) * dz(k - 1)); zu += LQ(0, i, j, k - 1) * e; zv += LQ(1, i, j, k - 1) * e; }
+        if (k <= nz - 2) { const double e = 1.0 / (dzb(k + 1) * dz(k + 1)); zu += LQ(0, i, j, k + 1) * e; zv += LQ(1, i, j, k + 1) * e; }
+        if (k == 0) { const double e = 1.0 / (dzb(0) * dz(0)); zu -= qu * e; zv -= qv * e; }
+        if (k == nz - 1) { const double e = (closed ? -1.0 : 1.0) / (dzt(k) * dz(k)); zu += qu * e; zv += qv * e; }
+        lu += hq[0] + cdif * zu;
+        lv += hq[1] + cdif * zv;
+    }
+    {   // w: second difference over faces (w = 0 below the first face), rows k <= nz-2
+        const double qw = LQ(2, i, j, k);
+        double zw = -qw * (1.0 / dz(k + 1) + 1.0 / dz(k)) / dzt(k);
+        if (k >= 1) zw += LQ(2, i, j, k - 1) / (dz(k) * dzt(k - 1));
+        zw += LQ(2, i, j, k + 1) / (dz(k + 1) * dzt(k + 1));
+        lw += hq[2] + cdif * zw;
+        // w^2 flux: ((w(k) + w(k+1)) / 2)^2 - ((w(k) + w(k-1)) / 2)^2 over dz_t at rows k' = k-1, k, k+1
+        auto Lfw = [&](int kk) -> double {
+            if (kk < 0 || kk > nz - 2) return 0.0;
+            const long long q = ((long long)kk * g.ny + j) * g.nx + i;
+            return dta * __ldg(m.lq[2] + q) + __ldg(m.lf_out[2] + q);
+        };
+        const double wm = A.W(i, j, k - 1), wc = A.W(i, j, k), wp = A.W(i, j, k + 1);
+        const double l0 = Lfw(k), lm = Lfw(k - 1), lp1 = Lfw(k + 1);
+        if (l0 != 0.0) lw += l0 / dzt(k) * (-0.5 * (wc + wp) + 0.5 * (wc + wm));
+        if (lm != 0.0) lw -= lm / dzt(k - 1) * 0.5 * (wm + wc);
+        if (lp1 != 0.0) lw += lp1 / dzt(k + 1) * 0.5 * (wp + wc);
+    }
+    // pressure gradients of the three equations
+    if (CDS == 1) {
+        lp = -crp / g.dx * (LQ(0, i - 1, j, k) - LQ(0, i, j, k)) - crp / g.dy * (LQ(1, i, j - 1, k) - LQ(1, i, j, k));
+    } else {
+        lp = -crp / (24.0 * g.dx) * (-LQ(0, i - 2, j, k) + 27.0 * LQ(0, i - 1, j, k) - 27.0 * LQ(0, i, j, k) + LQ(0, i + 1, j, k)) -
+             crp / (24.0 * g.dy) * (-LQ(1, i, j - 2, k) + 27.0 * LQ(1, i, j - 1, k) - 27.0 * LQ(1, i, j, k) + LQ(1, i, j + 1, k));
+    }
+    if (k >= 1) lp -= crp * LQ(2, i, j, k - 1) / dzt(k - 1);
+    lp += crp * LQ(2, i, j, k) / dzt(k);
+    m.out[0][id] = lu;
+    m.out[1][id] = lv;
+    m.out[2][id] = lw;
+    m.out[3][id] += lp;
 }
 
 // ---------------------------------------------------------------------------

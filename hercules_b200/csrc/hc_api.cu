@@ -1300,6 +1300,8 @@ template <typename R> static int step_dispatch(hc_handle* h)
 struct AdjBufs {
     double* lam[4];      // adjoint of u, v, w, p at the current point of the sweep
     double* lh[3];       // adjoint of the histories ff, gg, hh
+    double* lh2[3];      // the other half of the ping-pong pair for lh
+    double* ax[8];       // adjoints of the eight interpolants of the current sub-step
     double* lq[3];       // lambda_q of the current sub-step (physical)
     double* lbf[3];      // body-force gradient
     double* ckpt;        // checkpoint c: 7 fields (u, v, w, p, ff, gg, hh) at ckpt + 7 c n
@@ -1354,19 +1356,23 @@ template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* c
     const int add0[3] = {0, 0, 0};
     rc = fft_inverse<double>(h, S, lq, add0, 3);
     if (rc) return rc;
-    // adjoint of the right-hand side: lambda_u, v, w restart from zero, lambda_p
-    // keeps lambda_p' (p' = p + psi) and gains the pressure-gradient terms
-    const size_t fb = (size_t)h->g.n * sizeof(double);
-    for (int f = 0; f < 3; ++f) CK(cudaMemsetAsync(b.lam[f], 0, fb, h->st));
+    // adjoint of the right-hand side: lambda_u, v, w are rewritten, lambda_p
+    // keeps lambda_p' (p' = p + psi) and gains the pressure-gradient terms; the
+    // history adjoints move to the other buffer of their pair
     AdjRhsArgs m;
     m.a = make_acc<double>(h);
     m.a.f.u = st[0]; m.a.f.v = st[1]; m.a.f.w = st[2]; m.a.f.p = st[3];
-    for (int f = 0; f < 3; ++f) { m.lq[f] = b.lq[f]; m.lf_out[f] = b.lh[f]; m.lf_prev[f] = b.lh[f]; m.lbf[f] = b.lbf[f]; }
-    m.out.u = b.lam[0]; m.out.v = b.lam[1]; m.out.w = b.lam[2]; m.out.p = b.lam[3];
+    for (int f = 0; f < 3; ++f) { m.lq[f] = b.lq[f]; m.lf_out[f] = b.lh[f]; m.lf_prev[f] = b.lh2[f]; m.lbf[f] = b.lbf[f]; }
+    for (int f = 0; f < 8; ++f) m.ax[f] = b.ax[f];
+    for (int f = 0; f < 4; ++f) m.out[f] = b.lam[f];
     m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph;
     prof_begin(h, K_RHS_MOM);
-    k_rhs_momentum_adj<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
+    k_rhs_adj_interp<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
     CKL();
+    prof_begin(h, K_RHS_MOM);
+    k_rhs_adj_gather<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
+    CKL();
+    for (int f = 0; f < 3; ++f) { double* t = b.lh[f]; b.lh[f] = b.lh2[f]; b.lh2[f] = t; }
     return HC_OK;
 }
 
@@ -1391,6 +1397,8 @@ static AdjBufs adj_bufs(hc_handle* h)
     double* q = h->adj_buf;
     for (int f = 0; f < 4; ++f) { b.lam[f] = q; q += n; }
     for (int f = 0; f < 3; ++f) { b.lh[f] = q; q += n; }
+    for (int f = 0; f < 3; ++f) { b.lh2[f] = q; q += n; }
+    for (int f = 0; f < 8; ++f) { b.ax[f] = q; q += n; }
     for (int f = 0; f < 3; ++f) { b.lq[f] = q; q += n; }
     for (int f = 0; f < 3; ++f) { b.lbf[f] = q; q += n; }
     b.ckpt = q; q += (size_t)7 * h->adj_nseg * n;
@@ -2143,8 +2151,8 @@ int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
     const int nsub = p.dts == 2 ? 3 : 1;
     const int nseg = (nsteps + ckpt - 1) / ckpt;
     const int seglen = ckpt < nsteps ? ckpt : nsteps;
-    // 13 adjoint fields, 7 per checkpoint, 4 per taped sub-step, 7 for the final state
-    const size_t nfield = 13 + (size_t)7 * nseg + (size_t)4 * seglen * nsub + 7;
+    // 24 adjoint fields, 7 per checkpoint, 4 per taped sub-step, 7 for the final state
+    const size_t nfield = 24 + (size_t)7 * nseg + (size_t)4 * seglen * nsub + 7;
     const size_t bytes = nfield * (size_t)n * sizeof(double);
     if (bytes > h->adj_bytes) {
         if (h->adj_buf) cudaFree(h->adj_buf);

@@ -112,7 +112,7 @@ def test_adjoint_leaves_the_forward_state_and_repeats(engine):
         assert np.array_equal(c.download(f), ref[f]), f
     g2 = c.adjoint_reverse(seeds)
     for k in g1:
-        assert np.allclose(g1[k], g2[k], rtol=1e-12, atol=1e-15), k
+        assert np.array_equal(g1[k], g2[k]), k
     assert c.scalars()["step"] == 7
     t = c.adjoint_timing()
     assert t["forward_ms"] > 0 and t["reverse_ms"] > 0 and t["reverse_launches"] > 0
