@@ -49,32 +49,45 @@ __device__ __forceinline__ long long adj_at(const Geo& g, int i, int j, int k)
     return ((long long)k * g.ny + wrapi(j, g.ny)) * g.nx + wrapi(i, g.nx);
 }
 
+// Wrapped neighbour offsets of one point: i-2..i+2 and rows j-2..j+2 of level k.
+struct Nbr {
+    long long kz;
+    int xi[5];
+    int yj[5];
+    __device__ __forceinline__ Nbr(const Geo& g, int i, int j, int k)
+    {
+        kz = (long long)k * g.nxy;
+#pragma unroll
+        for (int d = -2; d <= 2; ++d) {
+            xi[d + 2] = wrapi(i + d, g.nx);
+            yj[d + 2] = wrapi(j + d, g.ny) * g.nx;
+        }
+    }
+    __device__ __forceinline__ long long at(int di, int dj) const { return kz + yj[dj + 2] + xi[di + 2]; }
+};
+
 // Pass 1, per point: the adjoint of every interpolant evaluated at this point,
 // gathered from the right-hand sides that read it (lambda_f = dt rk_a lambda_q +
 // lambda_f(out) at those points), and this point's history and body-force
-// adjoints. The interpolants are the forward ones (Acc, same wrap and ghosts).
+// adjoints. The interpolants are the forward ones (same weights and wall rules).
 template <int CDS>
 __global__ void __launch_bounds__(256) k_rhs_adj_interp(AdjRhsArgs m)
 {
-    const Acc<double>& A = m.a;
-    const Geo& g = A.g;
+    const Geo& g = m.a.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (i >= g.nx || j >= g.ny) return;
-    const long long id = ((long long)k * g.ny + j) * g.nx + i;
     const int nz = g.nz;
+    const Nbr N(g, i, j, k);
+    const long long id = N.at(0, 0), up = g.nxy;
+    const bool wrow = k <= nz - 2;           // this level carries a w equation
     const double dta = m.ph.dt * m.rk_a, dtb = m.ph.dt * m.rk_b;
-    // lambda_f of component c at a point; zero where the component has no equation
-    auto Lf = [&](int c, int ii, int jj, int kk) -> double {
-        if (kk < 0 || kk >= nz || (c == 2 && kk > nz - 2)) return 0.0;
-        const long long q = adj_at(g, ii, jj, kk);
-        return dta * __ldg(m.lq[c] + q) + __ldg(m.lf_out[c] + q);
-    };
+    auto L = [&](int c, long long q) { return dta * __ldg(m.lq[c] + q) + __ldg(m.lf_out[c] + q); };
     for (int c = 0; c < 3; ++c) {
-        if (c < 2 || k <= nz - 2) {
+        if (c < 2 || wrow) {
             m.lf_prev[c][id] = dtb * m.lq[c][id];
-            m.lbf[c][id] += Lf(c, i, j, k);
+            m.lbf[c][id] += L(c, id);
         } else {
             m.lf_prev[c][id] = m.lf_out[c][id];       // hh of the top-wall level is carried over
         }
@@ -84,27 +97,53 @@ __global__ void __launch_bounds__(256) k_rhs_adj_interp(AdjRhsArgs m)
     for (int q = 0; q < Dif<CDS>::n; ++q) {
         const int o = Dif<CDS>::off(q);
         const double cx = Dif<CDS>::c(q) / g.dx, cy = Dif<CDS>::c(q) / g.dy;
-        sxu += cx * Lf(0, i - o, j, k);          // uux: uhx(i) in the U equations at i - off
-        syu += cy * Lf(0, i, j - o + 1, k);      // uvy: uhy vhx(j) at j - off + 1
-        sxv += cx * Lf(1, i - o + 1, j, k);      // vux: vhx uhy(i) at i - off + 1
-        syv += cy * Lf(1, i, j - o, k);          // vvy: vhy(j) at j - off
-        sxw += cx * Lf(2, i - o + 1, j, k);      // wux: whx uhz(i)
-        syw += cy * Lf(2, i, j - o + 1, k);      // wvy: why vhz(j)
+        sxu += cx * L(0, N.at(-o, 0));          // uux: uhx(i) in the U equations at i - off
+        syu += cy * L(0, N.at(0, 1 - o));       // uvy: uhy vhx(j) at j - off + 1
+        sxv += cx * L(1, N.at(1 - o, 0));       // vux: vhx uhy(i) at i - off + 1
+        syv += cy * L(1, N.at(0, -o));          // vvy: vhy(j) at j - off
+        if (wrow) {
+            sxw += cx * L(2, N.at(1 - o, 0));   // wux: whx uhz(i)
+            syw += cy * L(2, N.at(0, 1 - o));   // wvy: why vhz(j)
+        }
     }
-    const double um = A.um, fc = m.ph.fc;
+    const double* U = m.a.f.u;
+    const double* V = m.a.f.v;
+    const double* W = m.a.f.w;
+    auto ld = [&](const double* f, int di, int dj) { return __ldg(f + N.at(di, dj)); };
+    double uhx, uhy, vhx, vhy;
+    if (CDS == 1) {
+        uhx = 0.5 * (ld(U, 0, 0) + ld(U, -1, 0));
+        uhy = 0.5 * (ld(U, 0, 1) + ld(U, 0, 0));
+        vhx = 0.5 * (ld(V, 1, 0) + ld(V, 0, 0));
+        vhy = 0.5 * (ld(V, 0, 0) + ld(V, 0, -1));
+    } else {
+        uhx = (-ld(U, 1, 0) + 9.0 * ld(U, 0, 0) + 9.0 * ld(U, -1, 0) - ld(U, -2, 0)) * 0.0625;
+        uhy = (-ld(U, 0, 2) + 9.0 * ld(U, 0, 1) + 9.0 * ld(U, 0, 0) - ld(U, 0, -1)) * 0.0625;
+        vhx = (-ld(V, 2, 0) + 9.0 * ld(V, 1, 0) + 9.0 * ld(V, 0, 0) - ld(V, -1, 0)) * 0.0625;
+        vhy = (-ld(V, 0, 1) + 9.0 * ld(V, 0, 0) + 9.0 * ld(V, 0, -1) - ld(V, 0, -2)) * 0.0625;
+    }
+    const double um = m.a.um, fc = m.ph.fc;
     const bool cor = m.ph.dp_opt == 3;
-    const double uhx = A.template uhx<CDS>(i, j, k), uhy = A.template uhy<CDS>(i, j, k);
-    const double vhx = A.template vhx<CDS>(i, j, k), vhy = A.template vhy<CDS>(i, j, k);
     m.ax[0][id] = -(2.0 * uhx + um) * sxu;
-    m.ax[1][id] = -vhx * (syu + sxv) - (cor ? 0.5 * fc * (Lf(1, i, j, k) + Lf(1, i + 1, j, k)) : 0.0);
-    m.ax[2][id] = -uhy * syu - (uhy + um) * sxv + (cor ? 0.5 * fc * (Lf(0, i, j, k) + Lf(0, i, j + 1, k)) : 0.0);
+    m.ax[1][id] = -vhx * (syu + sxv) - (cor ? 0.5 * fc * (L(1, id) + L(1, N.at(1, 0))) : 0.0);
+    m.ax[2][id] = -uhy * syu - (uhy + um) * sxv + (cor ? 0.5 * fc * (L(0, id) + L(0, N.at(0, 1))) : 0.0);
     m.ax[3][id] = -2.0 * vhy * syv;
-    if (k <= nz - 2) {
+    if (wrow) {
         // uwz, vwz: the face k between levels k and k+1 enters both with 1/dz
-        const double zu = -Lf(0, i, j, k) / ldz(g.z.dz, k) + Lf(0, i, j, k + 1) / ldz(g.z.dz, k + 1);
-        const double zv = -Lf(1, i, j, k) / ldz(g.z.dz, k) + Lf(1, i, j, k + 1) / ldz(g.z.dz, k + 1);
-        const double uhz = A.uhz(i, j, k), vhz = A.vhz(i, j, k);
-        const double whx = A.template whx<CDS>(i, j, k), why = A.template why<CDS>(i, j, k);
+        const double rz0 = 1.0 / ldz(g.z.dz, k), rz1 = 1.0 / ldz(g.z.dz, k + 1);
+        const double zu = -L(0, id) * rz0 + L(0, id + up) * rz1;
+        const double zv = -L(1, id) * rz0 + L(1, id + up) * rz1;
+        const double l = ldz(g.z.l_t, k);
+        const double uhz = __ldg(U + id + up) * l + __ldg(U + id) * (1.0 - l);
+        const double vhz = __ldg(V + id + up) * l + __ldg(V + id) * (1.0 - l);
+        double whx, why;
+        if (CDS == 1) {
+            whx = 0.5 * (ld(W, 1, 0) + ld(W, 0, 0));
+            why = 0.5 * (ld(W, 0, 1) + ld(W, 0, 0));
+        } else {
+            whx = (-ld(W, 2, 0) + 9.0 * ld(W, 1, 0) + 9.0 * ld(W, 0, 0) - ld(W, -1, 0)) * 0.0625;
+            why = (-ld(W, 0, 2) + 9.0 * ld(W, 0, 1) + 9.0 * ld(W, 0, 0) - ld(W, 0, -1)) * 0.0625;
+        }
         m.ax[4][id] = uhz * zu - (uhz + um) * sxw;
         m.ax[5][id] = vhz * zv - vhz * syw;
         m.ax[6][id] = whx * zu - whx * sxw;
@@ -123,100 +162,105 @@ __global__ void __launch_bounds__(256) k_rhs_adj_interp(AdjRhsArgs m)
 template <int CDS>
 __global__ void __launch_bounds__(256) k_rhs_adj_gather(AdjRhsArgs m)
 {
-    const Acc<double>& A = m.a;
-    const Geo& g = A.g;
+    const Geo& g = m.a.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (i >= g.nx || j >= g.ny) return;
-    const long long id = ((long long)k * g.ny + j) * g.nx + i;
     const int nz = g.nz;
+    const Nbr N(g, i, j, k);
+    const long long id = N.at(0, 0), up = g.nxy;
+    const bool wrow = k <= nz - 2;
     const double dt = m.ph.dt, cdif = m.rk_c * 0.5 * dt * m.ph.nu, crp = m.rk_c * dt, dta = dt * m.rk_a;
-    auto X = [&](int f, int ii, int jj, int kk) -> double { return __ldg(m.ax[f] + adj_at(g, ii, jj, kk)); };
-    auto LQ = [&](int c, int ii, int jj, int kk) -> double {
-        if (kk < 0 || kk >= nz || (c == 2 && kk > nz - 2)) return 0.0;
-        return __ldg(m.lq[c] + adj_at(g, ii, jj, kk));
-    };
+    auto X = [&](int f, int di, int dj) { return __ldg(m.ax[f] + N.at(di, dj)); };
+    auto Q = [&](int c, int di, int dj) { return __ldg(m.lq[c] + N.at(di, dj)); };
     auto dz = [&](int kk) { return ldz(g.z.dz, kk); };
     auto dzt = [&](int kk) { return ldz(g.z.dz_t, kk); };
     auto dzb = [&](int kk) { return ldz(g.z.dz_b, kk); };
     double lu, lv, lw, lp;
     // ---- transposed interpolation weights
     if (CDS == 1) {
-        lu = 0.5 * (X(0, i, j, k) + X(0, i + 1, j, k)) + 0.5 * (X(1, i, j - 1, k) + X(1, i, j, k));
-        lv = 0.5 * (X(2, i - 1, j, k) + X(2, i, j, k)) + 0.5 * (X(3, i, j, k) + X(3, i, j + 1, k));
-        lw = 0.5 * (X(4, i - 1, j, k) + X(4, i, j, k)) + 0.5 * (X(5, i, j - 1, k) + X(5, i, j, k));
+        lu = 0.5 * (X(0, 0, 0) + X(0, 1, 0)) + 0.5 * (X(1, 0, -1) + X(1, 0, 0));
+        lv = 0.5 * (X(2, -1, 0) + X(2, 0, 0)) + 0.5 * (X(3, 0, 0) + X(3, 0, 1));
+        lw = 0.5 * (X(4, -1, 0) + X(4, 0, 0)) + 0.5 * (X(5, 0, -1) + X(5, 0, 0));
     } else {
-        lu = (-X(0, i - 1, j, k) + 9.0 * X(0, i, j, k) + 9.0 * X(0, i + 1, j, k) - X(0, i + 2, j, k)) * 0.0625 +
-             (-X(1, i, j - 2, k) + 9.0 * X(1, i, j - 1, k) + 9.0 * X(1, i, j, k) - X(1, i, j + 1, k)) * 0.0625;
-        lv = (-X(2, i - 2, j, k) + 9.0 * X(2, i - 1, j, k) + 9.0 * X(2, i, j, k) - X(2, i + 1, j, k)) * 0.0625 +
-             (-X(3, i, j - 1, k) + 9.0 * X(3, i, j, k) + 9.0 * X(3, i, j + 1, k) - X(3, i, j + 2, k)) * 0.0625;
-        lw = (-X(4, i - 2, j, k) + 9.0 * X(4, i - 1, j, k) + 9.0 * X(4, i, j, k) - X(4, i + 1, j, k)) * 0.0625 +
-             (-X(5, i, j - 2, k) + 9.0 * X(5, i, j - 1, k) + 9.0 * X(5, i, j, k) - X(5, i, j + 1, k)) * 0.0625;
+        lu = (-X(0, -1, 0) + 9.0 * X(0, 0, 0) + 9.0 * X(0, 1, 0) - X(0, 2, 0)) * 0.0625 +
+             (-X(1, 0, -2) + 9.0 * X(1, 0, -1) + 9.0 * X(1, 0, 0) - X(1, 0, 1)) * 0.0625;
+        lv = (-X(2, -2, 0) + 9.0 * X(2, -1, 0) + 9.0 * X(2, 0, 0) - X(2, 1, 0)) * 0.0625 +
+             (-X(3, 0, -1) + 9.0 * X(3, 0, 0) + 9.0 * X(3, 0, 1) - X(3, 0, 2)) * 0.0625;
+        lw = (-X(4, -2, 0) + 9.0 * X(4, -1, 0) + 9.0 * X(4, 0, 0) - X(4, 1, 0)) * 0.0625 +
+             (-X(5, 0, -2) + 9.0 * X(5, 0, -1) + 9.0 * X(5, 0, 0) - X(5, 0, 1)) * 0.0625;
     }
     if (k >= 1) {
         const double l = ldz(g.z.l_t, k - 1);
-        lu += X(6, i, j, k - 1) * l;
-        lv += X(7, i, j, k - 1) * l;
+        lu += __ldg(m.ax[6] + id - up) * l;
+        lv += __ldg(m.ax[7] + id - up) * l;
     }
-    if (k <= nz - 2) {
+    if (wrow) {
         const double l = ldz(g.z.l_t, k);
-        lu += X(6, i, j, k) * (1.0 - l);
-        lv += X(7, i, j, k) * (1.0 - l);
+        lu += __ldg(m.ax[6] + id) * (1.0 - l);
+        lv += __ldg(m.ax[7] + id) * (1.0 - l);
     }
-    // ---- identity, diffusion (transposed), pressure gradient (transposed)
+    // ---- identity and horizontal diffusion (symmetric stencils)
     double hq[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const double q0 = LQ(c, i, j, k);
+        if (c == 2 && !wrow) { hq[c] = 0.0; continue; }
+        const double q0 = Q(c, 0, 0);
         double h;
         if (CDS == 1) {
-            h = (LQ(c, i + 1, j, k) - 2.0 * q0 + LQ(c, i - 1, j, k)) / g.dx2 +
-                (LQ(c, i, j + 1, k) - 2.0 * q0 + LQ(c, i, j - 1, k)) / g.dy2;
+            h = (Q(c, 1, 0) - 2.0 * q0 + Q(c, -1, 0)) / g.dx2 + (Q(c, 0, 1) - 2.0 * q0 + Q(c, 0, -1)) / g.dy2;
         } else {
-            h = (-LQ(c, i + 2, j, k) + 16.0 * LQ(c, i + 1, j, k) - 30.0 * q0 + 16.0 * LQ(c, i - 1, j, k) - LQ(c, i - 2, j, k)) / (12.0 * g.dx2) +
-                (-LQ(c, i, j + 2, k) + 16.0 * LQ(c, i, j + 1, k) - 30.0 * q0 + 16.0 * LQ(c, i, j - 1, k) - LQ(c, i, j - 2, k)) / (12.0 * g.dy2);
+            h = (-Q(c, 2, 0) + 16.0 * Q(c, 1, 0) - 30.0 * q0 + 16.0 * Q(c, -1, 0) - Q(c, -2, 0)) / (12.0 * g.dx2) +
+                (-Q(c, 0, 2) + 16.0 * Q(c, 0, 1) - 30.0 * q0 + 16.0 * Q(c, 0, -1) - Q(c, 0, -2)) / (12.0 * g.dy2);
         }
         hq[c] = q0 + cdif * h;
     }
-    const bool closed = A.closed;
+    // lambda_q of the same column at levels k-1, k, k+1 (zero where no equation)
+    auto qz = [&](int c, int kk) -> double {
+        if (kk < 0 || kk >= nz || (c == 2 && kk > nz - 2)) return 0.0;
+        return __ldg(m.lq[c] + id + (long long)(kk - k) * up);
+    };
+    const bool closed = m.a.closed;
     {   // u, v: second difference over cell centres with the no-slip / free-slip ghosts
-        const double qu = LQ(0, i, j, k), qv = LQ(1, i, j, k);
-        double zu = -qu * (1.0 / dzt(k) + 1.0 / dzb(k)) / dz(k), zv = -qv * (1.0 / dzt(k) + 1.0 / dzb(k)) / dz(k);
-        if (k >= 1) { const double e = 1.0 / (dzt(k - 1) * dz(k - 1)); zu += LQ(0, i, j, k - 1) * e; zv += LQ(1, i, j, k - 1) * e; }
-        if (k <= nz - 2) { const double e = 1.0 / (dzb(k + 1) * dz(k + 1)); zu += LQ(0, i, j, k + 1) * e; zv += LQ(1, i, j, k + 1) * e; }
+        const double qu = qz(0, k), qv = qz(1, k);
+        const double e0 = (1.0 / dzt(k) + 1.0 / dzb(k)) / dz(k);
+        double zu = -qu * e0, zv = -qv * e0;
+        if (k >= 1) { const double e = 1.0 / (dzt(k - 1) * dz(k - 1)); zu += qz(0, k - 1) * e; zv += qz(1, k - 1) * e; }
+        if (k <= nz - 2) { const double e = 1.0 / (dzb(k + 1) * dz(k + 1)); zu += qz(0, k + 1) * e; zv += qz(1, k + 1) * e; }
         if (k == 0) { const double e = 1.0 / (dzb(0) * dz(0)); zu -= qu * e; zv -= qv * e; }
         if (k == nz - 1) { const double e = (closed ? -1.0 : 1.0) / (dzt(k) * dz(k)); zu += qu * e; zv += qv * e; }
         lu += hq[0] + cdif * zu;
         lv += hq[1] + cdif * zv;
     }
+    const double qwm = qz(2, k - 1), qw0 = qz(2, k), qwp = qz(2, k + 1);
     {   // w: second difference over faces (w = 0 below the first face), rows k <= nz-2
-        const double qw = LQ(2, i, j, k);
-        double zw = -qw * (1.0 / dz(k + 1) + 1.0 / dz(k)) / dzt(k);
-        if (k >= 1) zw += LQ(2, i, j, k - 1) / (dz(k) * dzt(k - 1));
-        zw += LQ(2, i, j, k + 1) / (dz(k + 1) * dzt(k + 1));
+        double zw = wrow ? -qw0 * (1.0 / dz(k + 1) + 1.0 / dz(k)) / dzt(k) : 0.0;
+        if (k >= 1) zw += qwm / (dz(k) * dzt(k - 1));
+        if (k + 1 <= nz - 2) zw += qwp / (dz(k + 1) * dzt(k + 1));
         lw += hq[2] + cdif * zw;
         // w^2 flux: ((w(k) + w(k+1)) / 2)^2 - ((w(k) + w(k-1)) / 2)^2 over dz_t at rows k' = k-1, k, k+1
         auto Lfw = [&](int kk) -> double {
             if (kk < 0 || kk > nz - 2) return 0.0;
-            const long long q = ((long long)kk * g.ny + j) * g.nx + i;
+            const long long q = id + (long long)(kk - k) * up;
             return dta * __ldg(m.lq[2] + q) + __ldg(m.lf_out[2] + q);
         };
-        const double wm = A.W(i, j, k - 1), wc = A.W(i, j, k), wp = A.W(i, j, k + 1);
+        const double* W = m.a.f.w;
+        const double wm = k >= 1 ? __ldg(W + id - up) : 0.0, wc = __ldg(W + id);
+        const double wp = wrow ? __ldg(W + id + up) : 0.0;
         const double l0 = Lfw(k), lm = Lfw(k - 1), lp1 = Lfw(k + 1);
-        if (l0 != 0.0) lw += l0 / dzt(k) * (-0.5 * (wc + wp) + 0.5 * (wc + wm));
-        if (lm != 0.0) lw -= lm / dzt(k - 1) * 0.5 * (wm + wc);
-        if (lp1 != 0.0) lw += lp1 / dzt(k + 1) * 0.5 * (wp + wc);
+        if (wrow) lw += l0 / dzt(k) * (-0.5 * (wc + wp) + 0.5 * (wc + wm));
+        if (k >= 1) lw -= lm / dzt(k - 1) * 0.5 * (wm + wc);
+        if (k + 1 <= nz - 2) lw += lp1 / dzt(k + 1) * 0.5 * (wp + wc);
     }
     // pressure gradients of the three equations
     if (CDS == 1) {
-        lp = -crp / g.dx * (LQ(0, i - 1, j, k) - LQ(0, i, j, k)) - crp / g.dy * (LQ(1, i, j - 1, k) - LQ(1, i, j, k));
+        lp = -crp / g.dx * (Q(0, -1, 0) - Q(0, 0, 0)) - crp / g.dy * (Q(1, 0, -1) - Q(1, 0, 0));
     } else {
-        lp = -crp / (24.0 * g.dx) * (-LQ(0, i - 2, j, k) + 27.0 * LQ(0, i - 1, j, k) - 27.0 * LQ(0, i, j, k) + LQ(0, i + 1, j, k)) -
-             crp / (24.0 * g.dy) * (-LQ(1, i, j - 2, k) + 27.0 * LQ(1, i, j - 1, k) - 27.0 * LQ(1, i, j, k) + LQ(1, i, j + 1, k));
+        lp = -crp / (24.0 * g.dx) * (-Q(0, -2, 0) + 27.0 * Q(0, -1, 0) - 27.0 * Q(0, 0, 0) + Q(0, 1, 0)) -
+             crp / (24.0 * g.dy) * (-Q(1, 0, -2) + 27.0 * Q(1, 0, -1) - 27.0 * Q(1, 0, 0) + Q(1, 0, 1));
     }
-    if (k >= 1) lp -= crp * LQ(2, i, j, k - 1) / dzt(k - 1);
-    lp += crp * LQ(2, i, j, k) / dzt(k);
+    lp += crp * (qw0 / dzt(k) - (k >= 1 ? qwm / dzt(k - 1) : 0.0));
     m.out[0][id] = lu;
     m.out[1][id] = lv;
     m.out[2][id] = lw;

@@ -188,16 +188,20 @@ enum { F_U, F_V, F_W, F_P, F_T, F_FF, F_GG, F_HH, F_SS, F_QU, F_QV, F_QW, F_UHX,
 
 // kernel categories for the optional per-launch CUDA-event profile
 enum { K_BEGIN, K_RHS_MOM, K_FFT_X_FWD, K_FFT_Y_FWD, K_COLUMN, K_FFT_Y_INV, K_FFT_X_INV,
-       K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_SPEC_PROD, K_SPEC_ASM, K_SPEC_AUX, K_NCAT };
+       K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_SPEC_PROD, K_SPEC_ASM, K_SPEC_AUX, K_ADJ_COLUMN,
+       K_ADJ_RHS, K_NCAT };
 static const char* K_NAMES[K_NCAT] = {"substep_begin", "rhs_momentum", "fft_x_r2c", "fft_y_fwd", "column_fd",
                                       "fft_y_inv", "fft_x_c2r", "rhs_temperature", "column_t", "div_check",
-                                      "stats", "finalize", "spec_products", "spec_assemble", "aux"};
+                                      "stats", "finalize", "spec_products", "spec_assemble", "aux", "adj_column",
+                                      "adj_rhs"};
 
 // spectral-path buffers (cds = 3), each n values of the storage type: the half
 // spectra of the state and histories, phi, the divergence, the assembled
 // right-hand sides and work fields (physical products / their spectra)
 enum { SP_U, SP_V, SP_W, SP_P, SP_T, SP_FF, SP_GG, SP_HH, SP_SS, SP_PHI, SP_DIV, SP_QU, SP_QV, SP_QW, SP_W0,
        NSP = SP_W0 + 14 };
+
+#define ADJ_GRAPHS 4
 
 struct hc_handle {
     hc_params p;
@@ -223,6 +227,11 @@ struct hc_handle {
     double adj_ms[2];        // forward pass, reverse sweep (recomputation included)
     int adj_nsteps, adj_ckpt, adj_nseg, adj_seglen;
     int adj_ready;           // 1: checkpoints of the last hc_adjoint_forward are valid
+    int adj_tape_seg;        // segment whose sub-step start states the tape holds (-1: none)
+    cudaGraphExec_t adj_gexec[ADJ_GRAPHS];   // reverse segments, keyed by adj_gkey
+    int adj_gkey[ADJ_GRAPHS];
+    long long adj_glaunch[ADJ_GRAPHS];
+    int adj_gnext;
     long long adj_launches[2];
     // CUDA graph of one step (hc_set_graph): captured on first use, replayed per step
     int use_graph;
@@ -875,7 +884,9 @@ template <typename R> static int launch_column_t(hc_handle* h, const ColTArgs<R>
     return HC_OK;
 }
 
-template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
+// recompute = 1: a sub-step re-run for the adjoint's tape -- no divergence
+// check, no statistics snapshot, and the scalar update only when first = 1
+template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int recompute = 0, int first = 1)
 {
     typedef typename V2<R>::T T2;
     const hc_params& p = h->p;
@@ -883,14 +894,16 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     double rk_a, rk_b, rk_c;
     if (p.dts == 2) { rk_a = RKC1[sub]; rk_b = RKC2[sub]; rk_c = RKC3[sub]; }
     else { rk_a = 1.5; rk_b = -0.5; rk_c = 1.0; }
-    const int last = (p.dts == 2) ? (sub == 2) : 1;
+    const int last = ((p.dts == 2) ? (sub == 2) : 1) && !recompute;
 
     ScalarArgs sa;
     sa.sc = h->sc; sa.sub = sub; sa.dt = p.dt; sa.dp_opt = p.dp_opt; sa.dpx_coef = h->dpx_coef; sa.um = p.u_mrf;
     sa.is_ri_var = p.is_ri_var; sa.ri_str = p.ri_str; sa.ri_end = p.ri_end; sa.imax = p.imax;
-    prof_begin(h, K_BEGIN);
-    k_substep_begin<<<1, 1, 0, h->st>>>(sa);
-    CKL();
+    if (!recompute || first) {
+        prof_begin(h, K_BEGIN);
+        k_substep_begin<<<1, 1, 0, h->st>>>(sa);
+        CKL();
+    }
 
     // Rayleigh damping of the top layer (isdamp = 1), undamped copies kept for
     // the ghost reads of this sub-step's right-hand sides
@@ -934,7 +947,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph; m.sc = h->sc;
     m.with_t = p.isscalar == 1;
     // the divergence check of the previous sub-step rides along (slot sub-1)
-    m.part_div = (sub > 0 && h->div_in_rhs) ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
+    m.part_div = (sub > 0 && h->div_in_rhs && !recompute) ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
     m.kchunk = h->rhs_kc;
     m.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
     m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
@@ -1010,7 +1023,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub)
     fi.p = (const R*)h->fld[F_P]; fi.t = (const R*)h->fld[F_T];
     // the divergence check of this sub-step runs inside the next sub-step's RHS
     // (without damping, which changes the fields first); the last one has its own pass
-    if (!last && h->div_in_rhs) return HC_OK;
+    if (recompute || (!last && h->div_in_rhs)) return HC_OK;
     prof_begin(h, K_DIV);
     k_div_check<R, CDS><<<(unsigned)h->nbd, 256, 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->pd_stride * 3);
     CKL();
@@ -1297,6 +1310,9 @@ template <typename R> static int step_dispatch(hc_handle* h)
 // ---------------------------------------------------------------------------
 // discrete adjoint of the FD step (hc_adjoint)
 // ---------------------------------------------------------------------------
+extern "C" {
+static int graph_build(hc_handle* h);    // defined with the C-ABI below
+}
 struct AdjBufs {
     double* lam[4];      // adjoint of u, v, w, p at the current point of the sweep
     double* lh[3];       // adjoint of the histories ff, gg, hh
@@ -1349,7 +1365,7 @@ template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* c
     ColAdjArgs ca;
     ca.au = S[0]; ca.av = S[1]; ca.aw = S[2]; ca.apsi = S[3];
     ca.c = h->cc; ca.g = h->g; ca.rk_c = rk_c; ca.dt = p.dt; ca.nu = p.nu;
-    prof_begin(h, K_COLUMN);
+    prof_begin(h, K_ADJ_COLUMN);
     rc = launch_column_adj(h, ca);
     if (rc) return rc;
     double* lq[3] = {b.lq[0], b.lq[1], b.lq[2]};
@@ -1366,10 +1382,10 @@ template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* c
     for (int f = 0; f < 8; ++f) m.ax[f] = b.ax[f];
     for (int f = 0; f < 4; ++f) m.out[f] = b.lam[f];
     m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph;
-    prof_begin(h, K_RHS_MOM);
+    prof_begin(h, K_ADJ_RHS);
     k_rhs_adj_interp<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
     CKL();
-    prof_begin(h, K_RHS_MOM);
+    prof_begin(h, K_ADJ_RHS);
     k_rhs_adj_gather<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
     CKL();
     for (int f = 0; f < 3; ++f) { double* t = b.lh[f]; b.lh[f] = b.lh2[f]; b.lh2[f] = t; }
@@ -1408,24 +1424,48 @@ static AdjBufs adj_bufs(hc_handle* h)
 }
 
 // Forward pass with a checkpoint every ckpt steps: the state and scalars at
-// steps 0, ckpt, 2 ckpt, ... and at the end. The steps are plain steps (the
-// handle's statistics and diagnostics advance as in hc_step).
+// steps 0, ckpt, 2 ckpt, ... and at the end; the last segment also fills the
+// tape (the start state of each of its sub-steps), so the reverse sweep starts
+// without recomputation. The steps are plain steps (statistics and diagnostics
+// advance as in hc_step), replayed from the step graph outside the last segment.
 template <int CDS> static int adjoint_forward(hc_handle* h, AdjBufs& b)
 {
     const int nsteps = h->adj_nsteps, ckpt = h->adj_ckpt, nseg = h->adj_nseg;
+    const int nsub = h->p.dts == 2 ? 3 : 1;
     const long long n = h->g.n;
+    const bool graph = !h->prof;
     int rc;
+    if (graph && (rc = graph_build(h))) return rc;
     h->launches = 0;
     CK(cudaEventRecord(h->e0, h->st));
     for (int s = 0; s < nsteps; ++s) {
+        const int seg = s / ckpt;
         if (s % ckpt == 0) {
-            rc = adj_copy_state(h, b.ckpt + (size_t)(s / ckpt) * 7 * n, 7, 0);
+            rc = adj_copy_state(h, b.ckpt + (size_t)seg * 7 * n, 7, 0);
             if (rc) return rc;
-            CK(cudaMemcpyAsync(h->adj_sc + s / ckpt, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
+            CK(cudaMemcpyAsync(h->adj_sc + seg, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
         }
-        rc = step_fd<double, CDS>(h);
-        if (rc) return rc;
+        if (seg == nseg - 1) {
+            const int t0 = (s - seg * ckpt) * nsub;
+            for (int sub = 0; sub < nsub; ++sub) {
+                rc = adj_copy_state(h, b.tape + (size_t)(t0 + sub) * 4 * n, 4, 0);
+                if (rc) return rc;
+                rc = substep_fd<double, CDS>(h, sub);
+                if (rc) return rc;
+            }
+            rc = launch_stats<double>(h, 1);
+            if (rc) return rc;
+            rc = launch_finalize(h, nsub, 1);
+            if (rc) return rc;
+        } else if (graph) {
+            CK(cudaGraphLaunch(h->gexec, h->st));
+            h->launches += h->graph_launches;
+        } else {
+            rc = step_fd<double, CDS>(h);
+            if (rc) return rc;
+        }
     }
+    h->adj_tape_seg = nseg - 1;
     rc = adj_copy_state(h, b.fin, 7, 0);
     if (rc) return rc;
     CK(cudaMemcpyAsync(h->adj_sc + nseg, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
@@ -1438,9 +1478,86 @@ template <int CDS> static int adjoint_forward(hc_handle* h, AdjBufs& b)
     return HC_OK;
 }
 
-// Reverse sweep: per segment, last first, recompute the start state of each of
-// its sub-steps from the checkpoint, then run the sub-step adjoints backwards.
-// Ends with the final state and scalars of the forward pass restored.
+// One reverse segment of T sub-steps: with recompute, re-run the sub-steps from
+// the restored checkpoint (copying each start state into the tape; the last one
+// needs no re-run), then the sub-step adjoints from the last to the first.
+template <int CDS> static int adj_segment(hc_handle* h, AdjBufs& b, int T, int recompute)
+{
+    const int nsub = h->p.dts == 2 ? 3 : 1;
+    const long long n = h->g.n;
+    int rc;
+    if (recompute) {
+        for (int t = 0; t < T; ++t) {
+            rc = adj_copy_state(h, b.tape + (size_t)t * 4 * n, 4, 0);
+            if (rc) return rc;
+            if (t == T - 1) break;
+            rc = substep_fd<double, CDS>(h, t % nsub, 1, t == 0);
+            if (rc) return rc;
+        }
+    }
+    for (int t = T - 1; t >= 0; --t) {
+        const double* st[4];
+        for (int f = 0; f < 4; ++f) st[f] = b.tape + ((size_t)t * 4 + f) * n;
+        rc = adj_substep<CDS>(h, t % nsub, st, b);
+        if (rc) return rc;
+    }
+    return HC_OK;
+}
+
+static void adj_graph_drop(hc_handle* h)
+{
+    for (int q = 0; q < ADJ_GRAPHS; ++q) {
+        if (h->adj_gexec[q]) cudaGraphExecDestroy(h->adj_gexec[q]);
+        h->adj_gexec[q] = nullptr;
+        h->adj_gkey[q] = -1;
+    }
+}
+
+// adj_segment through a CUDA graph, captured once per (T, recompute, which
+// buffer of the history-adjoint pair is current) and replayed after that; the
+// host-side pointer swaps of the sub-steps are repeated on replay.
+template <int CDS> static int adj_segment_run(hc_handle* h, AdjBufs& b, int T, int recompute)
+{
+    if (h->prof) return adj_segment<CDS>(h, b, T, recompute);
+    const int parity = b.lh[0] == h->adj_buf + 4 * h->g.n ? 0 : 1;
+    const int key = (T * 2 + parity) * 2 + recompute;
+    int slot = -1;
+    for (int q = 0; q < ADJ_GRAPHS; ++q)
+        if (h->adj_gkey[q] == key) slot = q;
+    if (slot < 0) {
+        slot = h->adj_gnext;
+        h->adj_gnext = (h->adj_gnext + 1) % ADJ_GRAPHS;
+        if (h->adj_gexec[slot]) cudaGraphExecDestroy(h->adj_gexec[slot]);
+        h->adj_gexec[slot] = nullptr;
+        h->adj_gkey[slot] = -1;
+        const long long l0 = h->launches;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        int rc = adj_segment<CDS>(h, b, T, recompute);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(h->st, &g);
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            h->launches = l0;
+            return rc ? rc : HC_ERR_CUDA;
+        }
+        h->adj_glaunch[slot] = h->launches - l0;
+        h->launches = l0;
+        e = cudaGraphInstantiate(&h->adj_gexec[slot], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { h->adj_gexec[slot] = nullptr; return HC_ERR_CUDA; }
+        h->adj_gkey[slot] = key;
+    } else if (T & 1) {
+        for (int f = 0; f < 3; ++f) { double* t = b.lh[f]; b.lh[f] = b.lh2[f]; b.lh2[f] = t; }
+    }
+    CK(cudaGraphLaunch(h->adj_gexec[slot], h->st));
+    h->launches += h->adj_glaunch[slot];
+    return HC_OK;
+}
+
+// Reverse sweep over the segments, last first: restore the checkpoint and
+// recompute where the tape does not hold the segment, then its sub-step
+// adjoints. Ends with the final state and scalars of the forward pass restored.
 template <int CDS> static int adjoint_reverse(hc_handle* h, AdjBufs& b)
 {
     const int nsteps = h->adj_nsteps, ckpt = h->adj_ckpt, nseg = h->adj_nseg;
@@ -1450,24 +1567,16 @@ template <int CDS> static int adjoint_reverse(hc_handle* h, AdjBufs& b)
     h->launches = 0;
     CK(cudaEventRecord(h->e0, h->st));
     for (int seg = nseg - 1; seg >= 0; --seg) {
-        rc = adj_copy_state(h, b.ckpt + (size_t)seg * 7 * n, 7, 1);
-        if (rc) return rc;
-        CK(cudaMemcpyAsync(h->sc, h->adj_sc + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
         const int s0 = seg * ckpt, s1 = (s0 + ckpt < nsteps ? s0 + ckpt : nsteps);
-        int t = 0;
-        for (int s = s0; s < s1; ++s)
-            for (int sub = 0; sub < nsub; ++sub, ++t) {
-                rc = adj_copy_state(h, b.tape + (size_t)t * 4 * n, 4, 0);
-                if (rc) return rc;
-                rc = substep_fd<double, CDS>(h, sub);
-                if (rc) return rc;
-            }
-        for (--t; t >= 0; --t) {
-            const double* st[4];
-            for (int f = 0; f < 4; ++f) st[f] = b.tape + ((size_t)t * 4 + f) * n;
-            rc = adj_substep<CDS>(h, t % nsub, st, b);
+        const int recompute = h->adj_tape_seg != seg;
+        if (recompute) {
+            rc = adj_copy_state(h, b.ckpt + (size_t)seg * 7 * n, 7, 1);
             if (rc) return rc;
+            CK(cudaMemcpyAsync(h->sc, h->adj_sc + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
         }
+        rc = adj_segment_run<CDS>(h, b, (s1 - s0) * nsub, recompute);
+        if (rc) return rc;
+        h->adj_tape_seg = seg;
     }
     rc = adj_copy_state(h, b.fin, 7, 1);
     if (rc) return rc;
@@ -1506,6 +1615,7 @@ static void graph_drop(hc_handle* h)
 {
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     h->gexec = nullptr;
+    adj_graph_drop(h);
 }
 
 // Capture one full step (all sub-steps, statistics, finaliser) of this handle
@@ -1586,6 +1696,8 @@ int hc_create(const hc_params* p, hc_handle** out)
     h->dsig = nullptr; h->dmean = nullptr; h->dstale = nullptr; h->div_in_rhs = 0;
     h->bf[0] = h->bf[1] = h->bf[2] = nullptr; h->has_bf = 0;
     h->adj_buf = nullptr; h->adj_bytes = 0; h->adj_sc = nullptr; h->adj_nsc = 0;
+    h->adj_tape_seg = -1; h->adj_gnext = 0;
+    for (int q = 0; q < ADJ_GRAPHS; ++q) { h->adj_gexec[q] = nullptr; h->adj_gkey[q] = -1; }
     h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0;
     for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
@@ -2146,7 +2258,6 @@ int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
     DevScalars s0;
     CK(cudaMemcpy(&s0, h->sc, sizeof(s0), cudaMemcpyDeviceToHost));
     if (s0.nan_flag) return HC_ERR_NAN;
-    graph_drop(h);
     const long long n = h->g.n;
     const int nsub = p.dts == 2 ? 3 : 1;
     const int nseg = (nsteps + ckpt - 1) / ckpt;
@@ -2155,6 +2266,7 @@ int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
     const size_t nfield = 24 + (size_t)7 * nseg + (size_t)4 * seglen * nsub + 7;
     const size_t bytes = nfield * (size_t)n * sizeof(double);
     if (bytes > h->adj_bytes) {
+        adj_graph_drop(h);
         if (h->adj_buf) cudaFree(h->adj_buf);
         h->adj_buf = nullptr; h->adj_bytes = 0;
         if (cudaMalloc((void**)&h->adj_buf, bytes) != cudaSuccess) { cudaGetLastError(); return HC_ERR_NOMEM; }
@@ -2166,12 +2278,12 @@ int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
         if (cudaMalloc((void**)&h->adj_sc, (nseg + 1) * sizeof(DevScalars)) != cudaSuccess) { cudaGetLastError(); return HC_ERR_NOMEM; }
         h->adj_nsc = nseg + 1;
     }
+    if (nseg != h->adj_nseg || seglen != h->adj_seglen) adj_graph_drop(h);   // the tape moved
     h->adj_nsteps = nsteps; h->adj_ckpt = ckpt; h->adj_nseg = nseg; h->adj_seglen = seglen;
     AdjBufs b = adj_bufs(h);
-    const int prof = h->prof;
-    h->prof = 0;
     int rc = p.cds == 1 ? adjoint_forward<1>(h, b) : adjoint_forward<2>(h, b);
-    h->prof = prof;
+    if (rc) return rc;
+    rc = prof_collect(h);
     if (rc) return rc;
     DevScalars s1;
     CK(cudaMemcpy(&s1, h->sc, sizeof(s1), cudaMemcpyDeviceToHost));
@@ -2197,11 +2309,10 @@ int hc_adjoint_reverse(hc_handle* h, const double* lu, const double* lv, const d
         CK(cudaMemsetAsync(b.lh[f], 0, fb, h->st));
         CK(cudaMemsetAsync(b.lbf[f], 0, fb, h->st));
     }
-    const int prof = h->prof;
-    h->prof = 0;
     int rc = h->p.cds == 1 ? adjoint_reverse<1>(h, b) : adjoint_reverse<2>(h, b);
-    h->prof = prof;
     if (rc) { h->adj_ready = 0; return rc; }
+    rc = prof_collect(h);
+    if (rc) return rc;
     double* out[4] = {gu, gv, gw, gp};
     for (int f = 0; f < 4; ++f)
         if (out[f]) CK(cudaMemcpyAsync(out[f], b.lam[f], fb, cudaMemcpyDeviceToHost, h->st));
