@@ -181,3 +181,37 @@ def test_autograd_function_backward(engine):
         assert np.allclose(x.grad.numpy(), g[k], rtol=1e-12, atol=1e-15), k
     c.close()
     c2.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [
+    dict(cds=2, dts=2, dp_opt=3, ochannel=1, fc=0.5, ug=1.0, vg=0.2),
+    dict(cds=1, dts=2, dp_opt=1, ochannel=0, u_mrf=0.3),
+    dict(cds=2, dts=1, dp_opt=1, ochannel=0, u_mrf=-0.2),
+], ids=["fd4_rk3_ekman", "fd2_rk3_mrf", "fd4_ab2_mrf"])
+def test_adjoint_matches_torch_autograd(engine, case):
+    """The hand-written adjoint against autograd through the FP64 PyTorch
+    restatement of the same discrete step (tests/torch_step.py)."""
+    torch = pytest.importorskip("torch")
+    from torch_step import TorchFD
+    p = Params(**{**SMALL, **case})
+    f0 = inputs.small_random(p, seed=41)
+    bf = inputs.gaussian_body_force(p, seed=42, amp=0.02)
+    seeds = _random_seeds(p, 43)
+    nsteps = 3
+    T = lambda a, g=False: torch.tensor(a, dtype=torch.float64, requires_grad=g)
+    xs = [T(f0[f], True) for f in FIELDS] + [T(b, True) for b in bf]
+    hist = tuple(T(np.zeros_like(f0["u"])) for _ in range(3))
+    out = TorchFD(p).run(tuple(xs[:4]) + hist, nsteps, tuple(xs[4:]))
+    j = sum((T(seeds[f]) * out[q]).sum() for q, f in enumerate(FIELDS))
+    j.backward()
+    c = engine.Channel(p)
+    c.load({f: f0[f] for f in FIELDS})
+    c.set_body_force(*bf)
+    c.initialize()
+    g = c.adjoint(nsteps, seeds, ckpt=2)
+    c.close()
+    for x, k in zip(xs, ("u", "v", "w", "p", "fx", "fy", "fz")):
+        ref = x.grad.numpy()
+        err = np.max(np.abs(g[k] - ref)) / np.max(np.abs(ref))
+        assert err <= 1e-10, (k, err)
