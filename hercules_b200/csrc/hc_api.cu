@@ -202,6 +202,9 @@ enum { SP_U, SP_V, SP_W, SP_P, SP_T, SP_FF, SP_GG, SP_HH, SP_SS, SP_PHI, SP_DIV,
        NSP = SP_W0 + 14 };
 
 #define ADJ_GRAPHS 4
+// FP32 storage: mean accumulators sum each window of this many steps in FP32
+// before it is folded into their FP64 sums
+#define STATS_WINDOW 16
 
 struct hc_handle {
     hc_params p;
@@ -238,6 +241,8 @@ struct hc_handle {
     cudaGraphExec_t gexec;
     long long graph_launches;
     double* mean[11];
+    float* win[11];          // FP32 storage: the FP32 window sums of the mean accumulators
+    double* mtmp;            // FP32 storage: FP64 sums + window, assembled for a download
     double* zbuf;            // 5*(nz+4)
     double* coef;
     ColCoef cc;
@@ -790,7 +795,9 @@ template <typename R> static int launch_stats(hc_handle* h, int accumulate)
     s.f.p = (const R*)h->fld[F_P]; s.f.t = (const R*)h->fld[F_T];
     s.g = h->g;
     if (h->p.cds != 3) { s.uhx_s = (const R*)h->fld[F_UHX]; s.vhy_s = (const R*)h->fld[F_VHY]; }
-    for (int q = 0; q < 11; ++q) s.mean[q] = h->mean[q];
+    for (int q = 0; q < 11; ++q) { s.mean[q] = h->mean[q]; s.win[q] = h->win[q]; }
+    s.step = &h->sc->step;
+    s.window = STATS_WINDOW;
     s.accumulate = accumulate;
     s.um = h->p.u_mrf; s.dt = h->p.dt;
     s.part = h->part_st;
@@ -1657,6 +1664,8 @@ static void free_all(hc_handle* h)
     if (h->adj_sc) cudaFree(h->adj_sc);
     if (h->dmean) cudaFree(h->dmean);
     for (int q = 0; q < 11; ++q) if (h->mean[q]) cudaFree(h->mean[q]);
+    for (int q = 0; q < 11; ++q) if (h->win[q]) cudaFree(h->win[q]);
+    if (h->mtmp) cudaFree(h->mtmp);
     if (h->zbuf) cudaFree(h->zbuf);
     if (h->coef) cudaFree(h->coef);
     if (h->scratch) cudaFree(h->scratch);
@@ -1699,7 +1708,8 @@ int hc_create(const hc_params* p, hc_handle** out)
     h->adj_tape_seg = -1; h->adj_gnext = 0;
     for (int q = 0; q < ADJ_GRAPHS; ++q) { h->adj_gexec[q] = nullptr; h->adj_gkey[q] = -1; }
     h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0;
-    for (int q = 0; q < 11; ++q) h->mean[q] = nullptr;
+    for (int q = 0; q < 11; ++q) { h->mean[q] = nullptr; h->win[q] = nullptr; }
+    h->mtmp = nullptr;
     h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
     h->diag_cap = 0; h->last_ms = 0.0; h->launches = 0; h->initialized = 0;
@@ -1734,6 +1744,10 @@ int hc_create(const hc_params* p, hc_handle** out)
         for (int q = 0; q < 11; ++q) {
             if (cudaMalloc(&h->mean[q], n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
             if (cudaMemset(h->mean[q], 0, n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+            if (h->rsz == sizeof(float)) {
+                if (cudaMalloc(&h->win[q], n * sizeof(float)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+                if (cudaMemset(h->win[q], 0, n * sizeof(float)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+            }
         }
         if (p->cds == 3) {
             const int nsp = SP_W0 + (p->issk == 1 ? 14 : 8);
@@ -1885,6 +1899,7 @@ int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, 
             memcpy(&tmp[((long long)k * ny + j) * nx], host + (size_t)ghost + (size_t)ld1 * ((size_t)(j + ghost) + (size_t)ld2 * (size_t)(k + ghost)), nx * sizeof(double));
     if (is_mean || h->rsz == sizeof(double)) {
         CK(cudaMemcpy(d, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+        if (is_mean && h->win[0]) CK(cudaMemset(h->win[field_id - HC_FIELD_MEAN_U], 0, n * sizeof(float)));
     } else {
         std::vector<float> tf(n);
         for (long long q = 0; q < n; ++q) tf[q] = (float)tmp[q];
@@ -1923,7 +1938,19 @@ static void* download_source(hc_handle* h, int field_id, int* is_mean, int* rc)
     }
     if (field_id == HC_FIELD_PHI) { *rc = HC_ERR_UNSUPPORTED; return nullptr; }
     void* d = field_dev(h, field_id, is_mean);
-    if (!d) *rc = HC_ERR_ARG;
+    if (!d) { *rc = HC_ERR_ARG; return nullptr; }
+    if (*is_mean && h->win[0]) {
+        // the FP64 sums plus the FP32 window not folded in yet
+        if (!h->mtmp && cudaMalloc((void**)&h->mtmp, h->g.n * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            *rc = HC_ERR_NOMEM;
+            return nullptr;
+        }
+        const int q = field_id - HC_FIELD_MEAN_U;
+        k_mean_combine<<<RED_BLOCKS, 256, 0, h->st>>>(h->mtmp, h->mean[q], h->win[q], h->g.n);
+        if (cudaGetLastError() != cudaSuccess) { *rc = HC_ERR_CUDA; return nullptr; }
+        return h->mtmp;
+    }
     return d;
 }
 
@@ -1984,6 +2011,7 @@ int hc_upload_dev(hc_handle* h, int field_id, const void* dev)
     if (!d) return HC_ERR_ARG;
     const size_t bytes = h->g.n * (is_mean ? sizeof(double) : h->rsz);
     CK(cudaMemcpyAsync(d, dev, bytes, cudaMemcpyDeviceToDevice, h->st));
+    if (is_mean && h->win[0]) CK(cudaMemsetAsync(h->win[field_id - HC_FIELD_MEAN_U], 0, h->g.n * sizeof(float), h->st));
     CK(cudaStreamSynchronize(h->st));
     return HC_OK;
 }

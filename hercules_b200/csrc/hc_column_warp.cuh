@@ -662,11 +662,22 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     TT* TU = reinterpret_cast<TT*>(smem_raw);
     TT* TV = TU + CT_COLS * STR;
     TT* TW = TV + CT_COLS * STR;
+    // nrows * CT_COLS <= 32 K * CT_COLS = K * blockDim: at most K elements per
+    // thread, all loads issued before the first shared-memory store
     auto load = [&](const TT* __restrict__ q, TT* T, int nrows) {
-        for (int idx = threadIdx.x; idx < nrows * CT_COLS; idx += blockDim.x) {
+        TT v[K];
+#pragma unroll
+        for (int it = 0; it < K; ++it) {
+            const int idx = threadIdx.x + it * CT_COLS * 32;
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
             const long long cc = c0 + cb;
-            T[cb * STR + (r % K) * 32 + r / K] = cc < ncol ? q[(long long)r * ncol + cc] : mk2<R>(R(0), R(0));
+            v[it] = (idx < nrows * CT_COLS && cc < ncol) ? q[(long long)r * ncol + cc] : mk2<R>(R(0), R(0));
+        }
+#pragma unroll
+        for (int it = 0; it < K; ++it) {
+            const int idx = threadIdx.x + it * CT_COLS * 32;
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * 32 + r / K] = v[it];
         }
     };
     auto store = [&](TT* __restrict__ q, const TT* T, int nrows) {

@@ -455,18 +455,36 @@ template <typename R> struct StatsArgs {
     Geo g;
     const R* uhx_s; const R* vhy_s;     // null on the spectral path: u, v used directly
     double* mean[11];
+    // FP32 storage: the step's products go into FP32 sums of the current window
+    // of `window` steps, folded into the FP64 sums after every step whose number
+    // is a multiple of the window (null: straight into the FP64 sums)
+    float* win[11];
+    const int* step;                     // completed steps, this one included
+    int window;
     int accumulate;
     double um, dt;
     double* part;                        // per block: sum u*dz, CFL max
 };
 
+// FP64 sums plus the pending FP32 window: what the mean accumulators hold
+static __global__ void k_mean_combine(double* __restrict__ dst, const double* __restrict__ tot,
+                               const float* __restrict__ win, long long n)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = tot[q] + (double)win[q];
+}
+
 // calculate_mean_fields (src/module_tools.f90:362-404 / src/module_spectral.f90:1012-1052)
 // fused with the bulk velocity sum of calculate_ubar (src/module_parameters.f90:513-546)
 // and the CFL of screen_cpu_time (src/module_io.f90:43-61) for the next step.
+// A thread walks its (i,j) column through a chunk of levels, G levels at a time:
+// every load of a group (fields, then accumulators) is issued before its first
+// store, so the read-modify-writes of consecutive levels overlap in flight.
 template <typename R>
 __global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
 {
     // blockIdx.x: 256 consecutive (i,j) points of a plane; blockIdx.y: a chunk of levels
+    constexpr int G = 2;
     __shared__ double s_sum[8], s_cfl[8];
     const Geo& g = s.g;
     const int tid = threadIdx.x;
@@ -476,44 +494,95 @@ __global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
     const int k0 = blockIdx.y * kc, k1 = min(g.nz, k0 + kc);
     double ub = 0.0, cfl = 0.0;
     if (ij < g.nxy) {
-        // the fields are never written here and the accumulators never read as
-        // fields, so the loads of consecutive levels may overlap
         const R* __restrict__ fu = s.f.u; const R* __restrict__ fv = s.f.v;
         const R* __restrict__ fw = s.f.w; const R* __restrict__ ft = s.f.t;
         const R* __restrict__ fux = s.uhx_s; const R* __restrict__ fvy = s.vhy_s;
-        double* __restrict__ m0 = s.mean[0]; double* __restrict__ m1 = s.mean[1];
-        double* __restrict__ m2 = s.mean[2]; double* __restrict__ m3 = s.mean[3];
-        double* __restrict__ m4 = s.mean[4]; double* __restrict__ m5 = s.mean[5];
-        double* __restrict__ m6 = s.mean[6]; double* __restrict__ m7 = s.mean[7];
-        double* __restrict__ m8 = s.mean[8]; double* __restrict__ m9 = s.mean[9];
-        double* __restrict__ m10 = s.mean[10];
         const double um = s.um;
+        // FP32 storage always keeps the FP32 window sums (allocated with the handle)
+        const bool fold = sizeof(R) == sizeof(float) && s.accumulate && (*s.step % s.window) == 0;
         double wm = k0 > 0 ? (double)fw[(long long)(k0 - 1) * g.nxy + ij] : 0.0;
-#pragma unroll 2
-        for (int k = k0; k < k1; ++k) {
-            const long long q = (long long)k * g.nxy + ij;
-            const double u = (double)fu[q], v = (double)fv[q], w = (double)fw[q];
-            const double dzk = ldz(g.z.dz, k);
-            ub += u * dzk;
-            cfl = fmax(cfl, s.dt * fabs(u) * rdx + s.dt * fabs(v) * rdy + s.dt * fabs(w) / dzk);
-            if (s.accumulate) {
-                const double t = (double)ft[q];
-                const double wc = 0.5 * (w + wm);
-                const double ux = fux ? (double)fux[q] : u;
-                const double vy = fvy ? (double)fvy[q] : v;
-                m4[q] += (u + um) * (u + um);
-                m5[q] += v * v;
-                m6[q] += w * w;
-                m7[q] += wc * (ux + um);
-                m8[q] += wc * vy;
-                m9[q] += t * t;
-                m10[q] += t * 0.5 * (w + wm);
-                m0[q] += u + um;
-                m1[q] += v;
-                m2[q] += w;
-                m3[q] += t;
+        for (int kb = k0; kb < k1; kb += G) {
+            double u[G], v[G], w[G], t[G], ux[G], vy[G];
+            bool in[G];
+#pragma unroll
+            for (int e = 0; e < G; ++e) {
+                in[e] = kb + e < k1;
+                const long long q = (long long)(in[e] ? kb + e : kb) * g.nxy + ij;
+                u[e] = (double)fu[q]; v[e] = (double)fv[q]; w[e] = (double)fw[q];
+                if (s.accumulate) {
+                    t[e] = (double)ft[q];
+                    ux[e] = fux ? (double)fux[q] : u[e];
+                    vy[e] = fvy ? (double)fvy[q] : v[e];
+                } else {
+                    t[e] = 0.0; ux[e] = 0.0; vy[e] = 0.0;
+                }
             }
-            wm = w;
+            double wp[G];                   // w one level below each of the group's levels
+#pragma unroll
+            for (int e = 0; e < G; ++e) {
+                wp[e] = e == 0 ? wm : w[e - 1];
+                const double dzk = ldz(g.z.dz, in[e] ? kb + e : kb);
+                if (in[e]) {
+                    ub += u[e] * dzk;
+                    cfl = fmax(cfl, s.dt * fabs(u[e]) * rdx + s.dt * fabs(v[e]) * rdy + s.dt * fabs(w[e]) / dzk);
+                }
+            }
+            wm = w[G - 1];
+            if (!s.accumulate) continue;
+            // this step's product a at level kb + e
+            auto c = [&](int a, int e) -> double {
+                const double wc = 0.5 * (w[e] + wp[e]);
+                switch (a) {
+                case 0: return u[e] + um;
+                case 1: return v[e];
+                case 2: return w[e];
+                case 3: return t[e];
+                case 4: return (u[e] + um) * (u[e] + um);
+                case 5: return v[e] * v[e];
+                case 6: return w[e] * w[e];
+                case 7: return wc * (ux[e] + um);
+                case 8: return wc * vy[e];
+                case 9: return t[e] * t[e];
+                default: return t[e] * 0.5 * (w[e] + wp[e]);
+                }
+            };
+            if (sizeof(R) == sizeof(double)) {
+                // FP64 storage: straight into the FP64 sums
+                double m[11][G];
+#pragma unroll
+                for (int a = 0; a < 11; ++a)
+#pragma unroll
+                    for (int e = 0; e < G; ++e)
+                        if (in[e]) m[a][e] = s.mean[a][(long long)(kb + e) * g.nxy + ij];
+#pragma unroll
+                for (int a = 0; a < 11; ++a)
+#pragma unroll
+                    for (int e = 0; e < G; ++e)
+                        if (in[e]) s.mean[a][(long long)(kb + e) * g.nxy + ij] = m[a][e] + c(a, e);
+            } else if (!fold) {
+                float m[11][G];
+#pragma unroll
+                for (int a = 0; a < 11; ++a)
+#pragma unroll
+                    for (int e = 0; e < G; ++e)
+                        if (in[e]) m[a][e] = s.win[a][(long long)(kb + e) * g.nxy + ij];
+#pragma unroll
+                for (int a = 0; a < 11; ++a)
+#pragma unroll
+                    for (int e = 0; e < G; ++e)
+                        if (in[e]) s.win[a][(long long)(kb + e) * g.nxy + ij] = (float)((double)m[a][e] + c(a, e));
+            } else {
+                // end of a window: FP64 sum += window + this step, the window restarts at 0
+#pragma unroll
+                for (int a = 0; a < 11; ++a)
+#pragma unroll
+                    for (int e = 0; e < G; ++e)
+                        if (in[e]) {
+                            const long long q = (long long)(kb + e) * g.nxy + ij;
+                            s.mean[a][q] += (double)s.win[a][q] + c(a, e);
+                            s.win[a][q] = 0.0f;
+                        }
+            }
         }
     }
     ub = warp_sum(ub);
