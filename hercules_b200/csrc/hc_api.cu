@@ -647,11 +647,6 @@ template <typename R> static int set_smem_attrs()
         CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     }
-    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<4>()));
-    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<5>()));
-    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<6>()));
-    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<7>()));
-    CK(cudaFuncSetAttribute(k_column_fd_tile<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)column_tile_smem<8>()));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     return HC_OK;

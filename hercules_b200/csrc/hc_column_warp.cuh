@@ -322,200 +322,17 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_column_t_warp(ColTArgs<R> a)
 }
 
 // ---------------------------------------------------------------------------
-// Same fused FD column work as k_column_fd_warp, but the block stages the
-// columns of CT_COLS adjacent wavenumber pairs in shared memory, so that every
-// global load and store is a coalesced row segment of CT_COLS modes instead of
-// one scattered 16-byte access per lane. Tile layout per column: [i][lane]
-// (row r = lane*K + i), columns padded by one slot so that the row-wise global
-// loads land in distinct banks.
+// Columns of CT_COLS adjacent wavenumber pairs staged in shared memory, so that
+// every global load and store is a coalesced row segment of CT_COLS modes
+// instead of one scattered access per lane. Tile layout per column: [i][lane]
+// (row r = lane*K + i), rows of CT_RP = 32 slots (aligned for the per-lane
+// accesses of the solves), columns padded by one slot so that the row-wise
+// global loads spread over the banks.
 // ---------------------------------------------------------------------------
 #define CT_COLS 8
+#define CT_RP 32
 
-template <int K> __host__ __device__ constexpr int ct_stride() { return K * 32 + 1; }
-template <int K> __host__ size_t column_tile_smem() { return (size_t)3 * CT_COLS * ct_stride<K>() * sizeof(double2); }
-
-// rows [0, nrows) of CT_COLS columns starting at c0: global [r][c] <-> tile [c][r%K][r/K]
-template <typename R, int K>
-__device__ __forceinline__ void ct_load(const typename V2<R>::T* __restrict__ q, double2* T, long long c0, long long ncol,
-                                        int nrows)
-{
-    for (int idx = threadIdx.x; idx < nrows * CT_COLS; idx += blockDim.x) {
-        const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
-        const long long c = c0 + cb;
-        T[cb * ct_stride<K>() + (r % K) * 32 + r / K] = c < ncol ? ld2<R>(q, (long long)r * ncol + c) : make_double2(0, 0);
-    }
-}
-template <typename R, int K>
-__device__ __forceinline__ void ct_store(typename V2<R>::T* __restrict__ q, const double2* T, long long c0, long long ncol,
-                                         int nrows)
-{
-    for (int idx = threadIdx.x; idx < nrows * CT_COLS; idx += blockDim.x) {
-        const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
-        const long long c = c0 + cb;
-        if (c < ncol) st2<R>(q, (long long)r * ncol + c, T[cb * ct_stride<K>() + (r % K) * 32 + r / K]);
-    }
-}
-
-template <typename R, int K>
-__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile(ColArgs<R> a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (a.halt && *a.halt) return;
-    const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    const long long ncol = a.g.ncol;
-    const long long c0 = (long long)blockIdx.x * CT_COLS;
-    const long long c = c0 + wp;
-    const bool active = c < ncol;
-    const int nz = a.g.nz;
-    double2* TU = reinterpret_cast<double2*>(smem_raw);
-    double2* TV = TU + CT_COLS * ct_stride<K>();
-    double2* TW = TV + CT_COLS * ct_stride<K>();
-    ct_load<R, K>(a.qu, TU, c0, ncol, nz);
-    ct_load<R, K>(a.qv, TV, c0, ncol, nz);
-    ct_load<R, K>(a.qw, TW, c0, ncol, nz - 1);
-    __syncthreads();
-    double2* SU = TU + wp * ct_stride<K>();
-    double2* SV = TV + wp * ct_stride<K>();
-    double2* SW = TW + wp * ct_stride<K>();
-    const int l = (int)(c % a.g.nxh), m = (int)(c / a.g.nxh);
-    const bool is00 = (c == 0);
-    const double rk = a.rk_c, dt = a.dt;
-    const int r0 = ln * K;
-    double2 ph[1][K];
-    if (active) {
-        const double lam = __ldg(a.c.hx + l) + __ldg(a.c.hy + m);
-        const double lamp = __ldg(a.c.px + l) + __ldg(a.c.py + m);
-        const double* dgu = is00 ? a.c.d0u : a.c.dgu;
-        const double* dgw = is00 ? a.c.d0w : a.c.dgw;
-        const double* dgp = is00 ? a.c.d0p : a.c.dgp;
-        // ---- u*, v*: one matrix, two right-hand sides
-        {
-            double2 d[2][K];
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                const int r = r0 + i;
-                if (r < nz) {
-                    d[0][i] = SU[i * 32 + ln];
-                    d[1][i] = SV[i * 32 + ln];
-                    if (is00 && r == 0) d[0][i].x += a.bcu0;
-                    if (is00 && r == nz - 1) d[0][i].x += a.bcu1;
-                } else {
-                    d[0][i] = make_double2(0, 0);
-                    d[1][i] = make_double2(0, 0);
-                }
-            }
-            auto cf = [&](int r, double& aa, double& bb, double& cc) {
-                if (r < nz) {
-                    aa = rk * __ldg(a.c.au + r);
-                    cc = rk * __ldg(a.c.cu + r);
-                    bb = 1.0 + rk * (-lam + __ldg(dgu + r));
-                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
-            };
-            warp_partition_solve<K, 2>(cf, d, ln);
-#pragma unroll
-            for (int i = 0; i < K; ++i) { SU[i * 32 + ln] = d[0][i]; SV[i * 32 + ln] = d[1][i]; }
-        }
-        // ---- w*: rows 0..nz-2 (the top-wall row is an identity row with zero source)
-        {
-            double2 dw[1][K];
-#pragma unroll
-            for (int i = 0; i < K; ++i) dw[0][i] = r0 + i < nz - 1 ? SW[i * 32 + ln] : make_double2(0, 0);
-            auto cf = [&](int r, double& aa, double& bb, double& cc) {
-                if (r < nz - 1) {
-                    aa = rk * __ldg(a.c.aw + r);
-                    cc = rk * __ldg(a.c.cw + r);
-                    bb = 1.0 + rk * (-lam + __ldg(dgw + r));
-                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
-            };
-            warp_partition_solve<K, 1>(cf, dw, ln);
-#pragma unroll
-            for (int i = 0; i < K; ++i) SW[i * 32 + ln] = dw[0][i];
-        }
-        __syncwarp();
-        // ---- phi: source div(u*)/dt, Poisson with the null-space pin on (0,0)
-        const double2 DX = __ldg(a.c.dx + l), DY = __ldg(a.c.dy + m);
-        const double rdt = 1.0 / dt;
-        {
-            const double2 wlast = SW[(K - 1) * 32 + ln];
-            double2 wprev0 = shfl_up2(wlast, 1);
-            if (ln == 0) wprev0 = make_double2(0, 0);
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                const int r = r0 + i;
-                if (r < nz) {
-                    const double2 us = SU[i * 32 + ln], vs = SV[i * 32 + ln], ws = SW[i * 32 + ln];
-                    const double2 wm = i > 0 ? SW[(i - 1) * 32 + ln] : wprev0;
-                    const double rdz = __ldg(a.c.rdz + r);
-                    double2 div = zadd(zmul(DX, us), zmul(DY, vs));
-                    div = zadd(div, make_double2((ws.x - wm.x) * rdz, (ws.y - wm.y) * rdz));
-                    ph[0][i] = make_double2(div.x * rdt, div.y * rdt);
-                    if (is00 && r == 0) ph[0][i] = make_double2(0, 0);
-                } else {
-                    ph[0][i] = make_double2(0, 0);
-                }
-            }
-            auto cf = [&](int r, double& aa, double& bb, double& cc) {
-                if (r < nz) {
-                    aa = rk * __ldg(a.c.ap + r);
-                    cc = (is00 && r == 0) ? 0.0 : rk * __ldg(a.c.cp + r);
-                    bb = rk * (lamp + __ldg(dgp + r));
-                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
-            };
-            warp_partition_solve<K, 1>(cf, ph, ln);
-        }
-        // ---- projection of u*, v*, w* in place in the tiles
-        {
-            const double2 GX = __ldg(a.c.gx + l), GY = __ldg(a.c.gy + m);
-            const double cpr = rk * dt;
-            const double2 nxt0 = shfl_dn2(ph[0][0], 1);
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                const int r = r0 + i;
-                if (r >= nz) continue;
-                const double2 pc = ph[0][i];
-                const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
-                const double2 us = SU[i * 32 + ln], vs = SV[i * 32 + ln], ws = SW[i * 32 + ln];
-                const double rdzt = __ldg(a.c.rdzt + r);
-                SU[i * 32 + ln] = zsub(us, zscale(zmul(GX, pc), cpr));
-                SV[i * 32 + ln] = zsub(vs, zscale(zmul(GY, pc), cpr));
-                SW[i * 32 + ln] = r <= nz - 2 ? make_double2(ws.x - cpr * (pu.x - pc.x) * rdzt, ws.y - cpr * (pu.y - pc.y) * rdzt)
-                                              : make_double2(0, 0);
-            }
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < K; ++i) ph[0][i] = make_double2(0, 0);
-    }
-    __syncthreads();
-    ct_store<R, K>(a.qu, TU, c0, ncol, nz);
-    ct_store<R, K>(a.qv, TV, c0, ncol, nz);
-    ct_store<R, K>(a.qw, TW, c0, ncol, nz);
-    __syncthreads();
-    // ---- psi = phi - rk_c dt nu/2 lap(phi), staged through the u tile
-    {
-        const double2 nxt0 = shfl_dn2(ph[0][0], 1);
-        const double2 prv0 = shfl_up2(ph[0][K - 1], 1);
-        if (active) {
-            const double lxy = __ldg(a.c.lx + l) + __ldg(a.c.ly + m);
-            const double cps = rk * 0.5 * dt * a.nu;
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                const int r = r0 + i;
-                if (r >= nz) continue;
-                const double2 pc = ph[0][i];
-                const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
-                const double2 pd = (r == 0) ? pc : (i > 0 ? ph[0][i - 1] : prv0);
-                const double rdzt = __ldg(a.c.rdzt + r), rdzb = __ldg(a.c.rdzb + r), rdz = __ldg(a.c.rdz + r);
-                double2 lz;
-                lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
-                lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
-                SU[i * 32 + ln] = make_double2(pc.x - cps * (lxy * pc.x + lz.x), pc.y - cps * (lxy * pc.y + lz.y));
-            }
-        }
-    }
-    __syncthreads();
-    ct_store<R, K>(a.psi, TU, c0, ncol, nz);
-}
+template <int K> __host__ __device__ constexpr int ct_stride() { return K * CT_RP + 1; }
 
 // ---------------------------------------------------------------------------
 // The partition + PCR solve on a chosen arithmetic type T (float or double):
@@ -639,10 +456,10 @@ __device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename 
 }
 
 // ---------------------------------------------------------------------------
-// k_column_fd_tile with the tiles in the storage type and the Helmholtz solves
-// in the storage precision: in the mixed-precision mode the u, v, w solves run
-// in FP32 (the (0,0) mean mode, with its forcing, and the phi Poisson solve stay
-// FP64); in FP64 mode it computes exactly what k_column_fd_tile computes.
+// The fused FD column work of k_column_fd_warp over column tiles in the storage
+// type, with the Helmholtz solves in the storage precision: in the mixed mode
+// the u, v, w solves run in FP32 (the (0,0) mean mode, with its forcing, and the
+// phi Poisson solve stay FP64); in FP64 mode everything is FP64.
 // ---------------------------------------------------------------------------
 template <int K> __host__ size_t column_tile_smem_r(size_t elem) { return (size_t)3 * CT_COLS * ct_stride<K>() * elem; }
 
@@ -677,14 +494,14 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
         for (int it = 0; it < K; ++it) {
             const int idx = threadIdx.x + it * CT_COLS * 32;
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
-            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * 32 + r / K] = v[it];
+            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * CT_RP + r / K] = v[it];
         }
     };
     auto store = [&](TT* __restrict__ q, const TT* T, int nrows) {
         for (int idx = threadIdx.x; idx < nrows * CT_COLS; idx += blockDim.x) {
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
             const long long cc = c0 + cb;
-            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * 32 + r / K];
+            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * CT_RP + r / K];
         }
     };
     load(a.qu, TU, nz);
@@ -715,7 +532,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 for (int i = 0; i < K; ++i) {
                     const int r = r0 + i;
                     if (r < nz) {
-                        const TT xu = SU[i * 32 + ln], xv = SV[i * 32 + ln];
+                        const TT xu = SU[i * CT_RP + ln], xv = SV[i * CT_RP + ln];
                         double ux = (double)xu.x;
                         if (is00 && r == 0) ux += a.bcu0;
                         if (is00 && r == nz - 1) ux += a.bcu1;
@@ -736,15 +553,15 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 warp_partition_solve_t<T, K, 2>(cf, d, ln);
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
-                    SU[i * 32 + ln] = mk2<R>((R)d[0][i].x, (R)d[0][i].y);
-                    SV[i * 32 + ln] = mk2<R>((R)d[1][i].x, (R)d[1][i].y);
+                    SU[i * CT_RP + ln] = mk2<R>((R)d[0][i].x, (R)d[0][i].y);
+                    SV[i * CT_RP + ln] = mk2<R>((R)d[1][i].x, (R)d[1][i].y);
                 }
             }
             {
                 T2 dw[1][K];
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
-                    const TT x = SW[i * 32 + ln];
+                    const TT x = SW[i * CT_RP + ln];
                     dw[0][i] = r0 + i < nz - 1 ? mk2<T>((T)x.x, (T)x.y) : mk2<T>(T(0), T(0));
                 }
                 auto cf = [&](int r, T& aa, T& bb, T& cc) {
@@ -756,7 +573,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 };
                 warp_partition_solve_t<T, K, 1>(cf, dw, ln);
 #pragma unroll
-                for (int i = 0; i < K; ++i) SW[i * 32 + ln] = mk2<R>((R)dw[0][i].x, (R)dw[0][i].y);
+                for (int i = 0; i < K; ++i) SW[i * CT_RP + ln] = mk2<R>((R)dw[0][i].x, (R)dw[0][i].y);
             }
         };
         if (is00) helmholtz(double(0)); else helmholtz(R(0));
@@ -766,15 +583,15 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
         const double rdt = 1.0 / dt;
         {
             auto ldt = [&](const TT* S, int idx) { const TT x = S[idx]; return make_double2((double)x.x, (double)x.y); };
-            const double2 wlast = ldt(SW, (K - 1) * 32 + ln);
+            const double2 wlast = ldt(SW, (K - 1) * CT_RP + ln);
             double2 wprev0 = shfl_up2(wlast, 1);
             if (ln == 0) wprev0 = make_double2(0, 0);
 #pragma unroll
             for (int i = 0; i < K; ++i) {
                 const int r = r0 + i;
                 if (r < nz) {
-                    const double2 us = ldt(SU, i * 32 + ln), vs = ldt(SV, i * 32 + ln), ws = ldt(SW, i * 32 + ln);
-                    const double2 wm = i > 0 ? ldt(SW, (i - 1) * 32 + ln) : wprev0;
+                    const double2 us = ldt(SU, i * CT_RP + ln), vs = ldt(SV, i * CT_RP + ln), ws = ldt(SW, i * CT_RP + ln);
+                    const double2 wm = i > 0 ? ldt(SW, (i - 1) * CT_RP + ln) : wprev0;
                     const double rdz = __ldg(a.c.rdz + r);
                     double2 div = zadd(zmul(DX, us), zmul(DY, vs));
                     div = zadd(div, make_double2((ws.x - wm.x) * rdz, (ws.y - wm.y) * rdz));
@@ -804,12 +621,12 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 if (r >= nz) continue;
                 const double2 pc = ph[0][i];
                 const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
-                const TT us = SU[i * 32 + ln], vs = SV[i * 32 + ln], ws = SW[i * 32 + ln];
+                const TT us = SU[i * CT_RP + ln], vs = SV[i * CT_RP + ln], ws = SW[i * CT_RP + ln];
                 const double rdzt = __ldg(a.c.rdzt + r);
                 const double2 gu = zmul(GX, pc), gv = zmul(GY, pc);
-                SU[i * 32 + ln] = mk2<R>((R)((double)us.x - cpr * gu.x), (R)((double)us.y - cpr * gu.y));
-                SV[i * 32 + ln] = mk2<R>((R)((double)vs.x - cpr * gv.x), (R)((double)vs.y - cpr * gv.y));
-                SW[i * 32 + ln] = r <= nz - 2 ? mk2<R>((R)((double)ws.x - cpr * (pu.x - pc.x) * rdzt),
+                SU[i * CT_RP + ln] = mk2<R>((R)((double)us.x - cpr * gu.x), (R)((double)us.y - cpr * gu.y));
+                SV[i * CT_RP + ln] = mk2<R>((R)((double)vs.x - cpr * gv.x), (R)((double)vs.y - cpr * gv.y));
+                SW[i * CT_RP + ln] = r <= nz - 2 ? mk2<R>((R)((double)ws.x - cpr * (pu.x - pc.x) * rdzt),
                                                        (R)((double)ws.y - cpr * (pu.y - pc.y) * rdzt))
                                               : mk2<R>(R(0), R(0));
             }
@@ -841,7 +658,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 double2 lz;
                 lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
                 lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
-                SU[i * 32 + ln] = mk2<R>((R)(pc.x - cps * (lxy * pc.x + lz.x)), (R)(pc.y - cps * (lxy * pc.y + lz.y)));
+                SU[i * CT_RP + ln] = mk2<R>((R)(pc.x - cps * (lxy * pc.x + lz.x)), (R)(pc.y - cps * (lxy * pc.y + lz.y)));
             }
         }
     }
