@@ -534,15 +534,15 @@ template <typename R, int N> static int fft_t_op(hc_handle* h, int op, const voi
             CK(cudaFuncSetAttribute(k_fft_x_c2r_t<R, N, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx));
         }
         if (N == h->g.ny && h->fft_ty) {
-            CK(cudaFuncSetAttribute(k_fft_y_t<R, N, -1, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
-            CK(cudaFuncSetAttribute(k_fft_y_t<R, N, 1, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
+            CK(cudaFuncSetAttribute(FyKernel<R, N, -1, RM>::f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
+            CK(cudaFuncSetAttribute(FyKernel<R, N, 1, RM>::f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy));
         }
         return HC_OK;
     }
     if (op == 1) k_fft_x_r2c_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
     else if (op == 2) k_fft_x_c2r_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
-    else if (op == 3) k_fft_y_t<R, N, -1, RM><<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
-    else k_fft_y_t<R, N, 1, RM><<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
+    else if (op == 3) FyKernel<R, N, -1, RM>::f<<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
+    else FyKernel<R, N, 1, RM>::f<<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
     return HC_OK;
 }
 

@@ -277,6 +277,12 @@ template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_
 {
     return (size_t)FBufs<N, RMAX>::y * FyLines<N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
 }
+// y kernels in FP32: registers sized for as many resident blocks as the shared
+// memory allows, up to 4 (64 registers a thread)
+template <typename R, int N, int RMAX> struct FyMinBlocks {
+    static constexpr int bysmem = (int)((227 * 1024) / (fft_y_smem<R, N, RMAX>() + 1024));
+    static constexpr int v = bysmem < 1 ? 1 : (bysmem > 4 ? 4 : bysmem);
+};
 
 // ---- global accessors -------------------------------------------------------
 template <typename T2, int N> struct XRowsIn {       // rows row0.., zero past the last
@@ -440,7 +446,7 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
 // one plane k; grid (ceil(nxh/TL), nz, fields)
 // ----------------------------------------------------------------------------
 template <typename R, int N, int S, int RMAX>
-__global__ void __launch_bounds__(HC_FFT_NT) k_fft_y_t(FyArgs<R> a)
+__device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a)
 {
     typedef typename V2<R>::T T2;
     constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, TL = FyLines<N>::v;
@@ -472,3 +478,19 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_y_t(FyArgs<R> a)
     // element of the tile before its barrier, and only the last pass writes it
     run_passes<R, N, S, RMAX, TL, HC_FFT_NT, true, 0>(src, dst, A, B, a.tw);
 }
+
+// FP64: the compiler's own register budget
+template <typename R, int N, int S, int RMAX>
+__global__ void __launch_bounds__(HC_FFT_NT) k_fft_y_t(FyArgs<R> a) { fft_y_tile<R, N, S, RMAX>(a); }
+// FP32: registers sized for FyMinBlocks resident blocks
+template <int N, int S, int RMAX>
+__global__ void __launch_bounds__(HC_FFT_NT, FyMinBlocks<float, N, RMAX>::v) k_fft_y_t32(FyArgs<float> a)
+{
+    fft_y_tile<float, N, S, RMAX>(a);
+}
+template <typename R, int N, int S, int RMAX> struct FyKernel {
+    static constexpr void (*f)(FyArgs<R>) = k_fft_y_t<R, N, S, RMAX>;
+};
+template <int N, int S, int RMAX> struct FyKernel<float, N, S, RMAX> {
+    static constexpr void (*f)(FyArgs<float>) = k_fft_y_t32<N, S, RMAX>;
+};

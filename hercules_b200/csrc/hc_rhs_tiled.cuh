@@ -115,8 +115,12 @@ __device__ __forceinline__ void rt_put(R* dst, const R* v)
     }
 }
 
+// blocks per SM the register budget is sized for: FP32 fits three (80 registers,
+// no spills), FP64 two
+template <typename R> struct RhsMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 3 : 2; };
+
 template <typename R, int CDS>
-__global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled(RhsTArgs<R> a)
+__global__ void __launch_bounds__(256, RhsMinBlocks<R>::v) k_rhs_momentum_tiled(RhsTArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* sm = reinterpret_cast<R*>(smem_raw);
