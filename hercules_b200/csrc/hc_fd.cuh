@@ -403,6 +403,9 @@ __device__ __forceinline__ void decode_pt(long long q, const Geo& g, int& i, int
 
 // Divergence check (screen_div_error, src/module_io.f90:85-206): per block
 // sum |div|, the signed div of largest magnitude, and a NaN flag.
+// Work units are (256 consecutive (i,j) points) x (a chunk of levels); the
+// blocks take the units in a fixed order, each thread walks its column up the
+// chunk with the loads of two levels in flight and w(k-1) carried along.
 template <typename R, int CDS>
 __global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double* part)
 {
@@ -413,22 +416,51 @@ __global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double*
     __syncthreads();
     double sm = 0.0, mx = 0.0;
     int nan = 0;
-    for (long long q = (long long)blockIdx.x * blockDim.x + tid; q < g.n; q += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        decode_pt(q, g, i, j, k);
-        const double uc = (double)f.u[q], vc = (double)f.v[q], wc = (double)f.w[q];
-        double ux[4], vy[4];
-        ux[1] = uc; vy[1] = vc;
-        ux[2] = (double)ldf(f.u, g, i - 1, j, k); vy[2] = (double)ldf(f.v, g, i, j - 1, k);
-        if (CDS == 2) {
-            ux[0] = (double)ldf(f.u, g, i + 1, j, k); ux[3] = (double)ldf(f.u, g, i - 2, j, k);
-            vy[0] = (double)ldf(f.v, g, i, j + 1, k); vy[3] = (double)ldf(f.v, g, i, j - 2, k);
+    const long long ncb = (g.nxy + 255) / 256;
+    long long nch = (2LL * gridDim.x + ncb - 1) / ncb;
+    if (nch > g.nz) nch = g.nz;
+    const int kc = (int)((g.nz + nch - 1) / nch);
+    for (long long un = blockIdx.x; un < ncb * nch; un += gridDim.x) {
+        const long long cb = un % ncb;
+        const int k0 = (int)(un / ncb) * kc, k1 = min(g.nz, k0 + kc);
+        const long long ij = cb * 256 + tid;
+        if (ij >= g.nxy || k0 >= k1) continue;
+        const int j = (int)(ij / g.nx), i = (int)(ij - (long long)j * g.nx);
+        const int xp1 = wrapi(i + 1, g.nx) - i, xm1 = wrapi(i - 1, g.nx) - i, xm2 = wrapi(i - 2, g.nx) - i;
+        const long long yp1 = (long long)(wrapi(j + 1, g.ny) - j) * g.nx, ym1 = (long long)(wrapi(j - 1, g.ny) - j) * g.nx;
+        const long long ym2 = (long long)(wrapi(j - 2, g.ny) - j) * g.nx;
+        double wm = k0 > 0 ? (double)f.w[(long long)(k0 - 1) * g.nxy + ij] : 0.0;
+        for (int kb = k0; kb < k1; kb += 2) {
+            double ux[2][4], vy[2][4], wc[2];
+            bool in[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                in[e] = kb + e < k1;
+                const long long q = (long long)(in[e] ? kb + e : kb) * g.nxy + ij;
+                ux[e][1] = (double)f.u[q]; ux[e][2] = (double)f.u[q + xm1];
+                vy[e][1] = (double)f.v[q]; vy[e][2] = (double)f.v[q + ym1];
+                if (CDS == 2) {
+                    ux[e][0] = (double)f.u[q + xp1]; ux[e][3] = (double)f.u[q + xm2];
+                    vy[e][0] = (double)f.v[q + yp1]; vy[e][3] = (double)f.v[q + ym2];
+                } else {
+                    ux[e][0] = ux[e][3] = vy[e][0] = vy[e][3] = 0.0;
+                }
+                wc[e] = (double)f.w[q];
+            }
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                if (!in[e]) continue;
+                const double w_below = e == 0 ? wm : wc[0];
+                const double d = fd_div_point<CDS>(ux[e], vy[e], wc[e], w_below, g.dx, g.dy, ldz(g.z.dz, kb + e));
+                if (ux[e][1] != ux[e][1] || vy[e][1] != vy[e][1] || wc[e] != wc[e] || d != d) {
+                    nan = 1;
+                } else {
+                    sm += fabs(d);
+                    mx = absmax_pick(mx, d);
+                }
+            }
+            wm = wc[1];
         }
-        const double wm = k > 0 ? (double)f.w[q - g.nxy] : 0.0;
-        const double d = fd_div_point<CDS>(ux, vy, wc, wm, g.dx, g.dy, ldz(g.z.dz, k));
-        if (uc != uc || vc != vc || wc != wc || d != d) { nan = 1; continue; }
-        sm += fabs(d);
-        mx = absmax_pick(mx, d);
     }
     if (nan) s_nan = 1;
     sm = warp_sum(sm);
