@@ -512,8 +512,11 @@ static __global__ void k_mean_combine(double* __restrict__ dst, const double* __
 // A thread walks its (i,j) column through a chunk of levels, G levels at a time:
 // every load of a group (fields, then accumulators) is issued before its first
 // store, so the read-modify-writes of consecutive levels overlap in flight.
+// FP32 storage: registers sized for three resident blocks
+template <typename R> struct StatsMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 3 : 2; };
+
 template <typename R>
-__global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
+__global__ void __launch_bounds__(256, StatsMinBlocks<R>::v) k_stats(StatsArgs<R> s)
 {
     // blockIdx.x: 256 consecutive (i,j) points of a plane; blockIdx.y: a chunk of levels
     constexpr int G = 2;
@@ -534,48 +537,51 @@ __global__ void __launch_bounds__(256) k_stats(StatsArgs<R> s)
         const bool fold = sizeof(R) == sizeof(float) && s.accumulate && (*s.step % s.window) == 0;
         double wm = k0 > 0 ? (double)fw[(long long)(k0 - 1) * g.nxy + ij] : 0.0;
         for (int kb = k0; kb < k1; kb += G) {
-            double u[G], v[G], w[G], t[G], ux[G], vy[G];
+            // the fields stay in the storage type in registers; products in FP64
+            R u[G], v[G], w[G], t[G], ux[G], vy[G];
             bool in[G];
 #pragma unroll
             for (int e = 0; e < G; ++e) {
                 in[e] = kb + e < k1;
                 const long long q = (long long)(in[e] ? kb + e : kb) * g.nxy + ij;
-                u[e] = (double)fu[q]; v[e] = (double)fv[q]; w[e] = (double)fw[q];
+                u[e] = fu[q]; v[e] = fv[q]; w[e] = fw[q];
                 if (s.accumulate) {
-                    t[e] = (double)ft[q];
-                    ux[e] = fux ? (double)fux[q] : u[e];
-                    vy[e] = fvy ? (double)fvy[q] : v[e];
+                    t[e] = ft[q];
+                    ux[e] = fux ? fux[q] : u[e];
+                    vy[e] = fvy ? fvy[q] : v[e];
                 } else {
-                    t[e] = 0.0; ux[e] = 0.0; vy[e] = 0.0;
+                    t[e] = R(0); ux[e] = R(0); vy[e] = R(0);
                 }
             }
             double wp[G];                   // w one level below each of the group's levels
 #pragma unroll
             for (int e = 0; e < G; ++e) {
-                wp[e] = e == 0 ? wm : w[e - 1];
+                wp[e] = e == 0 ? wm : (double)w[e - 1];
                 const double dzk = ldz(g.z.dz, in[e] ? kb + e : kb);
                 if (in[e]) {
-                    ub += u[e] * dzk;
-                    cfl = fmax(cfl, s.dt * fabs(u[e]) * rdx + s.dt * fabs(v[e]) * rdy + s.dt * fabs(w[e]) / dzk);
+                    const double ue = u[e];
+                    ub += ue * dzk;
+                    cfl = fmax(cfl, s.dt * fabs(ue) * rdx + s.dt * fabs((double)v[e]) * rdy + s.dt * fabs((double)w[e]) / dzk);
                 }
             }
             wm = w[G - 1];
             if (!s.accumulate) continue;
             // this step's product a at level kb + e
             auto c = [&](int a, int e) -> double {
-                const double wc = 0.5 * (w[e] + wp[e]);
+                const double U = u[e], V = v[e], Wc = w[e], T = t[e];
+                const double wc = 0.5 * (Wc + wp[e]);
                 switch (a) {
-                case 0: return u[e] + um;
-                case 1: return v[e];
-                case 2: return w[e];
-                case 3: return t[e];
-                case 4: return (u[e] + um) * (u[e] + um);
-                case 5: return v[e] * v[e];
-                case 6: return w[e] * w[e];
-                case 7: return wc * (ux[e] + um);
-                case 8: return wc * vy[e];
-                case 9: return t[e] * t[e];
-                default: return t[e] * 0.5 * (w[e] + wp[e]);
+                case 0: return U + um;
+                case 1: return V;
+                case 2: return Wc;
+                case 3: return T;
+                case 4: return (U + um) * (U + um);
+                case 5: return V * V;
+                case 6: return Wc * Wc;
+                case 7: return wc * ((double)ux[e] + um);
+                case 8: return wc * (double)vy[e];
+                case 9: return T * T;
+                default: return T * 0.5 * (Wc + wp[e]);
                 }
             };
             if (sizeof(R) == sizeof(double)) {
