@@ -21,6 +21,7 @@
 #include "hc_fft_t.cuh"
 #include "hc_column.cuh"
 #include "hc_rhs_tiled.cuh"
+#include "hc_rhs_tiled2.cuh"
 #include "hc_column_warp.cuh"
 #include "hc_spec.cuh"
 #include "hc_adjoint.cuh"
@@ -649,6 +650,10 @@ template <typename R> static int set_smem_attrs()
     }
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
+    if (sizeof(R) == sizeof(float)) {
+        CK(cudaFuncSetAttribute(k_rhs_momentum_tiled2<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled2_smem(1)));
+        CK(cudaFuncSetAttribute(k_rhs_momentum_tiled2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled2_smem(1)));
+    }
     return HC_OK;
 }
 
@@ -954,7 +959,10 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     m.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
     m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
     prof_begin(h, K_RHS_MOM);
-    k_rhs_momentum_tiled<R, CDS><<<h->rhs_grid, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
+    if (sizeof(R) == sizeof(float))      // FP32: two x points a thread (64 x 8 tiles)
+        k_rhs_momentum_tiled2<CDS><<<h->rhs_grid, 256, rhs_tiled2_smem(m.with_t), h->st>>>(*(const RhsTArgs<float>*)&m);
+    else
+        k_rhs_momentum_tiled<R, CDS><<<h->rhs_grid, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
     CKL();
     }
 
@@ -1786,7 +1794,8 @@ int hc_create(const hc_params* p, hc_handle** out)
         if (h->nbd > RED_BLOCKS) h->nbd = RED_BLOCKS;
         {
             // momentum RHS tiles: enough blocks for ~4 per SM, chunks of 4..32 levels
-            const int bx = (g.nx + RT_TX - 1) / RT_TX, by = (g.ny + RT_TY - 1) / RT_TY;
+            const int tx_pts = h->rsz == sizeof(float) ? R2_TX : RT_TX;
+            const int bx = (g.nx + tx_pts - 1) / tx_pts, by = (g.ny + RT_TY - 1) / RT_TY;
             int kc = p->tile[2] > 0 ? p->tile[2] : (int)((long long)bx * by * p->nz / (4LL * 148));
             if (p->tile[2] <= 0) { if (kc < 4) kc = 4; if (kc > 32) kc = 32; }
             if (kc < 1) kc = 1;
