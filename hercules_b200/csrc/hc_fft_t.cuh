@@ -396,15 +396,30 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
         return mk2<R>(s.x - d.y, s.y + d.x);                   // s + i d
     };
     if constexpr (sizeof(R) == 8) {
-        // FP64: one thread per mode, the partner read again (measured faster here)
-        for (int idx = threadIdx.x; idx < L * N; idx += HC_FFT_NT) {
-            const int line = idx / N, l = idx - line * N;
-            T2 x = mk2<R>(R(0), R(0)), y = x;
-            if (line < nr) {
-                x = in[(long long)line * N + l];
-                if (l != 0) y = in[(long long)line * N + N - l];
+        // FP64: one thread per mode, the partner read again; the loads of four
+        // modes are issued before any of them is split
+        constexpr int IT = (L * N + HC_FFT_NT - 1) / HC_FFT_NT;
+#pragma unroll
+        for (int q0 = 0; q0 < IT; q0 += 4) {
+            T2 xs[4], ys[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int idx = threadIdx.x + (q0 + q) * HC_FFT_NT;
+                const int line = idx / N, l = idx - line * N;
+                xs[q] = mk2<R>(R(0), R(0));
+                ys[q] = xs[q];
+                if (q0 + q < IT && idx < L * N && line < nr) {
+                    xs[q] = in[(long long)line * N + l];
+                    if (l != 0) ys[q] = in[(long long)line * N + N - l];
+                }
             }
-            Zs[line * LS + fpi<G>(l)] = zsplit(x, y, l);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int idx = threadIdx.x + (q0 + q) * HC_FFT_NT;
+                if (q0 + q >= IT || idx >= L * N) break;
+                const int line = idx / N, l = idx - line * N;
+                Zs[line * LS + fpi<G>(l)] = zsplit(xs[q], ys[q], l);
+            }
         }
         __syncthreads();
         const SmemIO<T2, LS, G> src64{Zs};
