@@ -461,7 +461,11 @@ __device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename 
 // the u, v, w solves run in FP32 (the (0,0) mean mode, with its forcing, and the
 // phi Poisson solve stay FP64); in FP64 mode everything is FP64.
 // ---------------------------------------------------------------------------
-template <int K> __host__ size_t column_tile_smem_r(size_t elem) { return (size_t)3 * CT_COLS * ct_stride<K>() * elem; }
+// FP32 storage adds six per-level coefficient tables (u and w Helmholtz rows)
+template <int K> __host__ size_t column_tile_smem_r(size_t elem)
+{
+    return (size_t)3 * CT_COLS * ct_stride<K>() * elem + (elem == sizeof(float2) ? (size_t)6 * K * 32 * sizeof(float) : 0);
+}
 
 template <typename R, int K>
 __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R> a)
@@ -507,6 +511,23 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     load(a.qu, TU, nz);
     load(a.qv, TV, nz);
     load(a.qw, TW, nz - 1);
+    // FP32 storage: the per-level Helmholtz coefficients of the rk_c of this
+    // sub-step in FP32 (sub, super, and the diagonal without its -rk lam part),
+    // computed once per block instead of per row and lane
+    float* HT = reinterpret_cast<float*>(TW + CT_COLS * STR);
+    if constexpr (sizeof(R) == sizeof(float)) {
+        const double rkc = a.rk_c;
+        for (int r = threadIdx.x; r < nz; r += blockDim.x) {
+            HT[r] = (float)(rkc * __ldg(a.c.au + r));
+            HT[K * 32 + r] = (float)(rkc * __ldg(a.c.cu + r));
+            HT[2 * K * 32 + r] = (float)(1.0 + rkc * __ldg(a.c.dgu + r));
+            if (r < nz - 1) {
+                HT[3 * K * 32 + r] = (float)(rkc * __ldg(a.c.aw + r));
+                HT[4 * K * 32 + r] = (float)(rkc * __ldg(a.c.cw + r));
+                HT[5 * K * 32 + r] = (float)(1.0 + rkc * __ldg(a.c.dgw + r));
+            }
+        }
+    }
     __syncthreads();
     TT* SU = TU + wp * STR;
     TT* SV = TV + wp * STR;
@@ -543,11 +564,16 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                         d[1][i] = mk2<T>(T(0), T(0));
                     }
                 }
+                const float rlam = (float)(rk * lam);
                 auto cf = [&](int r, T& aa, T& bb, T& cc) {
                     if (r < nz) {
-                        aa = (T)(rk * __ldg(a.c.au + r));
-                        cc = (T)(rk * __ldg(a.c.cu + r));
-                        bb = (T)(1.0 + rk * (-lam + __ldg(dgu + r)));
+                        if constexpr (sizeof(T) == sizeof(float)) {
+                            aa = HT[r]; cc = HT[K * 32 + r]; bb = HT[2 * K * 32 + r] - rlam;
+                        } else {
+                            aa = (T)(rk * __ldg(a.c.au + r));
+                            cc = (T)(rk * __ldg(a.c.cu + r));
+                            bb = (T)(1.0 + rk * (-lam + __ldg(dgu + r)));
+                        }
                     } else { aa = T(0); bb = T(1); cc = T(0); }
                 };
                 warp_partition_solve_t<T, K, 2>(cf, d, ln);
@@ -564,11 +590,16 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                     const TT x = SW[i * CT_RP + ln];
                     dw[0][i] = r0 + i < nz - 1 ? mk2<T>((T)x.x, (T)x.y) : mk2<T>(T(0), T(0));
                 }
+                const float rlam = (float)(rk * lam);
                 auto cf = [&](int r, T& aa, T& bb, T& cc) {
                     if (r < nz - 1) {
-                        aa = (T)(rk * __ldg(a.c.aw + r));
-                        cc = (T)(rk * __ldg(a.c.cw + r));
-                        bb = (T)(1.0 + rk * (-lam + __ldg(dgw + r)));
+                        if constexpr (sizeof(T) == sizeof(float)) {
+                            aa = HT[3 * K * 32 + r]; cc = HT[4 * K * 32 + r]; bb = HT[5 * K * 32 + r] - rlam;
+                        } else {
+                            aa = (T)(rk * __ldg(a.c.aw + r));
+                            cc = (T)(rk * __ldg(a.c.cw + r));
+                            bb = (T)(1.0 + rk * (-lam + __ldg(dgw + r)));
+                        }
                     } else { aa = T(0); bb = T(1); cc = T(0); }
                 };
                 warp_partition_solve_t<T, K, 1>(cf, dw, ln);
