@@ -461,10 +461,14 @@ __device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename 
 // the u, v, w solves run in FP32 (the (0,0) mean mode, with its forcing, and the
 // phi Poisson solve stay FP64); in FP64 mode everything is FP64.
 // ---------------------------------------------------------------------------
-// FP32 storage adds six per-level coefficient tables (u and w Helmholtz rows)
+// FP32 storage: per-level tables after the tiles, six FP32 ones (u and w
+// Helmholtz rows) and six FP64 ones (Poisson rows, 1/dz, 1/dz_t, 1/dz_b). FP64
+// storage reads those coefficients through the read-only cache (its tiles
+// already fill the shared memory of two blocks).
 template <int K> __host__ size_t column_tile_smem_r(size_t elem)
 {
-    return (size_t)3 * CT_COLS * ct_stride<K>() * elem + (elem == sizeof(float2) ? (size_t)6 * K * 32 * sizeof(float) : 0);
+    return (size_t)3 * CT_COLS * ct_stride<K>() * elem +
+           (elem == sizeof(float2) ? (size_t)6 * K * 32 * (sizeof(float) + sizeof(double)) : 0);
 }
 
 template <typename R, int K>
@@ -515,6 +519,23 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     // sub-step in FP32 (sub, super, and the diagonal without its -rk lam part),
     // computed once per block instead of per row and lane
     float* HT = reinterpret_cast<float*>(TW + CT_COLS * STR);
+    double* DT = reinterpret_cast<double*>(HT + 6 * K * 32);
+    // table q (0..5: rk ap, rk cp, rk dgp, 1/dz, 1/dz_t, 1/dz_b) at level r
+    auto dtab = [&](int q, int r) -> double {
+        if constexpr (sizeof(R) == sizeof(float)) return DT[q * K * 32 + r];
+        const double* src[6] = {a.c.ap, a.c.cp, a.c.dgp, a.c.rdz, a.c.rdzt, a.c.rdzb};
+        return q < 3 ? a.rk_c * __ldg(src[q] + r) : __ldg(src[q] + r);
+    };
+    if constexpr (sizeof(R) == sizeof(float)) {
+        for (int r = threadIdx.x; r < nz; r += blockDim.x) {
+            DT[r] = a.rk_c * __ldg(a.c.ap + r);
+            DT[K * 32 + r] = a.rk_c * __ldg(a.c.cp + r);
+            DT[2 * K * 32 + r] = a.rk_c * __ldg(a.c.dgp + r);
+            DT[3 * K * 32 + r] = __ldg(a.c.rdz + r);
+            DT[4 * K * 32 + r] = __ldg(a.c.rdzt + r);
+            DT[5 * K * 32 + r] = __ldg(a.c.rdzb + r);
+        }
+    }
     if constexpr (sizeof(R) == sizeof(float)) {
         const double rkc = a.rk_c;
         for (int r = threadIdx.x; r < nz; r += blockDim.x) {
@@ -623,7 +644,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 if (r < nz) {
                     const double2 us = ldt(SU, i * CT_RP + ln), vs = ldt(SV, i * CT_RP + ln), ws = ldt(SW, i * CT_RP + ln);
                     const double2 wm = i > 0 ? ldt(SW, (i - 1) * CT_RP + ln) : wprev0;
-                    const double rdz = __ldg(a.c.rdz + r);
+                    const double rdz = dtab(3, r);
                     double2 div = zadd(zmul(DX, us), zmul(DY, vs));
                     div = zadd(div, make_double2((ws.x - wm.x) * rdz, (ws.y - wm.y) * rdz));
                     ph[0][i] = make_double2(div.x * rdt, div.y * rdt);
@@ -634,9 +655,13 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
             }
             auto cf = [&](int r, double& aa, double& bb, double& cc) {
                 if (r < nz) {
-                    aa = rk * __ldg(a.c.ap + r);
-                    cc = (is00 && r == 0) ? 0.0 : rk * __ldg(a.c.cp + r);
-                    bb = rk * (lamp + __ldg(dgp + r));
+                    if (sizeof(R) == sizeof(float) && !is00) {
+                        aa = dtab(0, r); cc = dtab(1, r); bb = dtab(2, r) + rk * lamp;
+                    } else {
+                        aa = rk * __ldg(a.c.ap + r);
+                        cc = (is00 && r == 0) ? 0.0 : rk * __ldg(a.c.cp + r);
+                        bb = rk * (lamp + __ldg(dgp + r));
+                    }
                 } else { aa = 0.0; bb = 1.0; cc = 0.0; }
             };
             warp_partition_solve<K, 1>(cf, ph, ln);
@@ -653,7 +678,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 const double2 pc = ph[0][i];
                 const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
                 const TT us = SU[i * CT_RP + ln], vs = SV[i * CT_RP + ln], ws = SW[i * CT_RP + ln];
-                const double rdzt = __ldg(a.c.rdzt + r);
+                const double rdzt = dtab(4, r);
                 const double2 gu = zmul(GX, pc), gv = zmul(GY, pc);
                 SU[i * CT_RP + ln] = mk2<R>((R)((double)us.x - cpr * gu.x), (R)((double)us.y - cpr * gu.y));
                 SV[i * CT_RP + ln] = mk2<R>((R)((double)vs.x - cpr * gv.x), (R)((double)vs.y - cpr * gv.y));
@@ -685,7 +710,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 const double2 pc = ph[0][i];
                 const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
                 const double2 pd = (r == 0) ? pc : (i > 0 ? ph[0][i - 1] : prv0);
-                const double rdzt = __ldg(a.c.rdzt + r), rdzb = __ldg(a.c.rdzb + r), rdz = __ldg(a.c.rdz + r);
+                const double rdzt = dtab(4, r), rdzb = dtab(5, r), rdz = dtab(3, r);
                 double2 lz;
                 lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
                 lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
