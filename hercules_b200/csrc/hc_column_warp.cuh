@@ -520,32 +520,37 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     // computed once per block instead of per row and lane
     float* HT = reinterpret_cast<float*>(TW + CT_COLS * STR);
     double* DT = reinterpret_cast<double*>(HT + 6 * K * 32);
+    // tables in the tiles' [i][lane] order (row r = lane*K + i at i*32 + lane),
+    // so that the 32 lanes of a warp read 32 consecutive entries
+    auto tpos = [](int r) { return (r % K) * 32 + r / K; };
     // table q (0..5: rk ap, rk cp, rk dgp, 1/dz, 1/dz_t, 1/dz_b) at level r
     auto dtab = [&](int q, int r) -> double {
-        if constexpr (sizeof(R) == sizeof(float)) return DT[q * K * 32 + r];
+        if constexpr (sizeof(R) == sizeof(float)) return DT[q * K * 32 + tpos(r)];
         const double* src[6] = {a.c.ap, a.c.cp, a.c.dgp, a.c.rdz, a.c.rdzt, a.c.rdzb};
         return q < 3 ? a.rk_c * __ldg(src[q] + r) : __ldg(src[q] + r);
     };
     if constexpr (sizeof(R) == sizeof(float)) {
         for (int r = threadIdx.x; r < nz; r += blockDim.x) {
-            DT[r] = a.rk_c * __ldg(a.c.ap + r);
-            DT[K * 32 + r] = a.rk_c * __ldg(a.c.cp + r);
-            DT[2 * K * 32 + r] = a.rk_c * __ldg(a.c.dgp + r);
-            DT[3 * K * 32 + r] = __ldg(a.c.rdz + r);
-            DT[4 * K * 32 + r] = __ldg(a.c.rdzt + r);
-            DT[5 * K * 32 + r] = __ldg(a.c.rdzb + r);
+            const int t = tpos(r);
+            DT[t] = a.rk_c * __ldg(a.c.ap + r);
+            DT[K * 32 + t] = a.rk_c * __ldg(a.c.cp + r);
+            DT[2 * K * 32 + t] = a.rk_c * __ldg(a.c.dgp + r);
+            DT[3 * K * 32 + t] = __ldg(a.c.rdz + r);
+            DT[4 * K * 32 + t] = __ldg(a.c.rdzt + r);
+            DT[5 * K * 32 + t] = __ldg(a.c.rdzb + r);
         }
     }
     if constexpr (sizeof(R) == sizeof(float)) {
         const double rkc = a.rk_c;
         for (int r = threadIdx.x; r < nz; r += blockDim.x) {
-            HT[r] = (float)(rkc * __ldg(a.c.au + r));
-            HT[K * 32 + r] = (float)(rkc * __ldg(a.c.cu + r));
-            HT[2 * K * 32 + r] = (float)(1.0 + rkc * __ldg(a.c.dgu + r));
+            const int t = tpos(r);
+            HT[t] = (float)(rkc * __ldg(a.c.au + r));
+            HT[K * 32 + t] = (float)(rkc * __ldg(a.c.cu + r));
+            HT[2 * K * 32 + t] = (float)(1.0 + rkc * __ldg(a.c.dgu + r));
             if (r < nz - 1) {
-                HT[3 * K * 32 + r] = (float)(rkc * __ldg(a.c.aw + r));
-                HT[4 * K * 32 + r] = (float)(rkc * __ldg(a.c.cw + r));
-                HT[5 * K * 32 + r] = (float)(1.0 + rkc * __ldg(a.c.dgw + r));
+                HT[3 * K * 32 + t] = (float)(rkc * __ldg(a.c.aw + r));
+                HT[4 * K * 32 + t] = (float)(rkc * __ldg(a.c.cw + r));
+                HT[5 * K * 32 + t] = (float)(1.0 + rkc * __ldg(a.c.dgw + r));
             }
         }
     }
@@ -589,7 +594,8 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 auto cf = [&](int r, T& aa, T& bb, T& cc) {
                     if (r < nz) {
                         if constexpr (sizeof(T) == sizeof(float)) {
-                            aa = HT[r]; cc = HT[K * 32 + r]; bb = HT[2 * K * 32 + r] - rlam;
+                            const int t = tpos(r);
+                            aa = HT[t]; cc = HT[K * 32 + t]; bb = HT[2 * K * 32 + t] - rlam;
                         } else {
                             aa = (T)(rk * __ldg(a.c.au + r));
                             cc = (T)(rk * __ldg(a.c.cu + r));
@@ -615,7 +621,8 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
                 auto cf = [&](int r, T& aa, T& bb, T& cc) {
                     if (r < nz - 1) {
                         if constexpr (sizeof(T) == sizeof(float)) {
-                            aa = HT[3 * K * 32 + r]; cc = HT[4 * K * 32 + r]; bb = HT[5 * K * 32 + r] - rlam;
+                            const int t = tpos(r);
+                            aa = HT[3 * K * 32 + t]; cc = HT[4 * K * 32 + t]; bb = HT[5 * K * 32 + t] - rlam;
                         } else {
                             aa = (T)(rk * __ldg(a.c.aw + r));
                             cc = (T)(rk * __ldg(a.c.cw + r));
