@@ -416,6 +416,49 @@ __global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double*
     __syncthreads();
     double sm = 0.0, mx = 0.0;
     int nan = 0;
+    if constexpr (sizeof(R) == sizeof(float)) {
+        // FP32 storage: two x points a thread (nx is even), 8-byte loads
+        const long long ncb2 = (g.nxy + 511) / 512;
+        long long nch2 = (2LL * gridDim.x + ncb2 - 1) / ncb2;
+        if (nch2 > g.nz) nch2 = g.nz;
+        const int kc2 = (int)((g.nz + nch2 - 1) / nch2);
+        for (long long un = blockIdx.x; un < ncb2 * nch2; un += gridDim.x) {
+            const long long cb = un % ncb2;
+            const int k0 = (int)(un / ncb2) * kc2, k1 = min(g.nz, k0 + kc2);
+            const long long ij = cb * 512 + 2 * tid;
+            if (ij >= g.nxy || k0 >= k1) continue;
+            const int j = (int)(ij / g.nx), i = (int)(ij - (long long)j * g.nx);
+            const int xm2 = wrapi(i - 2, g.nx) - i, xp2 = wrapi(i + 2, g.nx) - i;
+            const long long yp1 = (long long)(wrapi(j + 1, g.ny) - j) * g.nx, ym1 = (long long)(wrapi(j - 1, g.ny) - j) * g.nx;
+            const long long ym2 = (long long)(wrapi(j - 2, g.ny) - j) * g.nx;
+            auto l2 = [](const R* p, long long q) { return *reinterpret_cast<const float2*>(p + q); };
+            float2 wm = k0 > 0 ? l2(f.w, (long long)(k0 - 1) * g.nxy + ij) : make_float2(0.0f, 0.0f);
+#pragma unroll 2
+            for (int k = k0; k < k1; ++k) {
+                const long long q = (long long)k * g.nxy + ij;
+                const float2 um2 = l2(f.u, q + xm2), u0 = l2(f.u, q), up2 = l2(f.u, q + xp2);
+                const float2 vp = l2(f.v, q + yp1), v0 = l2(f.v, q), vm = l2(f.v, q + ym1), vmm = l2(f.v, q + ym2);
+                const float2 w0 = l2(f.w, q);
+                const double dzk = ldz(g.z.dz, k);
+                // x values i-2 .. i+3 of the pair
+                const double xs[6] = {um2.x, um2.y, u0.x, u0.y, up2.x, up2.y};
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    double ux[4] = {xs[3 + s], xs[2 + s], xs[1 + s], xs[s]};
+                    double vy[4] = {s ? vp.y : vp.x, s ? v0.y : v0.x, s ? vm.y : vm.x, s ? vmm.y : vmm.x};
+                    const double wc = s ? w0.y : w0.x, wb = s ? wm.y : wm.x;
+                    const double d = fd_div_point<CDS>(ux, vy, wc, wb, g.dx, g.dy, dzk);
+                    if (ux[1] != ux[1] || vy[1] != vy[1] || wc != wc || d != d) {
+                        nan = 1;
+                    } else {
+                        sm += fabs(d);
+                        mx = absmax_pick(mx, d);
+                    }
+                }
+                wm = w0;
+            }
+        }
+    } else {
     const long long ncb = (g.nxy + 255) / 256;
     long long nch = (2LL * gridDim.x + ncb - 1) / ncb;
     if (nch > g.nz) nch = g.nz;
@@ -461,6 +504,7 @@ __global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double*
             }
             wm = wc[1];
         }
+    }
     }
     if (nan) s_nan = 1;
     sm = warp_sum(sm);
