@@ -1804,7 +1804,7 @@ int hc_create(const hc_params* p, hc_handle** out)
             h->rhs_kc = kc;
             h->rhs_grid = dim3(bx, by, (p->nz + kc - 1) / kc);
         }
-        h->stx = (g.nxy + 255) / 256;
+        h->stx = h->rsz == sizeof(float) ? (g.nxy + 511) / 512 : (g.nxy + 255) / 256;   // k_stats: FP32 pairs
         h->sty = (2 * RED_BLOCKS) / h->stx;
         if (h->sty < 1) h->sty = 1;
         if (h->sty > p->nz) h->sty = p->nz;

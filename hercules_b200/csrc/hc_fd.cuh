@@ -572,7 +572,72 @@ __global__ void __launch_bounds__(256, StatsMinBlocks<R>::v) k_stats(StatsArgs<R
     const int kc = (g.nz + gridDim.y - 1) / gridDim.y;
     const int k0 = blockIdx.y * kc, k1 = min(g.nz, k0 + kc);
     double ub = 0.0, cfl = 0.0;
-    if (ij < g.nxy) {
+    if constexpr (sizeof(R) == sizeof(float)) {
+        // FP32 storage: a thread owns two adjacent points (nxy is even), so every
+        // field and window access is an 8-byte load or store; 512 points a block
+        const long long p2 = ij * 2;
+        if (p2 < g.nxy) {
+            auto l2 = [](const float* p, long long q) { return *reinterpret_cast<const float2*>(p + q); };
+            const double um = s.um;
+            const bool fold = s.accumulate && (*s.step % s.window) == 0;
+            float2 wm = k0 > 0 ? l2(s.f.w, (long long)(k0 - 1) * g.nxy + p2) : make_float2(0.0f, 0.0f);
+#pragma unroll 2
+            for (int k = k0; k < k1; ++k) {
+                const long long q = (long long)k * g.nxy + p2;
+                const float2 u = l2(s.f.u, q), v = l2(s.f.v, q), w = l2(s.f.w, q);
+                const double dzk = ldz(g.z.dz, k);
+                ub += (double)u.x * dzk;
+                cfl = fmax(cfl, s.dt * fabs((double)u.x) * rdx + s.dt * fabs((double)v.x) * rdy + s.dt * fabs((double)w.x) / dzk);
+                ub += (double)u.y * dzk;
+                cfl = fmax(cfl, s.dt * fabs((double)u.y) * rdx + s.dt * fabs((double)v.y) * rdy + s.dt * fabs((double)w.y) / dzk);
+                if (s.accumulate) {
+                    const float2 t = l2(s.f.t, q);
+                    const float2 ux = s.uhx_s ? l2(s.uhx_s, q) : u;
+                    const float2 vy = s.vhy_s ? l2(s.vhy_s, q) : v;
+                    auto c = [&](int a, int e) -> double {
+                        const double U = e ? u.y : u.x, V = e ? v.y : v.x, Wc = e ? w.y : w.x, T = e ? t.y : t.x;
+                        const double WP = e ? wm.y : wm.x;
+                        const double wc = 0.5 * (Wc + WP);
+                        switch (a) {
+                        case 0: return U + um;
+                        case 1: return V;
+                        case 2: return Wc;
+                        case 3: return T;
+                        case 4: return (U + um) * (U + um);
+                        case 5: return V * V;
+                        case 6: return Wc * Wc;
+                        case 7: return wc * ((double)(e ? ux.y : ux.x) + um);
+                        case 8: return wc * (double)(e ? vy.y : vy.x);
+                        case 9: return T * T;
+                        default: return T * 0.5 * (Wc + WP);
+                        }
+                    };
+                    if (!fold) {
+                        float2 m[11];
+#pragma unroll
+                        for (int a = 0; a < 11; ++a) m[a] = l2(s.win[a], q);
+#pragma unroll
+                        for (int a = 0; a < 11; ++a)
+                            *reinterpret_cast<float2*>(s.win[a] + q) =
+                                make_float2((float)((double)m[a].x + c(a, 0)), (float)((double)m[a].y + c(a, 1)));
+                    } else {
+                        // end of a window: FP64 sum += window + this step, the window restarts at 0
+#pragma unroll
+                        for (int a = 0; a < 11; ++a) {
+                            double2* mp = reinterpret_cast<double2*>(s.mean[a] + q);
+                            const float2 wv = l2(s.win[a], q);
+                            double2 mv = *mp;
+                            mv.x += (double)wv.x + c(a, 0);
+                            mv.y += (double)wv.y + c(a, 1);
+                            *mp = mv;
+                            *reinterpret_cast<float2*>(s.win[a] + q) = make_float2(0.0f, 0.0f);
+                        }
+                    }
+                }
+                wm = w;
+            }
+        }
+    } else if (ij < g.nxy) {
         const R* __restrict__ fu = s.f.u; const R* __restrict__ fv = s.f.v;
         const R* __restrict__ fw = s.f.w; const R* __restrict__ ft = s.f.t;
         const R* __restrict__ fux = s.uhx_s; const R* __restrict__ fvy = s.vhy_s;
