@@ -1887,6 +1887,30 @@ static void* field_dev(hc_handle* h, int id, int* is_mean)
     return nullptr;
 }
 
+// Device staging buffer of n doubles (shared with the mean-field download)
+static double* staging(hc_handle* h)
+{
+    if (!h->mtmp && cudaMalloc((void**)&h->mtmp, h->g.n * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return h->mtmp;
+}
+
+static __global__ void k_double_to_float(float* __restrict__ dst, const double* __restrict__ src, long long n)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (float)src[q];
+}
+static __global__ void k_float_to_double(double* __restrict__ dst, const float* __restrict__ src, long long n)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = (double)src[q];
+}
+
+// An interior-only host array (ghost 0, leading dimensions nx, ny) is copied as
+// it is -- straight from the caller's memory, pinned or not -- and converted to
+// the storage type on the device; ghosted arrays are packed on the host first.
 int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, int ghost)
 {
     if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
@@ -1897,18 +1921,30 @@ int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, 
     if (!d) return HC_ERR_ARG;
     const int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
     const long long n = (long long)nx * ny * nz;
-    std::vector<double> tmp(n);
-    for (int k = 0; k < nz; ++k)
-        for (int j = 0; j < ny; ++j)
-            memcpy(&tmp[((long long)k * ny + j) * nx], host + (size_t)ghost + (size_t)ld1 * ((size_t)(j + ghost) + (size_t)ld2 * (size_t)(k + ghost)), nx * sizeof(double));
-    if (is_mean || h->rsz == sizeof(double)) {
-        CK(cudaMemcpy(d, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-        if (is_mean && h->win[0]) CK(cudaMemset(h->win[field_id - HC_FIELD_MEAN_U], 0, n * sizeof(float)));
-    } else {
-        std::vector<float> tf(n);
-        for (long long q = 0; q < n; ++q) tf[q] = (float)tmp[q];
-        CK(cudaMemcpy(d, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    const bool contiguous = ghost == 0 && ld1 == nx && ld2 == ny;
+    std::vector<double> tmp;
+    const double* src = host;
+    if (!contiguous) {
+        tmp.resize(n);
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                memcpy(&tmp[((long long)k * ny + j) * nx], host + (size_t)ghost + (size_t)ld1 * ((size_t)(j + ghost) + (size_t)ld2 * (size_t)(k + ghost)), nx * sizeof(double));
+        src = tmp.data();
     }
+    CK(cudaStreamSynchronize(h->st));
+    // every copy and conversion on the handle's stream: a synchronous copy from
+    // pageable memory may return before its transfer has landed
+    if (is_mean || h->rsz == sizeof(double)) {
+        CK(cudaMemcpyAsync(d, src, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        if (is_mean && h->win[0]) CK(cudaMemsetAsync(h->win[field_id - HC_FIELD_MEAN_U], 0, n * sizeof(float), h->st));
+    } else {
+        double* st = staging(h);
+        if (!st) return HC_ERR_NOMEM;
+        CK(cudaMemcpyAsync(st, src, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        k_double_to_float<<<RED_BLOCKS, 256, 0, h->st>>>((float*)d, st, n);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(h->st));
     return HC_OK;
 }
 
@@ -1964,17 +2000,24 @@ int hc_download(hc_handle* h, int field_id, double* host, int ld1, int ld2, int 
     int is_mean, rc;
     void* d = download_source(h, field_id, &is_mean, &rc);
     if (!d) return rc;
-    CK(cudaStreamSynchronize(h->st));
     const int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
     const long long n = (long long)nx * ny * nz;
-    std::vector<double> tmp(n);
-    if (is_mean || h->rsz == sizeof(double)) {
-        CK(cudaMemcpy(tmp.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost));
-    } else {
-        std::vector<float> tf(n);
-        CK(cudaMemcpy(tf.data(), d, n * sizeof(float), cudaMemcpyDeviceToHost));
-        for (long long q = 0; q < n; ++q) tmp[q] = tf[q];
+    const double* src = (const double*)d;
+    if (!is_mean && h->rsz == sizeof(float)) {
+        double* st = staging(h);
+        if (!st) return HC_ERR_NOMEM;
+        k_float_to_double<<<RED_BLOCKS, 256, 0, h->st>>>(st, (const float*)d, n);
+        CK(cudaGetLastError());
+        src = st;
     }
+    if (ghost == 0 && ld1 == nx && ld2 == ny) {
+        CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        return HC_OK;
+    }
+    std::vector<double> tmp(n);
+    CK(cudaMemcpyAsync(tmp.data(), src, n * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
     for (int k = 0; k < nz; ++k)
         for (int j = 0; j < ny; ++j)
             memcpy(host + (size_t)ghost + (size_t)ld1 * ((size_t)(j + ghost) + (size_t)ld2 * (size_t)(k + ghost)), &tmp[((long long)k * ny + j) * nx], nx * sizeof(double));
