@@ -141,8 +141,15 @@ class Channel:
         for k, v in fields.items():
             self.upload(k, v)
 
-    def download(self, name: str, ghost: int = 0) -> np.ndarray:
-        a = np.zeros(self._shape(ghost), dtype=np.float64)
+    def download(self, name: str, ghost: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The field as a float64 array; `out` (C-contiguous float64 of the right
+        shape, e.g. in pinned memory) is filled instead of a new array."""
+        if out is not None:
+            if out.shape != self._shape(ghost) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"download({name}): out must be C-contiguous float64 of shape {self._shape(ghost)}")
+            a = out
+        else:
+            a = np.zeros(self._shape(ghost), dtype=np.float64)
         _check(self._L.hc_download(self.h, FIELD_IDS[name], a.ctypes.data,
                                    a.shape[2], a.shape[1], ghost), f"hc_download({name})")
         return a
