@@ -465,10 +465,13 @@ __device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename 
 // Helmholtz rows) and six FP64 ones (Poisson rows, 1/dz, 1/dz_t, 1/dz_b). FP64
 // storage reads those coefficients through the read-only cache (its tiles
 // already fill the shared memory of two blocks).
+// the three tiles; FP32 storage: the level tables and 16 wavenumber constants
+// of each column
 template <int K> __host__ size_t column_tile_smem_r(size_t elem)
 {
     return (size_t)3 * CT_COLS * ct_stride<K>() * elem +
-           (elem == sizeof(float2) ? (size_t)6 * K * 32 * (sizeof(float) + sizeof(double)) : 0);
+           (elem == sizeof(float2) ? (size_t)6 * K * 32 * (sizeof(float) + sizeof(double)) +
+                                         (size_t)CT_COLS * 16 * sizeof(double) : 0);
 }
 
 template <typename R, int K>
@@ -487,6 +490,38 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     TT* TU = reinterpret_cast<TT*>(smem_raw);
     TT* TV = TU + CT_COLS * STR;
     TT* TW = TV + CT_COLS * STR;
+    // FP32 storage: the per-level tables follow the tiles
+    float* HT = reinterpret_cast<float*>(TW + CT_COLS * STR);
+    double* DT = reinterpret_cast<double*>(HT + 6 * K * 32);
+    // FP32 storage: 16 wavenumber constants of each column (hx, hy, px, py, the
+    // divergence and gradient symbols, lx, ly), loaded together with the tiles so
+    // that no warp waits on them later: entry q of column cb at CW[cb * 16 + q]
+    // (904 -> 884 us a launch at 512 x 384 x 256). With FP64 storage the same
+    // staging was slower (1613 -> 1680 us): there the warps load them when needed.
+    constexpr bool kCW = sizeof(R) == sizeof(float);
+    double* CW = DT + 6 * K * 32;
+    double cwv = 0.0;
+    if (kCW) {
+        const int cq = threadIdx.x & 15, cb = threadIdx.x >> 4;
+        const long long cc = c0 + cb;
+        if (cb < CT_COLS && cc < ncol && cq < 14) {
+            const int l = (int)(cc % a.g.nxh), m = (int)(cc / a.g.nxh);
+            const double* q2l = nullptr;
+            switch (cq) {
+            case 0: q2l = a.c.hx + l; break;
+            case 1: q2l = a.c.hy + m; break;
+            case 2: q2l = a.c.px + l; break;
+            case 3: q2l = a.c.py + m; break;
+            case 4: case 5: q2l = reinterpret_cast<const double*>(a.c.dx + l) + (cq - 4); break;
+            case 6: case 7: q2l = reinterpret_cast<const double*>(a.c.dy + m) + (cq - 6); break;
+            case 8: case 9: q2l = reinterpret_cast<const double*>(a.c.gx + l) + (cq - 8); break;
+            case 10: case 11: q2l = reinterpret_cast<const double*>(a.c.gy + m) + (cq - 10); break;
+            case 12: q2l = a.c.lx + l; break;
+            default: q2l = a.c.ly + m; break;
+            }
+            cwv = __ldg(q2l);
+        }
+    }
     // nrows * CT_COLS <= 32 K * CT_COLS = K * blockDim: at most K elements per
     // thread, all loads issued before the first shared-memory store
     auto load = [&](const TT* __restrict__ q, TT* T, int nrows) {
@@ -515,12 +550,10 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     load(a.qu, TU, nz);
     load(a.qv, TV, nz);
     load(a.qw, TW, nz - 1);
+    if (kCW && (threadIdx.x >> 4) < CT_COLS) CW[threadIdx.x] = cwv;
     // FP32 storage: the per-level Helmholtz coefficients of the rk_c of this
     // sub-step in FP32 (sub, super, and the diagonal without its -rk lam part),
-    // computed once per block instead of per row and lane
-    float* HT = reinterpret_cast<float*>(TW + CT_COLS * STR);
-    double* DT = reinterpret_cast<double*>(HT + 6 * K * 32);
-    // tables in the tiles' [i][lane] order (row r = lane*K + i at i*32 + lane),
+    // computed once per block instead of per row and lane; tables in the tiles' [i][lane] order (row r = lane*K + i at i*32 + lane),
     // so that the 32 lanes of a warp read 32 consecutive entries
     auto tpos = [](int r) { return (r % K) * 32 + r / K; };
     // table q (0..5: rk ap, rk cp, rk dgp, 1/dz, 1/dz_t, 1/dz_b) at level r
@@ -562,10 +595,11 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     const bool is00 = (c == 0);
     const double rk = a.rk_c, dt = a.dt;
     const int r0 = ln * K;
+    const double* cw = CW + wp * 16;
     double2 ph[1][K];
     if (active) {
-        const double lam = __ldg(a.c.hx + l) + __ldg(a.c.hy + m);
-        const double lamp = __ldg(a.c.px + l) + __ldg(a.c.py + m);
+        const double lam = kCW ? cw[0] + cw[1] : __ldg(a.c.hx + l) + __ldg(a.c.hy + m);
+        const double lamp = kCW ? cw[2] + cw[3] : __ldg(a.c.px + l) + __ldg(a.c.py + m);
         const double* dgp = is00 ? a.c.d0p : a.c.dgp;
         // ---- u*, v* (one matrix, two right-hand sides) and w*, in the type T
         auto helmholtz = [&](auto tag) {
@@ -638,7 +672,8 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
         if (is00) helmholtz(double(0)); else helmholtz(R(0));
         __syncwarp();
         // ---- phi: source div(u*)/dt, Poisson with the null-space pin on (0,0), FP64
-        const double2 DX = __ldg(a.c.dx + l), DY = __ldg(a.c.dy + m);
+        const double2 DX = kCW ? make_double2(cw[4], cw[5]) : __ldg(a.c.dx + l);
+        const double2 DY = kCW ? make_double2(cw[6], cw[7]) : __ldg(a.c.dy + m);
         const double rdt = 1.0 / dt;
         {
             auto ldt = [&](const TT* S, int idx) { const TT x = S[idx]; return make_double2((double)x.x, (double)x.y); };
@@ -675,7 +710,8 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
         }
         // ---- projection of u*, v*, w* in place in the tiles
         {
-            const double2 GX = __ldg(a.c.gx + l), GY = __ldg(a.c.gy + m);
+            const double2 GX = kCW ? make_double2(cw[8], cw[9]) : __ldg(a.c.gx + l);
+            const double2 GY = kCW ? make_double2(cw[10], cw[11]) : __ldg(a.c.gy + m);
             const double cpr = rk * dt;
             const double2 nxt0 = shfl_dn2(ph[0][0], 1);
 #pragma unroll
@@ -708,7 +744,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
         const double2 nxt0 = shfl_dn2(ph[0][0], 1);
         const double2 prv0 = shfl_up2(ph[0][K - 1], 1);
         if (active) {
-            const double lxy = __ldg(a.c.lx + l) + __ldg(a.c.ly + m);
+            const double lxy = kCW ? cw[12] + cw[13] : __ldg(a.c.lx + l) + __ldg(a.c.ly + m);
             const double cps = rk * 0.5 * dt * a.nu;
 #pragma unroll
             for (int i = 0; i < K; ++i) {

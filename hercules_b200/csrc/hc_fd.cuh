@@ -406,8 +406,12 @@ __device__ __forceinline__ void decode_pt(long long q, const Geo& g, int& i, int
 // Work units are (256 consecutive (i,j) points) x (a chunk of levels); the
 // blocks take the units in a fixed order, each thread walks its column up the
 // chunk with the loads of two levels in flight and w(k-1) carried along.
+// registers sized for four resident blocks with FP32 storage, three with FP64
+// (at 512 x 384 x 256: 315 -> 239 us and 361 -> 309 us a launch; with the
+// compiler's own budget too few warps had their loads in flight)
+template <typename R> struct DivMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 4 : 3; };
 template <typename R, int CDS>
-__global__ void __launch_bounds__(256) k_div_check(FieldsIn<R> f, Geo g, double* part)
+__global__ void __launch_bounds__(256, DivMinBlocks<R>::v) k_div_check(FieldsIn<R> f, Geo g, double* part)
 {
     __shared__ double s_sum[8], s_max[8];
     __shared__ int s_nan;

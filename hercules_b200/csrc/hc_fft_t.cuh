@@ -28,8 +28,9 @@ __host__ __device__ constexpr int fft_log2(int r) { return r <= 1 ? 0 : 1 + fft_
 // Passes: the power-of-two part in passes of at most RMAX points, as evenly as
 // possible; one factor 3 folded with 8 or 4 of them into a radix-24 / radix-12
 // pass (so 384 = 16 x 24 and 192 = 8 x 24 take two passes); remaining factors
-// 3 and 5 as radix-3 / radix-5 passes.
-template <int N, int RMAX> struct FPlan {
+// 3 and 5 as radix-3 / radix-5 passes. FF puts the folded pass first (any order
+// of the radices is a valid Stockham plan; the spans follow the order).
+template <int N, int RMAX, bool FF = false> struct FPlan {
     static constexpr int e2all = fft_pow2_exp(N);
     static constexpr int e3 = fft_exp_of(N, 3);
     static constexpr int e5 = fft_exp_of(N, 5);
@@ -42,10 +43,15 @@ template <int N, int RMAX> struct FPlan {
     static constexpr int npass = q2 + nfold + (e3 - nfold) + e5;
     static constexpr bool valid = (N == (1 << e2all) * (e3 == 0 ? 1 : (e3 == 1 ? 3 : (e3 == 2 ? 9 : 27))) *
                                            (e5 == 0 ? 1 : (e5 == 1 ? 5 : 25)));
+    // radix of the p-th of the passes other than the folded one
+    __host__ __device__ static constexpr int rest(int p)
+    {
+        return p < q2 ? (1 << (e2 / qd + (p < e2 % qd ? 1 : 0))) : (p < q2 + e3 - nfold ? 3 : 5);
+    }
     __host__ __device__ static constexpr int rad(int p)
     {
-        return p < q2 ? (1 << (e2 / qd + (p < e2 % qd ? 1 : 0)))
-                      : (p < q2 + nfold ? (3 << fold) : (p < q2 + e3 ? 3 : 5));
+        return FF && nfold ? (p == 0 ? (3 << fold) : rest(p - 1))
+                           : (p < q2 ? rest(p) : (p < q2 + nfold ? (3 << fold) : rest(p - nfold)));
     }
     // product of the radices of passes 0..p-1 (the Stockham span Ns of pass p)
     __host__ __device__ static constexpr int span(int p) { return p == 0 ? 1 : span(p - 1) * rad(p - 1); }
@@ -213,11 +219,11 @@ __device__ __forceinline__ void stock_pass(const SRC& src, const DST& dst, const
 // Passes P..npass-1. Pass P reads SRC; passes after the first read shared
 // buffer A (ping-pong with B); the last pass writes DST. Every pass but the last
 // ends with a barrier.
-template <typename R, int N, int S, int RMAX, int LINES, int NT, bool LMINOR, int P, class SRC, class DST>
+template <typename R, int N, int S, int RMAX, int LINES, int NT, bool LMINOR, int P, bool FF = false, class SRC, class DST>
 __device__ __forceinline__ void run_passes(const SRC& src, const DST& dst, typename V2<R>::T* A, typename V2<R>::T* B,
                                            const typename V2<R>::T* tw)
 {
-    typedef FPlan<N, RMAX> PL;
+    typedef FPlan<N, RMAX, FF> PL;
     typedef typename V2<R>::T T2;
     constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride;
     if constexpr (P == PL::npass - 1) {
@@ -227,7 +233,7 @@ __device__ __forceinline__ void run_passes(const SRC& src, const DST& dst, typen
         stock_pass<R, N, S, PL::rad(P), PL::span(P), LINES, NT, LMINOR>(src, out, tw);
         __syncthreads();
         const SmemIO<T2, LS, G> in{A};
-        run_passes<R, N, S, RMAX, LINES, NT, LMINOR, P + 1>(in, dst, B, A, tw);
+        run_passes<R, N, S, RMAX, LINES, NT, LMINOR, P + 1, FF>(in, dst, B, A, tw);
     }
 }
 
@@ -460,6 +466,16 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
 // y direction on the half spectrum [k][m][l]: tiles of FyLines<N> columns l of
 // one plane k; grid (ceil(nxh/TL), nz, fields)
 // ----------------------------------------------------------------------------
+// y tiles in FP32 put the folded pass first where the other order would start
+// with a pass of fewer than 16 points: 192 = 24 x 8 then reads 24 elements a
+// thread in one round instead of 8 elements in 1.5 rounds (forward 85 -> 70 us,
+// inverse 107 -> 97 us at 256 x 192 x 256, 3 and 4 fields). 384 = 16 x 24 keeps
+// radix 16 first: radix 24 first gained nothing forward and spilled inverse
+// there, and in FP64 it was slower in both directions.
+template <typename R, int N, int RMAX> struct FyFoldFirst {
+    typedef FPlan<N, RMAX> PL;
+    static constexpr bool v = sizeof(R) == sizeof(float) && PL::nfold == 1 && PL::rad(0) < 16;
+};
 template <typename R, int N, int S, int RMAX>
 __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a)
 {
@@ -491,7 +507,7 @@ __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a)
     }
     // in place (s == d) with two or more passes: the first pass reads every
     // element of the tile before its barrier, and only the last pass writes it
-    run_passes<R, N, S, RMAX, TL, HC_FFT_NT, true, 0>(src, dst, A, B, a.tw);
+    run_passes<R, N, S, RMAX, TL, HC_FFT_NT, true, 0, FyFoldFirst<R, N, RMAX>::v>(src, dst, A, B, a.tw);
 }
 
 // FP64: the compiler's own register budget
