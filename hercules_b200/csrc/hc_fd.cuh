@@ -584,7 +584,9 @@ __global__ void __launch_bounds__(256, StatsMinBlocks<R>::v) k_stats(StatsArgs<R
             auto l2 = [](const float* p, long long q) { return *reinterpret_cast<const float2*>(p + q); };
             const double um = s.um;
             const bool fold = s.accumulate && (*s.step % s.window) == 0;
-            float2 wm = k0 > 0 ? l2(s.f.w, (long long)(k0 - 1) * g.nxy + p2) : make_float2(0.0f, 0.0f);
+            // ceil(nz / gridDim.y) levels a chunk: the last chunks can start at or past
+            // nz, and then read nothing (w below the chunk included)
+            float2 wm = (k0 > 0 && k0 < k1) ? l2(s.f.w, (long long)(k0 - 1) * g.nxy + p2) : make_float2(0.0f, 0.0f);
 #pragma unroll 2
             for (int k = k0; k < k1; ++k) {
                 const long long q = (long long)k * g.nxy + p2;
@@ -648,7 +650,7 @@ __global__ void __launch_bounds__(256, StatsMinBlocks<R>::v) k_stats(StatsArgs<R
         const double um = s.um;
         // FP32 storage always keeps the FP32 window sums (allocated with the handle)
         const bool fold = sizeof(R) == sizeof(float) && s.accumulate && (*s.step % s.window) == 0;
-        double wm = k0 > 0 ? (double)fw[(long long)(k0 - 1) * g.nxy + ij] : 0.0;
+        double wm = (k0 > 0 && k0 < k1) ? (double)fw[(long long)(k0 - 1) * g.nxy + ij] : 0.0;
         for (int kb = k0; kb < k1; kb += G) {
             // the fields stay in the storage type in registers; products in FP64
             R u[G], v[G], w[G], t[G], ux[G], vy[G];
