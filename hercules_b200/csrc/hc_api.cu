@@ -1154,7 +1154,7 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         for (int f = 0; f < 6; ++f) pa.d[f] = p.issk == 1 ? Q[SP_W0 + 8 + f] : nullptr;
         for (int f = 0; f < 8; ++f) pa.out[f] = Q[SP_W0 + f];
         for (int f = 0; f < 3; ++f) pa.bf[f] = h->has_bf ? (const R*)h->bf[f] : nullptr;
-        pa.g = g; pa.sc = h->sc;
+        pa.g = g; pa.sc = h->sc; pa.rdz = h->cc.rdz; pa.rdzt = h->cc.rdzt;
         pa.um = p.u_mrf; pa.fc = p.fc; pa.ug = p.ug; pa.vg = p.vg; pa.t_ref = p.t_ref; pa.tbot = p.tbot; pa.ttop = p.ttop;
         pa.inv_coe = 1.0 / (p.issk == 1 ? 0.5 : 1.0);
         pa.closed = p.ochannel == 0; pa.dp3 = p.dp_opt == 3; pa.scalar = p.isscalar == 1; pa.skew = p.issk == 1;
@@ -1175,6 +1175,7 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         aa.ff = S[SP_FF]; aa.gg = S[SP_GG]; aa.hh = S[SP_HH];
         aa.qu = S[SP_QU]; aa.qv = S[SP_QV]; aa.qw = S[SP_QW];
         aa.dt = dtab; aa.g = g; aa.tpx = tpx; aa.tpy = tpy;
+        aa.rdz = h->cc.rdz; aa.rdzt = h->cc.rdzt; aa.rdzb = h->cc.rdzb;
         aa.rk_a = rk_a; aa.rk_b = rk_b; aa.rk_c = rk_c; aa.dtime = p.dt; aa.nu = p.nu; aa.um = p.u_mrf;
         aa.coe = p.issk == 1 ? 0.5 : 1.0;
         aa.closed = p.ochannel == 0; aa.kchunk = spec_kchunk(h, g.ncol); aa.halt = halt;

@@ -172,14 +172,22 @@ template <typename R> struct ProdArgs {
     const R* bf[3];         // body force (null: none); enters the histories with factor 1
     R* out[8];
     Geo g;
+    const double* rdz; const double* rdzt;   // [nz] 1/dz, 1/dz_t
     const DevScalars* sc;
     double um, fc, ug, vg, t_ref, tbot, ttop, inv_coe;
     int closed, dp3, scalar, skew, kchunk;
     const int* halt;
 };
 
+// Products and assemble load each level one level ahead (below). Registers:
+// products at three resident blocks (at 256 x 256 x 128: FP32 storage 186 ->
+// 114 us, FP64 152 -> 143 us a launch); assemble at two blocks with FP32
+// storage (243 -> 98 us) and the compiler's own budget with FP64 (354 -> 161
+// us; bounded to two blocks it spilled and took 211 us)
+template <typename R> struct AsmMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 2 : 1; };
+
 template <typename R>
-__global__ void __launch_bounds__(256) k_spec_products(ProdArgs<R> a)
+__global__ void __launch_bounds__(256, 3) k_spec_products(ProdArgs<R> a)
 {
     if (a.halt && *a.halt) return;
     const Geo& g = a.g;
@@ -189,33 +197,58 @@ __global__ void __launch_bounds__(256) k_spec_products(ProdArgs<R> a)
     const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
     const long long nxy = g.nxy;
     const double um = a.um;
-    auto U = [&](int k) -> double {
-        if (k < 0) return -(double)a.u[ij] - 2.0 * um;
-        if (k >= nz) return a.closed ? -(double)a.u[(long long)(nz - 1) * nxy + ij] - 2.0 * um : (double)a.u[(long long)(nz - 1) * nxy + ij];
-        return (double)a.u[(long long)k * nxy + ij];
+    // stored value of the level a vertical neighbour reads (clamped; w reads
+    // nz-2 above the top) and the ghost rules of update_boundary_uvw / _t on it
+    const int nz1 = nz - 1;
+    auto iC = [&](int k) { return k < 0 ? 0 : (k > nz1 ? nz1 : k); };
+    auto iW = [&](int k) { return k < 0 ? 0 : (k > nz1 ? nz - 2 : k); };
+    auto raw = [&](const R* f, int kk) -> R { return f[(long long)kk * nxy + ij]; };
+    auto gU = [&](R r, int k) -> double {
+        return (k < 0 || (k >= nz && a.closed)) ? -(double)r - 2.0 * um : (double)r;
     };
-    auto V = [&](int k) -> double {
-        if (k < 0) return -(double)a.v[ij];
-        if (k >= nz) return a.closed ? -(double)a.v[(long long)(nz - 1) * nxy + ij] : (double)a.v[(long long)(nz - 1) * nxy + ij];
-        return (double)a.v[(long long)k * nxy + ij];
-    };
-    auto W = [&](int k) -> double {
-        if (k < 0) return 0.0;
-        if (k >= nz) return -(double)a.w[(long long)(nz - 2) * nxy + ij];
-        return (double)a.w[(long long)k * nxy + ij];
-    };
-    auto T = [&](int k) -> double {
+    auto gV = [&](R r, int k) -> double { return (k < 0 || (k >= nz && a.closed)) ? -(double)r : (double)r; };
+    auto gW = [&](R r, int k) -> double { return k < 0 ? 0.0 : (k >= nz ? -(double)r : (double)r); };
+    auto gT = [&](R r, int k) -> double {
         if (!a.scalar) return 0.0;
-        if (k < 0) return 2.0 * a.tbot - (double)a.t[ij];
-        if (k >= nz) return 2.0 * a.ttop - (double)a.t[(long long)(nz - 1) * nxy + ij];
-        return (double)a.t[(long long)k * nxy + ij];
+        return k < 0 ? 2.0 * a.tbot - (double)r : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
+    };
+    // the four fields at level L, in the storage type
+    struct Lv { R u, v, w, t; };
+    auto fetch = [&](int L, Lv& o) {
+        o.u = raw(a.u, iC(L)); o.v = raw(a.v, iC(L)); o.w = raw(a.w, iW(L));
+        o.t = a.scalar ? raw(a.t, iC(L)) : R(0);
     };
     const double dpx = a.sc->dpx_drive, got = a.sc->got, ic = a.inv_coe;
-    double um_ = U(k0 - 1), uk = U(k0), vm = V(k0 - 1), vk = V(k0), wm = W(k0 - 1), wk = W(k0), tk = T(k0);
+    Lv l0, l1;
+    fetch(k0 - 1, l0); fetch(k0, l1);
+    double um_ = gU(l0.u, k0 - 1), uk = gU(l1.u, k0), vm = gV(l0.v, k0 - 1), vk = gV(l1.v, k0);
+    double wm = gW(l0.w, k0 - 1), wk = gW(l1.w, k0), tk = gT(l1.t, k0);
+    // the loads a level needs (level k+1 of the fields, level k of the skew
+    // derivatives and of the z factors) are issued one level ahead, in the
+    // storage type, so that their latency overlaps the previous level's
+    // arithmetic and stores
+    Lv lp;
+    fetch(k0 + 1, lp);
+    R dd[6] = {0, 0, 0, 0, 0, 0};
+    auto ld_d = [&](int k, R* o) {
+        if (a.skew) {
+#pragma unroll
+            for (int f = 0; f < 6; ++f) o[f] = a.d[f][(long long)k * nxy + ij];
+        }
+    };
+    ld_d(k0, dd);
+    double zf[4] = {ldz(g.z.l_t, k0), ldz(g.z.l_b, k0), a.rdz[k0], a.rdzt[k0]};
     for (int k = k0; k < k1; ++k) {
-        const double up = U(k + 1), vp = V(k + 1), wp = W(k + 1), tp = T(k + 1);
-        const double lt = ldz(g.z.l_t, k), lb = ldz(g.z.l_b, k);
-        const double rdz = 1.0 / ldz(g.z.dz, k), rdzt = 1.0 / ldz(g.z.dz_t, k);
+        Lv ln;
+        R dn[6] = {0, 0, 0, 0, 0, 0};
+        double zn[4] = {0, 0, 0, 0};
+        if (k + 1 < k1) {
+            fetch(k + 2, ln);
+            ld_d(k + 1, dn);
+            zn[0] = ldz(g.z.l_t, k + 1); zn[1] = ldz(g.z.l_b, k + 1); zn[2] = a.rdz[k + 1]; zn[3] = a.rdzt[k + 1];
+        }
+        const double up = gU(lp.u, k + 1), vp = gV(lp.v, k + 1), wp = gW(lp.w, k + 1), tp = gT(lp.t, k + 1);
+        const double lt = zf[0], lb = zf[1], rdz = zf[2], rdzt = zf[3];
         const long long q = (long long)k * nxy + ij;
         const double a1u = up * lt + uk * (1.0 - lt), a2u = um_ * lb + uk * (1.0 - lb);
         const double a1v = vp * lt + vk * (1.0 - lt), a2v = vm * lb + vk * (1.0 - lb);
@@ -226,9 +259,9 @@ __global__ void __launch_bounds__(256) k_spec_products(ProdArgs<R> a)
         double cw = a.scalar ? ic * (got * ((1.0 - lt) * tk + lt * tp - a.t_ref)) - tmpw : -tmpw;
         if (a.skew) {
             const double wc = 0.5 * (wk + wm);
-            cu -= uk * (double)a.d[0][q] + vk * (double)a.d[1][q] + (a1u - a2u) * rdz * wc;
-            cv -= uk * (double)a.d[2][q] + vk * (double)a.d[3][q] + (a1v - a2v) * rdz * wc;
-            cw -= a1u * (double)a.d[4][q] + a1v * (double)a.d[5][q] + wk * ((hp - hm) * rdzt);
+            cu -= uk * (double)dd[0] + vk * (double)dd[1] + (a1u - a2u) * rdz * wc;
+            cv -= uk * (double)dd[2] + vk * (double)dd[3] + (a1v - a2v) * rdz * wc;
+            cw -= a1u * (double)dd[4] + a1v * (double)dd[5] + wk * ((hp - hm) * rdzt);
         }
         a.out[0][q] = (R)(uk * uk);
         a.out[1][q] = (R)(uk * vk);
@@ -244,6 +277,11 @@ __global__ void __launch_bounds__(256) k_spec_products(ProdArgs<R> a)
         a.out[6][q] = (R)cv;
         a.out[7][q] = (R)cw;
         um_ = uk; uk = up; vm = vk; vk = vp; wm = wk; wk = wp; tk = tp;
+        lp = ln;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) dd[f] = dn[f];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) zf[f] = zn[f];
     }
 }
 
@@ -266,6 +304,7 @@ template <typename R> struct AsmArgs {
     typename V2<R>::T* qu; typename V2<R>::T* qv; typename V2<R>::T* qw;
     DampTab dt;
     Geo g;
+    const double* rdz; const double* rdzt; const double* rdzb;   // [nz] 1/dz, 1/dz_t, 1/dz_b
     double tpx, tpy;
     double rk_a, rk_b, rk_c, dtime, nu, um, coe;
     int closed, kchunk;
@@ -273,7 +312,7 @@ template <typename R> struct AsmArgs {
 };
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_spec_assemble(AsmArgs<R> a)
+__global__ void __launch_bounds__(256, AsmMinBlocks<R>::v) k_spec_assemble(AsmArgs<R> a)
 {
     typedef typename V2<R>::T T2;
     if (a.halt && *a.halt) return;
@@ -285,43 +324,68 @@ __global__ void __launch_bounds__(256) k_spec_assemble(AsmArgs<R> a)
     const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
     const SpecWave wv = spec_wave(c, g, a.tpx, a.tpy);
     const double o00 = wv.is00 ? -2.0 * a.um : 0.0;     // u ghost offset, (0,0) mode only
-    auto ld = [&](const T2* f, int k) { return ld2<R>(f, (long long)k * ncol + c); };
-    auto SU = [&](int k) -> double2 {
-        if (k < 0) { double2 s = ld(a.su, 0); return make_double2(-s.x + o00, -s.y); }
-        if (k >= nz) {
-            double2 s = ld(a.su, nz - 1);
-            return a.closed ? make_double2(-s.x + o00, -s.y) : s;
-        }
-        return ld(a.su, k);
+    auto ldr = [&](const T2* f, int k) -> T2 { return f[(long long)k * ncol + c]; };
+    auto dbl = [](T2 v) { return make_double2((double)v.x, (double)v.y); };
+    const int nz1 = nz - 1;
+    // ghost rules of the vertical neighbours, applied to the stored value of the
+    // level they read (raw index: clamp for u, v, p; w reads nz-2 above the top)
+    auto gU = [&](T2 r, int k) -> double2 {
+        const double2 s = dbl(r);
+        return (k < 0 || (k >= nz && a.closed)) ? make_double2(-s.x + o00, -s.y) : s;
     };
-    auto SV = [&](int k) -> double2 {
-        if (k < 0) { double2 s = ld(a.sv, 0); return make_double2(-s.x, -s.y); }
-        if (k >= nz) { double2 s = ld(a.sv, nz - 1); return a.closed ? make_double2(-s.x, -s.y) : s; }
-        return ld(a.sv, k);
+    auto gV = [&](T2 r, int k) -> double2 {
+        const double2 s = dbl(r);
+        return (k < 0 || (k >= nz && a.closed)) ? make_double2(-s.x, -s.y) : s;
     };
     // w as the physical field sees it: 0 below the bottom wall and on the top wall
-    auto SW = [&](int k) -> double2 {
-        if (k < 0 || k == nz - 1) return make_double2(0, 0);
-        if (k >= nz) { double2 s = ld(a.sw, nz - 2); return make_double2(-s.x, -s.y); }
-        return ld(a.sw, k);
+    auto gW = [&](T2 r, int k) -> double2 {
+        if (k < 0 || k == nz1) return make_double2(0, 0);
+        const double2 s = dbl(r);
+        return k >= nz ? make_double2(-s.x, -s.y) : s;
     };
-    auto SP = [&](int k) -> double2 { return ld(a.sp, k < 0 ? 0 : (k >= nz ? nz - 1 : k)); };
+    auto iU = [&](int k) { return k < 0 ? 0 : (k > nz1 ? nz1 : k); };
+    auto iW = [&](int k) { return k < 0 ? 0 : (k > nz1 ? nz - 2 : k); };
     const double ad = a.rk_c * 0.5 * a.dtime * a.nu, cdt = a.rk_c * a.dtime;
     const double bdt = a.rk_b * a.dtime, adt = a.rk_a * a.dtime, coe = a.coe;
     const double k2 = wv.kx * wv.kx + wv.ky * wv.ky;
-    double2 um_ = SU(k0 - 1), uk = SU(k0), vm = SV(k0 - 1), vk = SV(k0), wm = SW(k0 - 1), wk = SW(k0);
-    double2 pk = SP(k0);
+    double2 um_ = gU(ldr(a.su, iU(k0 - 1)), k0 - 1), uk = gU(ldr(a.su, iU(k0)), k0);
+    double2 vm = gV(ldr(a.sv, iU(k0 - 1)), k0 - 1), vk = gV(ldr(a.sv, iU(k0)), k0);
+    double2 wm = gW(ldr(a.sw, iW(k0 - 1)), k0 - 1), wk = gW(ldr(a.sw, iW(k0)), k0);
+    double2 pk = dbl(ldr(a.sp, iU(k0)));
+    // everything a level reads from global memory (level k+1 of u, v, w, p, level
+    // k of the raw w spectrum, the eight product spectra and the histories) is
+    // loaded one level ahead in the storage type, so that its latency overlaps
+    // the previous level's arithmetic and stores
+    struct Lv { T2 up, vp, wp, pp, w0, F[8], h[3]; };
+    auto fetch = [&](int k, Lv& L) {
+        L.up = ldr(a.su, iU(k + 1)); L.vp = ldr(a.sv, iU(k + 1));
+        L.wp = ldr(a.sw, iW(k + 1)); L.pp = ldr(a.sp, iU(k + 1));
+        L.w0 = ldr(a.sw, k);
+#pragma unroll
+        for (int f = 0; f < 8; ++f) L.F[f] = ldr(a.F[f], k);
+        L.h[0] = ldr(a.ff, k); L.h[1] = ldr(a.gg, k); L.h[2] = ldr(a.hh, k);
+    };
+    auto zfac = [&](int k, double* z) {
+        z[0] = a.rdz[k]; z[1] = a.rdzt[k]; z[2] = a.rdzb[k];
+        z[3] = k + 1 < nz ? a.rdz[k + 1] : 1.0 / ldz(g.z.dz, k + 1);
+    };
+    Lv cur;
+    double zc[4];
+    fetch(k0, cur);
+    zfac(k0, zc);
     for (int k = k0; k < k1; ++k) {
-        const double2 up = SU(k + 1), vp = SV(k + 1), wp = SW(k + 1), pp = SP(k + 1);
+        Lv nxt;
+        double zn[4] = {0, 0, 0, 0};
+        if (k + 1 < k1) { fetch(k + 1, nxt); zfac(k + 1, zn); }
+        const double2 up = gU(cur.up, k + 1), vp = gV(cur.vp, k + 1), wp = gW(cur.wp, k + 1), pp = dbl(cur.pp);
         const long long id = (long long)k * ncol + c;
-        const double rdz = 1.0 / ldz(g.z.dz, k), rdzt = 1.0 / ldz(g.z.dz_t, k), rdzb = 1.0 / ldz(g.z.dz_b, k);
-        const double rdz1 = 1.0 / ldz(g.z.dz, k + 1);
+        const double rdz = zc[0], rdzt = zc[1], rdzb = zc[2], rdz1 = zc[3];
         const double2 Du = a.dt.at(uk, 0, k, nz);
         const double2 Dv = a.dt.at(vk, 1, k, nz);
-        const double2 Dw = a.dt.at(ld(a.sw, k), 2, k, nz);
+        const double2 Dw = a.dt.at(dbl(cur.w0), 2, k, nz);
         const double2 Dp = a.dt.at(pk, 3, k, nz);
-        const double2 Fuu = ld(a.F[0], k), Fuv = ld(a.F[1], k), Fvv = ld(a.F[2], k), Futw = ld(a.F[3], k);
-        const double2 Fvtw = ld(a.F[4], k), Fcu = ld(a.F[5], k), Fcv = ld(a.F[6], k), Fcw = ld(a.F[7], k);
+        const double2 Fuu = dbl(cur.F[0]), Fuv = dbl(cur.F[1]), Fvv = dbl(cur.F[2]), Futw = dbl(cur.F[3]);
+        const double2 Fvtw = dbl(cur.F[4]), Fcu = dbl(cur.F[5]), Fcv = dbl(cur.F[6]), Fcw = dbl(cur.F[7]);
         // vertical operators (zero on the Nyquist row, as the forward FFT leaves them)
         const double zs = wv.zp;
         const double2 lzu = make_double2(zs * (((up.x - uk.x) * rdzt - (uk.x - um_.x) * rdzb) * rdz),
@@ -334,7 +398,7 @@ __global__ void __launch_bounds__(256) k_spec_assemble(AsmArgs<R> a)
         // u
         double2 q = zfma(zfma(Du, Du, -ad * k2), lzu, ad);
         q = zfma(q, mul_i(Dp, wv.kx), -cdt);
-        q = zfma(q, ld(a.ff, k), bdt);
+        q = zfma(q, dbl(cur.h[0]), bdt);
         double2 h = make_double2(0, 0);
         h = zfma(h, mul_i(Du, wv.kx), -a.um);
         h = zfma(h, mul_i(Fuu, wv.kx), -coe);
@@ -345,7 +409,7 @@ __global__ void __launch_bounds__(256) k_spec_assemble(AsmArgs<R> a)
         // v
         q = zfma(zfma(Dv, Dv, -ad * k2), lzv, ad);
         q = zfma(q, mul_i(Dp, wv.ky), -cdt);
-        q = zfma(q, ld(a.gg, k), bdt);
+        q = zfma(q, dbl(cur.h[1]), bdt);
         h = make_double2(0, 0);
         h = zfma(h, mul_i(Dv, wv.kx), -a.um);
         h = zfma(h, mul_i(Fuv, wv.kx), -coe);
@@ -356,7 +420,7 @@ __global__ void __launch_bounds__(256) k_spec_assemble(AsmArgs<R> a)
         // w
         q = zfma(zfma(Dw, Dw, -ad * k2), lzw, ad);
         q = zfma(q, dpz, -cdt);
-        q = zfma(q, ld(a.hh, k), bdt);
+        q = zfma(q, dbl(cur.h[2]), bdt);
         h = make_double2(0, 0);
         h = zfma(h, mul_i(Dw, wv.kx), -a.um);
         h = zfma(h, mul_i(Futw, wv.kx), -coe);
@@ -365,6 +429,9 @@ __global__ void __launch_bounds__(256) k_spec_assemble(AsmArgs<R> a)
         st2<R>(a.hh, id, h);
         st2<R>(a.qw, id, zfma(q, h, adt));
         um_ = uk; uk = up; vm = vk; vk = vp; wm = wk; wk = wp; pk = pp;
+        cur = nxt;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) zc[f] = zn[f];
     }
 }
 
