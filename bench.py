@@ -171,8 +171,8 @@ ALG_WORDS_SUB = {
 # DRAM bytes (read + write) of one launch per kernel category, FP32-mixed, from
 # the ncu capture of the 256x192x256 case (profiles/traffic_fd_kernels_mixed_256x192x256.md)
 # scaled by the point ratio to the grids below (every kernel streams its fields once)
-_TRAFFIC_256x192x256 = {"rhs_momentum": 664.0e6, "column_fd": 296.6e6, "fft_x_r2c": 252.6e6, "fft_y_fwd": 239.9e6,
-                        "fft_y_inv": 339.1e6, "fft_x_c2r": 407.1e6, "div_check": 151.4e6, "stats": 1364.8e6}
+_TRAFFIC_256x192x256 = {"rhs_momentum": 647.9e6, "column_fd": 295.4e6, "fft_x_r2c": 253.1e6, "fft_y_fwd": 239.9e6,
+                        "fft_y_inv": 343.7e6, "fft_x_c2r": 406.8e6, "div_check": 155.0e6, "stats": 1362.9e6}
 TRAFFIC = {(w, k): v * (WORKLOADS[w][0] * WORKLOADS[w][1] * WORKLOADS[w][2]) / (256 * 192 * 256)
            for w in ("channel_fd4_512x384x256", "channel_fd4_256x192x256") for k, v in _TRAFFIC_256x192x256.items()}
 
