@@ -1224,6 +1224,7 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         for (int f = 0; f < 3; ++f) at.F[f] = S[SP_W0 + 4 + f];
         at.ss = S[SP_SS]; at.qt = S[SP_QU];
         at.dt = dtab; at.g = g; at.tpx = tpx; at.tpy = tpy;
+        at.rdz = h->cc.rdz; at.rdzt = h->cc.rdzt; at.rdzb = h->cc.rdzb;
         at.rk_a = rk_a; at.rk_b = rk_b; at.rk_c = rk_c; at.dtime = p.dt; at.alpha = p.alpha; at.um = p.u_mrf;
         at.tbot = p.tbot; at.ttop = p.ttop; at.kchunk = spec_kchunk(h, g.ncol); at.halt = halt;
         prof_begin(h, K_SPEC_ASM);

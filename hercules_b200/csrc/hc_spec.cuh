@@ -458,23 +458,37 @@ __global__ void __launch_bounds__(256) k_spec_products_t(ProdTArgs<R> a)
     const int nz = g.nz;
     const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
     const long long nxy = g.nxy;
-    auto T = [&](int k) -> double {
-        if (k < 0) return 2.0 * a.tbot - (double)a.t[ij];
-        if (k >= nz) return 2.0 * a.ttop - (double)a.t[(long long)(nz - 1) * nxy + ij];
-        return (double)a.t[(long long)k * nxy + ij];
+    // stored t of the level a neighbour reads (clamped) and the ghost rule of
+    // update_boundary_t on it; everything a level reads is loaded one level ahead
+    // in the storage type (see k_spec_products)
+    const int nz1 = nz - 1;
+    auto rawt = [&](int k) -> R { return a.t[(long long)(k < 0 ? 0 : (k > nz1 ? nz1 : k)) * nxy + ij]; };
+    auto gT = [&](R r, int k) -> double {
+        return k < 0 ? 2.0 * a.tbot - (double)r : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
     };
-    double tm = T(k0 - 1), tk = T(k0);
-    double wm = k0 > 0 ? (double)a.w[(long long)(k0 - 1) * nxy + ij] : 0.0;
-    for (int k = k0; k < k1; ++k) {
-        const double tp = T(k + 1);
+    struct Lv { R tp, u, v, w; double lt, lb, dz; };
+    auto fetch = [&](int k, Lv& L) {
         const long long q = (long long)k * nxy + ij;
-        const double uk = (double)a.u[q], vk = (double)a.v[q], wk = (double)a.w[q];
-        const double lt = ldz(g.z.l_t, k), lb = ldz(g.z.l_b, k);
+        L.tp = rawt(k + 1); L.u = a.u[q]; L.v = a.v[q]; L.w = a.w[q];
+        L.lt = ldz(g.z.l_t, k); L.lb = ldz(g.z.l_b, k); L.dz = ldz(g.z.dz, k);
+    };
+    double tm = gT(rawt(k0 - 1), k0 - 1), tk = gT(rawt(k0), k0);
+    double wm = k0 > 0 ? (double)a.w[(long long)(k0 - 1) * nxy + ij] : 0.0;
+    Lv cur;
+    fetch(k0, cur);
+    for (int k = k0; k < k1; ++k) {
+        Lv nxt;
+        if (k + 1 < k1) fetch(k + 1, nxt);
+        const double tp = gT(cur.tp, k + 1);
+        const long long q = (long long)k * nxy + ij;
+        const double uk = (double)cur.u, vk = (double)cur.v, wk = (double)cur.w;
+        const double lt = cur.lt, lb = cur.lb;
         const double a1 = tp * lt + tk * (1.0 - lt), a2 = tm * lb + tk * (1.0 - lb);
         a.out[0][q] = (R)(uk * tk);
         a.out[1][q] = (R)(tk * vk);
-        a.out[2][q] = (R)((a1 * wk - a2 * wm) / ldz(g.z.dz, k));
+        a.out[2][q] = (R)((a1 * wk - a2 * wm) / cur.dz);
         tm = tk; tk = tp; wm = wk;
+        cur = nxt;
     }
 }
 
@@ -485,6 +499,7 @@ template <typename R> struct AsmTArgs {
     typename V2<R>::T* qt;
     DampTab dt;
     Geo g;
+    const double* rdz; const double* rdzt; const double* rdzb;   // [nz] 1/dz, 1/dz_t, 1/dz_b
     double tpx, tpy;
     double rk_a, rk_b, rk_c, dtime, alpha, um, tbot, ttop;
     int kchunk;
@@ -503,34 +518,54 @@ __global__ void __launch_bounds__(256) k_spec_assemble_t(AsmTArgs<R> a)
     const int nz = g.nz;
     const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
     const SpecWave wv = spec_wave(c, g, a.tpx, a.tpy);
-    auto ld = [&](const T2* f, int k) { return ld2<R>(f, (long long)k * ncol + c); };
-    auto ST = [&](int k) -> double2 {
-        if (k < 0) { double2 s = ld(a.st, 0); return make_double2(-s.x + (wv.is00 ? 2.0 * a.tbot : 0.0), -s.y); }
-        if (k >= nz) { double2 s = ld(a.st, nz - 1); return make_double2(-s.x + (wv.is00 ? 2.0 * a.ttop : 0.0), -s.y); }
-        return ld(a.st, k);
+    auto ldr = [&](const T2* f, int k) -> T2 { return f[(long long)k * ncol + c]; };
+    auto dbl = [](T2 v) { return make_double2((double)v.x, (double)v.y); };
+    const int nz1 = nz - 1;
+    // stored spectrum of the level a neighbour reads (clamped) and the ghost rule
+    // of update_boundary_t on it (a constant offset lands on the (0,0) mode only)
+    auto gT = [&](T2 r, int k) -> double2 {
+        const double2 s = dbl(r);
+        if (k < 0) return make_double2(-s.x + (wv.is00 ? 2.0 * a.tbot : 0.0), -s.y);
+        if (k >= nz) return make_double2(-s.x + (wv.is00 ? 2.0 * a.ttop : 0.0), -s.y);
+        return s;
     };
+    auto iC = [&](int k) { return k < 0 ? 0 : (k > nz1 ? nz1 : k); };
     const double at = a.rk_c * 0.5 * a.dtime * a.alpha;
     const double bdt = a.rk_b * a.dtime, adt = a.rk_a * a.dtime;
     const double k2 = wv.kx * wv.kx + wv.ky * wv.ky;
-    double2 tm = ST(k0 - 1), tk = ST(k0);
+    double2 tm = gT(ldr(a.st, iC(k0 - 1)), k0 - 1), tk = gT(ldr(a.st, iC(k0)), k0);
+    // everything a level reads is loaded one level ahead in the storage type
+    // (see k_spec_assemble)
+    struct Lv { T2 tp, ss, F[3]; double rdz, rdzt, rdzb; };
+    auto fetch = [&](int k, Lv& L) {
+        L.tp = ldr(a.st, iC(k + 1)); L.ss = ldr(a.ss, k);
+#pragma unroll
+        for (int f = 0; f < 3; ++f) L.F[f] = ldr(a.F[f], k);
+        L.rdz = a.rdz[k]; L.rdzt = a.rdzt[k]; L.rdzb = a.rdzb[k];
+    };
+    Lv cur;
+    fetch(k0, cur);
     for (int k = k0; k < k1; ++k) {
-        const double2 tp = ST(k + 1);
+        Lv nxt;
+        if (k + 1 < k1) fetch(k + 1, nxt);
+        const double2 tp = gT(cur.tp, k + 1);
         const long long id = (long long)k * ncol + c;
-        const double rdz = 1.0 / ldz(g.z.dz, k), rdzt = 1.0 / ldz(g.z.dz_t, k), rdzb = 1.0 / ldz(g.z.dz_b, k);
+        const double rdz = cur.rdz, rdzt = cur.rdzt, rdzb = cur.rdzb;
         const double2 Dt = a.dt.at(tk, 4, k, nz);
         const double zs = wv.zp;
         const double2 lzt = make_double2(zs * (((tp.x - tk.x) * rdzt - (tk.x - tm.x) * rdzb) * rdz),
                                          zs * (((tp.y - tk.y) * rdzt - (tk.y - tm.y) * rdzb) * rdz));
         double2 q = zfma(zfma(Dt, Dt, -at * k2), lzt, at);
-        q = zfma(q, ld(a.ss, k), bdt);
+        q = zfma(q, dbl(cur.ss), bdt);
         double2 h = make_double2(0, 0);
         h = zfma(h, mul_i(Dt, wv.kx), -a.um);
-        h = zfma(h, mul_i(ld(a.F[0], k), wv.kx), -1.0);
-        h = zfma(h, mul_i(ld(a.F[1], k), wv.ky), -1.0);
-        h = zfma(h, ld(a.F[2], k), -1.0);
+        h = zfma(h, mul_i(dbl(cur.F[0]), wv.kx), -1.0);
+        h = zfma(h, mul_i(dbl(cur.F[1]), wv.ky), -1.0);
+        h = zfma(h, dbl(cur.F[2]), -1.0);
         st2<R>(a.ss, id, h);
         st2<R>(a.qt, id, zfma(q, h, adt));
         tm = tk; tk = tp;
+        cur = nxt;
     }
 }
 
@@ -705,6 +740,15 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_sp_warp(SpColArgs<R
     // ---- pressure update, projection, truncation
     const bool tr = spec_truncated(l, m, a.g.ny, A.ltr, A.mtr);
     {
+        // the old pressure spectrum of the lane's rows, all loaded before the
+        // first row's stores (read in the row loop, every row waited on its own load)
+        typename V2<R>::T spv[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            if (r < nz) spv[i] = A.sp[(long long)r * ncol + c];
+            else { spv[i].x = R(0); spv[i].y = R(0); }
+        }
         const double2 GX = __ldg(a.c.gx + l), GY = __ldg(a.c.gy + m);
         const double lxy = __ldg(a.c.lx + l) + __ldg(a.c.ly + m);
         const double cpr = rk * dt, cps = rk * 0.5 * dt * a.nu;
@@ -728,7 +772,7 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_sp_warp(SpColArgs<R
             lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
             lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
             const double2 psi = make_double2(pc.x - cps * (lxy * pc.x + lz.x), pc.y - cps * (lxy * pc.y + lz.y));
-            double2 fp = zadd(A.dt.at(ld2<R>(A.sp, id), 3, r, nz), psi);
+            double2 fp = zadd(A.dt.at(make_double2((double)spv[i].x, (double)spv[i].y), 3, r, nz), psi);
             if (tr) { fu = make_double2(0, 0); fv = fu; fw = fu; fp = fu; }
             st2<R>(A.phi, id, pc);
             st2<R>(A.su, id, fu);
