@@ -647,6 +647,11 @@ template <typename R> static int set_smem_attrs()
         CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         CK(cudaFuncSetAttribute(k_column_fd_tile_r<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        const int sp = (int)column_sp_tile_smem<4>(sizeof(typename V2<R>::T));
+        CK(cudaFuncSetAttribute(k_column_sp_tile<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
+        CK(cudaFuncSetAttribute(k_column_sp_tile<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
+        CK(cudaFuncSetAttribute(k_column_sp_tile<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
+        CK(cudaFuncSetAttribute(k_column_sp_tile<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
     }
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
@@ -1075,10 +1080,17 @@ template <typename R> static DampTab spec_damp_tab(hc_handle* h)
     return d;
 }
 
+// up to 128 levels (K <= 4) the tiled kernel: its FP64 registers for u*, v*, w*
+// grow with K, and beyond that the warp kernel keeps them in shared memory
 template <typename R, int K> static int col_sp_k(hc_handle* h, const SpColArgs<R>& a)
 {
-    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
-    k_column_sp_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(a);
+    if constexpr (K <= 4) {
+        const unsigned nb = (unsigned)((h->g.ncol + CT_COLS - 1) / CT_COLS);
+        k_column_sp_tile<R, K><<<nb, CT_COLS * 32, column_sp_tile_smem<K>(sizeof(typename V2<R>::T)), h->st>>>(a);
+    } else {
+        const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
+        k_column_sp_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(a);
+    }
     CKL();
     return HC_OK;
 }

@@ -803,3 +803,228 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_sp_warp(SpColArgs<R
         st2<R>(A.div, id, dv);
     }
 }
+
+// The same column work as k_column_sp_warp with the coalescing tiles of
+// k_column_fd_tile_r: a block of CT_COLS warps stages the rows of CT_COLS
+// adjacent columns (q_u, q_v, q_w and the old pressure spectrum) in shared
+// memory with row-contiguous loads, each warp solves one column from the tiles,
+// and the results (u, v, w, p, phi, the divergence spectrum) leave through the
+// tiles with row-contiguous stores; the warp kernel read and wrote every row of
+// its column with one access per lane (32 rows of one column per instruction).
+template <int K> __host__ size_t column_sp_tile_smem(size_t elem)
+{
+    return (size_t)4 * CT_COLS * ct_stride<K>() * elem;
+}
+
+template <typename R, int K>
+__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R> A)
+{
+    typedef typename V2<R>::T TT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const ColArgs<R>& a = A.b;
+    if (a.halt && *a.halt) return;
+    const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const long long ncol = a.g.ncol;
+    const long long c0 = (long long)blockIdx.x * CT_COLS;
+    const long long c = c0 + wp;
+    const bool active = c < ncol;
+    const int nz = a.g.nz;
+    constexpr int STR = ct_stride<K>();
+    TT* TU = reinterpret_cast<TT*>(smem_raw);
+    TT* TV = TU + CT_COLS * STR;
+    TT* TW = TV + CT_COLS * STR;
+    TT* TP = TW + CT_COLS * STR;
+    // element (column cb, row r) at cb * STR + (r % K) * CT_RP + r / K: lane ln of
+    // a warp holds rows ln K .. ln K + K - 1 of its column
+    auto load = [&](const TT* __restrict__ q, TT* T, int nrows) {
+        TT v[K];
+#pragma unroll
+        for (int it = 0; it < K; ++it) {
+            const int idx = threadIdx.x + it * CT_COLS * 32;
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            const long long cc = c0 + cb;
+            v[it] = (idx < nrows * CT_COLS && cc < ncol) ? q[(long long)r * ncol + cc] : mk2<R>(R(0), R(0));
+        }
+#pragma unroll
+        for (int it = 0; it < K; ++it) {
+            const int idx = threadIdx.x + it * CT_COLS * 32;
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * CT_RP + r / K] = v[it];
+        }
+    };
+    auto store = [&](TT* __restrict__ q, const TT* T) {
+        for (int idx = threadIdx.x; idx < nz * CT_COLS; idx += blockDim.x) {
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            const long long cc = c0 + cb;
+            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * CT_RP + r / K];
+        }
+    };
+    load(a.qu, TU, nz);
+    load(a.qv, TV, nz);
+    load(a.qw, TW, nz - 1);
+    load(A.sp, TP, nz);
+    __syncthreads();
+    TT* SU = TU + wp * STR;
+    TT* SV = TV + wp * STR;
+    TT* SW = TW + wp * STR;
+    TT* SP = TP + wp * STR;
+    auto dbl = [](TT v) { return make_double2((double)v.x, (double)v.y); };
+    auto put = [](TT* S, int q, double2 v) { S[q] = mk2<R>((R)v.x, (R)v.y); };
+    const int r0 = ln * K;
+    double2 ph[1][K];
+    double2 dvr[K];      // the divergence spectrum of the lane's rows
+    if (active) {
+        const int l = (int)(c % a.g.nxh), m = (int)(c / a.g.nxh);
+        const bool is00 = (c == 0), nyq = (m == a.g.ny / 2);
+        const double rk = a.rk_c, dt = a.dt;
+        const double lam = __ldg(a.c.hx + l) + __ldg(a.c.hy + m);
+        const double lamp = __ldg(a.c.px + l) + __ldg(a.c.py + m);
+        const double* dgu = is00 ? a.c.d0u : a.c.dgu;
+        const double* dgw = is00 ? a.c.d0w : a.c.dgw;
+        const double* dgp = is00 ? a.c.d0p : a.c.dgp;
+        // ---- u*, v*: one matrix, two right-hand sides. u*, v*, w* stay in FP64
+        //      registers until the projection, as the warp kernel keeps them in
+        //      FP64 shared memory (the tiles hold the storage type)
+        double2 us_[K], vs_[K], ws_[K];
+        {
+            double2 d[2][K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                if (r < nz) {
+                    d[0][i] = dbl(SU[i * CT_RP + ln]);
+                    d[1][i] = dbl(SV[i * CT_RP + ln]);
+                    if (is00 && r == 0) d[0][i].x += a.bcu0;
+                    if (is00 && r == nz - 1) d[0][i].x += a.bcu1;
+                } else {
+                    d[0][i] = make_double2(0, 0);
+                    d[1][i] = make_double2(0, 0);
+                }
+            }
+            auto cf = [&](int r, double& aa, double& bb, double& cc) {
+                if (r < nz) {
+                    aa = rk * __ldg(a.c.au + r);
+                    cc = rk * __ldg(a.c.cu + r);
+                    bb = 1.0 + rk * (-lam + __ldg(dgu + r));
+                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+            };
+            warp_partition_solve<K, 2>(cf, d, ln);
+#pragma unroll
+            for (int i = 0; i < K; ++i) { us_[i] = d[0][i]; vs_[i] = d[1][i]; }
+        }
+        {
+            double2 dw[1][K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                dw[0][i] = r < nz - 1 ? dbl(SW[i * CT_RP + ln]) : make_double2(0, 0);
+            }
+            auto cf = [&](int r, double& aa, double& bb, double& cc) {
+                if (r < nz - 1) {
+                    aa = rk * __ldg(a.c.aw + r);
+                    cc = rk * __ldg(a.c.cw + r);
+                    bb = 1.0 + rk * (-lam + __ldg(dgw + r));
+                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+            };
+            warp_partition_solve<K, 1>(cf, dw, ln);
+#pragma unroll
+            for (int i = 0; i < K; ++i) ws_[i] = dw[0][i];
+        }
+        // ---- phi: source (i kx u* + i ky v* + dw*/dz) / dt, zero on the Nyquist row
+        const double2 DX = __ldg(a.c.dx + l), DY = __ldg(a.c.dy + m);
+        const double rdt = 1.0 / dt;
+        {
+            double2 wprev0 = shfl_up2(ws_[K - 1], 1);
+            if (ln == 0) wprev0 = make_double2(0, 0);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                if (r < nz && !nyq) {
+                    const double2 wm = i > 0 ? ws_[i - 1] : wprev0;
+                    const double rdz = __ldg(a.c.rdz + r);
+                    double2 dv = zadd(zmul(DX, us_[i]), zmul(DY, vs_[i]));
+                    dv = zadd(dv, make_double2((ws_[i].x - wm.x) * rdz, (ws_[i].y - wm.y) * rdz));
+                    ph[0][i] = make_double2(dv.x * rdt, dv.y * rdt);
+                    if (is00 && r == 0) ph[0][i] = make_double2(0, 0);
+                } else {
+                    ph[0][i] = make_double2(0, 0);
+                }
+            }
+            auto cf = [&](int r, double& aa, double& bb, double& cc) {
+                if (r < nz) {
+                    aa = rk * __ldg(a.c.ap + r);
+                    cc = (is00 && r == 0) ? 0.0 : rk * __ldg(a.c.cp + r);
+                    bb = rk * (lamp + __ldg(dgp + r));
+                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+            };
+            warp_partition_solve<K, 1>(cf, ph, ln);
+        }
+        // ---- pressure update, projection, truncation: results into the tiles
+        const bool tr = spec_truncated(l, m, a.g.ny, A.ltr, A.mtr);
+        {
+            const double2 GX = __ldg(a.c.gx + l), GY = __ldg(a.c.gy + m);
+            const double lxy = __ldg(a.c.lx + l) + __ldg(a.c.ly + m);
+            const double cpr = rk * dt, cps = rk * 0.5 * dt * a.nu;
+            const double2 nxt0 = shfl_dn2(ph[0][0], 1);
+            const double2 prv0 = shfl_up2(ph[0][K - 1], 1);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                if (r >= nz) continue;
+                const double2 pc = ph[0][i];
+                const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
+                const double2 pd = (r == 0) ? pc : (i > 0 ? ph[0][i - 1] : prv0);
+                const double rdzt = __ldg(a.c.rdzt + r), rdzb = __ldg(a.c.rdzb + r), rdz = __ldg(a.c.rdz + r);
+                double2 fu = zsub(us_[i], zscale(zmul(GX, pc), cpr));
+                double2 fv = zsub(vs_[i], zscale(zmul(GY, pc), cpr));
+                double2 fw = r <= nz - 2 ? make_double2(ws_[i].x - cpr * (pu.x - pc.x) * rdzt, ws_[i].y - cpr * (pu.y - pc.y) * rdzt)
+                                         : make_double2(0, 0);
+                double2 lz;
+                lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
+                lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
+                const double2 psi = make_double2(pc.x - cps * (lxy * pc.x + lz.x), pc.y - cps * (lxy * pc.y + lz.y));
+                double2 fp = zadd(A.dt.at(dbl(SP[i * CT_RP + ln]), 3, r, nz), psi);
+                if (tr) { fu = make_double2(0, 0); fv = fu; fw = fu; fp = fu; }
+                put(SU, i * CT_RP + ln, fu);
+                put(SV, i * CT_RP + ln, fv);
+                put(SW, i * CT_RP + ln, fw);
+                put(SP, i * CT_RP + ln, fp);
+            }
+        }
+        __syncwarp();
+        // ---- divergence spectrum of the stored fields (the physical w is 0 below
+        //      the bottom wall and on the top wall)
+        const double2 wlast = dbl(SW[(K - 1) * CT_RP + ln]);
+        double2 wbelow0 = shfl_up2(wlast, 1);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            double2 dv = make_double2(0, 0);
+            if (r < nz && !nyq) {
+                const double2 fu = dbl(SU[i * CT_RP + ln]), fv = dbl(SV[i * CT_RP + ln]), fw = dbl(SW[i * CT_RP + ln]);
+                const double2 fwm = r == 0 ? make_double2(0, 0) : (i > 0 ? dbl(SW[(i - 1) * CT_RP + ln]) : wbelow0);
+                const double rdz = __ldg(a.c.rdz + r);
+                dv = zadd(zmul(DX, fu), zmul(DY, fv));
+                dv = zadd(dv, make_double2((fw.x - fwm.x) * rdz, (fw.y - fwm.y) * rdz));
+            }
+            dvr[i] = dv;
+        }
+    }
+    __syncthreads();
+    store(A.su, TU);
+    store(A.sv, TV);
+    store(A.sw, TW);
+    store(A.sp, TP);
+    __syncthreads();
+    // phi and the divergence spectrum through the first two tiles
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            put(SU, i * CT_RP + ln, ph[0][i]);
+            put(SV, i * CT_RP + ln, dvr[i]);
+        }
+    }
+    __syncthreads();
+    store(A.phi, TU);
+    store(A.div, TV);
+}
