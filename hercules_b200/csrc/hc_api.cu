@@ -542,8 +542,8 @@ template <typename R, int N> static int fft_t_op(hc_handle* h, int op, const voi
     }
     if (op == 1) k_fft_x_r2c_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
     else if (op == 2) k_fft_x_c2r_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
-    else if (op == 3) FyKernel<R, N, -1, RM>::f<<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
-    else FyKernel<R, N, 1, RM>::f<<<grid, HC_FFT_NT, sy, h->st>>>(*(const FyArgs<R>*)args);
+    else if (op == 3) FyKernel<R, N, -1, RM>::f<<<grid, FyThreads<R, N>::v, sy, h->st>>>(*(const FyArgs<R>*)args);
+    else FyKernel<R, N, 1, RM>::f<<<grid, FyThreads<R, N>::v, sy, h->st>>>(*(const FyArgs<R>*)args);
     return HC_OK;
 }
 
@@ -567,10 +567,10 @@ template <typename R> static int fft_t_setup(hc_handle* h)
 }
 
 // y tile width (columns l per block) of the length-n kernel
-static int fft_t_ytl(int n)
+template <typename R> static int fft_t_ytl(int n)
 {
     switch (n) {
-#define HC_LEN_CASE(N) case N: return FyLines<N>::v;
+#define HC_LEN_CASE(N) case N: return FyLines<R, N>::v;
     HC_FFT_T_LENGTHS(HC_LEN_CASE)
 #undef HC_LEN_CASE
     }
@@ -720,7 +720,7 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
         for (int f = 0; f < nf; ++f) a.dst[f] = out[f];
         a.nxh = h->g.nxh; a.tw = fft_tw<R>(h, 1); a.scale = (R)(1.0 / h->p.ny); a.halt = halt;
         prof_begin(h, K_FFT_Y_FWD);
-        int rc = fft_t_dispatch<R>(h, h->g.ny, 3, &a, dim3((h->g.nxh + fft_t_ytl(h->g.ny) - 1) / fft_t_ytl(h->g.ny), h->g.nz, nf));
+        int rc = fft_t_dispatch<R>(h, h->g.ny, 3, &a, dim3((h->g.nxh + fft_t_ytl<R>(h->g.ny) - 1) / fft_t_ytl<R>(h->g.ny), h->g.nz, nf));
         if (rc) return rc;
         CKL();
         return HC_OK;
@@ -751,7 +751,7 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
         for (int f = 0; f < nf; ++f) { a.dst[f] = in[f]; a.src[f] = ysrc ? ysrc[f] : nullptr; }
         a.nxh = h->g.nxh; a.tw = fft_tw<R>(h, 1); a.scale = (R)1; a.halt = halt;
         prof_begin(h, K_FFT_Y_INV);
-        int rc = fft_t_dispatch<R>(h, h->g.ny, 4, &a, dim3((h->g.nxh + fft_t_ytl(h->g.ny) - 1) / fft_t_ytl(h->g.ny), h->g.nz, nf));
+        int rc = fft_t_dispatch<R>(h, h->g.ny, 4, &a, dim3((h->g.nxh + fft_t_ytl<R>(h->g.ny) - 1) / fft_t_ytl<R>(h->g.ny), h->g.nz, nf));
         if (rc) return rc;
         CKL();
     } else {

@@ -271,9 +271,19 @@ template <typename R> struct FyArgs {
 
 // x: about 2048 complex values per block (at least one line)
 template <int N> struct FxLines { static constexpr int v = N >= 2048 ? 1 : 2048 / N; };
-// y: 16 columns per tile (128-byte row segments in FP32, 256 in FP64); 8 below 64 points
-template <int N> struct FyLines { static constexpr int v = N >= 64 ? 16 : 8; };
 #define HC_FFT_NT 256
+// y: tiles of 8 columns with 16 threads a column (64-byte row segments in FP32,
+// 128 in FP64), 4 columns for FP32 256-point columns; below 64 points 8 columns
+// with 256 threads. Narrower tiles keep more, smaller blocks resident: against
+// 16 columns with 256 threads, at 512 x 384 x 256 (3 and 4 fields) FP32 forward
+// 359 -> 322 us and inverse 480 -> 423 us, FP64 inverse 1034 -> 987 us; FP32
+// 256-point columns (256 x 256 x 128 spectral, 4 columns) 194 -> 105 and 132 ->
+// 75 us. 32 columns with 512 threads were slower (404 and 525 us), and 4 columns
+// of 384 points too (417 and 553 us).
+template <typename R, int N> struct FyLines {
+    static constexpr int v = N >= 64 ? ((sizeof(R) == sizeof(float) && N == 256) ? 4 : 8) : 8;
+};
+template <typename R, int N> struct FyThreads { static constexpr int v = N >= 64 ? FyLines<R, N>::v * 16 : HC_FFT_NT; };
 
 template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_x_smem()
 {
@@ -281,13 +291,14 @@ template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_
 }
 template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_y_smem()
 {
-    return (size_t)FBufs<N, RMAX>::y * FyLines<N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
+    return (size_t)FBufs<N, RMAX>::y * FyLines<R, N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
 }
 // y kernels in FP32: registers sized for as many resident blocks as the shared
-// memory allows, up to 4 (64 registers a thread)
+// memory allows, at 64 registers a thread at least (1024 threads an SM)
 template <typename R, int N, int RMAX> struct FyMinBlocks {
     static constexpr int bysmem = (int)((227 * 1024) / (fft_y_smem<R, N, RMAX>() + 1024));
-    static constexpr int v = bysmem < 1 ? 1 : (bysmem > 4 ? 4 : bysmem);
+    static constexpr int byreg = 4 * HC_FFT_NT / FyThreads<R, N>::v;
+    static constexpr int v = bysmem < 1 ? 1 : (bysmem > byreg ? byreg : bysmem);
 };
 
 // ---- global accessors -------------------------------------------------------
@@ -463,7 +474,7 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
 }
 
 // ----------------------------------------------------------------------------
-// y direction on the half spectrum [k][m][l]: tiles of FyLines<N> columns l of
+// y direction on the half spectrum [k][m][l]: tiles of FyLines<R, N> columns l of
 // one plane k; grid (ceil(nxh/TL), nz, fields)
 // ----------------------------------------------------------------------------
 // y tiles in FP32 put the folded pass first where the other order would start
@@ -480,7 +491,7 @@ template <typename R, int N, int S, int RMAX>
 __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a)
 {
     typedef typename V2<R>::T T2;
-    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, TL = FyLines<N>::v;
+    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, TL = FyLines<R, N>::v, NT = FyThreads<R, N>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
     T2* A = reinterpret_cast<T2*>(smem_raw);
@@ -496,26 +507,26 @@ __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a)
         if (s == d) {
             constexpr int LSz = FLine<N, G>::stride;
             const SmemIO<T2, LSz, G> stage{A};
-            for (int idx = threadIdx.x; idx < TL * N; idx += HC_FFT_NT) {
+            for (int idx = threadIdx.x; idx < TL * N; idx += NT) {
                 const int m = idx / TL, lt = idx - m * TL;
                 stage.st(lt, m, src.ld(lt, m));
             }
             __syncthreads();
-            stock_pass<R, N, S, FPlan<N, RMAX>::rad(0), 1, TL, HC_FFT_NT, true>(stage, dst, a.tw);
+            stock_pass<R, N, S, FPlan<N, RMAX>::rad(0), 1, TL, NT, true>(stage, dst, a.tw);
             return;
         }
     }
     // in place (s == d) with two or more passes: the first pass reads every
     // element of the tile before its barrier, and only the last pass writes it
-    run_passes<R, N, S, RMAX, TL, HC_FFT_NT, true, 0, FyFoldFirst<R, N, RMAX>::v>(src, dst, A, B, a.tw);
+    run_passes<R, N, S, RMAX, TL, NT, true, 0, FyFoldFirst<R, N, RMAX>::v>(src, dst, A, B, a.tw);
 }
 
 // FP64: the compiler's own register budget
 template <typename R, int N, int S, int RMAX>
-__global__ void __launch_bounds__(HC_FFT_NT) k_fft_y_t(FyArgs<R> a) { fft_y_tile<R, N, S, RMAX>(a); }
+__global__ void __launch_bounds__(FyThreads<R, N>::v) k_fft_y_t(FyArgs<R> a) { fft_y_tile<R, N, S, RMAX>(a); }
 // FP32: registers sized for FyMinBlocks resident blocks
 template <int N, int S, int RMAX>
-__global__ void __launch_bounds__(HC_FFT_NT, FyMinBlocks<float, N, RMAX>::v) k_fft_y_t32(FyArgs<float> a)
+__global__ void __launch_bounds__(FyThreads<float, N>::v, FyMinBlocks<float, N, RMAX>::v) k_fft_y_t32(FyArgs<float> a)
 {
     fft_y_tile<float, N, S, RMAX>(a);
 }
