@@ -279,15 +279,20 @@ def run_gpu(args, ws, rank):
         barrier()
         t0 = time.perf_counter()
         c = engine.Channel(p)
+        ta = time.perf_counter()
         c.load(host)
+        tb = time.perf_counter()
         c.initialize()
+        tc = time.perf_counter()
         for _ in range(args.steps):
             c.step(1)
+        td = time.perf_counter()
         outs = {f: c.download(f, out=res[f]) for f in ("u", "v", "w", "p", "t")}
         outs = None
         barrier()
         t1 = time.perf_counter()
         c.close()
+        parts = {"create": ta - t0, "upload": tb - ta, "initialize": tc - tb, "steps": td - tc, "download": t1 - td}
         el = max_over_ranks(t1 - t0)
         from hercules_b200.params import HcDiag
         import ctypes
@@ -295,7 +300,8 @@ def run_gpu(args, ws, rank):
                "h2d_bytes_per_step": int(5 * npts * 8 / args.steps),
                "d2h_bytes_per_step": int((5 * npts * 8) / args.steps + ctypes.sizeof(HcDiag)),
                "includes": "create + upload of 5 pinned host fields + initialize + K x (hc_step(1) with diag "
-                           "copy-back) + download of 5 fields into pinned host buffers, wall clock"}
+                           "copy-back) + download of 5 fields into pinned host buffers, wall clock",
+               "parts_ms": {k: round(v * 1e3, 2) for k, v in parts.items()}}
         del outs
 
     if ws > 1:

@@ -540,8 +540,8 @@ template <typename R, int N> static int fft_t_op(hc_handle* h, int op, const voi
         }
         return HC_OK;
     }
-    if (op == 1) k_fft_x_r2c_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
-    else if (op == 2) k_fft_x_c2r_t<R, N, RM><<<grid, HC_FFT_NT, sx, h->st>>>(*(const FxArgs<R>*)args);
+    if (op == 1) k_fft_x_r2c_t<R, N, RM><<<grid, FxThreads<R, N>::v, sx, h->st>>>(*(const FxArgs<R>*)args);
+    else if (op == 2) k_fft_x_c2r_t<R, N, RM><<<grid, FxThreads<R, N>::v, sx, h->st>>>(*(const FxArgs<R>*)args);
     else if (op == 3) FyKernel<R, N, -1, RM>::f<<<grid, FyThreads<R, N>::v, sy, h->st>>>(*(const FyArgs<R>*)args);
     else FyKernel<R, N, 1, RM>::f<<<grid, FyThreads<R, N>::v, sy, h->st>>>(*(const FyArgs<R>*)args);
     return HC_OK;
@@ -581,7 +581,7 @@ template <typename R> static long long fft_t_xblocks(int n, long long nrows)
 {
     long long lines = 1;
     switch (n) {
-#define HC_LEN_CASE(N) case N: lines = FxLines<N>::v; break;
+#define HC_LEN_CASE(N) case N: lines = FxLines<R, N>::v; break;
     HC_FFT_T_LENGTHS(HC_LEN_CASE)
 #undef HC_LEN_CASE
     }

@@ -269,8 +269,14 @@ template <typename R> struct FyArgs {
     const int* halt;
 };
 
-// x: about 2048 complex values per block (at least one line)
-template <int N> struct FxLines { static constexpr int v = N >= 2048 ? 1 : 2048 / N; };
+// x: about 2048 complex values per block of 256 threads in FP64; in FP32 1024
+// values per block of 128 threads (at 512 x 384 x 256, 4 fields: c2r 488 -> 463
+// us; 2048 values with 128 threads, or 1024 with 64, were slower)
+template <typename R, int N> struct FxLines {
+    static constexpr int pts = sizeof(R) == sizeof(float) ? 1024 : 2048;
+    static constexpr int v = N >= pts ? 1 : pts / N;
+};
+template <typename R, int N> struct FxThreads { static constexpr int v = sizeof(R) == sizeof(float) ? 128 : 256; };
 #define HC_FFT_NT 256
 // y: tiles of 8 columns with 16 threads a column (64-byte row segments in FP32,
 // 128 in FP64), 4 columns for FP32 256-point columns; below 64 points 8 columns
@@ -287,7 +293,7 @@ template <typename R, int N> struct FyThreads { static constexpr int v = N >= 64
 
 template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_x_smem()
 {
-    return (size_t)FBufs<N, RMAX>::x * FxLines<N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
+    return (size_t)FBufs<N, RMAX>::x * FxLines<R, N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
 }
 template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_y_smem()
 {
@@ -349,10 +355,11 @@ template <typename R, int N, int S> struct YColsOut {
 // x direction, forward: real rows -> nx/2 modes, divided by nx
 // ----------------------------------------------------------------------------
 template <typename R, int N, int RMAX>
-__global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_r2c_t(FxArgs<R> a)
+__global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_r2c_t(FxArgs<R> a)
 {
+    constexpr int NTX = FxThreads<R, N>::v;
     typedef typename V2<R>::T T2;
-    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, L = FxLines<N>::v;
+    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, L = FxLines<R, N>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
     // pass q (not the last) writes A for even q, B for odd q; the last pass lands
@@ -367,11 +374,11 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_r2c_t(FxArgs<R> a)
     constexpr int np = FPlan<N, RMAX>::npass;
     T2* Z = (np % 2 == 1) ? A : B;
     const SmemIO<T2, LS, G> zout{Z};
-    run_passes<R, N, -1, RMAX, L, HC_FFT_NT, false, 0>(src, zout, A, B, a.tw);
+    run_passes<R, N, -1, RMAX, L, NTX, false, 0>(src, zout, A, B, a.tw);
     __syncthreads();
     T2* out = reinterpret_cast<T2*>(a.out[f]) + row0 * N;
     const R sc = a.scale;
-    for (int idx = threadIdx.x; idx < nr * N; idx += HC_FFT_NT) {
+    for (int idx = threadIdx.x; idx < nr * N; idx += NTX) {
         const int line = idx / N, l = idx - line * N;
         const T2 z = Z[line * LS + fpi<G>(l)];
         T2 zc = Z[line * LS + fpi<G>(l == 0 ? 0 : N - l)];
@@ -387,10 +394,11 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_r2c_t(FxArgs<R> a)
 // x direction, inverse: nx/2 modes -> real rows (unnormalised), stored or added
 // ----------------------------------------------------------------------------
 template <typename R, int N, int RMAX>
-__global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
+__global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_c2r_t(FxArgs<R> a)
 {
+    constexpr int NTX = FxThreads<R, N>::v;
     typedef typename V2<R>::T T2;
-    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, L = FxLines<N>::v;
+    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, L = FxLines<R, N>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
     // the pre-split lines Zs feed pass 0; later passes alternate A and Zs
@@ -415,13 +423,13 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
     if constexpr (sizeof(R) == 8) {
         // FP64: one thread per mode, the partner read again; the loads of four
         // modes are issued before any of them is split
-        constexpr int IT = (L * N + HC_FFT_NT - 1) / HC_FFT_NT;
+        constexpr int IT = (L * N + NTX - 1) / NTX;
 #pragma unroll
         for (int q0 = 0; q0 < IT; q0 += 4) {
             T2 xs[4], ys[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int idx = threadIdx.x + (q0 + q) * HC_FFT_NT;
+                const int idx = threadIdx.x + (q0 + q) * NTX;
                 const int line = idx / N, l = idx - line * N;
                 xs[q] = mk2<R>(R(0), R(0));
                 ys[q] = xs[q];
@@ -432,7 +440,7 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int idx = threadIdx.x + (q0 + q) * HC_FFT_NT;
+                const int idx = threadIdx.x + (q0 + q) * NTX;
                 if (q0 + q >= IT || idx >= L * N) break;
                 const int line = idx / N, l = idx - line * N;
                 Zs[line * LS + fpi<G>(l)] = zsplit(xs[q], ys[q], l);
@@ -441,16 +449,16 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
         __syncthreads();
         const SmemIO<T2, LS, G> src64{Zs};
         const XRowsOut<T2, N> dst64{reinterpret_cast<T2*>(a.out[f]) + row0 * N, nr, a.add[f]};
-        run_passes<R, N, 1, RMAX, L, HC_FFT_NT, false, 0>(src64, dst64, A, B, a.tw);
+        run_passes<R, N, 1, RMAX, L, NTX, false, 0>(src64, dst64, A, B, a.tw);
         return;
     }
     // all of a thread's pairs are loaded before any is used, so the loads overlap
     constexpr int NP = N / 2 + 1;
-    constexpr int ROUNDS = (L * NP + HC_FFT_NT - 1) / HC_FFT_NT;
+    constexpr int ROUNDS = (L * NP + NTX - 1) / NTX;
     T2 xs[ROUNDS], ys[ROUNDS];
 #pragma unroll
     for (int q = 0; q < ROUNDS; ++q) {
-        const int idx = threadIdx.x + q * HC_FFT_NT;
+        const int idx = threadIdx.x + q * NTX;
         const int line = idx / NP, l = idx - line * NP;
         xs[q] = mk2<R>(R(0), R(0));
         ys[q] = xs[q];
@@ -461,7 +469,7 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
     }
 #pragma unroll
     for (int q = 0; q < ROUNDS; ++q) {
-        const int idx = threadIdx.x + q * HC_FFT_NT;
+        const int idx = threadIdx.x + q * NTX;
         if (idx >= L * NP) break;
         const int line = idx / NP, l = idx - line * NP;
         Zs[line * LS + fpi<G>(l)] = zsplit(xs[q], ys[q], l);
@@ -470,7 +478,7 @@ __global__ void __launch_bounds__(HC_FFT_NT) k_fft_x_c2r_t(FxArgs<R> a)
     __syncthreads();
     const SmemIO<T2, LS, G> src{Zs};
     const XRowsOut<T2, N> dst{reinterpret_cast<T2*>(a.out[f]) + row0 * N, nr, a.add[f]};
-    run_passes<R, N, 1, RMAX, L, HC_FFT_NT, false, 0>(src, dst, A, B, a.tw);
+    run_passes<R, N, 1, RMAX, L, NTX, false, 0>(src, dst, A, B, a.tw);
 }
 
 // ----------------------------------------------------------------------------
