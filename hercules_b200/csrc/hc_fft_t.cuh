@@ -269,25 +269,23 @@ template <typename R> struct FyArgs {
     const int* halt;
 };
 
-// x: about 2048 complex values per block of 256 threads in FP64; in FP32 1024
-// values per block of 128 threads (at 512 x 384 x 256, 4 fields: c2r 488 -> 463
-// us; 2048 values with 128 threads, or 1024 with 64, were slower)
-template <typename R, int N> struct FxLines {
-    static constexpr int pts = sizeof(R) == sizeof(float) ? 1024 : 2048;
-    static constexpr int v = N >= pts ? 1 : pts / N;
-};
-template <typename R, int N> struct FxThreads { static constexpr int v = sizeof(R) == sizeof(float) ? 128 : 256; };
+// x: 1024 complex values (at least one line) per block of 128 threads (against
+// 2048 values with 256 threads: FP32 c2r 488 -> 463 us at 512 x 384 x 256, 4
+// fields; FP64 r2c 179 -> 164 us and c2r 116 -> 106 us at 256 x 256 x 128;
+// 2048 values with 128 threads, or 1024 with 64, were slower)
+template <typename R, int N> struct FxLines { static constexpr int v = N >= 1024 ? 1 : 1024 / N; };
+template <typename R, int N> struct FxThreads { static constexpr int v = 128; };
 #define HC_FFT_NT 256
 // y: tiles of 8 columns with 16 threads a column (64-byte row segments in FP32,
-// 128 in FP64), 4 columns for FP32 256-point columns; below 64 points 8 columns
-// with 256 threads. Narrower tiles keep more, smaller blocks resident: against
-// 16 columns with 256 threads, at 512 x 384 x 256 (3 and 4 fields) FP32 forward
-// 359 -> 322 us and inverse 480 -> 423 us, FP64 inverse 1034 -> 987 us; FP32
-// 256-point columns (256 x 256 x 128 spectral, 4 columns) 194 -> 105 and 132 ->
-// 75 us. 32 columns with 512 threads were slower (404 and 525 us), and 4 columns
-// of 384 points too (417 and 553 us).
+// 128 in FP64), 4 columns for 256-point columns; below 64 points 8 columns with
+// 256 threads. Narrower tiles keep more, smaller blocks resident: against 16
+// columns with 256 threads, at 512 x 384 x 256 (3 and 4 fields) FP32 forward
+// 359 -> 322 us and inverse 480 -> 423 us, FP64 inverse 1034 -> 987 us;
+// 256-point columns (256 x 256 x 128 spectral, 4 columns) FP32 194 -> 105 and
+// 132 -> 75 us, FP64 244 -> 177 and 169 -> 122 us. 32 columns with 512 threads
+// were slower (404 and 525 us), and 4 columns of 384 points too (417 and 553 us).
 template <typename R, int N> struct FyLines {
-    static constexpr int v = N >= 64 ? ((sizeof(R) == sizeof(float) && N == 256) ? 4 : 8) : 8;
+    static constexpr int v = N >= 64 ? (N == 256 ? 4 : 8) : 8;
 };
 template <typename R, int N> struct FyThreads { static constexpr int v = N >= 64 ? FyLines<R, N>::v * 16 : HC_FFT_NT; };
 
