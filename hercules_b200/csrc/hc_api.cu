@@ -870,8 +870,8 @@ template <typename R> static int launch_column_fd(hc_handle* h, const ColArgs<R>
 }
 template <typename R, int K> static int col_t_k(hc_handle* h, const ColTArgs<R>& ct)
 {
-    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
-    k_column_t_warp<R, K><<<nb, CW_WARPS * 32, 0, h->st>>>(ct);
+    const unsigned nb = (unsigned)((h->g.ncol + CT_COLS - 1) / CT_COLS);
+    k_column_t_tile<R, K><<<nb, CT_COLS * 32, column_t_tile_smem<K>(sizeof(typename V2<R>::T)), h->st>>>(ct);
     CKL();
     return HC_OK;
 }

@@ -277,50 +277,6 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_fd_warp(ColArgs<R> 
     }
 }
 
-// Temperature Helmholtz solve (tbnd), warp per column.
-template <typename R, int K>
-__global__ void __launch_bounds__(CW_WARPS * 32) k_column_t_warp(ColTArgs<R> a)
-{
-    if (a.halt && *a.halt) return;
-    const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    const long long ncol = a.g.ncol;
-    const long long c = (long long)blockIdx.x * CW_WARPS + wp;
-    if (c >= ncol) return;
-    const int nz = a.g.nz;
-    const int l = (int)(c % a.g.nxh), m = (int)(c / a.g.nxh);
-    const bool is00 = (c == 0);
-    const double rk = a.rk_c;
-    const double lam = __ldg(a.c.hxt + l) + __ldg(a.c.hyt + m);
-    const double* dg = is00 ? a.c.d0t : a.c.dgt;
-    const int r0 = ln * K;
-    double2 d[1][K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-        const int r = r0 + i;
-        if (r < nz) {
-            d[0][i] = ld2<R>(a.qt, (long long)r * ncol + c);
-            if (is00 && r == 0) d[0][i].x += a.bct0;
-            if (is00 && r == nz - 1) d[0][i].x += a.bct1;
-        } else {
-            d[0][i] = make_double2(0, 0);
-        }
-    }
-    auto cf = [&](int r, double& aa, double& bb, double& cc) {
-        if (r < nz) {
-            aa = rk * __ldg(a.c.at + r);
-            cc = rk * __ldg(a.c.ct + r);
-            bb = 1.0 + rk * (-lam + __ldg(dg + r));
-        } else { aa = 0.0; bb = 1.0; cc = 0.0; }
-    };
-    warp_partition_solve<K, 1>(cf, d, ln);
-    const bool tr = spec_truncated(l, m, a.g.ny, a.ltr, a.mtr);
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-        const int r = r0 + i;
-        if (r < nz) st2<R>(a.out, (long long)r * ncol + c, tr ? make_double2(0, 0) : d[0][i]);
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Columns of CT_COLS adjacent wavenumber pairs staged in shared memory, so that
 // every global load and store is a coalesced row segment of CT_COLS modes
@@ -763,4 +719,89 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     }
     __syncthreads();
     store(a.psi, TU, nz);
+}
+
+// ---------------------------------------------------------------------------
+// Temperature Helmholtz solve (tbnd) through one coalescing tile: a block of
+// CT_COLS warps loads the rows of CT_COLS adjacent columns of q_t with
+// row-contiguous loads, each warp solves one column in FP64 from the tile, and
+// the solution (0 on truncated modes) leaves through the tile with
+// row-contiguous stores. All of a block's loads come before its stores, so the
+// solution may overwrite q_t. (One warp per column reading and writing a row a
+// lane: 76 -> 67 us mixed, 91 -> 68 us FP64 a launch at 256 x 256 x 128.)
+// ---------------------------------------------------------------------------
+template <int K> __host__ size_t column_t_tile_smem(size_t elem) { return (size_t)CT_COLS * ct_stride<K>() * elem; }
+
+template <typename R, int K>
+__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_t_tile(ColTArgs<R> a)
+{
+    typedef typename V2<R>::T TT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (a.halt && *a.halt) return;
+    const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const long long ncol = a.g.ncol;
+    const long long c0 = (long long)blockIdx.x * CT_COLS;
+    const long long c = c0 + wp;
+    const int nz = a.g.nz;
+    constexpr int STR = ct_stride<K>();
+    TT* TQ = reinterpret_cast<TT*>(smem_raw);
+    {
+        TT v[K];
+#pragma unroll
+        for (int it = 0; it < K; ++it) {
+            const int idx = threadIdx.x + it * CT_COLS * 32;
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            const long long cc = c0 + cb;
+            v[it] = (idx < nz * CT_COLS && cc < ncol) ? a.qt[(long long)r * ncol + cc] : mk2<R>(R(0), R(0));
+        }
+#pragma unroll
+        for (int it = 0; it < K; ++it) {
+            const int idx = threadIdx.x + it * CT_COLS * 32;
+            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            if (idx < nz * CT_COLS) TQ[cb * STR + (r % K) * CT_RP + r / K] = v[it];
+        }
+    }
+    __syncthreads();
+    TT* SQ = TQ + wp * STR;
+    if (c < ncol) {
+        const int l = (int)(c % a.g.nxh), m = (int)(c / a.g.nxh);
+        const bool is00 = (c == 0);
+        const double rk = a.rk_c;
+        const double lam = __ldg(a.c.hxt + l) + __ldg(a.c.hyt + m);
+        const double* dg = is00 ? a.c.d0t : a.c.dgt;
+        const int r0 = ln * K;
+        double2 d[1][K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const int r = r0 + i;
+            if (r < nz) {
+                const TT x = SQ[i * CT_RP + ln];
+                d[0][i] = make_double2((double)x.x, (double)x.y);
+                if (is00 && r == 0) d[0][i].x += a.bct0;
+                if (is00 && r == nz - 1) d[0][i].x += a.bct1;
+            } else {
+                d[0][i] = make_double2(0, 0);
+            }
+        }
+        auto cf = [&](int r, double& aa, double& bb, double& cc) {
+            if (r < nz) {
+                aa = rk * __ldg(a.c.at + r);
+                cc = rk * __ldg(a.c.ct + r);
+                bb = 1.0 + rk * (-lam + __ldg(dg + r));
+            } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+        };
+        warp_partition_solve<K, 1>(cf, d, ln);
+        const bool tr = spec_truncated(l, m, a.g.ny, a.ltr, a.mtr);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const double2 v = tr ? make_double2(0, 0) : d[0][i];
+            SQ[i * CT_RP + ln] = mk2<R>((R)v.x, (R)v.y);
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nz * CT_COLS; idx += blockDim.x) {
+        const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+        const long long cc = c0 + cb;
+        if (cc < ncol) a.out[(long long)r * ncol + cc] = TQ[cb * STR + (r % K) * CT_RP + r / K];
+    }
 }
