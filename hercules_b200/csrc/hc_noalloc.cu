@@ -10,6 +10,7 @@
 // of the library image instead of in memory obtained at run time.
 #include <cuda_runtime.h>
 #include <mutex>
+#include <stdint.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -27,7 +28,10 @@
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 
 // Host code may not use g_noalloc_scratch as an address: on the host that name is
-// only a stand-in. The device address is looked up once per device.
+// only a stand-in. The device address is looked up once per device, on the first
+// call made with that device current, and kept for the life of the process: after
+// cudaDeviceReset on that device the cached address is stale, so a process that
+// resets a device must not call this entry point on it again.
 #define NOALLOC_MAX_DEVICES 64
 static double* g_scratch_addr[NOALLOC_MAX_DEVICES];
 static std::mutex g_scratch_mu;
@@ -103,7 +107,12 @@ extern "C" int hc_divergence_noalloc(const hc_params* p, const double* dz, const
     if (!p || !dz || !u || !v || !w || !out_dev) return HC_ERR_ARG;
     if (p->cds != 1 && p->cds != 2) return HC_ERR_ARG;
     if (p->precision != HC_PREC_FP64 && p->precision != HC_PREC_MIXED) return HC_ERR_ARG;
-    if (p->nx < 4 || p->ny < 4 || p->nz < 2) return HC_ERR_ARG;
+    // the same grid rules as hc_create (even nx and ny, src/module_parameters.f90:266-270):
+    // with FP32 fields the kernel reads two adjacent x points as one 8-byte value, so an
+    // odd nx would put those reads at odd offsets
+    if (p->nx < 8 || p->ny < 4 || p->nz < 3 || (p->nx & 1) || (p->ny & 1)) return HC_ERR_PARAM;
+    // every load is 8 bytes wide (one double, or a pair of floats) and so is the result
+    if ((((uintptr_t)u) | ((uintptr_t)v) | ((uintptr_t)w) | ((uintptr_t)out_dev)) & 7u) return HC_ERR_ARG;
     const long long n = (long long)p->nx * p->ny * p->nz;
     if (p->nz > NOALLOC_NZ_MAX || n > 2147483647LL) {
         fprintf(stderr, "hercules_b200: hc_divergence_noalloc supports nz <= %d and nx*ny*nz < 2^31 "

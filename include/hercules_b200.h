@@ -194,10 +194,17 @@ int hc_kernel_profile(hc_handle* h, int max, char* names, double* total_ms,
  * receiving {mean |div|, signed div at the largest |div|, NaN flag} exactly as
  * hc_step's divergence diagnostic computes them. Scratch lives in one fixed
  * array per device (about 61 KB, held until exit): nz <= 4096 and
- * nx*ny*nz < 2^31, else HC_ERR_SIZE. The first call on a device looks up that
- * array's address; make it before any stream capture. Calls share the array, so
- * calls that overlap on the GPU race with each other. `stream` is a
- * cudaStream_t (NULL for the default stream); the call does not synchronise. */
+ * nx*ny*nz < 2^31, else HC_ERR_SIZE. nx and ny must be even (nx >= 8, ny >= 4,
+ * nz >= 3), else HC_ERR_PARAM; u, v, w and out_dev must be 8-byte aligned, else
+ * HC_ERR_ARG; cds must be 1 or 2. All of these are checked before any device
+ * work. The first call on a device looks up that array's address and keeps it
+ * for the life of the process (do not call again on a device after
+ * cudaDeviceReset); make it before any stream capture. Calls share the array,
+ * so calls that overlap on the GPU (several streams or host threads) race with
+ * each other. `stream` is a cudaStream_t (NULL for the default stream); the
+ * call does not synchronise: dz is copied asynchronously on that stream, so if
+ * it is page-locked host memory it must stay valid and unchanged until the
+ * stream has passed the call. */
 int hc_divergence_noalloc(const hc_params* p, const double* dz, const void* u,
                           const void* v, const void* w, double* out_dev, void* stream);
 

@@ -1,0 +1,159 @@
+"""GPU parity of the kernels the production grids instantiate, against the CPU
+FP64 oracle, through the C-ABI.
+
+The transforms are compiled once per length (x half-lengths and y lengths 8 ...
+512 of the form 2^a 3^b 5^c), each with its own passes, lines per block and
+first-pass folding, and the column solves once per depth class K = ceil(nz/32).
+The small parity cases of the other test files reach only the short lengths and
+K <= 3, so here every compiled length and depth is run at a size the oracle
+finishes in seconds: the transform length on one axis at full size with the
+other axes small, the production planes (512 x 384 and 256 x 256) with 8
+levels, and the column depths with a small plane.
+
+Tolerances (per field, max-norm of the difference over the oracle field's max):
+FP64 <= 1e-10 after the stated steps; FP32-mixed velocities (and temperature)
+<= 1e-5. The reference's FFT is `mpi_2d_fft` (src/module_tools.f90:518-700),
+its column solves `poisson_solver_fft` (src/module_poisson_solver.f90:483-658)
+and `poisson_solver_fft_spec` (src/module_spectral.f90:602-746).
+"""
+import numpy as np
+import pytest
+
+from hercules_b200 import inputs
+from hercules_b200.params import (PREC_MIXED, Params, config_channel_fd,
+                                  config_open_channel_spectral)
+from parity_util import rel_err
+
+FP64_TOL = 1e-10
+MIXED_TOL = 1e-5
+PI = 3.1415926535897932
+
+# every length with a compile-time transform (the x half-length nx/2 and ny)
+FFT_LENGTHS = (8, 12, 16, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512)
+
+
+def _fd(nx, ny, nz, **kw):
+    base = dict(lx=4.0, ly=3.0, lz=2.0, nx=nx, ny=ny, nz=nz, zstretch=1.0, ochannel=0, dp_opt=1,
+                cds=2, dts=2, nu=1.0 / 300.0, alpha=1.0 / 300.0 / 0.71, dt=1e-3, imax=100)
+    base.update(kw)
+    return Params(**base)
+
+
+def _sp(nx, ny, nz, **kw):
+    base = dict(lx=2 * PI, ly=PI, lz=1.0, nx=nx, ny=ny, nz=nz, zstretch=1.0, ochannel=1, dp_opt=1,
+                cds=3, issk=1, dts=2, nu=1.0 / 180.0, alpha=1.0 / 180.0 / 0.71, dt=1e-3, imax=100,
+                isscalar=1, got=0.3, tbot=-1.0, ttop=0.0)
+    base.update(kw)
+    return Params(**base)
+
+
+def _compare(p, fields, nsteps, oracle_lib, engine, precisions=(0, 1), extra=()):
+    """One oracle run, then the GPU engine in each precision from the same state."""
+    o = oracle_lib.Oracle(p)
+    o.load(fields)
+    o.initialize()
+    rc, od = o.step(nsteps)
+    assert rc == 0
+    names = ["u", "v", "w", "p"] + (["t"] if p.isscalar else []) + list(extra)
+    ref = {f: o.get(f) for f in names}
+    o.close()
+    errs = {}
+    for prec in precisions:
+        c = engine.Channel(p.replace(precision=prec))
+        c.load(fields)
+        c.initialize()
+        gd = c.step(nsteps)
+        assert gd[-1]["nan_flag"] == 0
+        for f in names:
+            errs[(prec, f)] = rel_err(c.download(f), ref[f])
+        c.close()
+    bad = []
+    for (prec, f), e in errs.items():
+        if prec == 0 and e > FP64_TOL:
+            bad.append(f"FP64 {f} {e:.3e}")
+        if prec == PREC_MIXED and f in ("u", "v", "w", "t") and e > MIXED_TOL:
+            bad.append(f"mixed {f} {e:.3e}")
+    assert not bad, "; ".join(bad)
+    return errs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", FFT_LENGTHS)
+@pytest.mark.parametrize("axis", ["x", "y"])
+@pytest.mark.parametrize("method", ["fd4", "spectral"])
+def test_every_transform_length(n, axis, method, oracle_lib, engine):
+    """Each compiled transform length on one axis (the other axis at 16 points,
+    5 levels), FD4 and pseudo-spectral, FP64 and mixed, 6 steps."""
+    nx, ny = (2 * n, 16) if axis == "x" else (16, n)
+    p = _fd(nx, ny, 5, isscalar=1, got=0.2) if method == "fd4" else _sp(nx, ny, 5)
+    _compare(p, inputs.small_random(p, seed=21), 6, oracle_lib, engine)
+
+
+PLANES = {
+    # the config-3 plane (x half-length 256, y 384) in config-3 physics
+    "fd4_512x384x8": config_channel_fd(nx=512, ny=384, nz=8),
+    # the config-2 plane (x half-length 128, y 256) in config-2 physics
+    "spectral_256x256x8": config_open_channel_spectral(nx=256, ny=256, nz=8),
+    # the other method on each plane, with temperature on the FD one
+    "fd4_256x256x8_scalar": _fd(256, 256, 8, ochannel=1, isscalar=1, got=0.5, tbot=-1.0, ttop=0.0),
+    "spectral_512x384x8": _sp(512, 384, 8, ochannel=0, isscalar=0, lx=4 * PI, ly=4 * PI / 3, lz=2.0),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(PLANES))
+def test_production_planes(name, oracle_lib, engine):
+    """The production x-y planes with 8 levels, FP64 and mixed, 4 steps."""
+    p = PLANES[name]
+    _compare(p, inputs.small_random(p, seed=5), 4, oracle_lib, engine)
+
+
+DEPTHS = {
+    # warp-per-column solves, K = ceil(nz/32) rows a lane
+    "fd4_nz128": _fd(32, 24, 128, isscalar=1, got=0.3),
+    "fd4_nz129": _fd(32, 24, 129, isscalar=1, got=0.3, ochannel=1, tbot=-1.0, ttop=0.0),
+    "fd4_nz200": _fd(32, 24, 200),
+    "fd4_nz256_config3_depth": config_channel_fd(nx=32, ny=24, nz=256),
+    "fd2_nz256_scalar": _fd(16, 12, 256, cds=1, isscalar=1, got=0.2),
+    # beyond 256 levels: one thread per column (k_column_fd, k_column_t)
+    "fd4_nz300_thread_per_column": _fd(16, 12, 300, isscalar=1, got=0.2),
+    # spectral column solves: the tiled kernel up to 128 levels, the warp kernel above
+    "spectral_nz128_config2_depth": config_open_channel_spectral(nx=32, ny=24, nz=128),
+    "spectral_nz129": _sp(16, 12, 129),
+    "spectral_nz256": _sp(16, 12, 256, ochannel=0, dp_opt=2),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(DEPTHS))
+def test_column_depths(name, oracle_lib, engine):
+    """Every column-solve depth class the production grids use, FP64 and mixed,
+    5 steps (histories and phi compared too in FP64)."""
+    p = DEPTHS[name]
+    extra = ("ff", "gg", "hh") if p.cds != 3 else ("phi",)
+    _compare(p, inputs.small_random(p, seed=13), 5, oracle_lib, engine, extra=extra)
+
+
+@pytest.mark.gpu
+def test_config3_grid_statistics_and_diagnostics(oracle_lib, engine):
+    """Config-3 plane: the statistics, bulk velocity and CFL of 3 FP64 steps."""
+    p = config_channel_fd(nx=512, ny=384, nz=8)
+    fields = inputs.poiseuille_noise(p, seed=3)
+    o = oracle_lib.Oracle(p)
+    o.load(fields)
+    o.initialize()
+    rc, od = o.step(3)
+    assert rc == 0
+    c = engine.Channel(p)
+    c.load(fields)
+    c.initialize()
+    gd = c.step(3)
+    for f in ("mean_u", "mean_v", "mean_w", "mean_uu", "mean_vv", "mean_ww", "mean_uw", "mean_vw"):
+        b = o.get(f)
+        assert rel_err(c.download(f), b) <= FP64_TOL, f
+    for a, b in zip(gd, od):
+        assert abs(a["cfl"] - b["cfl"]) <= FP64_TOL * abs(b["cfl"])
+        assert abs(a["ubar"] - b["ubar"]) <= FP64_TOL
+        assert abs(a["dpx_drive"] - b["dpx_drive"]) <= FP64_TOL * max(1.0, abs(b["dpx_drive"]))
+    c.close()
+    o.close()

@@ -55,12 +55,36 @@ def test_noalloc_divergence_matches_step_diagnostic(engine, prec, cds):
     c.close()
 
 
-@pytest.mark.gpu
-def test_noalloc_rejects_sizes_beyond_its_scratch(engine):
+HC_ERR_ARG, HC_ERR_PARAM, HC_ERR_SIZE = -1, -2, -8
+
+# Arguments the entry point refuses before it touches the GPU: the pointers are
+# never dereferenced, so these cases run without a device.
+REJECTED = {
+    "odd_nx": (dict(nx=33), 4096, HC_ERR_PARAM),
+    "odd_ny": (dict(ny=25), 4096, HC_ERR_PARAM),
+    "odd_nx_fp64": (dict(nx=33, precision=PREC_FP64), 4096, HC_ERR_PARAM),
+    "nz_too_small": (dict(nz=1), 4096, HC_ERR_PARAM),
+    "spectral_cds": (dict(cds=3), 4096, HC_ERR_ARG),
+    "unknown_precision": (dict(precision=7), 4096, HC_ERR_ARG),
+    "misaligned_u": (dict(), 4096 + 4, HC_ERR_ARG),
+    "misaligned_fp64": (dict(precision=PREC_FP64), 4096 + 4, HC_ERR_ARG),
+    "nz_beyond_scratch": (dict(nx=8, ny=8, nz=5000), 4096, HC_ERR_SIZE),
+    "points_beyond_2_31": (dict(nx=2048, ny=2048, nz=1024), 4096, HC_ERR_SIZE),
+}
+
+
+@pytest.mark.parametrize("case", list(REJECTED))
+def test_noalloc_refuses_bad_arguments_without_device_work(case):
+    from hercules_b200 import build, engine
+    build.build()
     L = engine.load_library()
-    p = Params(nx=8, ny=8, nz=5000, cds=2)
+    kw, uaddr, code = REJECTED[case]
+    base = dict(nx=32, ny=24, nz=17, cds=2, precision=PREC_MIXED)
+    base.update(kw)
+    p = Params(**base)
     cp = p.to_c()
     dz = np.ones(p.nz + 4)
-    dummy = ctypes.c_void_p(1)
-    rc = L.hc_divergence_noalloc(ctypes.byref(cp), dz.ctypes.data, dummy, dummy, dummy, dummy, None)
-    assert rc == -8     # HC_ERR_SIZE, before any device work
+    aligned = ctypes.c_void_p(4096)
+    rc = L.hc_divergence_noalloc(ctypes.byref(cp), dz.ctypes.data, ctypes.c_void_p(uaddr), aligned, aligned,
+                                 aligned, None)
+    assert rc == code, (case, rc)
