@@ -43,8 +43,10 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "channel_fd4_512x384x256"
 # CPU samples of the same physics, sized for 10-30 s of host work
-CPU_SAMPLE_GRID = (512, 384, 32)
-REF_STEP_GRID = (256, 192, 32)
+# (a 16-level slab of the configured 512 x 384 plane: the same transform lengths and
+# per-column work as the full grid, whose oracle step would take about a minute)
+CPU_SAMPLE_GRID = (512, 384, 16)
+REF_STEP_GRID = (512, 384, 16)
 
 
 def parse():
@@ -168,24 +170,46 @@ ALG_WORDS_SUB = {
 }
 
 
-# DRAM bytes (read + write) of one launch per kernel category, FP32-mixed, from
-# the ncu capture of the 256x192x256 case (profiles/traffic_fd_kernels_mixed_256x192x256.md)
-# scaled by the point ratio to the grids below (every kernel streams its fields once)
+# DRAM bytes (read + write) of one launch per kernel category, FP32-mixed, measured
+# by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the 256x192x256 case
+# and scaled by the point ratio to the grids below (every kernel streams its
+# fields once, so traffic grows in proportion to the points).
+TRAFFIC_CAPTURE = {"case": "channel_fd4_256x192x256 mixed", "metrics": "dram__bytes_read.sum + dram__bytes_write.sum",
+                   "scaled_by_points": True}
 _TRAFFIC_256x192x256 = {"rhs_momentum": 647.9e6, "column_fd": 295.4e6, "fft_x_r2c": 253.1e6, "fft_y_fwd": 239.9e6,
                         "fft_y_inv": 343.7e6, "fft_x_c2r": 406.8e6, "div_check": 155.0e6, "stats": 1362.9e6}
 TRAFFIC = {(w, k): v * (WORKLOADS[w][0] * WORKLOADS[w][1] * WORKLOADS[w][2]) / (256 * 192 * 256)
            for w in ("channel_fd4_512x384x256", "channel_fd4_256x192x256") for k, v in _TRAFFIC_256x192x256.items()}
 
+# FP32 storage: the statistics kernel sums each window of this many steps in FP32
+# and folds the window into the FP64 accumulators on its last step
+STATS_WINDOW = 16
+
+
+def stats_bytes_per_point(kind: str, wbytes: int) -> float:
+    """Bytes per point and step the statistics kernel must move: u, v, w, t (and the
+    uhx, vhy snapshots on the FD path) in the storage type, and the 11 accumulators
+    read and written -- FP64 sums with FP64 storage; with FP32 storage FP32 window
+    sums, plus once a window the fold (window read, FP64 sum read and written,
+    window cleared)."""
+    reads = (6 if kind == "fd" else 4) * wbytes
+    if wbytes == 8:
+        return reads + 11 * 2 * 8
+    return reads + 11 * 2 * 4 + 11 * (4 + 16 + 4) / STATS_WINDOW
+
 
 def alg_bytes_step(kernel: str, npts: int, wbytes: int, kind: str, nsub: int = 3) -> float:
     """Algorithmic bytes of one time step in one kernel category."""
     if kernel == "stats":
-        # reads u, v, w, t (+ uhx, vhy on the FD path) in the storage type; 11 FP64 accumulators RMW
-        return npts * ((6 if kind == "fd" else 4) * wbytes + 22 * 8)
+        return npts * stats_bytes_per_point(kind, wbytes)
+    if kind == "fd" and kernel == "div_check":
+        # sub-steps 1 and 2 check the divergence inside the next momentum RHS; the
+        # separate check runs once a step, after the last sub-step
+        nsub = 1
     return ALG_WORDS_SUB[kind].get(kernel, 0) * nsub * npts * wbytes
 
 
-def run_gpu(args, ws, rank):
+def run_gpu(args, ws, rank, hbm):
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -248,6 +272,15 @@ def run_gpu(args, ws, rank):
     pm = chans[PREC_MIXED].download("p")
     pf = chans[PREC_FP64].download("p")
     err["p"] = float(np.max(np.abs((pm - pm.mean()) - (pf - pf.mean()))) / np.max(np.abs(pf - pf.mean())))
+    if chans[PREC_FP64].p.isscalar:
+        a, b = chans[PREC_MIXED].download("t"), chans[PREC_FP64].download("t")
+        err["t"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    # the running statistics (sums over the same steps), each relative to its own max
+    for f in ("mean_u", "mean_v", "mean_w", "mean_uu", "mean_vv", "mean_ww", "mean_uw", "mean_vw") + \
+            (("mean_t", "mean_tt", "mean_tw") if chans[PREC_FP64].p.isscalar else ()):
+        a, b = chans[PREC_MIXED].download(f), chans[PREC_FP64].download(f)
+        den = float(np.max(np.abs(b)))
+        err[f] = float(np.max(np.abs(a - b)) / den) if den > 0 else float(np.max(np.abs(a)))
 
     # per-kernel CUDA-event profile of 2 steps of each run
     kern = {}
@@ -264,8 +297,10 @@ def run_gpu(args, ws, rank):
         for k, v in prof.items():
             avg = v["total_ms"] / max(v["launches"], 1)
             b = alg_bytes_step(k, npts, wb, kind) * nprof
+            gbs = (b / (v["total_ms"] * 1e-3) / 1e9) if b and v["total_ms"] > 0 else None
             kern[tag][k] = {"launches": v["launches"], "avg_ms": avg, "total_ms": v["total_ms"],
-                            "alg_gbs": (b / (v["total_ms"] * 1e-3) / 1e9) if b and v["total_ms"] > 0 else None}
+                            "alg_bytes_per_launch": b / max(v["launches"], 1) if b else None,
+                            "alg_gbs": gbs, "frac_of_hbm": gbs / hbm if gbs else None}
     for c in chans.values():
         c.close()
 
@@ -451,8 +486,10 @@ def main():
         line.update({"impl": "reference", "value": rate, "ms_per_step": el / args.steps * 1e3,
                      "dtype": "f64", "config": dict(cfg, sample_grid=list(g)),
                      "cpu_baseline": {"value": rate, "unit": "gridpoint-steps/s", "cores": ncores, "kind": "port",
-                                      "sample": f"{args.steps} steps of the same physics on {g[0]}x{g[1]}x{g[2]} "
-                                                "(the reference's Fortran/MPI code cannot be built here: no gfortran/MPI)"},
+                                      "sample": f"{args.steps} steps of the same physics on a {g[0]}x{g[1]}x{g[2]} "
+                                                f"slab of the {nx}x{ny}x{nz} grid (same plane and transform lengths; "
+                                                "per-point rate; the reference's Fortran/MPI code cannot be built "
+                                                "here: no gfortran/MPI)"},
                      "e2e": {"value": rate, "unit": "gridpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         print(json.dumps(line), flush=True)
         return
@@ -475,7 +512,7 @@ def main():
                      "roofline": None, "cpu_baseline": None, "e2e": None})
         print(json.dumps(line), flush=True)
         return
-    results, err, kern, e2e = run_gpu(args, ws, rank)
+    results, err, kern, e2e = run_gpu(args, ws, rank, hbm)
     if rank != 0:
         return
     from hercules_b200.params import PREC_FP64, PREC_MIXED
@@ -497,6 +534,7 @@ def main():
     npts = nx * ny * nz
     roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
             "frac": ach / hbm if ach else None, "peak_kind": peak_kind, "traffic": TRAFFIC.get((args.workload, dom)),
+            "traffic_capture": TRAFFIC_CAPTURE if (args.workload, dom) in TRAFFIC else None,
             "alg_bytes_per_launch": alg_bytes_step(dom, npts, 4, kind) / max(km[dom]["launches"] / 2, 1)}
     # whole-step HBM fraction with the fixed per-point accounting of an ideally
     # fused step: FD neutral RK3 131 words (117 field words + 14 FP64 mean words);
@@ -511,10 +549,10 @@ def main():
     adj = None if args.no_adjoint or is_spectral(args.workload) else run_adjoint()
     cpu = None
     if not args.no_cpu_baseline and args.gpus == 1:
-        rate, el = cpu_oracle_rate(CPU_SAMPLE_GRID, 1)
+        rate, el = cpu_oracle_rate(CPU_SAMPLE_GRID, 2)
         cpu = {"value": rate, "unit": "gridpoint-steps/s", "cores": ncores, "kind": "port",
-               "sample": f"1 step of the same physics on {CPU_SAMPLE_GRID[0]}x{CPU_SAMPLE_GRID[1]}x{CPU_SAMPLE_GRID[2]} "
-                         f"({el:.1f} s, OpenMP)"}
+               "sample": f"2 steps of the same physics on a {CPU_SAMPLE_GRID[0]}x{CPU_SAMPLE_GRID[1]}x{CPU_SAMPLE_GRID[2]} "
+                         f"slab of the {nx}x{ny}x{nz} grid ({el:.1f} s, OpenMP)"}
     line = dict(base)
     line.update({"value": mixed["value"], "ms_per_step": mixed["ms_per_step"], "dtype": "f32 fields/FFT + f64 Thomas",
                  "config": cfg, "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"]},
