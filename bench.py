@@ -62,6 +62,8 @@ def parse():
                     help="run one precision only (profiling); the headline needs both")
     ap.add_argument("--graph", action="store_true", help="replay each step from a captured CUDA graph")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing leg")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the adjoint/forward timing leg (Ekman 64x64x65) and print it")
     return ap.parse_args()
 
 
@@ -492,6 +494,11 @@ def main():
                                                 "here: no gfortran/MPI)"},
                      "e2e": {"value": rate, "unit": "gridpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         print(json.dumps(line), flush=True)
+        return
+
+    if args.adjoint_only:
+        if rank == 0:
+            print(json.dumps({"adjoint": run_adjoint(), "note": "adjoint leg only, not a headline line"}), flush=True)
         return
 
     if args.workload == "ensemble64":
