@@ -62,6 +62,7 @@ def parse():
                     help="run one precision only (profiling); the headline needs both")
     ap.add_argument("--graph", action="store_true", help="replay each step from a captured CUDA graph")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing leg")
+    ap.add_argument("--no-tune", action="store_true", help="ensemble: default tile shapes, no autotuner")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="run only the adjoint/forward timing leg (Ekman 64x64x65) and print it")
     return ap.parse_args()
@@ -413,8 +414,12 @@ def run_ensemble(args):
     from hercules_b200.params import PREC_FP64, PREC_MIXED
     torch.cuda.set_device(0)
     out = {}
+    tiles = {}
     for prec in (PREC_FP64, PREC_MIXED):
-        cases = inputs.ensemble_members(n=64, seed=1000, precision=prec)
+        # tile shapes of each of the four member grids from the autotuner
+        cases = inputs.ensemble_members(n=64, seed=1000, precision=prec, tune=not args.no_tune)
+        for p, _ in cases:
+            tiles[f"{p.nx}x{p.ny}x{p.nz}:{'mixed' if prec else 'fp64'}"] = list(p.tile)
         chans = []
         for p, fields in cases:
             c = engine.Channel(p)
@@ -429,7 +434,7 @@ def run_ensemble(args):
             e.step(args.steps)
         ms = e.last_ms
         out[prec] = {"value": npts * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps, "npts": npts,
-                     "launches": e.launches_per_step * args.steps, "clocks": clk.summary()}
+                     "launches": e.launches_per_step * args.steps, "clocks": clk.summary(), "tiles": tiles}
         e.close()
         for c in chans:
             c.close()
@@ -516,6 +521,7 @@ def main():
                      "fp64": {"value": r[PREC_FP64]["value"], "ms_per_step": r[PREC_FP64]["ms_per_step"]},
                      "mixed_speedup_vs_fp64": r[PREC_FP64]["ms_per_step"] / r[PREC_MIXED]["ms_per_step"],
                      "gpu_launches": int(r[PREC_MIXED]["launches"]), "clocks": r[PREC_MIXED]["clocks"],
+                     "tiles": r[PREC_MIXED]["tiles"],
                      "roofline": None, "cpu_baseline": None, "e2e": None})
         print(json.dumps(line), flush=True)
         return

@@ -104,12 +104,15 @@ def gaussian_body_force(p: Params, seed: int = 4, ell: float = 1.0, amp: float =
 ENSEMBLE_GRIDS = ((32, 32, 33), (48, 32, 49), (64, 48, 65), (96, 64, 65))
 
 
-def ensemble_members(n: int = 64, seed: int = 1000, precision: int = 0):
+def ensemble_members(n: int = 64, seed: int = 1000, precision: int = 0, tune: bool = False,
+                     tune_cache=None):
     """Seeded ensemble of independent closed channels: grid drawn uniformly from
     ENSEMBLE_GRIDS, Re_tau ~ U[100, 300] (nu = 1/Re_tau, constant pressure drive
     dp_opt=1), Richardson number ~ U[0, 1], Pr = 0.71, stable stratification
     (t: 0 at the bottom wall, 1 at the top), laminar Poiseuille plus 10% uniform
-    noise. Member q uses seed + q. Returns a list of (Params, fields)."""
+    noise. Member q uses seed + q. With tune=True the tile shapes of each distinct
+    grid come from the autotuner (needs the GPU; tune_cache: optional JSON path).
+    Returns a list of (Params, fields)."""
     from .params import config_channel_fd
     out = []
     for q in range(n):
@@ -130,4 +133,8 @@ def ensemble_members(n: int = 64, seed: int = 1000, precision: int = 0):
         w[-1] = 0.0
         t = (zc / p.lz)[:, None, None] + 0.01 * g.uniform(-1, 1, shape)
         out.append((p, {"u": u, "v": v, "w": w, "p": np.zeros(shape), "t": t}))
+    if tune:
+        from .autotune import tune_members
+        tuned = tune_members([p for p, _ in out], tune_cache)
+        out = [(q, f) for q, (_, f) in zip(tuned, out)]
     return out
