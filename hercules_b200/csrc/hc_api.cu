@@ -22,6 +22,7 @@
 #include "hc_column.cuh"
 #include "hc_rhs_tiled.cuh"
 #include "hc_rhs_tiled2.cuh"
+#include "hc_rhs_strip.cuh"
 #include "hc_column_warp.cuh"
 #include "hc_spec.cuh"
 #include "hc_adjoint.cuh"
@@ -255,6 +256,7 @@ struct hc_handle {
     long long pd_stride;     // partial slots per sub-step (max over the writers)
     dim3 rhs_grid;           // FD momentum RHS grid and its level chunk
     int rhs_kc;
+    int rhs_strip;           // FP32: the strip kernel (k_rhs_momentum_strip) runs the RHS
     DevScalars* sc;
     hc_diag* diag_dev;
     int diag_cap;
@@ -658,6 +660,8 @@ template <typename R> static int set_smem_attrs()
     if (sizeof(R) == sizeof(float)) {
         CK(cudaFuncSetAttribute(k_rhs_momentum_tiled2<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled2_smem(1)));
         CK(cudaFuncSetAttribute(k_rhs_momentum_tiled2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled2_smem(1)));
+        CK(cudaFuncSetAttribute(k_rhs_momentum_strip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem()));
+        CK(cudaFuncSetAttribute(k_rhs_momentum_strip<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem()));
     }
     return HC_OK;
 }
@@ -964,7 +968,9 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     m.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
     m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
     prof_begin(h, K_RHS_MOM);
-    if (sizeof(R) == sizeof(float))      // FP32: two x points a thread (64 x 8 tiles)
+    if (sizeof(R) == sizeof(float) && h->rhs_strip)   // FP32: products on strips (64 x 16 tiles)
+        k_rhs_momentum_strip<CDS><<<h->rhs_grid, 256, rhs_strip_smem(), h->st>>>(*(const RhsTArgs<float>*)&m);
+    else if (sizeof(R) == sizeof(float))      // FP32: two x points a thread (64 x 8 tiles)
         k_rhs_momentum_tiled2<CDS><<<h->rhs_grid, 256, rhs_tiled2_smem(m.with_t), h->st>>>(*(const RhsTArgs<float>*)&m);
     else
         k_rhs_momentum_tiled<R, CDS><<<h->rhs_grid, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
@@ -1808,8 +1814,10 @@ int hc_create(const hc_params* p, hc_handle** out)
         if (h->nbd > RED_BLOCKS) h->nbd = RED_BLOCKS;
         {
             // momentum RHS tiles: enough blocks for ~4 per SM, chunks of 4..32 levels
-            const int tx_pts = h->rsz == sizeof(float) ? R2_TX : RT_TX;
-            const int bx = (g.nx + tx_pts - 1) / tx_pts, by = (g.ny + RT_TY - 1) / RT_TY;
+            h->rhs_strip = h->rsz == sizeof(float) && rhs_strip_ok(p->nx, p->ny, p->u_mrf, p->dp_opt);
+            const int tx_pts = h->rhs_strip ? RS_TX : (h->rsz == sizeof(float) ? R2_TX : RT_TX);
+            const int ty_pts = h->rhs_strip ? RS_TY : RT_TY;
+            const int bx = (g.nx + tx_pts - 1) / tx_pts, by = (g.ny + ty_pts - 1) / ty_pts;
             int kc = p->tile[2] > 0 ? p->tile[2] : (int)((long long)bx * by * p->nz / (4LL * 148));
             if (p->tile[2] <= 0) { if (kc < 4) kc = 4; if (kc > 32) kc = 32; }
             if (kc < 1) kc = 1;

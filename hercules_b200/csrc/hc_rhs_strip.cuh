@@ -1,0 +1,507 @@
+// hc_rhs_strip.cuh -- FP32 momentum right-hand side (get_momentum_cnvdiff,
+// src/module_cnvdiff.f90:35-374) that evaluates every interpolant product only
+// where a flux difference reads it.
+//
+// In the reference's flux form, per equation and direction, a difference reads a
+// product on one axis only:
+//   U: d/dx uhx^2 (x),  d/dy uhy*vhx (y),  d/dz uhz*whx (own point)
+//   V: d/dx uhy*vhx (x), d/dy vhy^2 (y),   d/dz vhz*why (own point)
+//   W: d/dx uhz*whx (x), d/dy vhz*why (y),  w^2 in z (own point)
+// so uhx and uhz*whx are needed on an x strip of the tile (its rows, two extra
+// columns either side), vhy and vhz*why on a y strip (its columns, two extra rows
+// either side) and uhy*vhx on both strips -- never on the corners of the halo.
+// A block of 256 threads owns a 64 x 16 tile (a thread: two adjacent x points in
+// two adjacent rows) and marches up a chunk of k levels. Per level it
+//   1. computes the five products on their strips from the raw planes of level k
+//      (u, v, w, p with a 4-point x / 3-point y halo) and k+1 (shared memory);
+//   2. evaluates the three equations at its four points from the raw planes and
+//      the product strips, with the level-(k-1) values a thread needs (u, v, w,
+//      uhz*whx, vhz*why at its own points) carried in registers;
+// while the planes of level k+2 arrive in a third slot of each field's ring by
+// cp.async (16-byte copies, no registers). Ghost levels are never staged: below
+// the first level the no-slip / impermeable values follow from the first level
+// (update_boundary_uvw, src/module_boundary.f90:33-112) and above the last one
+// only the own-point values enter, also by formula. Built for the FP32 storage
+// of the mixed mode without a moving frame (u_mrf = 0) and without the Ekman
+// forcing (dp_opt 1 or 2); nx a multiple of 4 (16-byte rows), nx >= 64, ny >= 32.
+// Other cases run k_rhs_momentum_tiled2.
+#pragma once
+#include "hc_rhs_tiled2.cuh"
+
+#define RS_TX 64                      // tile points in x
+#define RS_TY 16                      // tile rows
+#define RS_HX 4                       // raw-window halo in x (keeps rows 16-byte aligned)
+#define RS_HY 3                       // raw-window halo in y
+#define RS_W (RS_TX + 2 * RS_HX)      // 72
+#define RS_H (RS_TY + 2 * RS_HY)      // 22
+#define RS_P (RS_W * RS_H)            // 1584 floats a plane
+#define RS_NC4 (RS_W / 4)             // 18 16-byte chunks a row
+#define RS_NPOS (RS_NC4 * RS_H)       // 396 chunks a plane
+// product strips (floats)
+#define RS_AW (RS_TX + 4)             // x strip width: x from -2 to 65
+#define RS_BH (RS_TY + 4)             // y strip height: y from -2 to 17
+#define RS_F_UHX 0                                  // [16][68]  uhx on the x strip
+#define RS_F_CZ (RS_F_UHX + RS_TY * RS_AW)          // [16][68]  uhz*whx on the x strip
+#define RS_F_B (RS_F_CZ + RS_TY * RS_AW)            // [20][68]  uhy*vhx on both strips
+#define RS_F_VHY (RS_F_B + RS_BH * RS_AW)           // [20][64]  vhy on the y strip
+#define RS_F_EZ (RS_F_VHY + RS_BH * RS_TX)          // [20][64]  vhz*why on the y strip
+#define RS_NF (RS_F_EZ + RS_BH * RS_TX)
+#define RS_KMAX 64
+#define RS_ZT (RS_KMAX + 1)
+
+__host__ inline size_t rhs_strip_smem() { return sizeof(float) * ((size_t)12 * RS_P + RS_NF + 5 * RS_ZT); }
+
+// the strip kernel covers this case (the host falls back to k_rhs_momentum_tiled2 otherwise)
+__host__ inline bool rhs_strip_ok(int nx, int ny, double u_mrf, int dp_opt)
+{
+    return nx % 4 == 0 && nx >= 64 && ny >= 32 && u_mrf == 0.0 && dp_opt != 3;
+}
+
+__device__ __forceinline__ void rs_cp16(float* dst, const float* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void rs_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void rs_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// fourth-order mid-point interpolant (-a + 9 b + 9 c - d) / 16 and its
+// second-order form (b + c) / 2 (get_interp_fields_uvwhxyz, src/module_tools.f90:410-468)
+template <int CDS> __device__ __forceinline__ float rs_mid(float a, float b, float c, float d)
+{
+    if (CDS == 1) return 0.5f * (b + c);
+    return (9.0f * (b + c) - (a + d)) * 0.0625f;
+}
+// staggered first difference (-a2 + 27 a1 - 27 a0 + am) (the 1/(24 h) applied by the caller);
+// second order: a1 - a0 (the 1/h applied by the caller)
+template <int CDS> __device__ __forceinline__ float rs_d1(float a2, float a1, float a0, float am)
+{
+    if (CDS == 1) return a1 - a0;
+    return 27.0f * (a1 - a0) - (a2 - am);
+}
+// centred second difference (-a2 + 16 a1 - 30 a0 + 16 am - am2) or a1 - 2 a0 + am
+template <int CDS> __device__ __forceinline__ float rs_d2(float a2, float a1, float a0, float am, float am2)
+{
+    if (CDS == 1) return (a1 + am) - 2.0f * a0;
+    return 16.0f * (a1 + am) - 30.0f * a0 - (a2 + am2);
+}
+
+template <int CDS>
+__global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* SR = reinterpret_cast<float*>(smem_raw);              // [4 fields][3 slots][RS_P]
+    float* FL = SR + 12 * RS_P;                                   // product strips
+    float* ZM = FL + RS_NF;                                       // per-level metrics
+    float* F_UHX = FL + RS_F_UHX;
+    float* F_CZ = FL + RS_F_CZ;
+    float* F_B = FL + RS_F_B;
+    float* F_VHY = FL + RS_F_VHY;
+    float* F_EZ = FL + RS_F_EZ;
+
+    const Geo& g = a.g;
+    const int nz = g.nz, nx = g.nx, ny = g.ny;
+    const int x0 = blockIdx.x * RS_TX, y0 = blockIdx.y * RS_TY;
+    const int kb = blockIdx.z * a.kchunk;
+    const int ke = min(nz, kb + a.kchunk);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int closed = a.ph.ochannel == 0;
+
+    // metric tables of the chunk: 1/dz, 1/dz_t, 1/dz_b, l_t, 1/dz(k+1)
+    for (int q = threadIdx.x; q < ke - kb; q += blockDim.x) {
+        const int k = kb + q;
+        ZM[q] = 1.0f / (float)ldz(g.z.dz, k);
+        ZM[RS_ZT + q] = 1.0f / (float)ldz(g.z.dz_t, k);
+        ZM[2 * RS_ZT + q] = 1.0f / (float)ldz(g.z.dz_b, k);
+        ZM[3 * RS_ZT + q] = (float)ldz(g.z.l_t, k);
+        ZM[4 * RS_ZT + q] = 1.0f / (float)ldz(g.z.dz, k + 1);
+    }
+
+    // this thread's two 16-byte chunk positions of a plane (wrapped source offsets)
+    int src0, src1 = 0, dst0, dst1 = 0;
+    const bool has1 = threadIdx.x + 256 < RS_NPOS;
+    {
+        int pos = threadIdx.x;
+        int row = pos / RS_NC4, c4 = pos - row * RS_NC4;
+        int ys = ((y0 - RS_HY + row) % ny + ny) % ny, xs = ((x0 - RS_HX + 4 * c4) % nx + nx) % nx;
+        src0 = ys * nx + xs;
+        dst0 = row * RS_W + 4 * c4;
+        if (has1) {
+            pos += 256;
+            row = pos / RS_NC4; c4 = pos - row * RS_NC4;
+            ys = ((y0 - RS_HY + row) % ny + ny) % ny; xs = ((x0 - RS_HX + 4 * c4) % nx + nx) % nx;
+            src1 = ys * nx + xs;
+            dst1 = row * RS_W + 4 * c4;
+        }
+    }
+    auto plane = [&](int f, int lvl) { return SR + (f * 3 + lvl % 3) * RS_P; };
+    auto stage = [&](int lvl) {       // cp.async of the four planes of an interior level
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            const float* src = f == 0 ? a.f.u : (f == 1 ? a.f.v : (f == 2 ? a.f.w : a.f.p));
+            const float* base = src + (long long)lvl * g.nxy;
+            float* d = plane(f, lvl);
+            rs_cp16(d + dst0, base + src0);
+            if (has1) rs_cp16(d + dst1, base + src1);
+        }
+    };
+    if (kb > 0) stage(kb - 1);
+    stage(kb);
+    if (kb + 1 < nz) stage(kb + 1);
+    rs_commit();
+    rs_wait_all();
+    __syncthreads();
+
+    const float rdx = 1.0f / (float)g.dx, rdy = 1.0f / (float)g.dy;
+    const float r24dx = 1.0f / (24.0f * (float)g.dx), r24dy = 1.0f / (24.0f * (float)g.dy);
+    const float r12dx2 = 1.0f / (12.0f * (float)g.dx2), r12dy2 = 1.0f / (12.0f * (float)g.dy2);
+    const float rdx2 = 1.0f / (float)g.dx2, rdy2 = 1.0f / (float)g.dy2;
+    const float sx1 = CDS == 1 ? rdx : r24dx, sy1 = CDS == 1 ? rdy : r24dy;     // first differences
+    const float sx2 = CDS == 1 ? rdx2 : r12dx2, sy2 = CDS == 1 ? rdy2 : r12dy2; // second differences
+    const float dt = (float)a.ph.dt, nu = (float)a.ph.nu;
+    const float rka = (float)a.rk_a, rkb = (float)a.rk_b, rkc = (float)a.rk_c;
+    const float cdif = rkc * 0.5f * dt * nu, cgp = rkc * dt;
+    const float dpx = (float)a.sc->dpx_drive;
+    const float got = (float)a.sc->got, tref = (float)a.ph.t_ref;
+    const bool scalar = a.ph.isscalar == 1;
+
+    // the thread's points: x = x0 + 2 lane + s, rows y0 + 2 wid + q (s, q in {0, 1})
+    const int xl = 2 * lane, rl0 = 2 * wid;
+    const int xi = x0 + xl;
+    const bool xin = xi < nx;
+    bool act[2];
+    int gid[2];
+    int rc[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        act[q] = xin && (y0 + rl0 + q) < ny;
+        gid[q] = (y0 + rl0 + q) * nx + xi;                             // + k nxy
+        rc[q] = (rl0 + q + RS_HY) * RS_W + xl + RS_HX;                 // own raw index (even)
+    }
+
+    // values of level k-1 at the own points: u, v, w, uhz*whx, vhz*why
+    float um1[2][2], vm1[2][2], wm1[2][2], czp[2][2], ezp[2][2];
+    if (kb == 0) {
+        // no-slip, impermeable bottom wall: u(-1) = -u(0), v(-1) = -v(0), w(-1) = 0;
+        // w vanishes below, so both level-(-1) products are 0
+        const float* u0 = plane(0, 0); const float* v0 = plane(1, 0);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const float2 uc = ld2s(u0, rc[q]), vc = ld2s(v0, rc[q]);
+            um1[q][0] = -uc.x; um1[q][1] = -uc.y; vm1[q][0] = -vc.x; vm1[q][1] = -vc.y;
+            wm1[q][0] = wm1[q][1] = 0.0f;
+            czp[q][0] = czp[q][1] = ezp[q][0] = ezp[q][1] = 0.0f;
+        }
+    } else {
+        const int L = kb - 1;
+        const float* u0 = plane(0, L); const float* v0 = plane(1, L); const float* w0 = plane(2, L);
+        const float* u1 = plane(0, L + 1); const float* v1 = plane(1, L + 1);
+        const float l = (float)ldz(g.z.l_t, L);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int r = rc[q];
+            float wx[6];
+            ld6(w0, r, wx);
+            const float2 wy1 = ld2s(w0, r + RS_W), wy2 = ld2s(w0, r + 2 * RS_W), wym = ld2s(w0, r - RS_W);
+            const float2 uc = ld2s(u0, r), vc = ld2s(v0, r), wc = ld2s(w0, r);
+            const float2 uu = ld2s(u1, r), vv = ld2s(v1, r);
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const float ucs = s ? uc.y : uc.x, vcs = s ? vc.y : vc.x;
+                const float whx = rs_mid<CDS>(wx[4 + s], wx[3 + s], wx[2 + s], wx[1 + s]);
+                const float why = rs_mid<CDS>(s ? wy2.y : wy2.x, s ? wy1.y : wy1.x, s ? wc.y : wc.x, s ? wym.y : wym.x);
+                const float uhz = (s ? uu.y : uu.x) * l + ucs * (1.0f - l);
+                const float vhz = (s ? vv.y : vv.x) * l + vcs * (1.0f - l);
+                czp[q][s] = uhz * whx;
+                ezp[q][s] = vhz * why;
+                um1[q][s] = ucs; vm1[q][s] = vcs; wm1[q][s] = s ? wc.y : wc.x;
+            }
+        }
+    }
+    __syncthreads();      // level kb-1's slot is refilled with level kb+2 below
+
+    double dv_sum = 0.0, dv_max = 0.0;
+    int dv_nan = 0;
+    for (int k = kb; k < ke; ++k) {
+        const bool next_in = k + 1 < nz;          // level k+1 is interior (staged)
+        if (k + 2 < nz && k + 1 < ke) { stage(k + 2); rs_commit(); }
+        const bool wface = k < nz - 1;
+        const float lt = ZM[3 * RS_ZT + (k - kb)];
+        const float* u0 = plane(0, k); const float* v0 = plane(1, k);
+        const float* w0 = plane(2, k); const float* p0 = plane(3, k);
+        const float* u1 = plane(0, k + 1); const float* v1 = plane(1, k + 1);
+        const float* w1 = plane(2, k + 1); const float* p1 = plane(3, k + 1);
+        const long long kofs = (long long)k * g.nxy;
+
+        // the thread's history values of this level, issued before the products so
+        // that their latency overlaps them
+        float2 hf[2], hg[2], hh[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            hf[q] = hg[q] = hh[q] = make_float2(0.0f, 0.0f);
+            if (act[q]) {
+                const long long id = kofs + gid[q];
+                hf[q] = *reinterpret_cast<const float2*>(a.ff + id);
+                hg[q] = *reinterpret_cast<const float2*>(a.gg + id);
+                if (wface) hh[q] = *reinterpret_cast<const float2*>(a.hh + id);
+            }
+        }
+        // optional own-point inputs (body force, temperature), read where they are used
+        auto ld_own = [&](const float* base, int q, long long extra) {
+            return act[q] ? *reinterpret_cast<const float2*>(base + kofs + gid[q] + extra) : make_float2(0.0f, 0.0f);
+        };
+
+        // ---- 1. the products on their strips (37 warp jobs of one row each)
+        for (int job = wid; job < 37; job += 8) {
+            if (job <= 16) {
+                // x strip: rows 0..15; job 16 is the two 2-column side pieces
+                int fx, fy;
+                if (job < 16) { fx = 2 * lane; fy = job; }
+                else { fy = lane & 15; fx = (lane >> 4) ? RS_TX : -2; }
+                const int r = (fy + RS_HY) * RS_W + fx + RS_HX;
+                float ux[6], vx[6], wx[6];
+                ld6(u0, r, ux); ld6(v0, r, vx);
+                const float2 uym = ld2s(u0, r - RS_W), uy1 = ld2s(u0, r + RS_W), uy2 = ld2s(u0, r + 2 * RS_W);
+                float2 up = make_float2(0.0f, 0.0f);
+                if (wface) { ld6(w0, r, wx); up = ld2s(u1, r); }
+                float o_uhx[2], o_cz[2], o_b[2];
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    o_uhx[s] = rs_mid<CDS>(ux[3 + s], ux[2 + s], ux[1 + s], ux[s]);
+                    const float uhy = rs_mid<CDS>(s ? uy2.y : uy2.x, s ? uy1.y : uy1.x, ux[2 + s], s ? uym.y : uym.x);
+                    const float vhx = rs_mid<CDS>(vx[4 + s], vx[3 + s], vx[2 + s], vx[1 + s]);
+                    o_b[s] = uhy * vhx;
+                    if (wface) {
+                        const float whx = rs_mid<CDS>(wx[4 + s], wx[3 + s], wx[2 + s], wx[1 + s]);
+                        const float uhz = (s ? up.y : up.x) * lt + ux[2 + s] * (1.0f - lt);
+                        o_cz[s] = uhz * whx;
+                    } else {
+                        o_cz[s] = 0.0f;       // w = 0 on the top face: whx = 0
+                    }
+                }
+                const int ea = fy * RS_AW + fx + 2;
+                st2s(F_UHX, ea, o_uhx[0], o_uhx[1]);
+                st2s(F_CZ, ea, o_cz[0], o_cz[1]);
+                st2s(F_B, (fy + 2) * RS_AW + fx + 2, o_b[0], o_b[1]);
+            } else {
+                // y strip: own columns, rows -2..17
+                const int fx = 2 * lane, fy = job - 17 - 2;
+                const int r = (fy + RS_HY) * RS_W + fx + RS_HX;
+                const float2 vc = ld2s(v0, r);
+                if (fy >= -1) {       // vhy at rows -1..17 (reads rows fy-2..fy+1)
+                    const float2 vm = ld2s(v0, r - RS_W), vm2 = ld2s(v0, r - 2 * RS_W), v1y = ld2s(v0, r + RS_W);
+                    st2s(F_VHY, (fy + 2) * RS_TX + fx, rs_mid<CDS>(v1y.x, vc.x, vm.x, vm2.x),
+                         rs_mid<CDS>(v1y.y, vc.y, vm.y, vm2.y));
+                }
+                if (fy <= 16) {       // vhz*why at rows -2..16 (reads w rows fy-1..fy+2)
+                    float e0 = 0.0f, e1 = 0.0f;
+                    if (wface) {
+                        const float2 wc = ld2s(w0, r), wym = ld2s(w0, r - RS_W), wy1 = ld2s(w0, r + RS_W),
+                                     wy2 = ld2s(w0, r + 2 * RS_W);
+                        const float2 vp = ld2s(v1, r);
+                        e0 = (vp.x * lt + vc.x * (1.0f - lt)) * rs_mid<CDS>(wy2.x, wy1.x, wc.x, wym.x);
+                        e1 = (vp.y * lt + vc.y * (1.0f - lt)) * rs_mid<CDS>(wy2.y, wy1.y, wc.y, wym.y);
+                    }
+                    st2s(F_EZ, (fy + 2) * RS_TX + fx, e0, e1);
+                }
+                if (fy < 0 || fy == 16) {     // uhy*vhx on the rows beyond the x strip
+                    float vx[6];
+                    ld6(v0, r, vx);
+                    const float2 uc = ld2s(u0, r), uym = ld2s(u0, r - RS_W), uy1 = ld2s(u0, r + RS_W),
+                                 uy2 = ld2s(u0, r + 2 * RS_W);
+                    const float b0 = rs_mid<CDS>(uy2.x, uy1.x, uc.x, uym.x) * rs_mid<CDS>(vx[4], vx[3], vx[2], vx[1]);
+                    const float b1 = rs_mid<CDS>(uy2.y, uy1.y, uc.y, uym.y) * rs_mid<CDS>(vx[5], vx[4], vx[3], vx[2]);
+                    st2s(F_B, (fy + 2) * RS_AW + fx + 2, b0, b1);
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- 2. the three equations at the thread's four points
+        const float rdz = ZM[k - kb], rdzt = ZM[RS_ZT + (k - kb)], rdzb = ZM[2 * RS_ZT + (k - kb)];
+        const float rdzp = ZM[4 * RS_ZT + (k - kb)];
+        const double dxd = g.dx, dyd = g.dy, dzd = ldz(g.z.dz, k);
+        const int fa0 = rl0 * RS_AW + xl + 2;                  // own index in the x strip
+        const int fb0 = (rl0 + 2) * RS_AW + xl + 2;            // own index in the uhy*vhx plane
+        const int fv0 = (rl0 + 2) * RS_TX + xl;                // own index in the y strip
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int r = rc[q];
+            // divergence of the incoming fields (FP64, the previous sub-step's check)
+            float ux[6];
+            ld6(u0, r, ux);
+            const float2 vc = ld2s(v0, r), vym = ld2s(v0, r - RS_W), vym2 = ld2s(v0, r - 2 * RS_W),
+                         vy1 = ld2s(v0, r + RS_W);
+            const float2 wc = ld2s(w0, r);
+            if (a.part_div && act[q]) {
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int c = 2 + s;
+                    const double uc = ux[c], vcs = s ? vc.y : vc.x, wcs = s ? wc.y : wc.x;
+                    double dux[4] = {(double)ux[c + 1], uc, (double)ux[c - 1], (double)ux[c - 2]};
+                    double dvy[4] = {(double)(s ? vy1.y : vy1.x), vcs, (double)(s ? vym.y : vym.x),
+                                     (double)(s ? vym2.y : vym2.x)};
+                    const double d = fd_div_point<CDS>(dux, dvy, wcs, k > 0 ? (double)wm1[q][s] : 0.0, dxd, dyd, dzd);
+                    if (uc != uc || vcs != vcs || wcs != wcs || d != d) dv_nan = 1;
+                    else { dv_sum += fabs(d); dv_max = absmax_pick(dv_max, d); }
+                }
+            }
+            float out_f[3][2], out_q[3][2];
+            // ---------------- U ----------------
+            {
+                float px[6], fh[6];
+                ld6(p0, r, px);
+                ld6(F_UHX, fa0 + q * RS_AW, fh);
+                const float2 uy2 = ld2s(u0, r + 2 * RS_W), uy1 = ld2s(u0, r + RS_W);
+                const float2 uym = ld2s(u0, r - RS_W), uym2 = ld2s(u0, r - 2 * RS_W);
+                const int fb = fb0 + q * RS_AW;
+                const float2 b1 = ld2s(F_B, fb + RS_AW), b0 = ld2s(F_B, fb), bm = ld2s(F_B, fb - RS_AW),
+                             bm2 = ld2s(F_B, fb - 2 * RS_AW);
+                const float2 cz = ld2s(F_CZ, fa0 + q * RS_AW);
+                const float2 uz1 = next_in ? ld2s(u1, r) : make_float2(0.0f, 0.0f);
+                const float2 bxq = a.bfx ? ld_own(a.bfx, q, 0) : make_float2(0.0f, 0.0f);
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int c = 2 + s;
+                    const float uc = ux[c];
+                    const float h2 = fh[c + 2], h1 = fh[c + 1], h0 = fh[c], hm = fh[c - 1];
+                    const float uux = rs_d1<CDS>(h2 * h2, h1 * h1, h0 * h0, hm * hm) * sx1;
+                    const float uvy = rs_d1<CDS>(s ? b1.y : b1.x, s ? b0.y : b0.x, s ? bm.y : bm.x, s ? bm2.y : bm2.x) * sy1;
+                    const float uxx = rs_d2<CDS>(ux[c + 2], ux[c + 1], uc, ux[c - 1], ux[c - 2]) * sx2;
+                    const float uyy = rs_d2<CDS>(s ? uy2.y : uy2.x, s ? uy1.y : uy1.x, uc, s ? uym.y : uym.x,
+                                                 s ? uym2.y : uym2.x) * sy2;
+                    const float dpdx = rs_d1<CDS>(px[c + 2], px[c + 1], px[c], px[c - 1]) * sx1;
+                    const float czs = s ? cz.y : cz.x;
+                    const float uwz = (czs - czp[q][s]) * rdz;
+                    czp[q][s] = czs;
+                    // above the last level: no-slip (closed) or free-slip (open) top
+                    const float up = next_in ? (s ? uz1.y : uz1.x) : (closed ? -uc : uc);
+                    const float uzz = ((up - uc) * rdzt - (uc - um1[q][s]) * rdzb) * rdz;
+                    um1[q][s] = uc;
+                    const float fu = -uux - uvy - uwz + dpx + (s ? bxq.y : bxq.x);
+                    out_f[0][s] = fu;
+                    out_q[0][s] = uc + dt * (rka * fu + rkb * (s ? hf[q].y : hf[q].x)) + cdif * (uxx + uyy + uzz) -
+                                  cgp * dpdx;
+                }
+                if (act[q] && a.uhx_s)
+                    *reinterpret_cast<float2*>(a.uhx_s + kofs + gid[q]) = make_float2(fh[2], fh[3]);
+            }
+            // ---------------- V ----------------
+            {
+                float vx[6], fbx[6];
+                ld6(v0, r, vx);
+                ld6(F_B, fb0 + q * RS_AW, fbx);
+                const float2 vy2 = ld2s(v0, r + 2 * RS_W);
+                const int fv = fv0 + q * RS_TX;
+                const float2 hy2 = ld2s(F_VHY, fv + 2 * RS_TX), hy1 = ld2s(F_VHY, fv + RS_TX), hy0 = ld2s(F_VHY, fv),
+                             hym = ld2s(F_VHY, fv - RS_TX);
+                const float2 ez = ld2s(F_EZ, fv);
+                const float2 pc = ld2s(p0, r), py2 = ld2s(p0, r + 2 * RS_W), py1 = ld2s(p0, r + RS_W),
+                             pym = ld2s(p0, r - RS_W);
+                const float2 vz1 = next_in ? ld2s(v1, r) : make_float2(0.0f, 0.0f);
+                const float2 byq = a.bfx ? ld_own(a.bfy, q, 0) : make_float2(0.0f, 0.0f);
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int c = 2 + s;
+                    const float vcs = vx[c];
+                    const float vux = rs_d1<CDS>(fbx[c + 1], fbx[c], fbx[c - 1], fbx[c - 2]) * sx1;
+                    const float y2 = s ? hy2.y : hy2.x, y1 = s ? hy1.y : hy1.x, y0v = s ? hy0.y : hy0.x,
+                                ym = s ? hym.y : hym.x;
+                    const float vvy = rs_d1<CDS>(y2 * y2, y1 * y1, y0v * y0v, ym * ym) * sy1;
+                    const float vxx = rs_d2<CDS>(vx[c + 2], vx[c + 1], vcs, vx[c - 1], vx[c - 2]) * sx2;
+                    const float vyy = rs_d2<CDS>(s ? vy2.y : vy2.x, s ? vy1.y : vy1.x, vcs, s ? vym.y : vym.x,
+                                                 s ? vym2.y : vym2.x) * sy2;
+                    const float dpdy = rs_d1<CDS>(s ? py2.y : py2.x, s ? py1.y : py1.x, s ? pc.y : pc.x,
+                                                  s ? pym.y : pym.x) * sy1;
+                    const float ezs = s ? ez.y : ez.x;
+                    const float vwz = (ezs - ezp[q][s]) * rdz;
+                    ezp[q][s] = ezs;
+                    const float vp = next_in ? (s ? vz1.y : vz1.x) : (closed ? -vcs : vcs);
+                    const float vzz = ((vp - vcs) * rdzt - (vcs - vm1[q][s]) * rdzb) * rdz;
+                    vm1[q][s] = vcs;
+                    const float fv_ = -vux - vvy - vwz + (s ? byq.y : byq.x);
+                    out_f[1][s] = fv_;
+                    out_q[1][s] = vcs + dt * (rka * fv_ + rkb * (s ? hg[q].y : hg[q].x)) + cdif * (vxx + vyy + vzz) -
+                                  cgp * dpdy;
+                }
+                if (act[q] && a.vhy_s)
+                    *reinterpret_cast<float2*>(a.vhy_s + kofs + gid[q]) = hy0;
+            }
+            // ---------------- W (k <= nz-2) ----------------
+            if (wface) {
+                float wx[6], fcz[6];
+                ld6(w0, r, wx);
+                ld6(F_CZ, fa0 + q * RS_AW, fcz);
+                const float2 wy2 = ld2s(w0, r + 2 * RS_W), wy1 = ld2s(w0, r + RS_W);
+                const float2 wym = ld2s(w0, r - RS_W), wym2 = ld2s(w0, r - 2 * RS_W);
+                const int fv = fv0 + q * RS_TX;
+                const float2 e1 = ld2s(F_EZ, fv + RS_TX), e0 = ld2s(F_EZ, fv), em = ld2s(F_EZ, fv - RS_TX),
+                             em2 = ld2s(F_EZ, fv - 2 * RS_TX);
+                const float2 wz1 = ld2s(w1, r), pz1 = ld2s(p1, r), pc = ld2s(p0, r);
+                const float2 bzq = a.bfx ? ld_own(a.bfz, q, 0) : make_float2(0.0f, 0.0f);
+                float2 tk = make_float2(0.0f, 0.0f), tk1 = tk;
+                if (scalar) { tk = ld_own(a.f.t, q, 0); tk1 = ld_own(a.f.t, q, g.nxy); }
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int c = 2 + s;
+                    const float wcs = wx[c], wp = s ? wz1.y : wz1.x, wm = wm1[q][s];
+                    const float wux = rs_d1<CDS>(fcz[c + 1], fcz[c], fcz[c - 1], fcz[c - 2]) * sx1;
+                    const float wvy = rs_d1<CDS>(s ? e1.y : e1.x, s ? e0.y : e0.x, s ? em.y : em.x, s ? em2.y : em2.x) * sy1;
+                    const float wxx = rs_d2<CDS>(wx[c + 2], wx[c + 1], wcs, wx[c - 1], wx[c - 2]) * sx2;
+                    const float wyy = rs_d2<CDS>(s ? wy2.y : wy2.x, s ? wy1.y : wy1.x, wcs, s ? wym.y : wym.x,
+                                                 s ? wym2.y : wym2.x) * sy2;
+                    float a1 = 0.5f * (wcs + wp); a1 = a1 * a1;
+                    float a2 = 0.5f * (wcs + wm); a2 = a2 * a2;
+                    const float wwz = (a1 - a2) * rdzt;
+                    const float wzz = ((wp - wcs) * rdzp - (wcs - wm) * rdz) * rdzt;
+                    float fw = -wux - wvy - wwz;
+                    if (scalar) fw = fw + got * ((1.0f - lt) * (s ? tk.y : tk.x) + lt * (s ? tk1.y : tk1.x) - tref);
+                    fw += s ? bzq.y : bzq.x;
+                    const float dpdz = ((s ? pz1.y : pz1.x) - (s ? pc.y : pc.x)) * rdzt;
+                    out_f[2][s] = fw;
+                    out_q[2][s] = wcs + dt * (rka * fw + rkb * (s ? hh[q].y : hh[q].x)) + cdif * (wxx + wyy + wzz) -
+                                  cgp * dpdz;
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < 2; ++s) wm1[q][s] = s ? wc.y : wc.x;
+            if (act[q]) {
+                const long long id = kofs + gid[q];
+                *reinterpret_cast<float2*>(a.ff + id) = make_float2(out_f[0][0], out_f[0][1]);
+                *reinterpret_cast<float2*>(a.qu + id) = make_float2(out_q[0][0], out_q[0][1]);
+                *reinterpret_cast<float2*>(a.gg + id) = make_float2(out_f[1][0], out_f[1][1]);
+                *reinterpret_cast<float2*>(a.qv + id) = make_float2(out_q[1][0], out_q[1][1]);
+                if (wface) {
+                    *reinterpret_cast<float2*>(a.hh + id) = make_float2(out_f[2][0], out_f[2][1]);
+                    *reinterpret_cast<float2*>(a.qw + id) = make_float2(out_q[2][0], out_q[2][1]);
+                }
+            }
+        }
+        rs_wait_all();
+        __syncthreads();
+    }
+
+    if (a.part_div) {
+        __shared__ double s_sum[8], s_max[8];
+        __shared__ int s_nan;
+        if (threadIdx.x == 0) s_nan = 0;
+        __syncthreads();
+        if (dv_nan) s_nan = 1;
+        dv_sum = warp_sum(dv_sum);
+        dv_max = warp_absmax(dv_max);
+        if (lane == 0) { s_sum[wid] = dv_sum; s_max[wid] = dv_max; }
+        __syncthreads();
+        if (wid == 0) {
+            dv_sum = lane < 8 ? s_sum[lane] : 0.0;
+            dv_max = lane < 8 ? s_max[lane] : 0.0;
+            dv_sum = warp_sum(dv_sum);
+            dv_max = warp_absmax(dv_max);
+            if (lane == 0) {
+                const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+                a.part_div[3 * b + 0] = dv_sum;
+                a.part_div[3 * b + 1] = dv_max;
+                a.part_div[3 * b + 2] = s_nan ? 1.0 : 0.0;
+            }
+        }
+    }
+}

@@ -59,7 +59,7 @@ def test_every_tile_choice_keeps_the_results(slot, value, engine):
         out.append({f: c.download(f) for f in ("u", "v", "w", "p")})
         c.close()
     for f in ("u", "v", "w", "p"):
-        assert rel_err(out[1][f], out[0][f]) <= 1e-12, (slot, value, f)
+        assert rel_err(out[1][f], out[0][f]) <= 1e-10, (slot, value, f)
 
 
 @pytest.mark.gpu
