@@ -157,3 +157,71 @@ def test_config3_grid_statistics_and_diagnostics(oracle_lib, engine):
         assert abs(a["dpx_drive"] - b["dpx_drive"]) <= FP64_TOL * max(1.0, abs(b["dpx_drive"]))
     c.close()
     o.close()
+
+
+# FP32 storage on grids of nx >= 64 (a multiple of 4) and ny >= 32 runs the strip
+# momentum RHS (k_rhs_momentum_strip): partial tiles, several level chunks (tile[2]),
+# both schemes, open/closed, temperature, AB2, and the body force
+STRIP = {
+    "fd4_closed_dp2_chunks": config_channel_fd(nx=96, ny=64, nz=40).replace(tile=[0, 0, 7, 0]),
+    "fd2_open_scalar": _fd(64, 48, 17, cds=1, ochannel=1, isscalar=1, got=0.7, tbot=-1.0, ttop=0.0),
+    "fd4_ab2_scalar_partial_tiles": _fd(132, 40, 9, dts=1, isscalar=1, got=0.3, tile=[0, 0, 4, 0]),
+    "fd4_open_dp1": _fd(64, 32, 12, ochannel=1),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(STRIP))
+def test_strip_rhs_mixed_against_oracle(name, oracle_lib, engine):
+    """Mixed precision through the strip RHS: velocities and temperature <= 1e-5
+    after 10 steps; the divergence of every sub-step is reported and small."""
+    p = STRIP[name]
+    errs = _compare(p, inputs.small_random(p, seed=17), 10, oracle_lib, engine, precisions=(PREC_MIXED,))
+    assert max(e for (q, f), e in errs.items() if f in ("u", "v", "w")) <= MIXED_TOL
+    c = engine.Channel(p.replace(precision=PREC_MIXED))
+    c.load(inputs.small_random(p, seed=17))
+    c.initialize()
+    d = c.step(2)[-1]
+    nsub = 3 if p.dts == 2 else 1
+    for s in range(nsub):
+        assert 0.0 < d["div_avg_sub"][s] < 1e-3, (s, d["div_avg_sub"])
+        assert abs(d["div_max_sub"][s]) >= d["div_avg_sub"][s]
+    c.close()
+
+
+@pytest.mark.gpu
+def test_strip_rhs_body_force_mixed(oracle_lib, engine):
+    p = config_channel_fd(nx=64, ny=32, nz=16).replace(dp_opt=1, nu=1.0 / 300.0)
+    fields = inputs.small_random(p, seed=9)
+    bf = inputs.gaussian_body_force(p, seed=4, amp=0.05)
+    o = oracle_lib.Oracle(p)
+    o.load(fields)
+    o.set_body_force(*bf)
+    o.initialize()
+    rc, _ = o.step(10)
+    assert rc == 0
+    c = engine.Channel(p.replace(precision=PREC_MIXED))
+    c.load(fields)
+    c.set_body_force(*bf)
+    c.initialize()
+    c.step(10)
+    for f in ("u", "v", "w"):
+        assert rel_err(c.download(f), o.get(f)) <= MIXED_TOL, f
+    c.close()
+    o.close()
+
+
+@pytest.mark.gpu
+def test_strip_rhs_reports_nan(engine):
+    """A NaN in the input reaches the check fused into the strip RHS (sub-step 2)
+    or the final check, and hc_step returns HC_ERR_NAN."""
+    p = config_channel_fd(nx=64, ny=32, nz=12, precision=PREC_MIXED)
+    fields = inputs.small_random(p, seed=1)
+    fields["v"][5, 7, 9] = np.nan
+    c = engine.Channel(p)
+    c.load(fields)
+    c.initialize()
+    with pytest.raises(engine.HerculesError) as ei:
+        c.step(2)
+    assert ei.value.code == -5
+    c.close()
