@@ -165,7 +165,7 @@ def test_config3_grid_statistics_and_diagnostics(oracle_lib, engine):
 STRIP = {
     "fd4_closed_dp2_chunks": config_channel_fd(nx=96, ny=64, nz=40).replace(tile=[0, 0, 7, 0]),
     "fd2_open_scalar": _fd(64, 48, 17, cds=1, ochannel=1, isscalar=1, got=0.7, tbot=-1.0, ttop=0.0),
-    "fd4_ab2_scalar_partial_tiles": _fd(132, 40, 9, dts=1, isscalar=1, got=0.3, tile=[0, 0, 4, 0]),
+    "fd4_ab2_scalar_partial_tiles": _fd(160, 40, 9, dts=1, isscalar=1, got=0.3, tile=[0, 0, 4, 0]),
     "fd4_open_dp1": _fd(64, 32, 12, ochannel=1),
 }
 
