@@ -245,7 +245,8 @@ struct hc_handle {
     double* mean[11];
     float* win[11];          // FP32 storage: the FP32 window sums of the mean accumulators
     double* mtmp;            // FP32 storage: FP64 sums + window, assembled for a download
-    double* zbuf;            // 5*(nz+4)
+    double* zbuf;            // 5*(nz+4) doubles, then the 5*nz floats of zm5
+    float* zm5;              // FP32 per-level metrics of the strip RHS
     double* coef;
     ColCoef cc;
     double* scratch;
@@ -498,11 +499,23 @@ static int build_tables(hc_handle* h)
 
 static int upload_zgrid(hc_handle* h)
 {
-    const int nka = h->p.nz + 4;
+    const int nka = h->p.nz + 4, nz = h->p.nz;
     for (int q = 0; q < 5; ++q)
         CK(cudaMemcpy(h->zbuf + q * nka, h->zhost[q].data(), nka * sizeof(double), cudaMemcpyHostToDevice));
     h->g.z.dz = h->zbuf; h->g.z.dz_t = h->zbuf + nka; h->g.z.dz_b = h->zbuf + 2 * nka;
     h->g.z.l_t = h->zbuf + 3 * nka; h->g.z.l_b = h->zbuf + 4 * nka;
+    // FP32 per-level metrics of the strip RHS, [5][nz]: 1/dz, 1/dz_t, 1/dz_b, l_t, 1/dz(k+1)
+    // (interior level k at Fortran index k+2 of the host arrays)
+    std::vector<float> zm(5 * (size_t)nz);
+    for (int k = 0; k < nz; ++k) {
+        zm[k] = 1.0f / (float)h->zhost[0][k + 2];
+        zm[nz + k] = 1.0f / (float)h->zhost[1][k + 2];
+        zm[2 * nz + k] = 1.0f / (float)h->zhost[2][k + 2];
+        zm[3 * nz + k] = (float)h->zhost[3][k + 2];
+        zm[4 * nz + k] = 1.0f / (float)h->zhost[0][k + 3];
+    }
+    h->zm5 = reinterpret_cast<float*>(h->zbuf + 5 * nka);
+    CK(cudaMemcpy(h->zm5, zm.data(), zm.size() * sizeof(float), cudaMemcpyHostToDevice));
     return HC_OK;
 }
 
@@ -622,8 +635,11 @@ static int build_fft(hc_handle* h)
     h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : (h->rsz == sizeof(double) ? 1024 : 2048) / nxh;
     if (h->rows_x < 1) h->rows_x = 1; if (h->rows_x > 64) h->rows_x = 64;
     h->smem_x = 2 * (size_t)h->rows_x * nxh * c2;
-    h->col_threads = h->p.tile[3] > 1 ? h->p.tile[3] : 128;
-    h->col_warp = h->p.tile[3] != 1 && h->p.nz <= 32 * 8;
+    // tile[3]: 0 the coalescing-tile column kernels, 1 one thread per column (128 a
+    // block), 2 one warp per column without tiles, >= 32 one thread per column with
+    // that many threads a block
+    h->col_threads = h->p.tile[3] >= 32 ? h->p.tile[3] : 128;
+    h->col_warp = (h->p.tile[3] == 0 || h->p.tile[3] == 2) && h->p.nz <= 32 * 8;
     if (h->col_threads < 32 || h->col_threads > 256 || (h->col_threads & 31)) return HC_ERR_PARAM;
     h->tl_y = h->p.tile[1] > 0 ? h->p.tile[1] : 1536 / ny;
     if (h->tl_y < 1) h->tl_y = 1; if (h->tl_y > 32) h->tl_y = 32; if (h->tl_y > nxh) h->tl_y = nxh;
@@ -965,6 +981,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     // the divergence check of the previous sub-step rides along (slot sub-1)
     m.part_div = (sub > 0 && h->div_in_rhs && !recompute) ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
     m.kchunk = h->rhs_kc;
+    m.zm = h->zm5;
     m.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
     m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
     prof_begin(h, K_RHS_MOM);
@@ -1733,7 +1750,7 @@ int hc_create(const hc_params* p, hc_handle** out)
     h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0;
     for (int q = 0; q < 11; ++q) { h->mean[q] = nullptr; h->win[q] = nullptr; }
     h->mtmp = nullptr;
-    h->zbuf = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
+    h->zbuf = nullptr; h->zm5 = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
     h->diag_cap = 0; h->last_ms = 0.0; h->launches = 0; h->initialized = 0;
     h->prof = 0; h->cur_cat = 0; h->ev_used = 0;
@@ -1804,7 +1821,8 @@ int hc_create(const hc_params* p, hc_handle** out)
         if (cudaMalloc(&h->scratch, cz * (3 * sizeof(double) + 4 * sizeof(double2))) != cudaSuccess) FAIL(HC_ERR_NOMEM);
         h->cs.bu = h->scratch; h->cs.bw = h->scratch + cz; h->cs.bp = h->scratch + 2 * cz;
         h->cs.su = (double2*)(h->scratch + 3 * cz); h->cs.sv = h->cs.su + cz; h->cs.sw = h->cs.sv + cz; h->cs.sp = h->cs.sw + cz;
-        if (cudaMalloc(&h->zbuf, 5 * (p->nz + 4) * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+        if (cudaMalloc(&h->zbuf, 5 * (p->nz + 4) * sizeof(double) + 5 * (size_t)p->nz * sizeof(float)) != cudaSuccess)
+            FAIL(HC_ERR_NOMEM);
         if ((rc = upload_zgrid(h)) != HC_OK) goto fail;
         if ((rc = build_tables(h)) != HC_OK) goto fail;
         if ((rc = build_fft(h)) != HC_OK) goto fail;
@@ -1825,6 +1843,18 @@ int hc_create(const hc_params* p, hc_handle** out)
             if (kc > p->nz) kc = p->nz;
             h->rhs_kc = kc;
             h->rhs_grid = dim3(bx, by, (p->nz + kc - 1) / kc);
+            if (h->rhs_strip) {
+                // persistent: two blocks an SM (or one per tile-level run of tile[2]
+                // levels when that asks for more), each an equal share of the
+                // (tile, level) work in level order
+                int dev_sm = 148;
+                cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, h->dev);
+                long long work = (long long)bx * by * p->nz;
+                long long nb = p->tile[2] > 0 ? (work + p->tile[2] - 1) / p->tile[2] : 2LL * dev_sm;
+                if (nb > work) nb = work;
+                if (nb < 1) nb = 1;
+                h->rhs_grid = dim3((unsigned)nb, 1, 1);
+            }
         }
         h->stx = h->rsz == sizeof(float) ? (g.nxy + 511) / 512 : (g.nxy + 255) / 256;   // k_stats: FP32 pairs
         h->sty = (2 * RED_BLOCKS) / h->stx;

@@ -46,10 +46,8 @@
 #define RS_F_VHY (RS_F_B + RS_BH * RS_AW)           // [20][64]  vhy on the y strip
 #define RS_F_EZ (RS_F_VHY + RS_BH * RS_TX)          // [20][64]  vhz*why on the y strip
 #define RS_NF (RS_F_EZ + RS_BH * RS_TX)
-#define RS_KMAX 64
-#define RS_ZT (RS_KMAX + 1)
 
-__host__ inline size_t rhs_strip_smem() { return sizeof(float) * ((size_t)12 * RS_P + RS_NF + 5 * RS_ZT); }
+__host__ inline size_t rhs_strip_smem() { return sizeof(float) * ((size_t)12 * RS_P + RS_NF); }
 
 // the strip kernel covers this case (the host falls back to k_rhs_momentum_tiled2 otherwise)
 __host__ inline bool rhs_strip_ok(int nx, int ny, double u_mrf, int dp_opt)
@@ -92,7 +90,6 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* SR = reinterpret_cast<float*>(smem_raw);              // [4 fields][3 slots][RS_P]
     float* FL = SR + 12 * RS_P;                                   // product strips
-    float* ZM = FL + RS_NF;                                       // per-level metrics
     float* F_UHX = FL + RS_F_UHX;
     float* F_CZ = FL + RS_F_CZ;
     float* F_B = FL + RS_F_B;
@@ -101,40 +98,56 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
 
     const Geo& g = a.g;
     const int nz = g.nz, nx = g.nx, ny = g.ny;
-    const int x0 = blockIdx.x * RS_TX, y0 = blockIdx.y * RS_TY;
-    const int kb = blockIdx.z * a.kchunk;
-    const int ke = min(nz, kb + a.kchunk);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int closed = a.ph.ochannel == 0;
-
-    // metric tables of the chunk: 1/dz, 1/dz_t, 1/dz_b, l_t, 1/dz(k+1)
-    for (int q = threadIdx.x; q < ke - kb; q += blockDim.x) {
-        const int k = kb + q;
-        ZM[q] = 1.0f / (float)ldz(g.z.dz, k);
-        ZM[RS_ZT + q] = 1.0f / (float)ldz(g.z.dz_t, k);
-        ZM[2 * RS_ZT + q] = 1.0f / (float)ldz(g.z.dz_b, k);
-        ZM[3 * RS_ZT + q] = (float)ldz(g.z.l_t, k);
-        ZM[4 * RS_ZT + q] = 1.0f / (float)ldz(g.z.dz, k + 1);
-    }
-
-    // this thread's two 16-byte chunk positions of a plane (wrapped source offsets)
-    int src0, src1 = 0, dst0, dst1 = 0;
-    const bool has1 = threadIdx.x + 256 < RS_NPOS;
-    {
-        int pos = threadIdx.x;
-        int row = pos / RS_NC4, c4 = pos - row * RS_NC4;
-        int ys = ((y0 - RS_HY + row) % ny + ny) % ny, xs = ((x0 - RS_HX + 4 * c4) % nx + nx) % nx;
-        src0 = ys * nx + xs;
-        dst0 = row * RS_W + 4 * c4;
-        if (has1) {
-            pos += 256;
-            row = pos / RS_NC4; c4 = pos - row * RS_NC4;
-            ys = ((y0 - RS_HY + row) % ny + ny) % ny; xs = ((x0 - RS_HX + 4 * c4) % nx + nx) % nx;
-            src1 = ys * nx + xs;
-            dst1 = row * RS_W + 4 * c4;
-        }
-    }
+    const int tiles_x = (nx + RS_TX - 1) / RS_TX;
+    const long long work = (long long)tiles_x * ((ny + RS_TY - 1) / RS_TY) * nz;
+    // this block's share of the (tile, level) work, tiles in order, levels ascending
+    long long wcur = work * blockIdx.x / gridDim.x;
+    const long long wend = work * (blockIdx.x + 1) / gridDim.x;
+    const float* zrdz = a.zm;
+    const float* zrdzt = a.zm + nz;
+    const float* zrdzb = a.zm + 2 * nz;
+    const float* zlt = a.zm + 3 * nz;
+    const float* zrdzp = a.zm + 4 * nz;
     auto plane = [&](int f, int lvl) { return SR + (f * 3 + lvl % 3) * RS_P; };
+
+    const float rdx = 1.0f / (float)g.dx, rdy = 1.0f / (float)g.dy;
+    const float r24dx = 1.0f / (24.0f * (float)g.dx), r24dy = 1.0f / (24.0f * (float)g.dy);
+    const float r12dx2 = 1.0f / (12.0f * (float)g.dx2), r12dy2 = 1.0f / (12.0f * (float)g.dy2);
+    const float rdx2 = 1.0f / (float)g.dx2, rdy2 = 1.0f / (float)g.dy2;
+    const float sx1 = CDS == 1 ? rdx : r24dx, sy1 = CDS == 1 ? rdy : r24dy;     // first differences
+    const float sx2 = CDS == 1 ? rdx2 : r12dx2, sy2 = CDS == 1 ? rdy2 : r12dy2; // second differences
+    const float dt = (float)a.ph.dt, nu = (float)a.ph.nu;
+    const float rka = (float)a.rk_a, rkb = (float)a.rk_b, rkc = (float)a.rk_c;
+    const float cdif = rkc * 0.5f * dt * nu, cgp = rkc * dt;
+    const float dpx = (float)a.sc->dpx_drive;
+    const float got = (float)a.sc->got, tref = (float)a.ph.t_ref;
+    const bool scalar = a.ph.isscalar == 1;
+
+    double dv_sum = 0.0, dv_max = 0.0;
+    int dv_nan = 0;
+    // the thread's points in a tile: x = x0 + 2 lane + s, rows y0 + 2 wid + q (s, q in {0, 1})
+    const int xl = 2 * lane, rl0 = 2 * wid;
+    int rc[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) rc[q] = (rl0 + q + RS_HY) * RS_W + xl + RS_HX;    // own raw index (even)
+    // this thread's two 16-byte chunk positions of a plane
+    const bool has1 = threadIdx.x + 256 < RS_NPOS;
+    const int row0 = threadIdx.x / RS_NC4, c40 = threadIdx.x - row0 * RS_NC4;
+    const int row1 = (threadIdx.x + 256) / RS_NC4, c41 = threadIdx.x + 256 - row1 * RS_NC4;
+    const int dst0 = row0 * RS_W + 4 * c40, dst1 = row1 * RS_W + 4 * c41;
+
+    while (wcur < wend) {
+    // ---- one segment: levels kb .. ke-1 of one tile
+    const long long tile = wcur / nz;
+    const int kb = (int)(wcur - tile * nz);
+    const int ke = (int)min((long long)nz, (long long)kb + (wend - wcur));
+    wcur += ke - kb;
+    const int x0 = (int)(tile % tiles_x) * RS_TX, y0 = (int)(tile / tiles_x) * RS_TY;
+    // wrapped source offsets of the chunk positions (the periodic comm_bound halo)
+    const int src0 = (((y0 - RS_HY + row0) % ny + ny) % ny) * nx + ((x0 - RS_HX + 4 * c40) % nx + nx) % nx;
+    const int src1 = has1 ? (((y0 - RS_HY + row1) % ny + ny) % ny) * nx + ((x0 - RS_HX + 4 * c41) % nx + nx) % nx : 0;
     auto stage = [&](int lvl) {       // cp.async of the four planes of an interior level
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
@@ -152,31 +165,14 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
     rs_wait_all();
     __syncthreads();
 
-    const float rdx = 1.0f / (float)g.dx, rdy = 1.0f / (float)g.dy;
-    const float r24dx = 1.0f / (24.0f * (float)g.dx), r24dy = 1.0f / (24.0f * (float)g.dy);
-    const float r12dx2 = 1.0f / (12.0f * (float)g.dx2), r12dy2 = 1.0f / (12.0f * (float)g.dy2);
-    const float rdx2 = 1.0f / (float)g.dx2, rdy2 = 1.0f / (float)g.dy2;
-    const float sx1 = CDS == 1 ? rdx : r24dx, sy1 = CDS == 1 ? rdy : r24dy;     // first differences
-    const float sx2 = CDS == 1 ? rdx2 : r12dx2, sy2 = CDS == 1 ? rdy2 : r12dy2; // second differences
-    const float dt = (float)a.ph.dt, nu = (float)a.ph.nu;
-    const float rka = (float)a.rk_a, rkb = (float)a.rk_b, rkc = (float)a.rk_c;
-    const float cdif = rkc * 0.5f * dt * nu, cgp = rkc * dt;
-    const float dpx = (float)a.sc->dpx_drive;
-    const float got = (float)a.sc->got, tref = (float)a.ph.t_ref;
-    const bool scalar = a.ph.isscalar == 1;
-
-    // the thread's points: x = x0 + 2 lane + s, rows y0 + 2 wid + q (s, q in {0, 1})
-    const int xl = 2 * lane, rl0 = 2 * wid;
     const int xi = x0 + xl;
     const bool xin = xi < nx;
     bool act[2];
     int gid[2];
-    int rc[2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         act[q] = xin && (y0 + rl0 + q) < ny;
         gid[q] = (y0 + rl0 + q) * nx + xi;                             // + k nxy
-        rc[q] = (rl0 + q + RS_HY) * RS_W + xl + RS_HX;                 // own raw index (even)
     }
 
     // values of level k-1 at the own points: u, v, w, uhz*whx, vhz*why
@@ -196,7 +192,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
         const int L = kb - 1;
         const float* u0 = plane(0, L); const float* v0 = plane(1, L); const float* w0 = plane(2, L);
         const float* u1 = plane(0, L + 1); const float* v1 = plane(1, L + 1);
-        const float l = (float)ldz(g.z.l_t, L);
+        const float l = zlt[L];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int r = rc[q];
@@ -220,13 +216,11 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
     }
     __syncthreads();      // level kb-1's slot is refilled with level kb+2 below
 
-    double dv_sum = 0.0, dv_max = 0.0;
-    int dv_nan = 0;
     for (int k = kb; k < ke; ++k) {
         const bool next_in = k + 1 < nz;          // level k+1 is interior (staged)
         if (k + 2 < nz && k + 1 < ke) { stage(k + 2); rs_commit(); }
         const bool wface = k < nz - 1;
-        const float lt = ZM[3 * RS_ZT + (k - kb)];
+        const float lt = __ldg(zlt + k);
         const float* u0 = plane(0, k); const float* v0 = plane(1, k);
         const float* w0 = plane(2, k); const float* p0 = plane(3, k);
         const float* u1 = plane(0, k + 1); const float* v1 = plane(1, k + 1);
@@ -318,8 +312,8 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
         __syncthreads();
 
         // ---- 2. the three equations at the thread's four points
-        const float rdz = ZM[k - kb], rdzt = ZM[RS_ZT + (k - kb)], rdzb = ZM[2 * RS_ZT + (k - kb)];
-        const float rdzp = ZM[4 * RS_ZT + (k - kb)];
+        const float rdz = __ldg(zrdz + k), rdzt = __ldg(zrdzt + k), rdzb = __ldg(zrdzb + k);
+        const float rdzp = __ldg(zrdzp + k);
         const double dxd = g.dx, dyd = g.dy, dzd = ldz(g.z.dz, k);
         const int fa0 = rl0 * RS_AW + xl + 2;                  // own index in the x strip
         const int fb0 = (rl0 + 2) * RS_AW + xl + 2;            // own index in the uhy*vhx plane
@@ -480,6 +474,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
         rs_wait_all();
         __syncthreads();
     }
+    }   // segments
 
     if (a.part_div) {
         __shared__ double s_sum[8], s_max[8];
