@@ -1844,15 +1844,27 @@ int hc_create(const hc_params* p, hc_handle** out)
             h->rhs_kc = kc;
             h->rhs_grid = dim3(bx, by, (p->nz + kc - 1) / kc);
             if (h->rhs_strip) {
-                // persistent: two blocks an SM (or one per tile-level run of tile[2]
-                // levels when that asks for more), each an equal share of the
-                // (tile, level) work in level order
+                // one block per (tile, level chunk), two resident an SM. Unless tile[2]
+                // sets it (a negative value: one wave of equal runs, no chunks), the
+                // chunk height in [8, 40] that wastes the least of the last wave of
+                // blocks, counting two staged levels of start-up per chunk
                 int dev_sm = 148;
                 cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, h->dev);
-                long long work = (long long)bx * by * p->nz;
-                long long nb = p->tile[2] > 0 ? (work + p->tile[2] - 1) / p->tile[2] : 2LL * dev_sm;
-                if (nb > work) nb = work;
-                if (nb < 1) nb = 1;
+                const long long slots = 2LL * dev_sm, ntl = (long long)bx * by;
+                int best = p->nz < 8 ? p->nz : 8;
+                double best_eff = -1.0;
+                for (int c = 8; c <= 40 && c <= p->nz; ++c) {
+                    const long long nb = ntl * ((p->nz + c - 1) / c);
+                    const double waves = (double)((nb + slots - 1) / slots);
+                    const double eff = (double)nb / (waves * slots) * c / (c + 2.0) *
+                                       (double)p->nz / (double)(c * ((p->nz + c - 1) / c));
+                    if (eff > best_eff + 1e-9) { best_eff = eff; best = c; }
+                }
+                int kcs = p->tile[2] > 0 ? p->tile[2] : best;
+                if (kcs > p->nz) kcs = p->nz;
+                long long nb = ntl * ((p->nz + kcs - 1) / kcs);
+                if (p->tile[2] < 0) { kcs = 0; nb = slots < ntl * p->nz ? slots : ntl * p->nz; }
+                h->rhs_kc = kcs;
                 h->rhs_grid = dim3((unsigned)nb, 1, 1);
             }
         }

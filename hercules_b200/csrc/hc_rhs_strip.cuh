@@ -101,10 +101,22 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_strip(RhsTArgs<float> a
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int closed = a.ph.ochannel == 0;
     const int tiles_x = (nx + RS_TX - 1) / RS_TX;
-    const long long work = (long long)tiles_x * ((ny + RS_TY - 1) / RS_TY) * nz;
-    // this block's share of the (tile, level) work, tiles in order, levels ascending
-    long long wcur = work * blockIdx.x / gridDim.x;
-    const long long wend = work * (blockIdx.x + 1) / gridDim.x;
+    const long long ntiles = (long long)tiles_x * ((ny + RS_TY - 1) / RS_TY);
+    // the (tile, level) work of this block: with a level chunk (a.kchunk > 0) block b
+    // takes chunk b / ntiles of tile b % ntiles, so that the blocks in flight cover
+    // neighbouring tiles at the same levels and share their halo rows in L2; with
+    // a.kchunk = 0 the blocks split the work, tiles in order and levels ascending,
+    // into equal runs (one wave, no tail)
+    long long wcur, wend;
+    if (a.kchunk > 0) {
+        const long long t = blockIdx.x % ntiles, c = blockIdx.x / ntiles;
+        wcur = t * nz + c * a.kchunk;
+        wend = t * nz + min((long long)nz, (c + 1) * a.kchunk);
+    } else {
+        const long long work = ntiles * nz;
+        wcur = work * blockIdx.x / gridDim.x;
+        wend = work * (blockIdx.x + 1) / gridDim.x;
+    }
     const float* zrdz = a.zm;
     const float* zrdzt = a.zm + nz;
     const float* zrdzb = a.zm + 2 * nz;
