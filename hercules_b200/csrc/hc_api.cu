@@ -245,7 +245,8 @@ struct hc_handle {
     double* mean[11];
     float* win[11];          // FP32 storage: the FP32 window sums of the mean accumulators
     double* mtmp;            // FP32 storage: FP64 sums + window, assembled for a download
-    double* zbuf;            // 5*(nz+4) doubles, then the 5*nz floats of zm5
+    double* zbuf;            // 5*(nz+4) doubles, then zm5d (5*nz doubles) and zm5 (5*nz floats)
+    double* zm5d;            // FP64 per-level metrics of the strip RHS
     float* zm5;              // FP32 per-level metrics of the strip RHS
     double* coef;
     ColCoef cc;
@@ -504,17 +505,25 @@ static int upload_zgrid(hc_handle* h)
         CK(cudaMemcpy(h->zbuf + q * nka, h->zhost[q].data(), nka * sizeof(double), cudaMemcpyHostToDevice));
     h->g.z.dz = h->zbuf; h->g.z.dz_t = h->zbuf + nka; h->g.z.dz_b = h->zbuf + 2 * nka;
     h->g.z.l_t = h->zbuf + 3 * nka; h->g.z.l_b = h->zbuf + 4 * nka;
-    // FP32 per-level metrics of the strip RHS, [5][nz]: 1/dz, 1/dz_t, 1/dz_b, l_t, 1/dz(k+1)
-    // (interior level k at Fortran index k+2 of the host arrays)
+    // per-level metrics of the strip RHS, [5][nz]: 1/dz, 1/dz_t, 1/dz_b, l_t, 1/dz(k+1)
+    // (interior level k at Fortran index k+2 of the host arrays), in FP64 and in FP32
+    std::vector<double> zd(5 * (size_t)nz);
     std::vector<float> zm(5 * (size_t)nz);
     for (int k = 0; k < nz; ++k) {
+        zd[k] = 1.0 / h->zhost[0][k + 2];
+        zd[nz + k] = 1.0 / h->zhost[1][k + 2];
+        zd[2 * nz + k] = 1.0 / h->zhost[2][k + 2];
+        zd[3 * nz + k] = h->zhost[3][k + 2];
+        zd[4 * nz + k] = 1.0 / h->zhost[0][k + 3];
         zm[k] = 1.0f / (float)h->zhost[0][k + 2];
         zm[nz + k] = 1.0f / (float)h->zhost[1][k + 2];
         zm[2 * nz + k] = 1.0f / (float)h->zhost[2][k + 2];
         zm[3 * nz + k] = (float)h->zhost[3][k + 2];
         zm[4 * nz + k] = 1.0f / (float)h->zhost[0][k + 3];
     }
-    h->zm5 = reinterpret_cast<float*>(h->zbuf + 5 * nka);
+    h->zm5d = h->zbuf + 5 * nka;
+    h->zm5 = reinterpret_cast<float*>(h->zm5d + 5 * nz);
+    CK(cudaMemcpy(h->zm5d, zd.data(), zd.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->zm5, zm.data(), zm.size() * sizeof(float), cudaMemcpyHostToDevice));
     return HC_OK;
 }
@@ -671,13 +680,14 @@ template <typename R> static int set_smem_attrs()
         CK(cudaFuncSetAttribute(k_column_sp_tile<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
         CK(cudaFuncSetAttribute(k_column_sp_tile<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
     }
+    CK(cudaFuncSetAttribute(k_rhs_momentum_strip<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem<R>()));
+    CK(cudaFuncSetAttribute(k_rhs_momentum_strip<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem<R>()));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
     if (sizeof(R) == sizeof(float)) {
         CK(cudaFuncSetAttribute(k_rhs_momentum_tiled2<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled2_smem(1)));
         CK(cudaFuncSetAttribute(k_rhs_momentum_tiled2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled2_smem(1)));
-        CK(cudaFuncSetAttribute(k_rhs_momentum_strip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem()));
-        CK(cudaFuncSetAttribute(k_rhs_momentum_strip<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem()));
+
     }
     return HC_OK;
 }
@@ -981,12 +991,12 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     // the divergence check of the previous sub-step rides along (slot sub-1)
     m.part_div = (sub > 0 && h->div_in_rhs && !recompute) ? h->part_div + (long long)(sub - 1) * h->pd_stride * 3 : nullptr;
     m.kchunk = h->rhs_kc;
-    m.zm = h->zm5;
+    m.zm = sizeof(R) == sizeof(float) ? (const void*)h->zm5 : (const void*)h->zm5d;
     m.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
     m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
     prof_begin(h, K_RHS_MOM);
-    if (sizeof(R) == sizeof(float) && h->rhs_strip)   // FP32: products on strips (64 x 16 tiles)
-        k_rhs_momentum_strip<CDS><<<h->rhs_grid, 256, rhs_strip_smem(), h->st>>>(*(const RhsTArgs<float>*)&m);
+    if (h->rhs_strip)                    // products on strips (64 x 16 tiles)
+        k_rhs_momentum_strip<R, CDS><<<h->rhs_grid, RsCfg<R>::NT, rhs_strip_smem<R>(), h->st>>>(m);
     else if (sizeof(R) == sizeof(float))      // FP32: two x points a thread (64 x 8 tiles)
         k_rhs_momentum_tiled2<CDS><<<h->rhs_grid, 256, rhs_tiled2_smem(m.with_t), h->st>>>(*(const RhsTArgs<float>*)&m);
     else
@@ -1750,7 +1760,7 @@ int hc_create(const hc_params* p, hc_handle** out)
     h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0;
     for (int q = 0; q < 11; ++q) { h->mean[q] = nullptr; h->win[q] = nullptr; }
     h->mtmp = nullptr;
-    h->zbuf = nullptr; h->zm5 = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
+    h->zbuf = nullptr; h->zm5 = nullptr; h->zm5d = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
     h->diag_cap = 0; h->last_ms = 0.0; h->launches = 0; h->initialized = 0;
     h->prof = 0; h->cur_cat = 0; h->ev_used = 0;
@@ -1821,7 +1831,8 @@ int hc_create(const hc_params* p, hc_handle** out)
         if (cudaMalloc(&h->scratch, cz * (3 * sizeof(double) + 4 * sizeof(double2))) != cudaSuccess) FAIL(HC_ERR_NOMEM);
         h->cs.bu = h->scratch; h->cs.bw = h->scratch + cz; h->cs.bp = h->scratch + 2 * cz;
         h->cs.su = (double2*)(h->scratch + 3 * cz); h->cs.sv = h->cs.su + cz; h->cs.sw = h->cs.sv + cz; h->cs.sp = h->cs.sw + cz;
-        if (cudaMalloc(&h->zbuf, 5 * (p->nz + 4) * sizeof(double) + 5 * (size_t)p->nz * sizeof(float)) != cudaSuccess)
+        if (cudaMalloc(&h->zbuf, 5 * (p->nz + 4) * sizeof(double) + 5 * (size_t)p->nz * (sizeof(double) + sizeof(float))) !=
+            cudaSuccess)
             FAIL(HC_ERR_NOMEM);
         if ((rc = upload_zgrid(h)) != HC_OK) goto fail;
         if ((rc = build_tables(h)) != HC_OK) goto fail;
@@ -1832,7 +1843,7 @@ int hc_create(const hc_params* p, hc_handle** out)
         if (h->nbd > RED_BLOCKS) h->nbd = RED_BLOCKS;
         {
             // momentum RHS tiles: enough blocks for ~4 per SM, chunks of 4..32 levels
-            h->rhs_strip = h->rsz == sizeof(float) && rhs_strip_ok(p->nx, p->ny, p->u_mrf, p->dp_opt);
+            h->rhs_strip = rhs_strip_ok(p->nx, p->ny, p->u_mrf, p->dp_opt, h->rsz);
             const int tx_pts = h->rhs_strip ? RS_TX : (h->rsz == sizeof(float) ? R2_TX : RT_TX);
             const int ty_pts = h->rhs_strip ? RS_TY : RT_TY;
             const int bx = (g.nx + tx_pts - 1) / tx_pts, by = (g.ny + ty_pts - 1) / ty_pts;
@@ -1844,13 +1855,14 @@ int hc_create(const hc_params* p, hc_handle** out)
             h->rhs_kc = kc;
             h->rhs_grid = dim3(bx, by, (p->nz + kc - 1) / kc);
             if (h->rhs_strip) {
-                // one block per (tile, level chunk), two resident an SM. Unless tile[2]
+                // one block per (tile, level chunk), RsCfg::MINB resident an SM. Unless tile[2]
                 // sets it (a negative value: one wave of equal runs, no chunks), the
                 // chunk height in [8, 40] that wastes the least of the last wave of
                 // blocks, counting two staged levels of start-up per chunk
                 int dev_sm = 148;
                 cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, h->dev);
-                const long long slots = 2LL * dev_sm, ntl = (long long)bx * by;
+                const long long slots = (long long)(h->rsz == sizeof(float) ? RsCfg<float>::MINB : RsCfg<double>::MINB) * dev_sm;
+                const long long ntl = (long long)bx * by;
                 int best = p->nz < 8 ? p->nz : 8;
                 double best_eff = -1.0;
                 for (int c = 8; c <= 40 && c <= p->nz; ++c) {

@@ -40,7 +40,7 @@ template <typename R> struct RhsTArgs {
     // largest magnitude, NaN flag; null when not wanted
     double* part_div;
     const R* bfx; const R* bfy; const R* bfz;   // body force added to ff, gg, hh (null: none)
-    const float* zm;     // FP32 per-level metrics [5][nz] (the strip kernel)
+    const void* zm;      // per-level metrics [5][nz] in the storage type (the strip kernel)
 };
 
 #define RT_KMAX 64

@@ -159,9 +159,9 @@ def test_config3_grid_statistics_and_diagnostics(oracle_lib, engine):
     o.close()
 
 
-# FP32 storage on grids of nx >= 64 (a multiple of 4) and ny >= 32 runs the strip
-# momentum RHS (k_rhs_momentum_strip): partial tiles, several level chunks (tile[2]),
-# both schemes, open/closed, temperature, AB2, and the body force
+# Grids of nx >= 64 and ny >= 32 run the strip momentum RHS (k_rhs_momentum_strip)
+# in both precisions: partial tiles, several level chunks (tile[2]), both schemes,
+# open/closed, temperature, AB2, and the body force
 STRIP = {
     "fd4_closed_dp2_chunks": config_channel_fd(nx=96, ny=64, nz=40).replace(tile=[0, 0, 7, 0]),
     "fd2_open_scalar": _fd(64, 48, 17, cds=1, ochannel=1, isscalar=1, got=0.7, tbot=-1.0, ttop=0.0),
@@ -172,12 +172,13 @@ STRIP = {
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(STRIP))
-def test_strip_rhs_mixed_against_oracle(name, oracle_lib, engine):
-    """Mixed precision through the strip RHS: velocities and temperature <= 1e-5
-    after 10 steps; the divergence of every sub-step is reported and small."""
+def test_strip_rhs_against_oracle(name, oracle_lib, engine):
+    """Both precisions through the strip RHS: FP64 <= 1e-10 and FP32-mixed
+    velocities and temperature <= 1e-5 after 10 steps (histories too in FP64);
+    the mixed divergence of every sub-step is reported and small."""
     p = STRIP[name]
-    errs = _compare(p, inputs.small_random(p, seed=17), 10, oracle_lib, engine, precisions=(PREC_MIXED,))
-    assert max(e for (q, f), e in errs.items() if f in ("u", "v", "w")) <= MIXED_TOL
+    errs = _compare(p, inputs.small_random(p, seed=17), 10, oracle_lib, engine, extra=("ff", "gg", "hh"))
+    assert max(e for (q, f), e in errs.items() if q == PREC_MIXED and f in ("u", "v", "w")) <= MIXED_TOL
     c = engine.Channel(p.replace(precision=PREC_MIXED))
     c.load(inputs.small_random(p, seed=17))
     c.initialize()
@@ -190,7 +191,7 @@ def test_strip_rhs_mixed_against_oracle(name, oracle_lib, engine):
 
 
 @pytest.mark.gpu
-def test_strip_rhs_body_force_mixed(oracle_lib, engine):
+def test_strip_rhs_body_force(oracle_lib, engine):
     p = config_channel_fd(nx=64, ny=32, nz=16).replace(dp_opt=1, nu=1.0 / 300.0)
     fields = inputs.small_random(p, seed=9)
     bf = inputs.gaussian_body_force(p, seed=4, amp=0.05)
@@ -200,14 +201,15 @@ def test_strip_rhs_body_force_mixed(oracle_lib, engine):
     o.initialize()
     rc, _ = o.step(10)
     assert rc == 0
-    c = engine.Channel(p.replace(precision=PREC_MIXED))
-    c.load(fields)
-    c.set_body_force(*bf)
-    c.initialize()
-    c.step(10)
-    for f in ("u", "v", "w"):
-        assert rel_err(c.download(f), o.get(f)) <= MIXED_TOL, f
-    c.close()
+    for prec, tol in ((0, FP64_TOL), (PREC_MIXED, MIXED_TOL)):
+        c = engine.Channel(p.replace(precision=prec))
+        c.load(fields)
+        c.set_body_force(*bf)
+        c.initialize()
+        c.step(10)
+        for f in ("u", "v", "w"):
+            assert rel_err(c.download(f), o.get(f)) <= tol, (prec, f)
+        c.close()
     o.close()
 
 
