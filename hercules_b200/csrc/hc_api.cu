@@ -26,6 +26,7 @@
 #include "hc_column_warp.cuh"
 #include "hc_spec.cuh"
 #include "hc_adjoint.cuh"
+#include "hc_group.cuh"
 
 // ---------------------------------------------------------------------------
 // small device kernels for the scalar state
@@ -44,7 +45,7 @@ struct ScalarArgs {
 // screen_cpu_time's time_sim += dt (src/module_io.f90:68), update_ri
 // (src/module_parameters.f90:580-590) and update_dpx_drive (:594-613), which the
 // reference calls at the start of every sub-step's RHS.
-__global__ void k_substep_begin(ScalarArgs a)
+__device__ __forceinline__ void k_substep_begin_body(const ScalarArgs& a, const uint3 blockIdx, const dim3 gridDim)
 {
     DevScalars* s = a.sc;
     if (s->nan_flag) return;
@@ -56,6 +57,7 @@ __global__ void k_substep_begin(ScalarArgs a)
     if (a.dp_opt == 1) s->dpx_drive = 1.0;
     else if (a.dp_opt == 2) s->dpx_drive = s->dpx_drive - (s->ubar + a.um - 1.0) * a.dpx_coef;
 }
+__global__ void k_substep_begin(ScalarArgs a) { k_substep_begin_body(a, blockIdx, gridDim); }
 
 struct FinalArgs {
     DevScalars* sc;
@@ -116,7 +118,7 @@ __device__ double block_absmax_fixed(double v, double* sh)
 }
 
 // End-of-step finaliser (one block of 256 threads, fixed reduction order).
-__global__ void __launch_bounds__(256) k_finalize(FinalArgs a)
+__device__ __forceinline__ void k_finalize_body(const FinalArgs& a, const uint3 blockIdx, const dim3 gridDim)
 {
     __shared__ double sh[256];
     DevScalars* s = a.sc;
@@ -175,6 +177,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinalArgs a)
         d->step = s->step;
     }
 }
+__global__ void __launch_bounds__(256) k_finalize(FinalArgs a) { k_finalize_body(a, blockIdx, gridDim); }
 
 template <typename R>
 __global__ void k_convert_in(const double* src, R* dst, long long n)
@@ -258,7 +261,8 @@ struct hc_handle {
     long long pd_stride;     // partial slots per sub-step (max over the writers)
     dim3 rhs_grid;           // FD momentum RHS grid and its level chunk
     int rhs_kc;
-    int rhs_strip;           // FP32: the strip kernel (k_rhs_momentum_strip) runs the RHS
+    int rhs_strip;           // the strip kernel (k_rhs_momentum_strip) runs the RHS
+    std::vector<GroupRec>* rec;   // non-null: launches are recorded (ensemble plans), not run
     DevScalars* sc;
     hc_diag* diag_dev;
     int diag_cap;
@@ -323,6 +327,25 @@ static int prof_collect(hc_handle* h)
         h->cat_n[h->ev_cat[q / 2]] += 1;
     }
     h->ev_used = 0;
+    return HC_OK;
+}
+
+// Launch KFN (whose body is BODY, launched with at most NT threads and MINB
+// resident blocks) on the handle's stream, or, while the handle records, keep the
+// launch for a grouped ensemble launch of the same body.
+template <typename A, void (*KFN)(A), void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
+static int hc_launch(hc_handle* h, dim3 grid, dim3 block, size_t smem, const A& args)
+{
+    if (h->rec) {
+        GroupRec r;
+        r.key = (const void*)&k_group<A, BODY, NT, MINB>;
+        r.build = &group_build<A, BODY, NT, MINB>;
+        r.args.assign(reinterpret_cast<const unsigned char*>(&args), reinterpret_cast<const unsigned char*>(&args) + sizeof(A));
+        r.grid = grid; r.block = block; r.smem = smem;
+        h->rec->push_back(std::move(r));
+        return HC_OK;
+    }
+    KFN<<<grid, block, smem, h->st>>>(args);
     return HC_OK;
 }
 
@@ -564,11 +587,18 @@ template <typename R, int N> static int fft_t_op(hc_handle* h, int op, const voi
         }
         return HC_OK;
     }
-    if (op == 1) k_fft_x_r2c_t<R, N, RM><<<grid, FxThreads<R, N>::v, sx, h->st>>>(*(const FxArgs<R>*)args);
-    else if (op == 2) k_fft_x_c2r_t<R, N, RM><<<grid, FxThreads<R, N>::v, sx, h->st>>>(*(const FxArgs<R>*)args);
-    else if (op == 3) FyKernel<R, N, -1, RM>::f<<<grid, FyThreads<R, N>::v, sy, h->st>>>(*(const FyArgs<R>*)args);
-    else FyKernel<R, N, 1, RM>::f<<<grid, FyThreads<R, N>::v, sy, h->st>>>(*(const FyArgs<R>*)args);
-    return HC_OK;
+    constexpr int TX = FxThreads<R, N>::v, TY = FyThreads<R, N>::v;
+    if (op == 1)
+        return hc_launch<FxArgs<R>, k_fft_x_r2c_t<R, N, RM>, k_fft_x_r2c_t_body<R, N, RM>, TX, 1>(
+            h, grid, dim3(TX), sx, *(const FxArgs<R>*)args);
+    if (op == 2)
+        return hc_launch<FxArgs<R>, k_fft_x_c2r_t<R, N, RM>, k_fft_x_c2r_t_body<R, N, RM>, TX, 1>(
+            h, grid, dim3(TX), sx, *(const FxArgs<R>*)args);
+    if (op == 3)
+        return hc_launch<FyArgs<R>, FyKernel<R, N, -1, RM>::f, k_fft_y_t_body<R, N, -1, RM>, TY, FyKernel<R, N, -1, RM>::minb>(
+            h, grid, dim3(TY), sy, *(const FyArgs<R>*)args);
+    return hc_launch<FyArgs<R>, FyKernel<R, N, 1, RM>::f, k_fft_y_t_body<R, N, 1, RM>, TY, FyKernel<R, N, 1, RM>::minb>(
+        h, grid, dim3(TY), sy, *(const FyArgs<R>*)args);
 }
 
 template <typename R> static int fft_t_dispatch(hc_handle* h, int n, int op, const void* args, dim3 grid)
@@ -741,7 +771,7 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     ax.rows = h->rows_x; ax.pl = h->px; ax.wpack = h->wpack; ax.scale = 1.0 / h->p.nx; ax.halt = halt;
     dim3 gx((unsigned)((ax.nrows + ax.rows - 1) / ax.rows), nf, 1);
     prof_begin(h, K_FFT_X_FWD);
-    k_fft_x_r2c<R><<<gx, 256, h->smem_x, h->st>>>(ax);
+    { int lrc = hc_launch<FftXArgs<R>, k_fft_x_r2c<R>, k_fft_x_r2c_body<R>, 256, 1>(h, gx, dim3(256), h->smem_x, ax); if (lrc) return lrc; }
     CKL();
     }
     if (h->fft_ty) {
@@ -761,7 +791,7 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     ay.nxh = h->g.nxh; ay.ny = h->g.ny; ay.tl = h->tl_y; ay.pl = h->py; ay.scale = 1.0 / h->p.ny; ay.halt = halt;
     dim3 gy((h->g.nxh + ay.tl - 1) / ay.tl, h->g.nz, nf);
     prof_begin(h, K_FFT_Y_FWD);
-    k_fft_y<R, -1><<<gy, 256, h->smem_y, h->st>>>(ay);
+    { int lrc = hc_launch<FftYArgs<R>, k_fft_y<R, -1>, k_fft_y_body<R, -1>, 256, 1>(h, gy, dim3(256), h->smem_y, ay); if (lrc) return lrc; }
     CKL();
     (void)sizeof(T2);
     return HC_OK;
@@ -791,7 +821,7 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
     ay.nxh = h->g.nxh; ay.ny = h->g.ny; ay.tl = h->tl_y; ay.pl = h->py; ay.scale = 1.0; ay.halt = halt;
     dim3 gy((h->g.nxh + ay.tl - 1) / ay.tl, h->g.nz, nf);
     prof_begin(h, K_FFT_Y_INV);
-    k_fft_y<R, 1><<<gy, 256, h->smem_y, h->st>>>(ay);
+    { int lrc = hc_launch<FftYArgs<R>, k_fft_y<R, 1>, k_fft_y_body<R, 1>, 256, 1>(h, gy, dim3(256), h->smem_y, ay); if (lrc) return lrc; }
     CKL();
     }
     if (h->fft_tx) {
@@ -813,7 +843,7 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
     ax.rows = h->rows_x; ax.pl = h->px; ax.wpack = h->wpack; ax.halt = halt;
     dim3 gx((unsigned)((ax.nrows + ax.rows - 1) / ax.rows), nf, 1);
     prof_begin(h, K_FFT_X_INV);
-    k_fft_x_c2r<R><<<gx, 256, h->smem_x, h->st>>>(ax);
+    { int lrc = hc_launch<FftXInvArgs<R>, k_fft_x_c2r<R>, k_fft_x_c2r_body<R>, 256, 1>(h, gx, dim3(256), h->smem_x, ax); if (lrc) return lrc; }
     CKL();
     return HC_OK;
 }
@@ -837,7 +867,8 @@ template <typename R> static int launch_stats(hc_handle* h, int accumulate)
     s.um = h->p.u_mrf; s.dt = h->p.dt;
     s.part = h->part_st;
     prof_begin(h, K_STATS);
-    k_stats<R><<<dim3((unsigned)h->stx, (unsigned)h->sty), 256, 0, h->st>>>(s);
+    { int lrc = hc_launch<StatsArgs<R>, k_stats<R>, k_stats_body<R>, 256, StatsMinBlocks<R>::v>(
+          h, dim3((unsigned)h->stx, (unsigned)h->sty), dim3(256), 0, s); if (lrc) return lrc; }
     CKL();
     return HC_OK;
 }
@@ -858,7 +889,7 @@ static int launch_finalize(hc_handle* h, int nsub, int write_diag, int set_ubar 
     f.cds = h->p.cds;
     f.set_ubar = set_ubar;
     prof_begin(h, K_FINAL);
-    k_finalize<<<1, 256, 0, h->st>>>(f);
+    { int lrc = hc_launch<FinalArgs, k_finalize, k_finalize_body, 256, 1>(h, dim3(1), dim3(256), 0, f); if (lrc) return lrc; }
     CKL();
     return HC_OK;
 }
@@ -869,12 +900,14 @@ template <typename R, int K> static int col_fd_k(hc_handle* h, const ColArgs<R>&
 {
     if (h->p.tile[3] == 2) {      // per-warp variant without the coalescing tiles
         const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
-        k_column_fd_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(ca);
+        { int lrc = hc_launch<ColArgs<R>, k_column_fd_warp<R, K>, k_column_fd_warp_body<R, K>, CW_WARPS * 32, 4>(
+              h, dim3(nb), dim3(CW_WARPS * 32), column_warp_smem<K>(), ca); if (lrc) return lrc; }
         CKL();
         return HC_OK;
     }
     const unsigned nb = (unsigned)((h->g.ncol + CT_COLS - 1) / CT_COLS);
-    k_column_fd_tile_r<R, K><<<nb, CT_COLS * 32, column_tile_smem_r<K>(sizeof(typename V2<R>::T)), h->st>>>(ca);
+    { int lrc = hc_launch<ColArgs<R>, k_column_fd_tile_r<R, K>, k_column_fd_tile_r_body<R, K>, CT_COLS * 32, 2>(
+          h, dim3(nb), dim3(CT_COLS * 32), column_tile_smem_r<K>(sizeof(typename V2<R>::T)), ca); if (lrc) return lrc; }
     CKL();
     return HC_OK;
 }
@@ -894,14 +927,16 @@ template <typename R> static int launch_column_fd(hc_handle* h, const ColArgs<R>
         default: break;
         }
     }
-    k_column_fd<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ca);
+    { int lrc = hc_launch<ColArgs<R>, k_column_fd<R>, k_column_fd_body<R>, 256, 1>(
+          h, dim3((unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads)), dim3(h->col_threads), 0, ca); if (lrc) return lrc; }
     CKL();
     return HC_OK;
 }
 template <typename R, int K> static int col_t_k(hc_handle* h, const ColTArgs<R>& ct)
 {
     const unsigned nb = (unsigned)((h->g.ncol + CT_COLS - 1) / CT_COLS);
-    k_column_t_tile<R, K><<<nb, CT_COLS * 32, column_t_tile_smem<K>(sizeof(typename V2<R>::T)), h->st>>>(ct);
+    { int lrc = hc_launch<ColTArgs<R>, k_column_t_tile<R, K>, k_column_t_tile_body<R, K>, CT_COLS * 32, 2>(
+          h, dim3(nb), dim3(CT_COLS * 32), column_t_tile_smem<K>(sizeof(typename V2<R>::T)), ct); if (lrc) return lrc; }
     CKL();
     return HC_OK;
 }
@@ -921,7 +956,8 @@ template <typename R> static int launch_column_t(hc_handle* h, const ColTArgs<R>
         default: break;
         }
     }
-    k_column_t<R><<<(unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads), h->col_threads, 0, h->st>>>(ct);
+    { int lrc = hc_launch<ColTArgs<R>, k_column_t<R>, k_column_t_body<R>, 256, 1>(
+          h, dim3((unsigned)((h->g.ncol + h->col_threads - 1) / h->col_threads)), dim3(h->col_threads), 0, ct); if (lrc) return lrc; }
     CKL();
     return HC_OK;
 }
@@ -943,7 +979,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     sa.is_ri_var = p.is_ri_var; sa.ri_str = p.ri_str; sa.ri_end = p.ri_end; sa.imax = p.imax;
     if (!recompute || first) {
         prof_begin(h, K_BEGIN);
-        k_substep_begin<<<1, 1, 0, h->st>>>(sa);
+        { int lrc = hc_launch<ScalarArgs, k_substep_begin, k_substep_begin_body, 32, 1>(h, dim3(1), dim3(1), 0, sa); if (lrc) return lrc; }
         CKL();
     }
 
@@ -996,11 +1032,19 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
     prof_begin(h, K_RHS_MOM);
     if (h->rhs_strip)                    // products on strips (64 x 16 tiles)
-        k_rhs_momentum_strip<R, CDS><<<h->rhs_grid, RsCfg<R>::NT, rhs_strip_smem<R>(), h->st>>>(m);
-    else if (sizeof(R) == sizeof(float))      // FP32: two x points a thread (64 x 8 tiles)
-        k_rhs_momentum_tiled2<CDS><<<h->rhs_grid, 256, rhs_tiled2_smem(m.with_t), h->st>>>(*(const RhsTArgs<float>*)&m);
-    else
-        k_rhs_momentum_tiled<R, CDS><<<h->rhs_grid, RT_TX * RT_TY, rhs_tiled_smem<R>(m.with_t), h->st>>>(m);
+    {
+        int lrc;
+        if (h->rhs_strip)
+            lrc = hc_launch<RhsTArgs<R>, k_rhs_momentum_strip<R, CDS>, k_rhs_momentum_strip_body<R, CDS>, RsCfg<R>::NT,
+                            RsCfg<R>::MINB>(h, h->rhs_grid, dim3(RsCfg<R>::NT), rhs_strip_smem<R>(), m);
+        else if constexpr (sizeof(R) == sizeof(float))      // FP32: two x points a thread (64 x 8 tiles)
+            lrc = hc_launch<RhsTArgs<float>, k_rhs_momentum_tiled2<CDS>, k_rhs_momentum_tiled2_body<CDS>, 256, 2>(
+                h, h->rhs_grid, dim3(256), rhs_tiled2_smem(m.with_t), m);
+        else
+            lrc = hc_launch<RhsTArgs<R>, k_rhs_momentum_tiled<R, CDS>, k_rhs_momentum_tiled_body<R, CDS>, 256,
+                            RhsMinBlocks<R>::v>(h, h->rhs_grid, dim3(RT_TX * RT_TY), rhs_tiled_smem<R>(m.with_t), m);
+        if (lrc) return lrc;
+    }
     CKL();
     }
 
@@ -1041,7 +1085,8 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
         ta.ss = (R*)h->fld[F_SS]; ta.qt = (R*)h->fld[F_QU];
         ta.rk_a = rk_a; ta.rk_b = rk_b; ta.rk_c = rk_c; ta.ph = h->ph;
         prof_begin(h, K_RHS_T);
-        k_rhs_temperature<R, CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(ta);
+        { int lrc = hc_launch<TempArgs<R>, k_rhs_temperature<R, CDS>, k_rhs_temperature_body<R, CDS>, 256, 1>(
+              h, pt_grid(h->g), pt_block(), 0, ta); if (lrc) return lrc; }
         CKL();
         const R* tin[1] = {(const R*)h->fld[F_QU]};
         rc = fft_forward<R>(h, tin, S, 1);
@@ -1073,7 +1118,13 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     // (without damping, which changes the fields first); the last one has its own pass
     if (recompute || (!last && h->div_in_rhs)) return HC_OK;
     prof_begin(h, K_DIV);
-    k_div_check<R, CDS><<<(unsigned)h->nbd, 256, 0, h->st>>>(fi, h->g, h->part_div + (long long)sub * h->pd_stride * 3);
+    {
+        DivArgs<R> da;
+        da.f = fi; da.g = h->g; da.part = h->part_div + (long long)sub * h->pd_stride * 3;
+        int lrc = hc_launch<DivArgs<R>, k_div_check<R, CDS>, k_div_check_body<R, CDS>, 256, DivMinBlocks<R>::v>(
+            h, dim3((unsigned)h->nbd), dim3(256), 0, da);
+        if (lrc) return lrc;
+    }
     CKL();
     return HC_OK;
 }
@@ -1757,7 +1808,7 @@ int hc_create(const hc_params* p, hc_handle** out)
     h->adj_buf = nullptr; h->adj_bytes = 0; h->adj_sc = nullptr; h->adj_nsc = 0;
     h->adj_tape_seg = -1; h->adj_gnext = 0;
     for (int q = 0; q < ADJ_GRAPHS; ++q) { h->adj_gexec[q] = nullptr; h->adj_gkey[q] = -1; }
-    h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0;
+    h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0; h->rec = nullptr; h->rhs_strip = 0;
     for (int q = 0; q < 11; ++q) { h->mean[q] = nullptr; h->win[q] = nullptr; }
     h->mtmp = nullptr;
     h->zbuf = nullptr; h->zm5 = nullptr; h->zm5d = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
@@ -2281,9 +2332,14 @@ int hc_set_graph(hc_handle* h, int enable)
 }
 
 // ---------------------------------------------------------------------------
-// ensemble: independent channels advanced together, one graph per step with a
-// branch per member (the members' own streams, forked from and joined into the
-// ensemble stream), so small members run concurrently
+// ensemble: independent channels advanced together. FD members (no damping)
+// advance through grouped launches: each member records the launches of one step
+// (its own kernels, grids and arguments), and the n-th launch of every member is
+// issued as one launch per distinct kernel variant over all members that run it
+// (k_group), so a step takes a few dozen launches whatever the member count.
+// Otherwise one graph per step holds a branch per member (the members' own
+// streams, forked from and joined into the ensemble stream). Either way the
+// step is replayed from a CUDA graph.
 // ---------------------------------------------------------------------------
 struct hc_ensemble {
     std::vector<hc_handle*> m;
@@ -2293,10 +2349,12 @@ struct hc_ensemble {
     cudaGraphExec_t gexec;
     long long launches_per_step;
     double last_ms;
+    std::vector<GroupLaunch> plan;     // grouped launches of one step (empty: branch graph)
 };
 
 static void ensemble_free(hc_ensemble* e)
 {
+    for (size_t q = 0; q < e->plan.size(); ++q) cudaFree(e->plan[q].dbuf);
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     for (size_t q = 0; q < e->join.size(); ++q) if (e->join[q]) cudaEventDestroy(e->join[q]);
     if (e->fork) cudaEventDestroy(e->fork);
@@ -2304,6 +2362,53 @@ static void ensemble_free(hc_ensemble* e)
     if (e->e1) cudaEventDestroy(e->e1);
     if (e->st) cudaStreamDestroy(e->st);
     delete e;
+}
+
+// The grouped plan of one ensemble step; 1 if some member's step cannot be
+// recorded (spectral or damped members), then nothing is kept.
+static int ensemble_plan(hc_ensemble* e)
+{
+    const int n = (int)e->m.size();
+    std::vector<std::vector<GroupRec>> recs(n);
+    size_t len = 0;
+    for (int q = 0; q < n; ++q) {
+        hc_handle* h = e->m[q];
+        if (h->p.cds == 3 || h->p.isdamp == 1) return 1;
+        const int prof = h->prof;
+        const long long l0 = h->launches;
+        h->prof = 0;
+        h->rec = &recs[q];
+        const int rc = h->rsz == sizeof(float) ? step_dispatch<float>(h) : step_dispatch<double>(h);
+        h->rec = nullptr;
+        h->prof = prof;
+        h->launches = l0;
+        if (rc != HC_OK) return 1;
+        if (recs[q].size() > len) len = recs[q].size();
+    }
+    // the i-th launch of every member, grouped by kernel variant in member order
+    for (size_t i = 0; i < len; ++i) {
+        std::vector<const void*> keys;
+        std::vector<std::vector<const GroupRec*>> groups;
+        for (int q = 0; q < n; ++q) {
+            if (i >= recs[q].size()) continue;
+            const GroupRec* r = &recs[q][i];
+            size_t g = 0;
+            while (g < keys.size() && keys[g] != r->key) ++g;
+            if (g == keys.size()) { keys.push_back(r->key); groups.emplace_back(); }
+            groups[g].push_back(r);
+        }
+        for (size_t g = 0; g < groups.size(); ++g) {
+            GroupLaunch gl;
+            if (groups[g][0]->build(groups[g].data(), (int)groups[g].size(), &gl) != 0) {
+                for (size_t q = 0; q < e->plan.size(); ++q) cudaFree(e->plan[q].dbuf);
+                e->plan.clear();
+                cudaGetLastError();
+                return 1;
+            }
+            e->plan.push_back(gl);
+        }
+    }
+    return 0;
 }
 
 int hc_ensemble_create(hc_handle* const* members, int n, hc_ensemble** out)
@@ -2328,6 +2433,14 @@ int hc_ensemble_create(hc_handle* const* members, int n, hc_ensemble** out)
         cudaEventCreate(&e->e0) != cudaSuccess || cudaEventCreate(&e->e1) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
     for (int q = 0; q < n; ++q)
         if (cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
+    if (ensemble_plan(e) == 0) {
+        if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
+        for (size_t q = 0; q < e->plan.size(); ++q) {
+            if (e->plan[q].nblk) e->plan[q].run(e->plan[q], e->st);
+            if (cudaGetLastError() != cudaSuccess) rc = HC_ERR_CUDA;
+        }
+        total = (long long)e->plan.size();
+    } else {
     if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
     cudaEventRecord(e->fork, e->st);
     for (int q = 0; q < n && rc == HC_OK; ++q) {
@@ -2342,6 +2455,7 @@ int hc_ensemble_create(hc_handle* const* members, int n, hc_ensemble** out)
         h->prof = prof;
         cudaEventRecord(e->join[q], h->st);
         cudaStreamWaitEvent(e->st, e->join[q], 0);
+    }
     }
     {
         cudaError_t ce = cudaStreamEndCapture(e->st, &g);

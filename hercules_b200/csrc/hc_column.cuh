@@ -80,7 +80,7 @@ __device__ __forceinline__ double2 zscale(double2 a, double s) { return make_dou
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_column_fd(ColArgs<R> a)
+__device__ __forceinline__ void k_column_fd_body(const ColArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     if (a.halt && *a.halt) return;
     const long long ncol = a.g.ncol;
@@ -233,6 +233,8 @@ __global__ void __launch_bounds__(256) k_column_fd(ColArgs<R> a)
         }
     }
 }
+template <typename R>
+__global__ void __launch_bounds__(256) k_column_fd(ColArgs<R> a) { k_column_fd_body<R>(a, blockIdx, gridDim); }
 
 // Temperature Helmholtz solve (poisson_solver_fft with tbnd=1), in place.
 template <typename R> struct ColTArgs {
@@ -257,7 +259,7 @@ __device__ __forceinline__ bool spec_truncated(int l, int m, int ny, int ltr, in
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_column_t(ColTArgs<R> a)
+__device__ __forceinline__ void k_column_t_body(const ColTArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     if (a.halt && *a.halt) return;
     const long long ncol = a.g.ncol;
@@ -302,3 +304,5 @@ __global__ void __launch_bounds__(256) k_column_t(ColTArgs<R> a)
         st2<R>(a.out, id, tr ? make_double2(0, 0) : x);
     }
 }
+template <typename R>
+__global__ void __launch_bounds__(256) k_column_t(ColTArgs<R> a) { k_column_t_body<R>(a, blockIdx, gridDim); }

@@ -143,7 +143,7 @@ __device__ __forceinline__ void warp_partition_solve(const CF& coef, double2 (&d
 template <int K> __host__ size_t column_warp_smem() { return (size_t)CW_WARPS * 3 * K * 32 * sizeof(double2); }
 
 template <typename R, int K>
-__global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_fd_warp(ColArgs<R> a)
+__device__ __forceinline__ void k_column_fd_warp_body(const ColArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
@@ -276,6 +276,8 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_fd_warp(ColArgs<R> 
         }
     }
 }
+template <typename R, int K>
+__global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_fd_warp(ColArgs<R> a) { k_column_fd_warp_body<R, K>(a, blockIdx, gridDim); }
 
 // ---------------------------------------------------------------------------
 // Columns of CT_COLS adjacent wavenumber pairs staged in shared memory, so that
@@ -431,7 +433,7 @@ template <int K> __host__ size_t column_tile_smem_r(size_t elem)
 }
 
 template <typename R, int K>
-__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R> a)
+__device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     typedef typename V2<R>::T TT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -720,6 +722,8 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
     __syncthreads();
     store(a.psi, TU, nz);
 }
+template <typename R, int K>
+__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R> a) { k_column_fd_tile_r_body<R, K>(a, blockIdx, gridDim); }
 
 // ---------------------------------------------------------------------------
 // Temperature Helmholtz solve (tbnd) through one coalescing tile: a block of
@@ -733,7 +737,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
 template <int K> __host__ size_t column_t_tile_smem(size_t elem) { return (size_t)CT_COLS * ct_stride<K>() * elem; }
 
 template <typename R, int K>
-__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_t_tile(ColTArgs<R> a)
+__device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     typedef typename V2<R>::T TT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -805,3 +809,5 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_t_tile(ColTArgs<R> a
         if (cc < ncol) a.out[(long long)r * ncol + cc] = TQ[cb * STR + (r % K) * CT_RP + r / K];
     }
 }
+template <typename R, int K>
+__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_t_tile(ColTArgs<R> a) { k_column_t_tile_body<R, K>(a, blockIdx, gridDim); }

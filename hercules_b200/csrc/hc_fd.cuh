@@ -302,7 +302,7 @@ template <typename R> struct TempArgs {
 // get_temperature_cnvdiff (src/module_cnvdiff.f90:381-473); u, v, w are the
 // projected velocities of this sub-step, t the one from before it.
 template <typename R, int CDS>
-__global__ void __launch_bounds__(256) k_rhs_temperature(TempArgs<R> m)
+__device__ __forceinline__ void k_rhs_temperature_body(const TempArgs<R>& m, const uint3 blockIdx, const dim3 gridDim)
 {
     const Acc<R>& A = m.a;
     const Geo& g = A.g;
@@ -340,6 +340,8 @@ __global__ void __launch_bounds__(256) k_rhs_temperature(TempArgs<R> m)
     m.ss[id] = s;
     m.qt[id] = tc + dt * ((R)m.rk_a * s + (R)m.rk_b * s0) + (R)m.rk_c * R(0.5) * dt * al * (txx + tyy + tzz);
 }
+template <typename R, int CDS>
+__global__ void __launch_bounds__(256) k_rhs_temperature(TempArgs<R> m) { k_rhs_temperature_body<R, CDS>(m, blockIdx, gridDim); }
 
 // ---------------------------------------------------------------------------
 // block reductions
@@ -410,9 +412,18 @@ __device__ __forceinline__ void decode_pt(long long q, const Geo& g, int& i, int
 // (at 512 x 384 x 256: 315 -> 239 us and 361 -> 309 us a launch; with the
 // compiler's own budget too few warps had their loads in flight)
 template <typename R> struct DivMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 4 : 3; };
+template <typename R>
+struct DivArgs {
+    FieldsIn<R> f;
+    Geo g;
+    double* part;    // 3 doubles per block: sum |div|, signed div at max |div|, NaN flag
+};
 template <typename R, int CDS>
-__global__ void __launch_bounds__(256, DivMinBlocks<R>::v) k_div_check(FieldsIn<R> f, Geo g, double* part)
+__device__ __forceinline__ void k_div_check_body(const DivArgs<R>& da, const uint3 blockIdx, const dim3 gridDim)
 {
+    const FieldsIn<R>& f = da.f;
+    const Geo& g = da.g;
+    double* part = da.part;
     __shared__ double s_sum[8], s_max[8];
     __shared__ int s_nan;
     const int tid = threadIdx.x;
@@ -529,6 +540,8 @@ __global__ void __launch_bounds__(256, DivMinBlocks<R>::v) k_div_check(FieldsIn<
         }
     }
 }
+template <typename R, int CDS>
+__global__ void __launch_bounds__(256, DivMinBlocks<R>::v) k_div_check(DivArgs<R> a) { k_div_check_body<R, CDS>(a, blockIdx, gridDim); }
 
 template <typename R> struct StatsArgs {
     FieldsIn<R> f;
@@ -564,7 +577,7 @@ static __global__ void k_mean_combine(double* __restrict__ dst, const double* __
 template <typename R> struct StatsMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 3 : 2; };
 
 template <typename R>
-__global__ void __launch_bounds__(256, StatsMinBlocks<R>::v) k_stats(StatsArgs<R> s)
+__device__ __forceinline__ void k_stats_body(const StatsArgs<R>& s, const uint3 blockIdx, const dim3 gridDim)
 {
     // blockIdx.x: 256 consecutive (i,j) points of a plane; blockIdx.y: a chunk of levels
     constexpr int G = 2;
@@ -756,6 +769,8 @@ __global__ void __launch_bounds__(256, StatsMinBlocks<R>::v) k_stats(StatsArgs<R
         }
     }
 }
+template <typename R>
+__global__ void __launch_bounds__(256, StatsMinBlocks<R>::v) k_stats(StatsArgs<R> s) { k_stats_body<R>(s, blockIdx, gridDim); }
 
 // ---------------------------------------------------------------------------
 // rayleigh_damping (src/module_tools.f90:705-749) of u, v, w, p, t on levels

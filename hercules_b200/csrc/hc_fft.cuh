@@ -143,7 +143,7 @@ template <typename R> struct FftXArgs {
 };
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_fft_x_r2c(FftXArgs<R> a)
+__device__ __forceinline__ void k_fft_x_r2c_body(const FftXArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     typedef typename V2<R>::T T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -177,6 +177,8 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c(FftXArgs<R> a)
         out[idx] = X;
     }
 }
+template <typename R>
+__global__ void __launch_bounds__(256) k_fft_x_r2c(FftXArgs<R> a) { k_fft_x_r2c_body<R>(a, blockIdx, gridDim); }
 
 // ---------------------------------------------------------------------------
 // x direction, inverse: nx/2 modes -> real rows (unnormalised), stored or added
@@ -193,7 +195,7 @@ template <typename R> struct FftXInvArgs {
 };
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_fft_x_c2r(FftXInvArgs<R> a)
+__device__ __forceinline__ void k_fft_x_c2r_body(const FftXInvArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     typedef typename V2<R>::T T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -230,6 +232,8 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r(FftXInvArgs<R> a)
         out[idx] = v;
     }
 }
+template <typename R>
+__global__ void __launch_bounds__(256) k_fft_x_c2r(FftXInvArgs<R> a) { k_fft_x_c2r_body<R>(a, blockIdx, gridDim); }
 
 // ---------------------------------------------------------------------------
 // y direction, in place on the half spectrum [k][m][l]
@@ -244,7 +248,7 @@ template <typename R> struct FftYArgs {
 };
 
 template <typename R, int S>
-__global__ void __launch_bounds__(256) k_fft_y(FftYArgs<R> a)
+__device__ __forceinline__ void k_fft_y_body(const FftYArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     typedef typename V2<R>::T T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -279,3 +283,5 @@ __global__ void __launch_bounds__(256) k_fft_y(FftYArgs<R> a)
         d[(long long)m * a.nxh + l] = v;
     }
 }
+template <typename R, int S>
+__global__ void __launch_bounds__(256) k_fft_y(FftYArgs<R> a) { k_fft_y_body<R, S>(a, blockIdx, gridDim); }

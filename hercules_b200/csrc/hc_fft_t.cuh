@@ -353,7 +353,7 @@ template <typename R, int N, int S> struct YColsOut {
 // x direction, forward: real rows -> nx/2 modes, divided by nx
 // ----------------------------------------------------------------------------
 template <typename R, int N, int RMAX>
-__global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_r2c_t(FxArgs<R> a)
+__device__ __forceinline__ void k_fft_x_r2c_t_body(const FxArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     constexpr int NTX = FxThreads<R, N>::v;
     typedef typename V2<R>::T T2;
@@ -387,12 +387,14 @@ __global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_r2c_t(FxArgs<R> a)
         out[idx] = mk2<R>((e.x + wd.y) * sc, (e.y - wd.x) * sc);
     }
 }
+template <typename R, int N, int RMAX>
+__global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_r2c_t(FxArgs<R> a) { k_fft_x_r2c_t_body<R, N, RMAX>(a, blockIdx, gridDim); }
 
 // ----------------------------------------------------------------------------
 // x direction, inverse: nx/2 modes -> real rows (unnormalised), stored or added
 // ----------------------------------------------------------------------------
 template <typename R, int N, int RMAX>
-__global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_c2r_t(FxArgs<R> a)
+__device__ __forceinline__ void k_fft_x_c2r_t_body(const FxArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     constexpr int NTX = FxThreads<R, N>::v;
     typedef typename V2<R>::T T2;
@@ -478,6 +480,8 @@ __global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_c2r_t(FxArgs<R> a)
     const XRowsOut<T2, N> dst{reinterpret_cast<T2*>(a.out[f]) + row0 * N, nr, a.add[f]};
     run_passes<R, N, 1, RMAX, L, NTX, false, 0>(src, dst, A, B, a.tw);
 }
+template <typename R, int N, int RMAX>
+__global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_c2r_t(FxArgs<R> a) { k_fft_x_c2r_t_body<R, N, RMAX>(a, blockIdx, gridDim); }
 
 // ----------------------------------------------------------------------------
 // y direction on the half spectrum [k][m][l]: tiles of FyLines<R, N> columns l of
@@ -494,7 +498,7 @@ template <typename R, int N, int RMAX> struct FyFoldFirst {
     static constexpr bool v = sizeof(R) == sizeof(float) && PL::nfold == 1 && PL::rad(0) < 16;
 };
 template <typename R, int N, int S, int RMAX>
-__device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a)
+__device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a, const uint3 blockIdx)
 {
     typedef typename V2<R>::T T2;
     constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, TL = FyLines<R, N>::v, NT = FyThreads<R, N>::v;
@@ -527,18 +531,26 @@ __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a)
     run_passes<R, N, S, RMAX, TL, NT, true, 0, FyFoldFirst<R, N, RMAX>::v>(src, dst, A, B, a.tw);
 }
 
+template <typename R, int N, int S, int RMAX>
+__device__ __forceinline__ void k_fft_y_t_body(const FyArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
+{
+    fft_y_tile<R, N, S, RMAX>(a, blockIdx);
+}
 // FP64: the compiler's own register budget
 template <typename R, int N, int S, int RMAX>
-__global__ void __launch_bounds__(FyThreads<R, N>::v) k_fft_y_t(FyArgs<R> a) { fft_y_tile<R, N, S, RMAX>(a); }
+__global__ void __launch_bounds__(FyThreads<R, N>::v) k_fft_y_t(FyArgs<R> a) { k_fft_y_t_body<R, N, S, RMAX>(a, blockIdx, gridDim); }
 // FP32: registers sized for FyMinBlocks resident blocks
 template <int N, int S, int RMAX>
 __global__ void __launch_bounds__(FyThreads<float, N>::v, FyMinBlocks<float, N, RMAX>::v) k_fft_y_t32(FyArgs<float> a)
 {
-    fft_y_tile<float, N, S, RMAX>(a);
+    k_fft_y_t_body<float, N, S, RMAX>(a, blockIdx, gridDim);
 }
+// the y kernel of a length and its launch bounds (threads, resident blocks)
 template <typename R, int N, int S, int RMAX> struct FyKernel {
     static constexpr void (*f)(FyArgs<R>) = k_fft_y_t<R, N, S, RMAX>;
+    static constexpr int minb = 1;
 };
 template <int N, int S, int RMAX> struct FyKernel<float, N, S, RMAX> {
     static constexpr void (*f)(FyArgs<float>) = k_fft_y_t32<N, S, RMAX>;
+    static constexpr int minb = FyMinBlocks<float, N, RMAX>::v;
 };

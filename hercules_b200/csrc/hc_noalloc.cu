@@ -94,7 +94,9 @@ static int run_div(const Geo& g, const void* u, const void* v, const void* w, do
 {
     FieldsIn<R> f;
     f.u = (const R*)u; f.v = (const R*)v; f.w = (const R*)w; f.p = nullptr; f.t = nullptr;
-    k_div_check<R, CDS><<<(unsigned)nb, 256, 0, st>>>(f, g, part);
+    DivArgs<R> da;
+    da.f = f; da.g = g; da.part = part;
+    k_div_check<R, CDS><<<(unsigned)nb, 256, 0, st>>>(da);
     if (cudaGetLastError() != cudaSuccess) return HC_ERR_CUDA;
     k_noalloc_div_final<<<1, 256, 0, st>>>(part, nb, (double)g.nx, (double)g.ny, (double)g.nz, out);
     if (cudaGetLastError() != cudaSuccess) return HC_ERR_CUDA;

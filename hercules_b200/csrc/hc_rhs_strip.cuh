@@ -114,7 +114,7 @@ template <typename R> __device__ __forceinline__ void ld6r(const R* p, int i, R*
 }
 
 template <typename R, int CDS>
-__global__ void __launch_bounds__(RsCfg<R>::NT, RsCfg<R>::MINB) k_rhs_momentum_strip(RhsTArgs<R> a)
+__device__ __forceinline__ void k_rhs_momentum_strip_body(const RhsTArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     typedef typename V2<R>::T R2;
     constexpr int RQ = RsCfg<R>::RQ, NT = RsCfg<R>::NT, NW = RsCfg<R>::NW;
@@ -544,3 +544,5 @@ __global__ void __launch_bounds__(RsCfg<R>::NT, RsCfg<R>::MINB) k_rhs_momentum_s
         }
     }
 }
+template <typename R, int CDS>
+__global__ void __launch_bounds__(RsCfg<R>::NT, RsCfg<R>::MINB) k_rhs_momentum_strip(RhsTArgs<R> a) { k_rhs_momentum_strip_body<R, CDS>(a, blockIdx, gridDim); }

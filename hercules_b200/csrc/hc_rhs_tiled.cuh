@@ -121,7 +121,7 @@ __device__ __forceinline__ void rt_put(R* dst, const R* v)
 template <typename R> struct RhsMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 3 : 2; };
 
 template <typename R, int CDS>
-__global__ void __launch_bounds__(256, RhsMinBlocks<R>::v) k_rhs_momentum_tiled(RhsTArgs<R> a)
+__device__ __forceinline__ void k_rhs_momentum_tiled_body(const RhsTArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* sm = reinterpret_cast<R*>(smem_raw);
@@ -424,3 +424,5 @@ __global__ void __launch_bounds__(256, RhsMinBlocks<R>::v) k_rhs_momentum_tiled(
         }
     }
 }
+template <typename R, int CDS>
+__global__ void __launch_bounds__(256, RhsMinBlocks<R>::v) k_rhs_momentum_tiled(RhsTArgs<R> a) { k_rhs_momentum_tiled_body<R, CDS>(a, blockIdx, gridDim); }

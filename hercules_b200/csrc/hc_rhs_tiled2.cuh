@@ -79,7 +79,7 @@ __device__ __forceinline__ void r2_put(float* dst, const float* v)
 }
 
 template <int CDS>
-__global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled2(RhsTArgs<float> a)
+__device__ __forceinline__ void k_rhs_momentum_tiled2_body(const RhsTArgs<float>& a, const uint3 blockIdx, const dim3 gridDim)
 {
     typedef float R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -480,3 +480,5 @@ __global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled2(RhsTArgs<float> 
         }
     }
 }
+template <int CDS>
+__global__ void __launch_bounds__(256, 2) k_rhs_momentum_tiled2(RhsTArgs<float> a) { k_rhs_momentum_tiled2_body<CDS>(a, blockIdx, gridDim); }

@@ -82,3 +82,41 @@ def test_ensemble_config_generator_runs(engine):
     e.close()
     for c in chans:
         c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [0, PREC_MIXED])
+def test_grouped_ensemble_equals_individual_runs(engine, prec):
+    """FD members advance through grouped launches (the i-th kernel of every member
+    in one launch per kernel variant): a step of 12 members of four grids, with
+    temperature, a body force and an AB2 member, takes far fewer launches than
+    the members' own, and every member ends bit-equal to stepping it alone."""
+    grids = inputs.ENSEMBLE_GRIDS
+    members = []
+    for q in range(12):
+        nx, ny, nz = grids[q % 4]
+        p = config_channel_fd(nx, ny, nz, precision=prec).replace(
+            dp_opt=1, nu=1.0 / (100.0 + 15 * q), alpha=1.0 / (71.0 + 10 * q), isscalar=1, got=0.05 * q,
+            tbot=0.0, ttop=1.0, dt=2e-4)
+        if q == 5:
+            p = p.replace(dts=1)
+        members.append(p)
+    bf = inputs.gaussian_body_force(members[2], seed=4, amp=0.02)
+    ens_ch = [_channel(engine, p, 40 + q, bf=bf if q == 2 else None) for q, p in enumerate(members)]
+    ref_ch = [_channel(engine, p, 40 + q, bf=bf if q == 2 else None) for q, p in enumerate(members)]
+    e = engine.Ensemble(ens_ch)
+    e.step(5)
+    solo = 0
+    for c in ref_ch:
+        c.step(5)
+        solo = max(solo, c.last_launches // 5)
+    # grouped: at most a few launches per kernel position, not one per member
+    assert e.launches_per_step <= 5 * solo, (e.launches_per_step, solo)
+    assert e.launches_per_step < len(members) * solo // 2
+    for q, (x, y) in enumerate(zip(ens_ch, ref_ch)):
+        for f in ("u", "v", "w", "p", "t", "ff", "mean_u", "mean_tw"):
+            assert np.array_equal(x.download(f), y.download(f)), (q, f)
+        assert x.scalars() == y.scalars()
+    e.close()
+    for c in ens_ch + ref_ch:
+        c.close()
