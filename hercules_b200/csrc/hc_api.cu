@@ -13,6 +13,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/hercules_b200.h"
@@ -338,7 +339,8 @@ static int hc_launch(hc_handle* h, dim3 grid, dim3 block, size_t smem, const A& 
 {
     if (h->rec) {
         GroupRec r;
-        r.key = (const void*)&k_group<A, BODY, NT, MINB>;
+        r.key = (const void*)&k_group<A, BODY, NT, MINB, GroupCap<A>::v>;
+        r.cap = GroupCap<A>::v;
         r.build = &group_build<A, BODY, NT, MINB>;
         r.args.assign(reinterpret_cast<const unsigned char*>(&args), reinterpret_cast<const unsigned char*>(&args) + sizeof(A));
         r.grid = grid; r.block = block; r.smem = smem;
@@ -2350,11 +2352,14 @@ struct hc_ensemble {
     long long launches_per_step;
     double last_ms;
     std::vector<GroupLaunch> plan;     // grouped launches of one step (empty: branch graph)
+    std::vector<cudaStream_t> side;    // branches for the independent groups of one position
+    std::vector<cudaEvent_t> sev;
 };
 
 static void ensemble_free(hc_ensemble* e)
 {
-    for (size_t q = 0; q < e->plan.size(); ++q) cudaFree(e->plan[q].dbuf);
+    for (size_t q = 0; q < e->side.size(); ++q) cudaStreamDestroy(e->side[q]);
+    for (size_t q = 0; q < e->sev.size(); ++q) cudaEventDestroy(e->sev[q]);
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     for (size_t q = 0; q < e->join.size(); ++q) if (e->join[q]) cudaEventDestroy(e->join[q]);
     if (e->fork) cudaEventDestroy(e->fork);
@@ -2398,14 +2403,19 @@ static int ensemble_plan(hc_ensemble* e)
             groups[g].push_back(r);
         }
         for (size_t g = 0; g < groups.size(); ++g) {
-            GroupLaunch gl;
-            if (groups[g][0]->build(groups[g].data(), (int)groups[g].size(), &gl) != 0) {
-                for (size_t q = 0; q < e->plan.size(); ++q) cudaFree(e->plan[q].dbuf);
-                e->plan.clear();
-                cudaGetLastError();
-                return 1;
+            // at most cap members a launch
+            const int cap = groups[g][0]->cap;
+            for (size_t c0 = 0; c0 < groups[g].size(); c0 += (size_t)cap) {
+                const int cnt = (int)std::min(groups[g].size() - c0, (size_t)cap);
+                GroupLaunch gl;
+                gl.pos = (int)i;
+                if (groups[g][0]->build(groups[g].data() + c0, cnt, &gl) != 0) {
+                    e->plan.clear();
+                    cudaGetLastError();
+                    return 1;
+                }
+                e->plan.push_back(std::move(gl));
             }
-            e->plan.push_back(gl);
         }
     }
     return 0;
@@ -2434,10 +2444,36 @@ int hc_ensemble_create(hc_handle* const* members, int n, hc_ensemble** out)
     for (int q = 0; q < n; ++q)
         if (cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
     if (ensemble_plan(e) == 0) {
+        // the groups of one position are independent: all but the first run on
+        // side branches forked from and joined back into the ensemble stream
+        size_t width = 1;
+        for (size_t q = 0, w = 0; q < e->plan.size(); ++q) {
+            w = (q > 0 && e->plan[q].pos == e->plan[q - 1].pos) ? w + 1 : 1;
+            if (w > width) width = w;
+        }
+        for (size_t q = 1; q < width; ++q) {
+            cudaStream_t sq;
+            if (cudaStreamCreateWithFlags(&sq, cudaStreamNonBlocking) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
+            e->side.push_back(sq);
+        }
+        for (size_t q = 0; q < 2 * width; ++q) {
+            cudaEvent_t ev;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
+            e->sev.push_back(ev);
+        }
         if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { rc = HC_ERR_CUDA; goto fail; }
-        for (size_t q = 0; q < e->plan.size(); ++q) {
-            if (e->plan[q].nblk) e->plan[q].run(e->plan[q], e->st);
+        for (size_t q = 0; q < e->plan.size();) {
+            size_t r = q;
+            while (r < e->plan.size() && e->plan[r].pos == e->plan[q].pos) ++r;
+            if (r - q > 1) cudaEventRecord(e->sev[0], e->st);
+            for (size_t g = q; g < r; ++g) {
+                cudaStream_t sg = g == q ? e->st : e->side[g - q - 1];
+                if (g > q) cudaStreamWaitEvent(sg, e->sev[0], 0);
+                if (e->plan[g].nblk) e->plan[g].run(e->plan[g], sg);
+                if (g > q) { cudaEventRecord(e->sev[1 + (g - q - 1)], sg); cudaStreamWaitEvent(e->st, e->sev[1 + (g - q - 1)], 0); }
+            }
             if (cudaGetLastError() != cudaSuccess) rc = HC_ERR_CUDA;
+            q = r;
         }
         total = (long long)e->plan.size();
     } else {

@@ -7,31 +7,47 @@
 // of the 1-D launch are the concatenated grids of the members, and each block
 // finds its member (binary search over the prefix sums of the members' block
 // counts), its block index in that member's grid, and the member's arguments in
-// a device table. Every member's block then does exactly what it does in the
-// member's own launch, so the results are the same bit for bit.
+// the launch's parameter block. Every member's block then does exactly what it
+// does in the member's own launch: the table is a __grid_constant__ parameter, so
+// the body reads its arguments from the constant bank exactly as in its own
+// kernel (read from global memory they could alias the kernel's stores, and the
+// compiler then contracted FP32 products differently), and the results are the
+// same bit for bit.
 #pragma once
 #include <cuda_runtime.h>
 #include <string.h>
 #include <vector>
 
-template <typename A> struct GroupTab {
-    int n;                 // members
-    const int* start;      // n+1 prefix sums of the members' block counts
-    const dim3* grid;      // the members' own grids
-    const A* args;         // the members' arguments
+// Members a grouped launch carries in its parameter block (kernel parameters may
+// take up to 32 KB on this architecture).
+template <typename A> struct GroupCap {
+    static constexpr int v = (32000 - 16) / (int)(sizeof(A) + sizeof(int) + sizeof(dim3)) < 64
+                                 ? (32000 - 16) / (int)(sizeof(A) + sizeof(int) + sizeof(dim3)) : 64;
 };
 
-template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_group(GroupTab<A> t)
+// The table of a grouped launch, passed as the kernel's parameter block: the
+// members' arguments are read from the constant bank, as in their own kernels.
+// Two capacities: up to 8 members (a few KB of parameters a launch) and up to
+// GroupCap<A> members.
+#define HC_GROUP_SMALL 8
+template <typename A, int CAP> struct GroupTab {
+    int n;                 // members
+    int start[CAP + 1];    // prefix sums of the members' block counts
+    dim3 grid[CAP];        // the members' own grids
+    A args[CAP];           // the members' arguments
+};
+
+template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB, int CAP>
+__global__ void __launch_bounds__(NT, MINB) k_group(const __grid_constant__ GroupTab<A, CAP> t)
 {
     const int b = blockIdx.x;
     int lo = 0, hi = t.n - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(t.start + mid) <= b) lo = mid; else hi = mid - 1;
+        if (t.start[mid] <= b) lo = mid; else hi = mid - 1;
     }
     const dim3 gd = t.grid[lo];
-    const int lb = b - __ldg(t.start + lo);
+    const int lb = b - t.start[lo];
     uint3 bi;
     bi.x = lb % gd.x;
     bi.y = (lb / gd.x) % gd.y;
@@ -42,85 +58,74 @@ __global__ void __launch_bounds__(NT, MINB) k_group(GroupTab<A> t)
 struct GroupLaunch;
 
 // One recorded launch of one channel: the grouped kernel that can run its body
-// (which identifies the kernel variant), how to build a group of such launches,
-// and the launch's own arguments and shape.
+// (which identifies the kernel variant), the most members one grouped launch
+// takes, how to build a group of such launches, and the launch's own arguments
+// and shape.
 struct GroupRec {
     const void* key;
+    int cap;
     int (*build)(const GroupRec* const* recs, int n, GroupLaunch* out);
     std::vector<unsigned char> args;
     dim3 grid, block;
     size_t smem;
 };
 
-// A built group: its device table (one allocation) and how to launch it.
+// A built group: its parameter block and how to launch it.
 struct GroupLaunch {
     void (*run)(const GroupLaunch& g, cudaStream_t st);
-    void* dbuf;
-    int n;
+    int pos;               // position in the members' launch sequences
     unsigned nblk;
     dim3 block;
     size_t smem;
-    const void* args;
-    const int* start;
-    const dim3* grid;
+    std::vector<unsigned char> params;
 };
 
-template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
+template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB, int CAP>
 static void group_run(const GroupLaunch& gl, cudaStream_t st)
 {
-    GroupTab<A> t;
-    t.n = gl.n; t.start = gl.start; t.grid = gl.grid; t.args = (const A*)gl.args;
-    k_group<A, BODY, NT, MINB><<<gl.nblk, gl.block, gl.smem, st>>>(t);
+    k_group<A, BODY, NT, MINB, CAP><<<gl.nblk, gl.block, gl.smem, st>>>(
+        *reinterpret_cast<const GroupTab<A, CAP>*>(gl.params.data()));
 }
 
-static inline size_t group_align(size_t x) { return (x + 255) & ~(size_t)255; }
-
-// Build the device table of a group of recorded launches of the same body.
-// Returns 0, or -1 if the members' block shapes differ or the table cannot be
-// allocated (the caller then runs the members apart).
-template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
-static int group_build(const GroupRec* const* recs, int n, GroupLaunch* out)
+// Build a grouped launch of at most GroupCap<A> recorded launches of the same
+// body. Returns 0, or -1 if the members' block shapes differ (the caller then
+// runs the members apart).
+template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB, int CAP>
+static int group_build_cap(const GroupRec* const* recs, int n, GroupLaunch* out)
 {
-    std::vector<int> start(n + 1);
-    std::vector<dim3> grid(n);
-    std::vector<unsigned char> args((size_t)n * sizeof(A));
+    if (n < 1 || n > CAP) return -1;
+    out->params.assign(sizeof(GroupTab<A, CAP>), 0);
+    GroupTab<A, CAP>* t = reinterpret_cast<GroupTab<A, CAP>*>(out->params.data());
     long long tot = 0;
     size_t smem = 0;
     const dim3 blk = recs[0]->block;
+    t->n = n;
     for (int m = 0; m < n; ++m) {
         const GroupRec& r = *recs[m];
         if (r.block.x != blk.x || r.block.y != blk.y || r.block.z != blk.z || r.args.size() != sizeof(A)) return -1;
-        start[m] = (int)tot;
-        grid[m] = r.grid;
-        memcpy(args.data() + (size_t)m * sizeof(A), r.args.data(), sizeof(A));
+        t->start[m] = (int)tot;
+        t->grid[m] = r.grid;
+        memcpy(&t->args[m], r.args.data(), sizeof(A));
         tot += (long long)r.grid.x * r.grid.y * r.grid.z;
         if (r.smem > smem) smem = r.smem;
     }
     if (tot > 0x7fffffffLL) return -1;
-    start[n] = (int)tot;
-    const size_t oa = 0, os = group_align((size_t)n * sizeof(A)), og = os + group_align((size_t)(n + 1) * sizeof(int));
-    const size_t total = og + (size_t)n * sizeof(dim3);
-    unsigned char* d = nullptr;
-    if (cudaMalloc(&d, total) != cudaSuccess) return -1;
-    if (cudaMemcpy(d + oa, args.data(), args.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(d + os, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(d + og, grid.data(), n * sizeof(dim3), cudaMemcpyHostToDevice) != cudaSuccess) {
-        cudaFree(d);
-        return -1;
-    }
+    t->start[n] = (int)tot;
     if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k_group<A, BODY, NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-        cudaFree(d);
+        cudaFuncSetAttribute(k_group<A, BODY, NT, MINB, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
         return -1;
-    }
-    out->run = &group_run<A, BODY, NT, MINB>;
-    out->dbuf = d;
-    out->n = n;
+    out->run = &group_run<A, BODY, NT, MINB, CAP>;
     out->nblk = (unsigned)tot;
     out->block = blk;
     out->smem = smem;
-    out->args = d + oa;
-    out->start = (const int*)(d + os);
-    out->grid = (const dim3*)(d + og);
     return 0;
+}
+
+template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
+static int group_build(const GroupRec* const* recs, int n, GroupLaunch* out)
+{
+    constexpr int big = GroupCap<A>::v, small = HC_GROUP_SMALL < big ? HC_GROUP_SMALL : big;
+    if (n <= small) return group_build_cap<A, BODY, NT, MINB, small>(recs, n, out);
+    return group_build_cap<A, BODY, NT, MINB, big>(recs, n, out);
 }
