@@ -9,8 +9,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SO = os.path.join(HERE, "libhercules_b200.so")
 SRCS = [os.path.join(HERE, "csrc", f) for f in ("hc_api.cu", "hc_noalloc.cu")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+# -split-compile: the device code's kernels are optimised by parallel jobs
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-         "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+         "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr", "-split-compile", str(os.cpu_count() or 4)]
 
 
 def sources():

@@ -712,6 +712,8 @@ template <typename R> static int set_smem_attrs()
         CK(cudaFuncSetAttribute(k_column_sp_tile<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
         CK(cudaFuncSetAttribute(k_column_sp_tile<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
     }
+    CK(cudaFuncSetAttribute(k_rhs_t_strip<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_t_strip_smem<R>()));
+    CK(cudaFuncSetAttribute(k_rhs_t_strip<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_t_strip_smem<R>()));
     CK(cudaFuncSetAttribute(k_rhs_momentum_strip<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem<R>()));
     CK(cudaFuncSetAttribute(k_rhs_momentum_strip<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_strip_smem<R>()));
     CK(cudaFuncSetAttribute(k_rhs_momentum_tiled<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tiled_smem<R>(1)));
@@ -1087,8 +1089,16 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
         ta.ss = (R*)h->fld[F_SS]; ta.qt = (R*)h->fld[F_QU];
         ta.rk_a = rk_a; ta.rk_b = rk_b; ta.rk_c = rk_c; ta.ph = h->ph;
         prof_begin(h, K_RHS_T);
-        { int lrc = hc_launch<TempArgs<R>, k_rhs_temperature<R, CDS>, k_rhs_temperature_body<R, CDS>, 256, 1>(
-              h, pt_grid(h->g), pt_block(), 0, ta); if (lrc) return lrc; }
+        ta.kchunk = h->rhs_kc;
+        ta.zm = sizeof(R) == sizeof(float) ? (const void*)h->zm5 : (const void*)h->zm5d;
+        int lrc;
+        if (h->rhs_strip && h->rhs_kc > 0 && p.isdamp == 0)    // fluxes on strips (64 x 16 tiles)
+            lrc = hc_launch<TempArgs<R>, k_rhs_t_strip<R, CDS>, k_rhs_t_strip_body<R, CDS>, RsCfg<R>::NT, RsCfg<R>::MINB>(
+                h, h->rhs_grid, dim3(RsCfg<R>::NT), rhs_t_strip_smem<R>(), ta);
+        else
+            lrc = hc_launch<TempArgs<R>, k_rhs_temperature<R, CDS>, k_rhs_temperature_body<R, CDS>, 256, 1>(
+                h, pt_grid(h->g), pt_block(), 0, ta);
+        if (lrc) return lrc;
         CKL();
         const R* tin[1] = {(const R*)h->fld[F_QU]};
         rc = fft_forward<R>(h, tin, S, 1);

@@ -297,6 +297,8 @@ template <typename R> struct TempArgs {
     R* ss; R* qt;
     double rk_a, rk_b, rk_c;
     Phys ph;
+    int kchunk;          // the strip kernel: levels a block
+    const void* zm;      // the strip kernel: per-level metrics [5][nz] in the storage type
 };
 
 // get_temperature_cnvdiff (src/module_cnvdiff.f90:381-473); u, v, w are the

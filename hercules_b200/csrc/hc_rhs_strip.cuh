@@ -546,3 +546,197 @@ __device__ __forceinline__ void k_rhs_momentum_strip_body(const RhsTArgs<R>& a, 
 }
 template <typename R, int CDS>
 __global__ void __launch_bounds__(RsCfg<R>::NT, RsCfg<R>::MINB) k_rhs_momentum_strip(RhsTArgs<R> a) { k_rhs_momentum_strip_body<R, CDS>(a, blockIdx, gridDim); }
+
+// ---------------------------------------------------------------------------
+// Temperature right-hand side on strips (get_temperature_cnvdiff,
+// src/module_cnvdiff.f90:381-473): the fluxes thx*u (x strip) and thy*v (y
+// strip) are formed once per face from the staged planes of T, u and v of the
+// level (a two-slot cp.async ring: level k+1 arrives while k is computed), and
+// thz*w of the level below is carried in registers. T ghosts by formula: 2 tbot -
+// T(0) below, 2 ttop - T(nz-1) above (update_boundary_t, src/module_boundary.f90:
+// 176-183), thz = tbot / ttop at the walls where w = 0. Same tiles, threads and
+// grid as the momentum strip kernel; no damping.
+// ---------------------------------------------------------------------------
+#define RT_F_THX 0                                   // [16][68] thx on the x strip
+#define RT_F_FX (RT_F_THX + RS_TY * RS_AW)           // [16][68] thx*u on the x strip
+#define RT_F_FY (RT_F_FX + RS_TY * RS_AW)            // [20][64] thy*v on the y strip
+#define RT_NF (RT_F_FY + RS_BH * RS_TX)
+
+template <typename R> __host__ inline size_t rhs_t_strip_smem() { return sizeof(R) * ((size_t)6 * RS_P + RT_NF); }
+
+template <typename R, int CDS>
+__device__ __forceinline__ void k_rhs_t_strip_body(const TempArgs<R>& m, const uint3 blockIdx, const dim3 gridDim)
+{
+    typedef typename V2<R>::T R2;
+    constexpr int RQ = RsCfg<R>::RQ, NT = RsCfg<R>::NT, NW = RsCfg<R>::NW;
+    constexpr int EPC = RsCfg<R>::EPC, NCH = RsCfg<R>::NCH, NPOS = RsCfg<R>::NPOS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* SR = reinterpret_cast<R*>(smem_raw);              // [3 fields: T, u, v][2 slots][RS_P]
+    R* FL = SR + 6 * RS_P;
+    R* F_THX = FL + RT_F_THX;
+    R* F_FX = FL + RT_F_FX;
+    R* F_FY = FL + RT_F_FY;
+    const Acc<R>& A = m.a;
+    const Geo& g = A.g;
+    const int nz = g.nz, nx = g.nx, ny = g.ny;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int tiles_x = (nx + RS_TX - 1) / RS_TX;
+    const long long ntiles = (long long)tiles_x * ((ny + RS_TY - 1) / RS_TY);
+    const int kch = m.kchunk;
+    const long long t = blockIdx.x % ntiles, c = blockIdx.x / ntiles;
+    const int kb = (int)(c * kch), ke = min(nz, (int)((c + 1) * kch));
+    const int x0 = (int)(t % tiles_x) * RS_TX, y0 = (int)(t / tiles_x) * RS_TY;
+    const R* zrdz = (const R*)m.zm;
+    const R* zrdzt = (const R*)m.zm + nz;
+    const R* zrdzb = (const R*)m.zm + 2 * nz;
+    const R* zlt = (const R*)m.zm + 3 * nz;
+    auto plane = [&](int f, int lvl) { return SR + (f * 2 + (lvl & 1)) * RS_P; };
+
+    const bool has1 = threadIdx.x + NT < NPOS;
+    const int row0 = threadIdx.x / NCH, c40 = threadIdx.x - row0 * NCH;
+    const int row1 = (threadIdx.x + NT) / NCH, c41 = threadIdx.x + NT - row1 * NCH;
+    const int dst0 = row0 * RS_W + EPC * c40, dst1 = row1 * RS_W + EPC * c41;
+    const int src0 = (((y0 - RS_HY + row0) % ny + ny) % ny) * nx + ((x0 - RS_HX + EPC * c40) % nx + nx) % nx;
+    const int src1 = has1 ? (((y0 - RS_HY + row1) % ny + ny) % ny) * nx + ((x0 - RS_HX + EPC * c41) % nx + nx) % nx : 0;
+    auto stage = [&](int lvl) {
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            const R* src = f == 0 ? A.f.t : (f == 1 ? A.f.u : A.f.v);
+            const R* base = src + (long long)lvl * g.nxy;
+            R* d = plane(f, lvl);
+            rs_cp16(d + dst0, base + src0);
+            if (has1) rs_cp16(d + dst1, base + src1);
+        }
+    };
+    stage(kb);
+    rs_commit();
+    rs_wait_all();
+    __syncthreads();
+
+    const R rdx = R(1) / (R)g.dx, rdy = R(1) / (R)g.dy;
+    const R sx1 = CDS == 1 ? rdx : R(1) / (R(24) * (R)g.dx), sy1 = CDS == 1 ? rdy : R(1) / (R(24) * (R)g.dy);
+    const R sx2 = CDS == 1 ? R(1) / (R)g.dx2 : R(1) / (R(12) * (R)g.dx2);
+    const R sy2 = CDS == 1 ? R(1) / (R)g.dy2 : R(1) / (R(12) * (R)g.dy2);
+    const R dt = (R)m.ph.dt, al = (R)m.ph.alpha, um = A.um;
+    const R rka = (R)m.rk_a, rkb = (R)m.rk_b, cdif = (R)m.rk_c * R(0.5) * dt * al;
+    const R tbot = A.tbot, ttop = A.ttop;
+    const int xl = 2 * lane, rl0 = RQ * wid;
+    const int xi = x0 + xl;
+    bool act[2];
+    int gid[2], rc[2];
+#pragma unroll
+    for (int q = 0; q < RQ; ++q) {
+        act[q] = xi < nx && (y0 + rl0 + q) < ny;
+        gid[q] = (y0 + rl0 + q) * nx + xi;
+        rc[q] = (rl0 + q + RS_HY) * RS_W + xl + RS_HX;
+    }
+    auto ld_own = [&](const R* base, int q, long long ofs) {
+        return act[q] ? *reinterpret_cast<const R2*>(base + ofs + gid[q]) : mk2<R>(R(0), R(0));
+    };
+    // level k-1 at the own points: T and thz*w (0 below the bottom wall, where w = 0)
+    R tm1[2][2], fzp[2][2];
+#pragma unroll
+    for (int q = 0; q < RQ; ++q) {
+        if (kb == 0) {
+            const R2 tc = ld2r(plane(0, 0), rc[q]);
+            tm1[q][0] = R(2) * tbot - tc.x; tm1[q][1] = R(2) * tbot - tc.y;
+            fzp[q][0] = fzp[q][1] = R(0);
+        } else {
+            const long long o = (long long)(kb - 1) * g.nxy;
+            const R2 ta = ld_own(A.f.t, q, o), tb = ld2r(plane(0, kb), rc[q]), wa = ld_own(A.f.w, q, o);
+            const R l = zlt[kb - 1];
+            tm1[q][0] = ta.x; tm1[q][1] = ta.y;
+            fzp[q][0] = (tb.x * l + ta.x * (R(1) - l)) * wa.x;
+            fzp[q][1] = (tb.y * l + ta.y * (R(1) - l)) * wa.y;
+        }
+    }
+
+    for (int k = kb; k < ke; ++k) {
+        if (k + 1 < ke) { stage(k + 1); rs_commit(); }
+        const R* T0 = plane(0, k); const R* U0 = plane(1, k); const R* V0 = plane(2, k);
+        const long long kofs = (long long)k * g.nxy;
+        // own-point inputs: w(k), T(k+1), the history
+        R2 wk[2], tp[2], s0[2];
+#pragma unroll
+        for (int q = 0; q < RQ; ++q) {
+            wk[q] = ld_own(A.f.w, q, kofs);
+            tp[q] = k + 1 < nz ? ld_own(A.f.t, q, kofs + g.nxy) : mk2<R>(R(0), R(0));
+            s0[q] = ld_own(m.ss, q, kofs);
+        }
+        // ---- fluxes on their strips: 17 x-strip jobs (rows 0..15, then the side
+        // pieces), 19 y-strip jobs (rows -2..16)
+        for (int job = wid; job < 36; job += NW) {
+            if (job <= 16) {
+                int fx, fy;
+                if (job < 16) { fx = 2 * lane; fy = job; }
+                else { fy = lane & 15; fx = (lane >> 4) ? RS_TX : -2; }
+                const int r = (fy + RS_HY) * RS_W + fx + RS_HX;
+                R tx[6];
+                ld6r(T0, r, tx);
+                const R2 uc = ld2r(U0, r);
+                const R h0 = rs_mid<R, CDS>(tx[4], tx[3], tx[2], tx[1]);
+                const R h1 = rs_mid<R, CDS>(tx[5], tx[4], tx[3], tx[2]);
+                const int ea = fy * RS_AW + fx + 2;
+                st2r(F_THX, ea, h0, h1);
+                st2r(F_FX, ea, h0 * uc.x, h1 * uc.y);
+            } else {
+                const int fx = 2 * lane, fy = job - 17 - 2;
+                const int r = (fy + RS_HY) * RS_W + fx + RS_HX;
+                const R2 tc = ld2r(T0, r), tym = ld2r(T0, r - RS_W), ty1 = ld2r(T0, r + RS_W), ty2 = ld2r(T0, r + 2 * RS_W);
+                const R2 vc = ld2r(V0, r);
+                st2r(F_FY, (fy + 2) * RS_TX + fx, rs_mid<R, CDS>(ty2.x, ty1.x, tc.x, tym.x) * vc.x,
+                     rs_mid<R, CDS>(ty2.y, ty1.y, tc.y, tym.y) * vc.y);
+            }
+        }
+        __syncthreads();
+        const R rdz = zrdz[k], rdzt = zrdzt[k], rdzb = zrdzb[k], lt = zlt[k];
+        const int fa0 = rl0 * RS_AW + xl + 2, fv0 = (rl0 + 2) * RS_TX + xl;
+#pragma unroll
+        for (int q = 0; q < RQ; ++q) {
+            const int r = rc[q];
+            R tx[6], fx6[6], hx6[6];
+            ld6r(T0, r, tx);
+            ld6r(F_FX, fa0 + q * RS_AW, fx6);
+            if (um != R(0)) ld6r(F_THX, fa0 + q * RS_AW, hx6);
+            const R2 ty2 = ld2r(T0, r + 2 * RS_W), ty1 = ld2r(T0, r + RS_W), tym = ld2r(T0, r - RS_W),
+                     tym2 = ld2r(T0, r - 2 * RS_W);
+            const int fv = fv0 + q * RS_TX;
+            const R2 y1 = ld2r(F_FY, fv + RS_TX), y0v = ld2r(F_FY, fv), ym = ld2r(F_FY, fv - RS_TX),
+                     ym2 = ld2r(F_FY, fv - 2 * RS_TX);
+            R out_s[2], out_q[2];
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const int c = 2 + s;
+                const R tc = tx[c];
+                const R tux = rs_d1<R, CDS>(fx6[c + 1], fx6[c], fx6[c - 1], fx6[c - 2]) * sx1;
+                const R tvy = rs_d1<R, CDS>(s ? y1.y : y1.x, s ? y0v.y : y0v.x, s ? ym.y : ym.x, s ? ym2.y : ym2.x) * sy1;
+                const R txx = rs_d2<R, CDS>(tx[c + 2], tx[c + 1], tc, tx[c - 1], tx[c - 2]) * sx2;
+                const R tyy = rs_d2<R, CDS>(s ? ty2.y : ty2.x, s ? ty1.y : ty1.x, tc, s ? tym.y : tym.x,
+                                            s ? tym2.y : tym2.x) * sy2;
+                // thz*w at the top face of the level; 0 on the top wall (w = 0 there)
+                const R tpv = k + 1 < nz ? (s ? tp[q].y : tp[q].x) : R(2) * ttop - tc;
+                const R fz = k < nz - 1 ? (tpv * lt + tc * (R(1) - lt)) * (s ? wk[q].y : wk[q].x) : R(0);
+                const R twz = (fz - fzp[q][s]) * rdz;
+                fzp[q][s] = fz;
+                const R tzz = ((tpv - tc) * rdzt - (tc - tm1[q][s]) * rdzb) * rdz;
+                tm1[q][s] = tc;
+                R sv = -tux - tvy - twz;
+                if (um != R(0)) sv -= um * (rs_d1<R, CDS>(hx6[c + 1], hx6[c], hx6[c - 1], hx6[c - 2]) * sx1);
+                out_s[s] = sv;
+                out_q[s] = tc + dt * (rka * sv + rkb * (s ? s0[q].y : s0[q].x)) + cdif * (txx + tyy + tzz);
+            }
+            if (act[q]) {
+                const long long id = kofs + gid[q];
+                *reinterpret_cast<R2*>(m.ss + id) = mk2<R>(out_s[0], out_s[1]);
+                *reinterpret_cast<R2*>(m.qt + id) = mk2<R>(out_q[0], out_q[1]);
+            }
+        }
+        rs_wait_all();
+        __syncthreads();
+    }
+}
+template <typename R, int CDS>
+__global__ void __launch_bounds__(RsCfg<R>::NT, RsCfg<R>::MINB) k_rhs_t_strip(TempArgs<R> m)
+{
+    k_rhs_t_strip_body<R, CDS>(m, blockIdx, gridDim);
+}
