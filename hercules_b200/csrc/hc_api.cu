@@ -1035,10 +1035,9 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
     m.bfx = h->has_bf ? (const R*)h->bf[0] : nullptr;
     m.bfy = (const R*)h->bf[1]; m.bfz = (const R*)h->bf[2];
     prof_begin(h, K_RHS_MOM);
-    if (h->rhs_strip)                    // products on strips (64 x 16 tiles)
     {
         int lrc;
-        if (h->rhs_strip)
+        if (h->rhs_strip)                // products on strips (64 x 16 tiles)
             lrc = hc_launch<RhsTArgs<R>, k_rhs_momentum_strip<R, CDS>, k_rhs_momentum_strip_body<R, CDS>, RsCfg<R>::NT,
                             RsCfg<R>::MINB>(h, h->rhs_grid, dim3(RsCfg<R>::NT), rhs_strip_smem<R>(), m);
         else if constexpr (sizeof(R) == sizeof(float))      // FP32: two x points a thread (64 x 8 tiles)
