@@ -27,9 +27,15 @@ template <typename A> struct GroupCap {
 
 // The table of a grouped launch, passed as the kernel's parameter block: the
 // members' arguments are read from the constant bank, as in their own kernels.
-// Two capacities: up to 8 members (a few KB of parameters a launch) and up to
-// GroupCap<A> members.
+// Every launch, a channel's own included, uses the capacity GroupSmall (8
+// members, a few KB of parameters), so that a channel runs the same kernel alone
+// and in an ensemble; larger groups are split into launches of 8 members.
 #define HC_GROUP_SMALL 8
+template <typename A> struct GroupSmall {
+    static constexpr int v = HC_GROUP_SMALL < GroupCap<A>::v ? HC_GROUP_SMALL : GroupCap<A>::v;
+};
+// the largest dynamic shared memory any launch of a kernel may ask for
+template <typename A> struct GroupSmem { static constexpr int max = 227 * 1024; };
 template <typename A, int CAP> struct GroupTab {
     int n;                 // members
     int start[CAP + 1];    // prefix sums of the members' block counts
@@ -111,9 +117,10 @@ static int group_build_cap(const GroupRec* const* recs, int n, GroupLaunch* out)
     }
     if (tot > 0x7fffffffLL) return -1;
     t->start[n] = (int)tot;
+    // the same limit a channel's own launches set (a lower one would refuse them)
     if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k_group<A, BODY, NT, MINB, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
+        cudaFuncSetAttribute(k_group<A, BODY, NT, MINB, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GroupSmem<A>::max) != cudaSuccess)
         return -1;
     out->run = &group_run<A, BODY, NT, MINB, CAP>;
     out->nblk = (unsigned)tot;
@@ -125,7 +132,5 @@ static int group_build_cap(const GroupRec* const* recs, int n, GroupLaunch* out)
 template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
 static int group_build(const GroupRec* const* recs, int n, GroupLaunch* out)
 {
-    constexpr int big = GroupCap<A>::v, small = HC_GROUP_SMALL < big ? HC_GROUP_SMALL : big;
-    if (n <= small) return group_build_cap<A, BODY, NT, MINB, small>(recs, n, out);
-    return group_build_cap<A, BODY, NT, MINB, big>(recs, n, out);
+    return group_build_cap<A, BODY, NT, MINB, GroupSmall<A>::v>(recs, n, out);
 }
