@@ -355,8 +355,7 @@ static int hc_launch(hc_handle* h, dim3 grid, dim3 block, size_t smem, const A& 
         // the grouped kernel's shared-memory limit, raised once per device
         static unsigned long long raised = 0;
         if (h->dev < 64 && !(raised >> h->dev & 1ull)) {
-            CK(cudaFuncSetAttribute(k_group<A, BODY, NT, MINB, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    GroupSmem<A>::max));
+            CK(group_raise_smem((const void*)k_group<A, BODY, NT, MINB, CAP>));
             raised |= 1ull << h->dev;
         }
     }

@@ -34,8 +34,19 @@ template <typename A> struct GroupCap {
 template <typename A> struct GroupSmall {
     static constexpr int v = HC_GROUP_SMALL < GroupCap<A>::v ? HC_GROUP_SMALL : GroupCap<A>::v;
 };
-// the largest dynamic shared memory any launch of a kernel may ask for
-template <typename A> struct GroupSmem { static constexpr int max = 227 * 1024; };
+// Raise a kernel's dynamic shared-memory limit to what the device allows next to
+// the kernel's own static shared memory (the same limit from every call site).
+static inline cudaError_t group_raise_smem(const void* kernel)
+{
+    int dev = 0, optin = 0;
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    return e;
+}
 template <typename A, int CAP> struct GroupTab {
     int n;                 // members
     int start[CAP + 1];    // prefix sums of the members' block counts
@@ -118,9 +129,7 @@ static int group_build_cap(const GroupRec* const* recs, int n, GroupLaunch* out)
     if (tot > 0x7fffffffLL) return -1;
     t->start[n] = (int)tot;
     // the same limit a channel's own launches set (a lower one would refuse them)
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k_group<A, BODY, NT, MINB, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             GroupSmem<A>::max) != cudaSuccess)
+    if (smem > 48 * 1024 && group_raise_smem((const void*)k_group<A, BODY, NT, MINB, CAP>) != cudaSuccess)
         return -1;
     out->run = &group_run<A, BODY, NT, MINB, CAP>;
     out->nblk = (unsigned)tot;
