@@ -331,43 +331,26 @@ static int prof_collect(hc_handle* h)
     return HC_OK;
 }
 
-// Launch the body BODY (KFN is its single-channel kernel; NT threads, MINB
-// resident blocks) on the handle's stream as a one-member k_group launch, or,
-// while the handle records, keep the launch for a grouped ensemble launch. A
-// channel's own steps and its steps inside an ensemble thus run the same kernel
-// (the same compiled code, hence the same rounding): only the member table
-// differs.
+// Launch KFN (whose body is BODY, launched with at most NT threads and MINB
+// resident blocks) on the handle's stream, or, while the handle records, keep the
+// launch for a grouped ensemble launch of the same body. (Running a channel's own
+// launches through k_group too would make them the same compiled code as in an
+// ensemble, but reading the arguments through the member table cost 5-6 % of the
+// 512 x 384 x 256 step, so a channel alone runs its named kernels.)
 template <typename A, void (*KFN)(A), void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
 static int hc_launch(hc_handle* h, dim3 grid, dim3 block, size_t smem, const A& args)
 {
-    constexpr int CAP = GroupSmall<A>::v;
     if (h->rec) {
         GroupRec r;
-        r.key = (const void*)&k_group<A, BODY, NT, MINB, CAP>;
-        r.cap = CAP;
+        r.key = (const void*)&k_group<A, BODY, NT, MINB, GroupCap<A>::v>;
+        r.cap = GroupCap<A>::v;
         r.build = &group_build<A, BODY, NT, MINB>;
         r.args.assign(reinterpret_cast<const unsigned char*>(&args), reinterpret_cast<const unsigned char*>(&args) + sizeof(A));
         r.grid = grid; r.block = block; r.smem = smem;
         h->rec->push_back(std::move(r));
         return HC_OK;
     }
-    if (smem > 48 * 1024) {
-        // the grouped kernel's shared-memory limit, raised once per device
-        static unsigned long long raised = 0;
-        if (h->dev < 64 && !(raised >> h->dev & 1ull)) {
-            CK(group_raise_smem((const void*)k_group<A, BODY, NT, MINB, CAP>));
-            raised |= 1ull << h->dev;
-        }
-    }
-    GroupTab<A, CAP> t;
-    memset(&t, 0, sizeof(t));
-    t.n = 1;
-    t.start[0] = 0;
-    t.start[1] = (int)(grid.x * grid.y * grid.z);
-    t.grid[0] = grid;
-    t.args[0] = args;
-    k_group<A, BODY, NT, MINB, CAP><<<grid.x * grid.y * grid.z, block, smem, h->st>>>(t);
-    (void)KFN;
+    KFN<<<grid, block, smem, h->st>>>(args);
     return HC_OK;
 }
 

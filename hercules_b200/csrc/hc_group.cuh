@@ -8,11 +8,13 @@
 // finds its member (binary search over the prefix sums of the members' block
 // counts), its block index in that member's grid, and the member's arguments in
 // the launch's parameter block. Every member's block then does exactly what it
-// does in the member's own launch: the table is a __grid_constant__ parameter, so
-// the body reads its arguments from the constant bank exactly as in its own
-// kernel (read from global memory they could alias the kernel's stores, and the
-// compiler then contracted FP32 products differently), and the results are the
-// same bit for bit.
+// does in the member's own launch. The table is a __grid_constant__ parameter, so
+// the body reads its arguments from the constant bank as in its own kernel (read
+// from global memory they may alias the kernel's stores, which changed how the
+// compiler contracted FP32 products). The grouped kernel is still a separate
+// compilation of the body: FP64 results have matched the member's own launches
+// bit for bit, FP32 ones agree to a few units in the last place where the
+// compiler fused a multiply and an add differently.
 #pragma once
 #include <cuda_runtime.h>
 #include <string.h>
@@ -27,9 +29,8 @@ template <typename A> struct GroupCap {
 
 // The table of a grouped launch, passed as the kernel's parameter block: the
 // members' arguments are read from the constant bank, as in their own kernels.
-// Every launch, a channel's own included, uses the capacity GroupSmall (8
-// members, a few KB of parameters), so that a channel runs the same kernel alone
-// and in an ensemble; larger groups are split into launches of 8 members.
+// Two capacities: up to 8 members (a few KB of parameters a launch) and up to
+// GroupCap<A> members.
 #define HC_GROUP_SMALL 8
 template <typename A> struct GroupSmall {
     static constexpr int v = HC_GROUP_SMALL < GroupCap<A>::v ? HC_GROUP_SMALL : GroupCap<A>::v;
@@ -141,5 +142,6 @@ static int group_build_cap(const GroupRec* const* recs, int n, GroupLaunch* out)
 template <typename A, void (*BODY)(const A&, const uint3, const dim3), int NT, int MINB>
 static int group_build(const GroupRec* const* recs, int n, GroupLaunch* out)
 {
-    return group_build_cap<A, BODY, NT, MINB, GroupSmall<A>::v>(recs, n, out);
+    if (n <= GroupSmall<A>::v) return group_build_cap<A, BODY, NT, MINB, GroupSmall<A>::v>(recs, n, out);
+    return group_build_cap<A, BODY, NT, MINB, GroupCap<A>::v>(recs, n, out);
 }
