@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--graph", action="store_true", help="replay each step from a captured CUDA graph")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing leg")
     ap.add_argument("--no-tune", action="store_true", help="ensemble: default tile shapes, no autotuner")
+    ap.add_argument("--stats-gate", choices=["config3", "config2"], default=None,
+                    help="run the mixed-vs-FP64 statistics gate (long runs) and print its lines")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="run only the adjoint/forward timing leg (Ekman 64x64x65) and print it")
     return ap.parse_args()
@@ -441,6 +443,78 @@ def run_ensemble(args):
     return out
 
 
+def run_stats_gate(which: str):
+    """The statistical gate of the mixed mode: the FP32-mixed and FP64 runs of the
+    same seeded start, their running means turned into mean profiles, Reynolds
+    stresses, wall friction and (with temperature) heat flux, compared as
+    max |mixed - fp64| / max |fp64| per profile (gate: 1 %).
+
+    config3: the 512x384x256 neutral closed channel (FD4, dp_opt=2), statistics of
+    all 2000 steps; also with temperature (Ri_b = 0.1, Dirichlet walls) for the
+    heat flux. config2: the 256x256x128 stratified open channel (pseudo-spectral),
+    1000 steps at each Ri_b in {0, 0.1, 0.5, 1.0}, statistics of the last 500."""
+    import numpy as np
+    import torch
+    from hercules_b200 import engine, inputs, stats
+    from hercules_b200.params import PREC_FP64, PREC_MIXED, config_channel_fd, config_open_channel_spectral
+    torch.cuda.set_device(0)
+    cases = []
+    if which == "config3":
+        for scal in (0, 1):
+            cases.append((f"fd4_512x384x256{'_Ri0.1' if scal else ''}", 2000, 0,
+                          lambda prec, scal=scal: config_channel_fd(512, 384, 256, precision=prec).replace(
+                              **({"isscalar": 1, "got": 0.1, "tbot": 0.0, "ttop": 1.0} if scal else {}))))
+    else:
+        for ri in (0.0, 0.1, 0.5, 1.0):
+            cases.append((f"spectral_256x256x128_Ri{ri}", 1000, 500,
+                          lambda prec, ri=ri: config_open_channel_spectral(256, 256, 128, got=ri, precision=prec)))
+    out = []
+    for name, nsteps, skip, mk in cases:
+        prof, fric, flux, ms = {}, {}, {}, {}
+        for prec in (PREC_FP64, PREC_MIXED):
+            p = mk(prec)
+            fields = inputs.loglaw_stratified(p, seed=10) if p.cds == 3 else inputs.poiseuille_noise(p, seed=3)
+            if p.isscalar and p.cds != 3:
+                zc = __import__("hercules_b200.params", fromlist=["mesh"]).mesh(p)["zc"]
+                fields["t"] = np.broadcast_to((p.tbot + (p.ttop - p.tbot) * zc / p.lz)[:, None, None],
+                                              (p.nz, p.ny, p.nx)).copy()
+            c = engine.Channel(p)
+            c.load(fields)
+            c.initialize()
+            base = None
+            t_ms = 0.0
+            if skip:
+                rc = c.step_nodiag(skip)
+                assert rc == 0, rc
+                t_ms += c.last_ms
+                base = {m: c.download(m) for m in stats.MEAN_FILES}
+            rc = c.step_nodiag(nsteps - skip)
+            assert rc == 0, rc
+            t_ms += c.last_ms
+            means = {}
+            for m in stats.MEAN_FILES:
+                a = c.download(m)
+                means[m] = (a - base[m] if base else a) / float(nsteps - skip)
+            c.close()
+            pr = stats.profiles(means, p)
+            prof[prec] = pr
+            fric[prec] = stats.wall_friction(pr, p)
+            flux[prec] = stats.heat_flux(pr, p) if p.isscalar else None
+            ms[prec] = t_ms / nsteps
+        keys = ("U", "uu", "vv", "ww", "uw") + (("T", "tt", "tw") if flux[PREC_FP64] is not None else ())
+        d = stats.relative_difference(prof[PREC_MIXED], prof[PREC_FP64], keys=keys)
+        d["tau_w"] = abs(fric[PREC_MIXED]["tau_w"] - fric[PREC_FP64]["tau_w"]) / abs(fric[PREC_FP64]["tau_w"])
+        if flux[PREC_FP64] is not None:
+            qb = flux[PREC_FP64]["wall_bottom"]
+            d["q_wall_bottom"] = abs(flux[PREC_MIXED]["wall_bottom"] - qb) / max(abs(qb), 1e-300)
+        out.append({"case": name, "steps": nsteps, "statistics_over": nsteps - skip,
+                    "rel_diff_mixed_vs_fp64": d, "max_rel_diff": max(d.values()),
+                    "gate_1pct": max(d.values()) <= 0.01, "ms_per_step": {"fp64": ms[PREC_FP64], "mixed": ms[PREC_MIXED]},
+                    "u_tau": {"fp64": fric[PREC_FP64]["u_tau"], "mixed": fric[PREC_MIXED]["u_tau"]}})
+        print(json.dumps(out[-1]), flush=True)
+    return out
+
+
 def cpu_oracle_rate(grid, steps, warm=1):
     """Time the CPU restatement of the reference step (OpenMP, all host cores)."""
     from oracle import oracle as O
@@ -499,6 +573,11 @@ def main():
                                                 "here: no gfortran/MPI)"},
                      "e2e": {"value": rate, "unit": "gridpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         print(json.dumps(line), flush=True)
+        return
+
+    if args.stats_gate:
+        if rank == 0:
+            run_stats_gate(args.stats_gate)
         return
 
     if args.adjoint_only:
