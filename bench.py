@@ -451,12 +451,13 @@ def run_stats_gate(which: str):
 
     config3: the 512x384x256 neutral closed channel (FD4, dp_opt=2), statistics of
     all 2000 steps; also with temperature (Ri_b = 0.1, Dirichlet walls) for the
-    heat flux. config2: the 256x256x128 stratified open channel (pseudo-spectral),
-    1000 steps at each Ri_b in {0, 0.1, 0.5, 1.0}, statistics of the last 500."""
+    heat flux. config2: the 256x256x128 stratified open channel (pseudo-spectral,
+    fixed bottom-cooling flux), 1000 steps at each Ri_b in {0, 0.1, 0.5, 1.0},
+    statistics of the last 500."""
     import numpy as np
     import torch
     from hercules_b200 import engine, inputs, stats
-    from hercules_b200.params import PREC_FP64, PREC_MIXED, config_channel_fd, config_open_channel_spectral
+    from hercules_b200.params import PREC_FP64, PREC_MIXED, config_channel_fd, config_open_channel_spectral, t_line
     torch.cuda.set_device(0)
     cases = []
     if which == "config3":
@@ -476,8 +477,7 @@ def run_stats_gate(which: str):
             fields = inputs.loglaw_stratified(p, seed=10) if p.cds == 3 else inputs.poiseuille_noise(p, seed=3)
             if p.isscalar and p.cds != 3:
                 zc = __import__("hercules_b200.params", fromlist=["mesh"]).mesh(p)["zc"]
-                fields["t"] = np.broadcast_to((p.tbot + (p.ttop - p.tbot) * zc / p.lz)[:, None, None],
-                                              (p.nz, p.ny, p.nx)).copy()
+                fields["t"] = np.broadcast_to(t_line(p, zc)[:, None, None], (p.nz, p.ny, p.nx)).copy()
             c = engine.Channel(p)
             c.load(fields)
             c.initialize()
@@ -505,8 +505,14 @@ def run_stats_gate(which: str):
         d = stats.relative_difference(prof[PREC_MIXED], prof[PREC_FP64], keys=keys)
         d["tau_w"] = abs(fric[PREC_MIXED]["tau_w"] - fric[PREC_FP64]["tau_w"]) / abs(fric[PREC_FP64]["tau_w"])
         if flux[PREC_FP64] is not None:
-            qb = flux[PREC_FP64]["wall_bottom"]
-            d["q_wall_bottom"] = abs(flux[PREC_MIXED]["wall_bottom"] - qb) / max(abs(qb), 1e-300)
+            # the wall flux, or under a fixed bottom flux the wall temperature it sets
+            # (relative to the temperature range across the channel)
+            if p.tbc_bot:
+                tb = flux[PREC_FP64]["t_wall_bottom"]
+                d["t_wall_bottom"] = abs(flux[PREC_MIXED]["t_wall_bottom"] - tb) / max(abs(p.ttop - tb), 1e-300)
+            else:
+                qb = flux[PREC_FP64]["wall_bottom"]
+                d["q_wall_bottom"] = abs(flux[PREC_MIXED]["wall_bottom"] - qb) / max(abs(qb), 1e-300)
         out.append({"case": name, "steps": nsteps, "statistics_over": nsteps - skip,
                     "rel_diff_mixed_vs_fp64": d, "max_rel_diff": max(d.values()),
                     "gate_1pct": max(d.values()) <= 0.01, "ms_per_step": {"fp64": ms[PREC_FP64], "mixed": ms[PREC_MIXED]},
@@ -546,7 +552,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded Poiseuille + 10% uniform noise)"}
     if is_spectral(args.workload):
         physics = ("stably stratified open channel, pseudo-spectral horizontal (2/3 rule, skew form), FD2 vertical, "
-                   "RK3, dp_opt=1, nu=1/180, Pr=0.71, Ri_b=0.1, Dirichlet T, dt=1e-3")
+                   "RK3, dp_opt=1, nu=1/180, Pr=0.71, Ri_b=0.1, fixed bottom-cooling flux dT/dz=1, T=0 at the top, dt=1e-3")
         base["data"] = "synthetic (seeded log-law + 5% Gaussian noise, linear T + 1% noise)"
     else:
         physics = "neutral closed channel, FD4 horizontal, FD2 vertical, RK3, dp_opt=2, nu=1/2800, dt=1e-3, zstretch=1"

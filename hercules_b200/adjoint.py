@@ -35,6 +35,20 @@ def wall_shear_seed(p: Params) -> np.ndarray:
     return s
 
 
+def wall_heat_flux(t, p: Params):
+    """alpha dT/dz at the bottom wall, averaged over the wall, with the Dirichlet
+    ghost T(0) = 2 tbot - T(1) (src/module_boundary.f90:180): alpha (T(1) - tbot) / (dz(1)/2)."""
+    dz1 = mesh(p)["dz"][2]
+    return p.alpha * ((t[0] - p.tbot).mean()) / (0.5 * dz1)
+
+
+def wall_heat_flux_seed(p: Params) -> np.ndarray:
+    """d(wall_heat_flux)/dT as a field: alpha / (dz(1)/2) / (nx ny) on the first level."""
+    s = np.zeros((p.nz, p.ny, p.nx))
+    s[0] = p.alpha / (0.5 * mesh(p)["dz"][2]) / (p.nx * p.ny)
+    return s
+
+
 def kinetic_energy(u, v, w):
     """Mean of (u^2 + v^2 + w^2) / 2 over the stored points."""
     return 0.5 * ((u ** 2).mean() + (v ** 2).mean() + (w ** 2).mean())

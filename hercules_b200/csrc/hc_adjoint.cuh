@@ -1,6 +1,7 @@
 // hc_adjoint.cuh -- discrete adjoint of the FD sub-step (no counterpart in the
 // reference). Scope: FP64, cds = 1 or 2, constant forcing (dp_opt = 1 or 3),
-// no temperature, no damping; RK3 or AB2; body force.
+// temperature with a constant Richardson number, no damping; RK3 or AB2; body
+// force.
 //
 // One forward sub-step maps (u, v, w, p, f_prev) to (u', v', w', p', f):
 //   f   = F(u, v, w) + body force                    (momentum RHS, k_rhs_momentum)
@@ -32,6 +33,8 @@ struct AdjRhsArgs {
     double* lbf[3];                // body-force gradient, accumulated
     double* ax[8];                 // adjoints of the interpolants uhx, uhy, vhx, vhy, whx, why, uhz, vhz
     double* out[4];                // lambda_u, v, w (written), lambda_p (accumulated)
+    double* out_t;                 // lambda_T (accumulated: the buoyancy of the w equation); null: none
+    double got;                    // g/T0 of the buoyancy term
     double rk_a, rk_b, rk_c;
     Phys ph;
 };
@@ -252,6 +255,13 @@ __global__ void __launch_bounds__(256) k_rhs_adj_gather(AdjRhsArgs m)
         if (wrow) lw += l0 / dzt(k) * (-0.5 * (wc + wp) + 0.5 * (wc + wm));
         if (k >= 1) lw -= lm / dzt(k - 1) * 0.5 * (wm + wc);
         if (k + 1 <= nz - 2) lw += lp1 / dzt(k + 1) * 0.5 * (wp + wc);
+        // buoyancy got ((1 - l_t(k')) T(k') + l_t(k') T(k'+1)) in the w equations k' = k, k-1
+        if (m.out_t) {
+            double bt = 0.0;
+            if (wrow) bt += (1.0 - ldz(g.z.l_t, k)) * l0;
+            if (k >= 1) bt += ldz(g.z.l_t, k - 1) * lm;
+            m.out_t[id] += m.got * bt;
+        }
     }
     // pressure gradients of the three equations
     if (CDS == 1) {
@@ -413,4 +423,165 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_column_fd_adj(ColAdjArgs a)
         a.av[id] = d[1][i];
         a.aw[id] = r <= nz - 2 ? dw[0][i] : make_double2(0, 0);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Temperature (isscalar = 1). The forward sub-step ends with
+//   ss  = -Dx(thx u') - Dy(thy v') - Dz(thz w') - um Dx(thx)     (get_temperature_cnvdiff,
+//   qt  = T + dt (rk_a ss + rk_b ss_prev) + c_t L T               src/module_cnvdiff.f90:381-473)
+//   T'  = M_T qt,   M_T = iFFT . H_T^-1 . FFT                     (the Dirichlet T Helmholtz solve)
+// where u', v', w' are the velocities this sub-step produced and T the
+// temperature it started from; the momentum right-hand side of the same
+// sub-step read T through the buoyancy term got ((1 - l_t) T(k) + l_t T(k+1)) of
+// the w equation. Its adjoint runs first in the reverse sweep:
+//   lambda_qt = M_T^T lambda_T',  lambda_ss = dt rk_a lambda_qt + lambda_ss(out),
+//   lambda_ss_prev = dt rk_b lambda_qt,
+//   lambda_T  = lambda_qt + c_t L^T lambda_qt + (dss/dT)^T lambda_ss,
+//   lambda_u' += (dss/du')^T lambda_ss (and v', w'),
+// again as two gather passes (interpolant adjoints, then raw values).
+// ---------------------------------------------------------------------------
+struct AdjTArgs {
+    Acc<double> a;                 // T at the sub-step's start; f.u, f.v, f.w = u', v', w'
+    const double* lqt;             // lambda_qt (physical)
+    const double* lss_out;         // adjoint of the new history ss
+    double* lss_prev;              // out: adjoint of the old history
+    double* ax[3];                 // adjoints of thx, thy, thz at each point
+    double* lvel[3];               // lambda_u', v', w': accumulated
+    double* out_t;                 // lambda_T: written
+    double rk_a, rk_b, rk_c;
+    Phys ph;
+};
+
+// Pass 1: the adjoints of thx, thy, thz at this point, its velocity adjoints
+// (the fluxes thx u' etc. are products at this point), and the history adjoint.
+template <int CDS>
+__global__ void __launch_bounds__(256) k_t_adj_interp(AdjTArgs m)
+{
+    const Geo& g = m.a.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const int nz = g.nz;
+    const Nbr N(g, i, j, k);
+    const long long id = N.at(0, 0), up = g.nxy;
+    const double dta = m.ph.dt * m.rk_a;
+    auto L = [&](long long q) { return dta * __ldg(m.lqt + q) + __ldg(m.lss_out + q); };
+    m.lss_prev[id] = m.ph.dt * m.rk_b * m.lqt[id];
+    // the x (y) differences at i - off read the flux of face i
+    double sx = 0.0, sy = 0.0;
+#pragma unroll
+    for (int q = 0; q < Dif<CDS>::n; ++q) {
+        const int o = Dif<CDS>::off(q);
+        sx += Dif<CDS>::c(q) / g.dx * L(N.at(-o, 0));
+        sy += Dif<CDS>::c(q) / g.dy * L(N.at(0, -o));
+    }
+    const Acc<double>& A = m.a;
+    const double thx = A.template thx<CDS>(i, j, k), thy = A.template thy<CDS>(i, j, k);
+    const double u1 = __ldg(A.f.u + id), v1 = __ldg(A.f.v + id);
+    m.ax[0][id] = -(u1 + A.um) * sx;
+    m.ax[1][id] = -v1 * sy;
+    m.lvel[0][id] += -thx * sx;
+    m.lvel[1][id] += -thy * sy;
+    // z: Dz(FZ)(k) = (FZ(k) - FZ(k-1)) / dz(k); FZ(k) = thz(k) w'(k), w'(nz-1) = 0
+    if (k <= nz - 2) {
+        const double lfz = -L(id) / ldz(g.z.dz, k) + L(id + up) / ldz(g.z.dz, k + 1);
+        const double l = ldz(g.z.l_t, k);
+        const double thz = __ldg(A.f.t + id + up) * l + __ldg(A.f.t + id) * (1.0 - l);
+        m.ax[2][id] = __ldg(A.f.w + id) * lfz;
+        m.lvel[2][id] += thz * lfz;
+    } else {
+        m.ax[2][id] = 0.0;
+    }
+}
+
+// Pass 2: lambda_T by the transposed interpolation weights, the identity, the
+// transposed diffusion (the ghosts fold back with weight tbs at the bottom: -1
+// for 2 tbot - T(0), +1 for a fixed gradient; -1 for 2 ttop - T(nz-1) at the top)
+// and thz's z weights.
+template <int CDS>
+__global__ void __launch_bounds__(256) k_t_adj_gather(AdjTArgs m)
+{
+    const Geo& g = m.a.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const int nz = g.nz;
+    const Nbr N(g, i, j, k);
+    const long long id = N.at(0, 0), up = g.nxy;
+    auto X = [&](int f, int di, int dj) { return __ldg(m.ax[f] + N.at(di, dj)); };
+    auto Q = [&](int di, int dj) { return __ldg(m.lqt + N.at(di, dj)); };
+    auto dz = [&](int kk) { return ldz(g.z.dz, kk); };
+    auto dzt = [&](int kk) { return ldz(g.z.dz_t, kk); };
+    auto dzb = [&](int kk) { return ldz(g.z.dz_b, kk); };
+    const double ct = m.rk_c * 0.5 * m.ph.dt * m.ph.alpha;
+    double lt;
+    // thx(i) = (-T(i+2) + 9 T(i+1) + 9 T(i) - T(i-1)) / 16, thy alike
+    if (CDS == 1) {
+        lt = 0.5 * (X(0, -1, 0) + X(0, 0, 0)) + 0.5 * (X(1, 0, -1) + X(1, 0, 0));
+    } else {
+        lt = (-X(0, -2, 0) + 9.0 * X(0, -1, 0) + 9.0 * X(0, 0, 0) - X(0, 1, 0)) * 0.0625 +
+             (-X(1, 0, -2) + 9.0 * X(1, 0, -1) + 9.0 * X(1, 0, 0) - X(1, 0, 1)) * 0.0625;
+    }
+    // thz(k) = l_t(k) T(k+1) + (1 - l_t(k)) T(k) on the faces k <= nz-2
+    if (k <= nz - 2) lt += (1.0 - ldz(g.z.l_t, k)) * __ldg(m.ax[2] + id);
+    if (k >= 1) lt += ldz(g.z.l_t, k - 1) * __ldg(m.ax[2] + id - up);
+    // identity and horizontal diffusion (symmetric stencils)
+    const double q0 = Q(0, 0);
+    double h;
+    if (CDS == 1) {
+        h = (Q(1, 0) - 2.0 * q0 + Q(-1, 0)) / g.dx2 + (Q(0, 1) - 2.0 * q0 + Q(0, -1)) / g.dy2;
+    } else {
+        h = (-Q(2, 0) + 16.0 * Q(1, 0) - 30.0 * q0 + 16.0 * Q(-1, 0) - Q(-2, 0)) / (12.0 * g.dx2) +
+            (-Q(0, 2) + 16.0 * Q(0, 1) - 30.0 * q0 + 16.0 * Q(0, -1) - Q(0, -2)) / (12.0 * g.dy2);
+    }
+    lt += q0 + ct * h;
+    // tzz(k) = ((T(k+1) - T(k)) / dz_t(k) - (T(k) - T(k-1)) / dz_b(k)) / dz(k), transposed
+    auto qz = [&](int kk) -> double { return (kk < 0 || kk >= nz) ? 0.0 : __ldg(m.lqt + id + (long long)(kk - k) * up); };
+    double zt = -q0 * (1.0 / dzt(k) + 1.0 / dzb(k)) / dz(k);
+    if (k >= 1) zt += qz(k - 1) / (dzt(k - 1) * dz(k - 1));
+    if (k <= nz - 2) zt += qz(k + 1) / (dzb(k + 1) * dz(k + 1));
+    if (k == 0) zt += m.a.tbs * q0 / (dzb(0) * dz(0));        // T(-1) = tbs T(0) + tba
+    if (k == nz - 1) zt -= q0 / (dzt(k) * dz(k));             // T(nz) = 2 ttop - T(nz-1)
+    lt += ct * zt;
+    m.out_t[id] = lt;
+}
+
+// H_T^-T per wavenumber column (the T Helmholtz matrix is real, so its adjoint is
+// its transpose): in place on the spectra of lambda_T', giving those of lambda_qt.
+struct ColTAdjArgs {
+    double2* at;
+    ColCoef c;
+    Geo g;
+    double rk_c;
+};
+
+template <int K>
+__global__ void __launch_bounds__(CW_WARPS * 32) k_column_t_adj(ColTAdjArgs a)
+{
+    const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const long long ncol = a.g.ncol;
+    const long long c = (long long)blockIdx.x * CW_WARPS + wp;
+    if (c >= ncol) return;
+    const int nz = a.g.nz;
+    const int l = (int)(c % a.g.nxh), m = (int)(c / a.g.nxh);
+    const double rk = a.rk_c;
+    const double lam = __ldg(a.c.hxt + l) + __ldg(a.c.hyt + m);
+    const double* dg = c == 0 ? a.c.d0t : a.c.dgt;
+    const int r0 = ln * K;
+    double2 d[1][K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) d[0][i] = r0 + i < nz ? a.at[(long long)(r0 + i) * ncol + c] : make_double2(0, 0);
+    auto cf = [&](int r, double& aa, double& bb, double& cc) {
+        if (r < nz) {
+            aa = r >= 1 ? rk * __ldg(a.c.ct + r - 1) : 0.0;
+            cc = r + 1 <= nz - 1 ? rk * __ldg(a.c.at + r + 1) : 0.0;
+            bb = 1.0 + rk * (-lam + __ldg(dg + r));
+        } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+    };
+    warp_partition_solve<K, 1>(cf, d, ln);
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+        if (r0 + i < nz) a.at[(long long)(r0 + i) * ncol + c] = d[0][i];
 }

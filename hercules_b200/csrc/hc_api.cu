@@ -491,7 +491,8 @@ static int build_tables(hc_handle* h)
         ct[k] = k == nz - 1 ? 0.0 : c0t;
         dgt[k] = -(k == 0 ? 0.0 : a0t) - (k == nz - 1 ? 0.0 : c0t);
         d0t[k] = -a0t - c0t;
-        if (k == 0) d0t[k] = d0t[k] - a0t;
+        // the bottom ghost folds with -1 (fixed T) or +1 (fixed gradient)
+        if (k == 0) d0t[k] = p.tbc_bot ? d0t[k] + a0t : d0t[k] - a0t;
         if (k == nz - 1) d0t[k] = d0t[k] - c0t;
         // p (get_p_eqn_coeff :49-118)
         double a0p = 1.0 / dz(k) / dzb(k), c0p = 1.0 / dz(k) / dzt(k);
@@ -735,13 +736,37 @@ template <typename R> static int set_smem_attrs()
 static dim3 pt_block() { return dim3(32, 8, 1); }
 static dim3 pt_grid(const Geo& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
 
+// The bottom ghost of T as T(-1) = tbs T(0) + tba: a fixed wall temperature (the
+// reference, src/module_boundary.f90:176-183) gives tbs = -1, tba = 2 tbot; the
+// fixed wall gradient dT/dz = tbot (tbc_bot = 1) gives tbs = 1, tba = -tbot dz_b(0).
+static void t_ghost_bottom(const hc_handle* h, double& tbs, double& tba)
+{
+    if (h->p.tbc_bot) { tbs = 1.0; tba = -h->p.tbot * h->zhost[2][2]; }
+    else { tbs = -1.0; tba = 2.0 * h->p.tbot; }
+}
+// The constants the wall ghosts of T add to the (0,0) mode of the T solve's
+// source (src/module_poisson_solver.f90:575-582): the ghost's constant part times
+// the coupling aa of the first level (cc of the last).
+static void t_bc_src(const hc_handle* h, double rk_c, double& b0, double& b1)
+{
+    const hc_params& p = h->p;
+    const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
+    const int ks = 2, ke = p.nz + 1;
+    const double aa_t_zstr = -0.5 * rk_c * p.dt * p.alpha / DZ[ks] / DZB[ks];
+    const double cc_t_zend = -0.5 * rk_c * p.dt * p.alpha / DZ[ke] / DZT[ke];
+    b0 = p.tbc_bot ? aa_t_zstr * p.tbot * DZB[ks] : -2.0 * aa_t_zstr * p.tbot;
+    b1 = -2.0 * cc_t_zend * p.ttop;
+}
+
 template <typename R> static Acc<R> make_acc(hc_handle* h)
 {
     Acc<R> a;
     a.f.u = (const R*)h->fld[F_U]; a.f.v = (const R*)h->fld[F_V]; a.f.w = (const R*)h->fld[F_W];
     a.f.p = (const R*)h->fld[F_P]; a.f.t = (const R*)h->fld[F_T];
     a.g = h->g;
-    a.um = (R)h->p.u_mrf; a.tbot = (R)h->p.tbot; a.ttop = (R)h->p.ttop;
+    double tbs, tba;
+    t_ghost_bottom(h, tbs, tba);
+    a.um = (R)h->p.u_mrf; a.tbs = (R)tbs; a.tba = (R)tba; a.ttop = (R)h->p.ttop;
     a.closed = h->p.ochannel == 0;
     a.su = a.sv = a.sw = a.sp = a.st = nullptr;
     a.kd = h->p.nz;
@@ -1108,14 +1133,7 @@ template <typename R, int CDS> static int substep_fd(hc_handle* h, int sub, int 
         ColTArgs<R> ct;
         ct.qt = S[0]; ct.c = h->cc; ct.s = h->cs; ct.g = h->g; ct.rk_c = rk_c; ct.halt = halt;
         ct.out = S[0]; ct.ltr = 0; ct.mtr = 0;
-        {
-            const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
-            const int ks = 2, ke = p.nz + 1;
-            double aa_t_zstr = -0.5 * rk_c * p.dt * p.alpha / DZ[ks] / DZB[ks];
-            double cc_t_zend = -0.5 * rk_c * p.dt * p.alpha / DZ[ke] / DZT[ke];
-            ct.bct0 = -2.0 * aa_t_zstr * p.tbot;
-            ct.bct1 = -2.0 * cc_t_zend * p.ttop;
-        }
+        t_bc_src(h, rk_c, ct.bct0, ct.bct1);
         prof_begin(h, K_COLUMN_T);
         rc = launch_column_t<R>(h, ct);
         if (rc) return rc;
@@ -1265,7 +1283,8 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         for (int f = 0; f < 8; ++f) pa.out[f] = Q[SP_W0 + f];
         for (int f = 0; f < 3; ++f) pa.bf[f] = h->has_bf ? (const R*)h->bf[f] : nullptr;
         pa.g = g; pa.sc = h->sc; pa.rdz = h->cc.rdz; pa.rdzt = h->cc.rdzt;
-        pa.um = p.u_mrf; pa.fc = p.fc; pa.ug = p.ug; pa.vg = p.vg; pa.t_ref = p.t_ref; pa.tbot = p.tbot; pa.ttop = p.ttop;
+        pa.um = p.u_mrf; pa.fc = p.fc; pa.ug = p.ug; pa.vg = p.vg; pa.t_ref = p.t_ref; pa.ttop = p.ttop;
+        t_ghost_bottom(h, pa.tbs, pa.tba);
         pa.inv_coe = 1.0 / (p.issk == 1 ? 0.5 : 1.0);
         pa.closed = p.ochannel == 0; pa.dp3 = p.dp_opt == 3; pa.scalar = p.isscalar == 1; pa.skew = p.issk == 1;
         pa.kchunk = spec_kchunk(h, g.nxy); pa.halt = halt;
@@ -1322,7 +1341,8 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         ProdTArgs<R> pt;
         pt.u = (const R*)h->fld[F_U]; pt.v = (const R*)h->fld[F_V]; pt.w = (const R*)h->fld[F_W]; pt.t = (const R*)h->fld[F_T];
         for (int f = 0; f < 3; ++f) pt.out[f] = Q[SP_W0 + 4 + f];
-        pt.g = g; pt.tbot = p.tbot; pt.ttop = p.ttop; pt.kchunk = spec_kchunk(h, g.nxy); pt.halt = halt;
+        t_ghost_bottom(h, pt.tbs, pt.tba);
+        pt.g = g; pt.ttop = p.ttop; pt.kchunk = spec_kchunk(h, g.nxy); pt.halt = halt;
         prof_begin(h, K_SPEC_PROD);
         k_spec_products_t<R><<<dim3((unsigned)((g.nxy + 255) / 256), (p.nz + pt.kchunk - 1) / pt.kchunk), 256, 0, h->st>>>(pt);
         CKL();
@@ -1336,17 +1356,15 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         at.dt = dtab; at.g = g; at.tpx = tpx; at.tpy = tpy;
         at.rdz = h->cc.rdz; at.rdzt = h->cc.rdzt; at.rdzb = h->cc.rdzb;
         at.rk_a = rk_a; at.rk_b = rk_b; at.rk_c = rk_c; at.dtime = p.dt; at.alpha = p.alpha; at.um = p.u_mrf;
-        at.tbot = p.tbot; at.ttop = p.ttop; at.kchunk = spec_kchunk(h, g.ncol); at.halt = halt;
+        t_ghost_bottom(h, at.tbs, at.tba);
+        at.ttop = p.ttop; at.kchunk = spec_kchunk(h, g.ncol); at.halt = halt;
         prof_begin(h, K_SPEC_ASM);
         k_spec_assemble_t<R><<<dim3((unsigned)((g.ncol + 255) / 256), (p.nz + at.kchunk - 1) / at.kchunk), 256, 0, h->st>>>(at);
         CKL();
         ColTArgs<R> ct;
         ct.qt = S[SP_QU]; ct.out = S[SP_T]; ct.ltr = ltr; ct.mtr = mtr;
         ct.c = h->cc; ct.s = h->cs; ct.g = g; ct.rk_c = rk_c; ct.halt = halt;
-        const double* DZ = h->zhost[0].data(); const double* DZT = h->zhost[1].data(); const double* DZB = h->zhost[2].data();
-        const int ks = 2, ke = p.nz + 1;
-        ct.bct0 = -2.0 * (-0.5 * rk_c * p.dt * p.alpha / DZ[ks] / DZB[ks]) * p.tbot;
-        ct.bct1 = -2.0 * (-0.5 * rk_c * p.dt * p.alpha / DZ[ke] / DZT[ke]) * p.ttop;
+        t_bc_src(h, rk_c, ct.bct0, ct.bct1);
         prof_begin(h, K_COLUMN_T);
         if ((rc = launch_column_t<R>(h, ct))) return rc;
         const T2* ys[1] = {S[SP_T]};
@@ -1442,12 +1460,17 @@ struct AdjBufs {
     double* ax[8];       // adjoints of the eight interpolants of the current sub-step
     double* lq[3];       // lambda_q of the current sub-step (physical)
     double* lbf[3];      // body-force gradient
-    double* ckpt;        // checkpoint c: 7 fields (u, v, w, p, ff, gg, hh) at ckpt + 7 c n
-    double* tape;        // sub-step t of a segment: its start state u, v, w, p at tape + 4 t n
-    double* fin;         // the final state, 7 fields
+    double* lt;          // adjoint of T (temperature runs)
+    double* ls; double* ls2;   // adjoint of the history ss, ping-pong pair
+    double* nxt;         // u, v, w at the end of the segment being reversed (temperature runs)
+    int nst, ntp;        // fields a checkpoint / a taped sub-step holds
+    double* ckpt;        // checkpoint c: nst fields (u, v, w, p, ff, gg, hh[, t, ss]) at ckpt + nst c n
+    double* tape;        // sub-step t of a segment: its start state u, v, w, p[, t] at tape + ntp t n
+    double* fin;         // the final state, nst fields
 };
 
-static const int ADJ_STATE[7] = {F_U, F_V, F_W, F_P, F_FF, F_GG, F_HH};
+static const int ADJ_STATE[9] = {F_U, F_V, F_W, F_P, F_FF, F_GG, F_HH, F_T, F_SS};
+static const int ADJ_TAPE[5] = {F_U, F_V, F_W, F_P, F_T};
 
 template <int K> static int col_adj_k(hc_handle* h, const ColAdjArgs& a)
 {
@@ -1471,14 +1494,86 @@ static int launch_column_adj(hc_handle* h, const ColAdjArgs& a)
     }
 }
 
-// Adjoint of one FD sub-step: on entry b.lam / b.lh hold the adjoints of the
-// sub-step's outputs, on return those of its inputs (the state st[] it started from).
-template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* const* st, AdjBufs& b)
+template <int K> static int col_t_adj_k(hc_handle* h, const ColTAdjArgs& a)
+{
+    const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
+    k_column_t_adj<K><<<nb, CW_WARPS * 32, 0, h->st>>>(a);
+    CKL();
+    return HC_OK;
+}
+static int launch_column_t_adj(hc_handle* h, const ColTAdjArgs& a)
+{
+    switch ((h->p.nz + 31) / 32) {
+    case 1: return col_t_adj_k<1>(h, a);
+    case 2: return col_t_adj_k<2>(h, a);
+    case 3: return col_t_adj_k<3>(h, a);
+    case 4: return col_t_adj_k<4>(h, a);
+    case 5: return col_t_adj_k<5>(h, a);
+    case 6: return col_t_adj_k<6>(h, a);
+    case 7: return col_t_adj_k<7>(h, a);
+    case 8: return col_t_adj_k<8>(h, a);
+    default: return HC_ERR_UNSUPPORTED;
+    }
+}
+
+// Adjoint of the temperature part of one FD sub-step (it runs after the
+// momentum part in the forward step, so first here): on entry b.lt / b.ls hold
+// the adjoints of T' and of the new history; on return b.lt holds the adjoint of
+// the T the sub-step started from (the buoyancy share still to come from the
+// momentum part), b.ls that of the old history, and the adjoints of the
+// sub-step's velocities u', v', w' (nx[]) in b.lam have gained the advection terms.
+template <int CDS> static int adj_substep_t(hc_handle* h, int sub, const double* const* st, const double* const* nx,
+                                            AdjBufs& b)
 {
     const hc_params& p = h->p;
     double rk_a, rk_b, rk_c;
     if (p.dts == 2) { rk_a = RKC1[sub]; rk_b = RKC2[sub]; rk_c = RKC3[sub]; }
     else { rk_a = 1.5; rk_b = -0.5; rk_c = 1.0; }
+    double2* S0 = (double2*)h->spec[0];
+    const double* lin[1] = {b.lt};
+    double2* sout[1] = {S0};
+    int rc = fft_forward<double>(h, lin, sout, 1);
+    if (rc) return rc;
+    ColTAdjArgs ct;
+    ct.at = S0; ct.c = h->cc; ct.g = h->g; ct.rk_c = rk_c;
+    prof_begin(h, K_ADJ_COLUMN);
+    rc = launch_column_t_adj(h, ct);
+    if (rc) return rc;
+    double* lqt[1] = {b.lq[0]};
+    const int add0[1] = {0};
+    rc = fft_inverse<double>(h, sout, lqt, add0, 1);
+    if (rc) return rc;
+    AdjTArgs m;
+    m.a = make_acc<double>(h);
+    m.a.f.t = st[4]; m.a.f.u = nx[0]; m.a.f.v = nx[1]; m.a.f.w = nx[2];
+    m.lqt = b.lq[0]; m.lss_out = b.ls; m.lss_prev = b.ls2;
+    for (int f = 0; f < 3; ++f) { m.ax[f] = b.ax[f]; m.lvel[f] = b.lam[f]; }
+    m.out_t = b.lt;
+    m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph;
+    prof_begin(h, K_ADJ_RHS);
+    k_t_adj_interp<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
+    CKL();
+    prof_begin(h, K_ADJ_RHS);
+    k_t_adj_gather<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
+    CKL();
+    double* t = b.ls; b.ls = b.ls2; b.ls2 = t;
+    return HC_OK;
+}
+
+// Adjoint of one FD sub-step: on entry b.lam / b.lh (and b.lt / b.ls) hold the
+// adjoints of the sub-step's outputs, on return those of its inputs (the state
+// st[] it started from; nx[] is the u, v, w it produced).
+template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* const* st, const double* const* nx,
+                                          AdjBufs& b)
+{
+    const hc_params& p = h->p;
+    double rk_a, rk_b, rk_c;
+    if (p.dts == 2) { rk_a = RKC1[sub]; rk_b = RKC2[sub]; rk_c = RKC3[sub]; }
+    else { rk_a = 1.5; rk_b = -0.5; rk_c = 1.0; }
+    if (p.isscalar == 1) {
+        int rc = adj_substep_t<CDS>(h, sub, st, nx, b);
+        if (rc) return rc;
+    }
     double2* S[4] = {(double2*)h->spec[0], (double2*)h->spec[1], (double2*)h->spec[2], (double2*)h->spec[3]};
     // M^T = iFFT . C^H . FFT applied to the adjoints of (u', v', w', psi = p' - p)
     const double* lin[4] = {b.lam[0], b.lam[1], b.lam[2], b.lam[3]};
@@ -1503,6 +1598,8 @@ template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* c
     for (int f = 0; f < 3; ++f) { m.lq[f] = b.lq[f]; m.lf_out[f] = b.lh[f]; m.lf_prev[f] = b.lh2[f]; m.lbf[f] = b.lbf[f]; }
     for (int f = 0; f < 8; ++f) m.ax[f] = b.ax[f];
     for (int f = 0; f < 4; ++f) m.out[f] = b.lam[f];
+    m.out_t = p.isscalar == 1 ? b.lt : nullptr;
+    m.got = p.got;
     m.rk_a = rk_a; m.rk_b = rk_b; m.rk_c = rk_c; m.ph = h->ph;
     prof_begin(h, K_ADJ_RHS);
     k_rhs_adj_interp<CDS><<<pt_grid(h->g), pt_block(), 0, h->st>>>(m);
@@ -1514,12 +1611,12 @@ template <int CDS> static int adj_substep(hc_handle* h, int sub, const double* c
     return HC_OK;
 }
 
-static int adj_copy_state(hc_handle* h, double* dst, int nf, int to_fields)
+static int adj_copy_state(hc_handle* h, double* dst, int nf, int to_fields, const int* list = ADJ_STATE)
 {
     const size_t fb = (size_t)h->g.n * sizeof(double);
     for (int f = 0; f < nf; ++f) {
         double* a = dst + (size_t)f * h->g.n;
-        void* fld = h->fld[ADJ_STATE[f]];
+        void* fld = h->fld[list[f]];
         if (to_fields) CK(cudaMemcpyAsync(fld, a, fb, cudaMemcpyDeviceToDevice, h->st));
         else CK(cudaMemcpyAsync(a, fld, fb, cudaMemcpyDeviceToDevice, h->st));
     }
@@ -1539,8 +1636,14 @@ static AdjBufs adj_bufs(hc_handle* h)
     for (int f = 0; f < 8; ++f) { b.ax[f] = q; q += n; }
     for (int f = 0; f < 3; ++f) { b.lq[f] = q; q += n; }
     for (int f = 0; f < 3; ++f) { b.lbf[f] = q; q += n; }
-    b.ckpt = q; q += (size_t)7 * h->adj_nseg * n;
-    b.tape = q; q += (size_t)4 * h->adj_seglen * (h->p.dts == 2 ? 3 : 1) * n;
+    b.lt = q; q += n;
+    b.ls = q; q += n;
+    b.ls2 = q; q += n;
+    b.nxt = q; q += 3 * n;
+    b.nst = h->p.isscalar == 1 ? 9 : 7;
+    b.ntp = h->p.isscalar == 1 ? 5 : 4;
+    b.ckpt = q; q += (size_t)b.nst * h->adj_nseg * n;
+    b.tape = q; q += (size_t)b.ntp * h->adj_seglen * (h->p.dts == 2 ? 3 : 1) * n;
     b.fin = q;
     return b;
 }
@@ -1563,14 +1666,14 @@ template <int CDS> static int adjoint_forward(hc_handle* h, AdjBufs& b)
     for (int s = 0; s < nsteps; ++s) {
         const int seg = s / ckpt;
         if (s % ckpt == 0) {
-            rc = adj_copy_state(h, b.ckpt + (size_t)seg * 7 * n, 7, 0);
+            rc = adj_copy_state(h, b.ckpt + (size_t)seg * b.nst * n, b.nst, 0);
             if (rc) return rc;
             CK(cudaMemcpyAsync(h->adj_sc + seg, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
         }
         if (seg == nseg - 1) {
             const int t0 = (s - seg * ckpt) * nsub;
             for (int sub = 0; sub < nsub; ++sub) {
-                rc = adj_copy_state(h, b.tape + (size_t)(t0 + sub) * 4 * n, 4, 0);
+                rc = adj_copy_state(h, b.tape + (size_t)(t0 + sub) * b.ntp * n, b.ntp, 0, ADJ_TAPE);
                 if (rc) return rc;
                 rc = substep_fd<double, CDS>(h, sub);
                 if (rc) return rc;
@@ -1588,7 +1691,7 @@ template <int CDS> static int adjoint_forward(hc_handle* h, AdjBufs& b)
         }
     }
     h->adj_tape_seg = nseg - 1;
-    rc = adj_copy_state(h, b.fin, 7, 0);
+    rc = adj_copy_state(h, b.fin, b.nst, 0);
     if (rc) return rc;
     CK(cudaMemcpyAsync(h->adj_sc + nseg, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
     CK(cudaEventRecord(h->e1, h->st));
@@ -1610,7 +1713,7 @@ template <int CDS> static int adj_segment(hc_handle* h, AdjBufs& b, int T, int r
     int rc;
     if (recompute) {
         for (int t = 0; t < T; ++t) {
-            rc = adj_copy_state(h, b.tape + (size_t)t * 4 * n, 4, 0);
+            rc = adj_copy_state(h, b.tape + (size_t)t * b.ntp * n, b.ntp, 0, ADJ_TAPE);
             if (rc) return rc;
             if (t == T - 1) break;
             rc = substep_fd<double, CDS>(h, t % nsub, 1, t == 0);
@@ -1618,9 +1721,13 @@ template <int CDS> static int adj_segment(hc_handle* h, AdjBufs& b, int T, int r
         }
     }
     for (int t = T - 1; t >= 0; --t) {
-        const double* st[4];
-        for (int f = 0; f < 4; ++f) st[f] = b.tape + ((size_t)t * 4 + f) * n;
-        rc = adj_substep<CDS>(h, t % nsub, st, b);
+        const double* st[5];
+        const double* nx[3];
+        for (int f = 0; f < b.ntp; ++f) st[f] = b.tape + ((size_t)t * b.ntp + f) * n;
+        // the velocities the sub-step produced: the next sub-step's start, or the
+        // segment's end staged in b.nxt
+        for (int f = 0; f < 3; ++f) nx[f] = t + 1 < T ? b.tape + ((size_t)(t + 1) * b.ntp + f) * n : b.nxt + (size_t)f * n;
+        rc = adj_substep<CDS>(h, t % nsub, st, nx, b);
         if (rc) return rc;
     }
     return HC_OK;
@@ -1671,6 +1778,7 @@ template <int CDS> static int adj_segment_run(hc_handle* h, AdjBufs& b, int T, i
         h->adj_gkey[slot] = key;
     } else if (T & 1) {
         for (int f = 0; f < 3; ++f) { double* t = b.lh[f]; b.lh[f] = b.lh2[f]; b.lh2[f] = t; }
+        if (h->p.isscalar == 1) { double* t = b.ls; b.ls = b.ls2; b.ls2 = t; }
     }
     CK(cudaGraphLaunch(h->adj_gexec[slot], h->st));
     h->launches += h->adj_glaunch[slot];
@@ -1692,15 +1800,20 @@ template <int CDS> static int adjoint_reverse(hc_handle* h, AdjBufs& b)
         const int s0 = seg * ckpt, s1 = (s0 + ckpt < nsteps ? s0 + ckpt : nsteps);
         const int recompute = h->adj_tape_seg != seg;
         if (recompute) {
-            rc = adj_copy_state(h, b.ckpt + (size_t)seg * 7 * n, 7, 1);
+            rc = adj_copy_state(h, b.ckpt + (size_t)seg * b.nst * n, b.nst, 1);
             if (rc) return rc;
             CK(cudaMemcpyAsync(h->sc, h->adj_sc + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
+        }
+        if (h->p.isscalar == 1) {
+            // u, v, w at the segment's end: the next checkpoint, or the final state
+            const double* end = seg == nseg - 1 ? b.fin : b.ckpt + (size_t)(seg + 1) * b.nst * n;
+            CK(cudaMemcpyAsync(b.nxt, end, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
         }
         rc = adj_segment_run<CDS>(h, b, (s1 - s0) * nsub, recompute);
         if (rc) return rc;
         h->adj_tape_seg = seg;
     }
-    rc = adj_copy_state(h, b.fin, 7, 1);
+    rc = adj_copy_state(h, b.fin, b.nst, 1);
     if (rc) return rc;
     CK(cudaMemcpyAsync(h->sc, h->adj_sc + nseg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->st));
     CK(cudaEventRecord(h->e1, h->st));
@@ -1805,6 +1918,7 @@ int hc_create(const hc_params* p, hc_handle** out)
     if (p->nx < 8 || p->ny < 4 || p->nz < 3) return HC_ERR_PARAM;
     if (p->cds < 1 || p->cds > 3 || (p->dts != 1 && p->dts != 2) || p->dt <= 0.0) return HC_ERR_PARAM;
     if (p->isscalar != 0 && p->isscalar != 1) return HC_ERR_PARAM;
+    if (p->tbc_bot != 0 && p->tbc_bot != 1) return HC_ERR_PARAM;
     if (p->dp_opt < 1 || p->dp_opt > 3) return HC_ERR_PARAM;
     if (p->precision != HC_PREC_FP64 && p->precision != HC_PREC_MIXED) return HC_ERR_PARAM;
     if (p->isdamp == 1 && (p->nzdamp < 1 || p->nzdamp > p->nz - 1)) return HC_ERR_PARAM;
@@ -2565,7 +2679,7 @@ int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
     if (!h->initialized) return HC_ERR_STATE;
     const hc_params& p = h->p;
     if (h->rsz != sizeof(double) || (p.cds != 1 && p.cds != 2) || (p.dp_opt != 1 && p.dp_opt != 3) ||
-        p.isscalar != 0 || p.isdamp != 0 || p.nz > 256)
+        (p.isscalar == 1 && p.is_ri_var != 0) || p.isdamp != 0 || p.nz > 256)
         return HC_ERR_UNSUPPORTED;
     h->adj_ready = 0;
     DevScalars s0;
@@ -2575,8 +2689,9 @@ int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
     const int nsub = p.dts == 2 ? 3 : 1;
     const int nseg = (nsteps + ckpt - 1) / ckpt;
     const int seglen = ckpt < nsteps ? ckpt : nsteps;
-    // 24 adjoint fields, 7 per checkpoint, 4 per taped sub-step, 7 for the final state
-    const size_t nfield = 24 + (size_t)7 * nseg + (size_t)4 * seglen * nsub + 7;
+    // 30 adjoint fields, nst per checkpoint, ntp per taped sub-step, nst for the final state
+    const size_t nst = p.isscalar == 1 ? 9 : 7, ntp = p.isscalar == 1 ? 5 : 4;
+    const size_t nfield = 30 + nst * nseg + ntp * seglen * nsub + nst;
     const size_t bytes = nfield * (size_t)n * sizeof(double);
     if (bytes > h->adj_bytes) {
         adj_graph_drop(h);
@@ -2608,8 +2723,15 @@ int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt)
 int hc_adjoint_reverse(hc_handle* h, const double* lu, const double* lv, const double* lw, const double* lp,
                        double* gu, double* gv, double* gw, double* gp, double* gbf)
 {
+    return hc_adjoint_reverse_t(h, lu, lv, lw, lp, nullptr, gu, gv, gw, gp, nullptr, gbf);
+}
+
+int hc_adjoint_reverse_t(hc_handle* h, const double* lu, const double* lv, const double* lw, const double* lp,
+                         const double* lt, double* gu, double* gv, double* gw, double* gp, double* gt, double* gbf)
+{
     if (!h) return HC_ERR_ARG;
     if (!h->adj_ready) return HC_ERR_STATE;
+    if ((lt || gt) && h->p.isscalar != 1) return HC_ERR_ARG;
     AdjBufs b = adj_bufs(h);
     const long long n = h->g.n;
     const size_t fb = (size_t)n * sizeof(double);
@@ -2622,6 +2744,9 @@ int hc_adjoint_reverse(hc_handle* h, const double* lu, const double* lv, const d
         CK(cudaMemsetAsync(b.lh[f], 0, fb, h->st));
         CK(cudaMemsetAsync(b.lbf[f], 0, fb, h->st));
     }
+    if (lt) CK(cudaMemcpyAsync(b.lt, lt, fb, cudaMemcpyHostToDevice, h->st));
+    else CK(cudaMemsetAsync(b.lt, 0, fb, h->st));
+    CK(cudaMemsetAsync(b.ls, 0, fb, h->st));
     int rc = h->p.cds == 1 ? adjoint_reverse<1>(h, b) : adjoint_reverse<2>(h, b);
     if (rc) { h->adj_ready = 0; return rc; }
     rc = prof_collect(h);
@@ -2631,6 +2756,7 @@ int hc_adjoint_reverse(hc_handle* h, const double* lu, const double* lv, const d
         if (out[f]) CK(cudaMemcpyAsync(out[f], b.lam[f], fb, cudaMemcpyDeviceToHost, h->st));
     if (gbf)
         for (int f = 0; f < 3; ++f) CK(cudaMemcpyAsync(gbf + (size_t)f * n, b.lbf[f], fb, cudaMemcpyDeviceToHost, h->st));
+    if (gt) CK(cudaMemcpyAsync(gt, b.lt, fb, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     DevScalars s1;
     CK(cudaMemcpy(&s1, h->sc, sizeof(s1), cudaMemcpyDeviceToHost));

@@ -27,16 +27,26 @@ __device__ __forceinline__ double2 shfl_dn2(double2 v, int s)
     return make_double2(__shfl_down_sync(0xffffffffu, v.x, s), __shfl_down_sync(0xffffffffu, v.y, s));
 }
 
+// The hardware's single-precision reciprocal approximation (PTX rcp.approx.ftz:
+// within about one FP32 ulp; subnormal inputs flush to zero, and no pivot of the
+// column systems comes near that range).
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Reciprocal by Newton-Raphson iteration on f(y) = 1/y - x, i.e.
-// y <- y + y (1 - x y), seeded with the single-precision reciprocal. Each step
-// doubles the number of correct bits (about 23 -> 46 -> 92), so two steps reach
+// y <- y + y (1 - x y), seeded with the single-precision approximation. Each step
+// squares the relative error (about 2^-23 -> 2^-46 -> 2^-92), so two steps reach
 // FP64 round-off. The pivots of the diagonally dominant column systems stay far
 // inside the FP32 range; anything outside it (and NaN) takes the IEEE division.
 __device__ __forceinline__ double rcp_nr(double x)
 {
     const double ax = fabs(x);
     if (!(ax > 1e-30 && ax < 1e30)) return 1.0 / x;
-    double y = (double)__frcp_rn((float)x);
+    double y = (double)rcp_approx((float)x);
     double e = fma(-x, y, 1.0);
     y = fma(y, e, y);
     e = fma(-x, y, 1.0);
@@ -297,7 +307,9 @@ template <int K> __host__ __device__ constexpr int ct_stride() { return K * CT_R
 // the mixed-precision column kernel runs its Helmholtz solves in FP32 and keeps
 // the Poisson solve and the (0,0) mean mode in FP64.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float rcp_t(float x) { return __frcp_rn(x); }
+// FP32 solves (the mixed mode's Helmholtz systems): the approximation alone; its
+// error is of the order of the elimination's own FP32 rounding
+__device__ __forceinline__ float rcp_t(float x) { return rcp_approx(x); }
 __device__ __forceinline__ double rcp_t(double x) { return rcp_nr(x); }
 
 template <typename T> __device__ __forceinline__ typename V2<T>::T t2sub(typename V2<T>::T a, typename V2<T>::T b)

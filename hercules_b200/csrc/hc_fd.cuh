@@ -30,7 +30,7 @@ template <typename R> __device__ __forceinline__ R ldf(const R* f, const Geo& g,
 template <typename R> struct Acc {
     FieldsIn<R> f;
     Geo g;
-    R um, tbot, ttop;
+    R um, tbs, tba, ttop;   // bottom ghost of T: T(-1) = tbs T(0) + tba
     int closed;   // ochannel == 0
     // pre-damping copies of levels kd..nz-1 ([k-kd][j][i]); null: no damping
     const R* su; const R* sv; const R* sw; const R* sp; const R* st;
@@ -69,7 +69,7 @@ template <typename R> struct Acc {
         return raw(f.p, sp, i, j, k);
     }
     __device__ __forceinline__ R T(int i, int j, int k) const {
-        if (k < 0) return R(2) * tbot - gsrc(f.t, st, i, j, 0);
+        if (k < 0) return tbs * gsrc(f.t, st, i, j, 0) + tba;
         if (k >= g.nz) return R(2) * ttop - gsrc(f.t, st, i, j, g.nz - 1);
         return raw(f.t, st, i, j, k);
     }
@@ -137,7 +137,7 @@ template <typename R> struct Acc {
     }
     __device__ __forceinline__ R thz(int i, int j, int k) const {
         i = wrapi(i, g.nx); j = wrapi(j, g.ny);
-        if (k < 0) return tbot;
+        if (k < 0) return tbs < R(0) ? R(0.5) * tba : R(0.5) * (T(i, j, -1) + T(i, j, 0));   // the wall value
         if (k >= g.nz - 1) return ttop;
         R l = lt(k);
         return T(i, j, k + 1) * l + T(i, j, k) * (R(1) - l);

@@ -619,7 +619,7 @@ __device__ __forceinline__ void k_rhs_t_strip_body(const TempArgs<R>& m, const u
     const R sy2 = CDS == 1 ? R(1) / (R)g.dy2 : R(1) / (R(12) * (R)g.dy2);
     const R dt = (R)m.ph.dt, al = (R)m.ph.alpha, um = A.um;
     const R rka = (R)m.rk_a, rkb = (R)m.rk_b, cdif = (R)m.rk_c * R(0.5) * dt * al;
-    const R tbot = A.tbot, ttop = A.ttop;
+    const R tbs = A.tbs, tba = A.tba, ttop = A.ttop;
     const int xl = 2 * lane, rl0 = RQ * wid;
     const int xi = x0 + xl;
     bool act[2];
@@ -639,7 +639,7 @@ __device__ __forceinline__ void k_rhs_t_strip_body(const TempArgs<R>& m, const u
     for (int q = 0; q < RQ; ++q) {
         if (kb == 0) {
             const R2 tc = ld2r(plane(0, 0), rc[q]);
-            tm1[q][0] = R(2) * tbot - tc.x; tm1[q][1] = R(2) * tbot - tc.y;
+            tm1[q][0] = tbs * tc.x + tba; tm1[q][1] = tbs * tc.y + tba;
             fzp[q][0] = fzp[q][1] = R(0);
         } else {
             const long long o = (long long)(kb - 1) * g.nxy;

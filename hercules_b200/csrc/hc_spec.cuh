@@ -174,7 +174,7 @@ template <typename R> struct ProdArgs {
     Geo g;
     const double* rdz; const double* rdzt;   // [nz] 1/dz, 1/dz_t
     const DevScalars* sc;
-    double um, fc, ug, vg, t_ref, tbot, ttop, inv_coe;
+    double um, fc, ug, vg, t_ref, tbs, tba, ttop, inv_coe;   // T(-1) = tbs T(0) + tba
     int closed, dp3, scalar, skew, kchunk;
     const int* halt;
 };
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(256, 3) k_spec_products(ProdArgs<R> a)
     auto gW = [&](R r, int k) -> double { return k < 0 ? 0.0 : (k >= nz ? -(double)r : (double)r); };
     auto gT = [&](R r, int k) -> double {
         if (!a.scalar) return 0.0;
-        return k < 0 ? 2.0 * a.tbot - (double)r : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
+        return k < 0 ? a.tbs * (double)r + a.tba : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
     };
     // the four fields at level L, in the storage type
     struct Lv { R u, v, w, t; };
@@ -443,7 +443,7 @@ template <typename R> struct ProdTArgs {
     const R* u; const R* v; const R* w; const R* t;
     R* out[3];
     Geo g;
-    double tbot, ttop;
+    double tbs, tba, ttop;   // T(-1) = tbs T(0) + tba
     int kchunk;
     const int* halt;
 };
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(256) k_spec_products_t(ProdTArgs<R> a)
     const int nz1 = nz - 1;
     auto rawt = [&](int k) -> R { return a.t[(long long)(k < 0 ? 0 : (k > nz1 ? nz1 : k)) * nxy + ij]; };
     auto gT = [&](R r, int k) -> double {
-        return k < 0 ? 2.0 * a.tbot - (double)r : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
+        return k < 0 ? a.tbs * (double)r + a.tba : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
     };
     struct Lv { R tp, u, v, w; double lt, lb, dz; };
     auto fetch = [&](int k, Lv& L) {
@@ -501,7 +501,7 @@ template <typename R> struct AsmTArgs {
     Geo g;
     const double* rdz; const double* rdzt; const double* rdzb;   // [nz] 1/dz, 1/dz_t, 1/dz_b
     double tpx, tpy;
-    double rk_a, rk_b, rk_c, dtime, alpha, um, tbot, ttop;
+    double rk_a, rk_b, rk_c, dtime, alpha, um, tbs, tba, ttop;   // T(-1) = tbs T(0) + tba
     int kchunk;
     const int* halt;
 };
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(256) k_spec_assemble_t(AsmTArgs<R> a)
     // of update_boundary_t on it (a constant offset lands on the (0,0) mode only)
     auto gT = [&](T2 r, int k) -> double2 {
         const double2 s = dbl(r);
-        if (k < 0) return make_double2(-s.x + (wv.is00 ? 2.0 * a.tbot : 0.0), -s.y);
+        if (k < 0) return make_double2(a.tbs * s.x + (wv.is00 ? a.tba : 0.0), a.tbs * s.y);
         if (k >= nz) return make_double2(-s.x + (wv.is00 ? 2.0 * a.ttop : 0.0), -s.y);
         return s;
     };

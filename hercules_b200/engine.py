@@ -32,7 +32,7 @@ ABI_SYMBOLS = ["hc_create", "hc_set_grid", "hc_get_grid", "hc_upload", "hc_downl
                "hc_last_step_ms", "hc_last_launch_count", "hc_set_profiling", "hc_kernel_profile",
                "hc_divergence_noalloc", "hc_set_body_force", "hc_set_graph", "hc_ensemble_create",
                "hc_ensemble_step", "hc_ensemble_last_ms", "hc_ensemble_destroy", "hc_adjoint_forward",
-               "hc_adjoint_reverse", "hc_adjoint", "hc_adjoint_last_ms", "hc_destroy", "hc_error_string"]
+               "hc_adjoint_reverse", "hc_adjoint_reverse_t", "hc_adjoint", "hc_adjoint_last_ms", "hc_destroy", "hc_error_string"]
 
 
 class HerculesError(RuntimeError):
@@ -78,6 +78,7 @@ def load_library(path: str = LIB_PATH):
     L.hc_adjoint.argtypes = [vp, ip, ip] + [ctypes.c_void_p] * 9
     L.hc_adjoint_forward.argtypes = [vp, ip, ip]
     L.hc_adjoint_reverse.argtypes = [vp] + [ctypes.c_void_p] * 9
+    L.hc_adjoint_reverse_t.argtypes = [vp] + [ctypes.c_void_p] * 11
     L.hc_adjoint_last_ms.argtypes = [vp, ctypes.POINTER(dp), ctypes.POINTER(dp),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.hc_destroy.argtypes = [vp]
@@ -181,25 +182,31 @@ class Channel:
         _check(self._L.hc_adjoint_forward(self.h, nsteps, ckpt), "hc_adjoint_forward")
 
     def adjoint_reverse(self, seeds: Dict[str, np.ndarray], body_force: bool = True) -> Dict[str, np.ndarray]:
-        """Gradient of J = sum over f in seeds of <seeds[f], f_N> (f in u, v, w, p;
-        the fields after the last adjoint_forward) with respect to the fields that
-        pass started from (keys "u", "v", "w", "p") and, with body_force, to the
-        body force ("fx", "fy", "fz")."""
+        """Gradient of J = sum over f in seeds of <seeds[f], f_N> (f in u, v, w, p and,
+        with temperature, t; the fields after the last adjoint_forward) with respect
+        to the fields that pass started from (keys "u", "v", "w", "p"[, "t"]) and,
+        with body_force, to the body force ("fx", "fy", "fz")."""
         shp = self._shape(0)
-        sd = []
-        for f in ("u", "v", "w", "p"):
+        names = ("u", "v", "w", "p") + (("t",) if self.p.isscalar else ())
+        sd = {}
+        for f in names:
             a = seeds.get(f)
             if a is not None:
                 a = np.ascontiguousarray(a, dtype=np.float64)
                 if a.shape != shp:
                     raise ValueError(f"seed {f}: shape {a.shape} != {shp}")
-            sd.append(a)
-        g = {f: np.zeros(shp) for f in ("u", "v", "w", "p")}
+            sd[f] = a
+        g = {f: np.zeros(shp) for f in names}
         gbf = np.zeros((3,) + shp) if body_force else None
         ptr = lambda a: None if a is None else ctypes.c_void_p(a.ctypes.data)
-        _check(self._L.hc_adjoint_reverse(self.h, *[ptr(a) for a in sd],
-                                          *[ptr(g[f]) for f in ("u", "v", "w", "p")], ptr(gbf)),
-               "hc_adjoint_reverse")
+        if self.p.isscalar:
+            _check(self._L.hc_adjoint_reverse_t(self.h, *[ptr(sd[f]) for f in names],
+                                                *[ptr(g[f]) for f in names], ptr(gbf)),
+                   "hc_adjoint_reverse_t")
+        else:
+            _check(self._L.hc_adjoint_reverse(self.h, *[ptr(sd[f]) for f in names],
+                                              *[ptr(g[f]) for f in names], ptr(gbf)),
+                   "hc_adjoint_reverse")
         if body_force:
             g.update(fx=gbf[0], fy=gbf[1], fz=gbf[2])
         return g

@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .params import Params, mesh
+from .params import Params, mesh, t_line
 
 
 def _rng(seed):
@@ -36,8 +36,8 @@ def poiseuille_noise(p: Params, seed: int = 1, amp: float = 0.15):
 
 def loglaw_stratified(p: Params, seed: int = 10):
     """Open-channel log-law (u+ = z+ below 11, else 2.44 ln z+ + 5.2, z+ = 180 z)
-    with 5% Gaussian noise on u and 5% of u_max on v, w; linear temperature
-    between tbot and ttop plus 1% noise."""
+    with 5% Gaussian noise on u and 5% of u_max on v, w; the linear temperature
+    between the walls (params.t_line) plus 1% of its range as noise."""
     g = _rng(seed)
     zc = mesh(p)["zc"]
     zp = 180.0 * zc
@@ -48,8 +48,8 @@ def loglaw_stratified(p: Params, seed: int = 10):
     v = 0.05 * umax * g.standard_normal(shape)
     w = 0.05 * umax * g.standard_normal(shape)
     w[-1] = 0.0
-    dT = p.ttop - p.tbot
-    tl = p.tbot + dT * zc / p.lz
+    tl = t_line(p, zc)
+    dT = p.tbot * p.lz if p.tbc_bot else p.ttop - p.tbot
     t = tl[:, None, None] + 0.01 * abs(dT) * g.standard_normal(shape)
     return {"u": u - p.u_mrf, "v": v, "w": w, "p": np.zeros(shape), "t": t}
 
@@ -66,7 +66,7 @@ def small_random(p: Params, seed: int = 0, amp: float = 0.1):
     w = amp * g.uniform(-1, 1, shape)
     w[-1] = 0.0
     pr = amp * g.uniform(-1, 1, shape)
-    t = (p.tbot + (p.ttop - p.tbot) * zc / p.lz)[:, None, None] + amp * g.uniform(-1, 1, shape)
+    t = t_line(p, zc)[:, None, None] + amp * g.uniform(-1, 1, shape)
     out = {"u": u, "v": v, "w": w, "p": pr, "t": t}
     if p.dts == 1:
         for k in ("ff", "gg", "hh", "ss"):

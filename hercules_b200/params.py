@@ -49,7 +49,8 @@ class HcParams(ctypes.Structure):
         ("ri_str", ctypes.c_double), ("ri_end", ctypes.c_double),
         ("precision", ctypes.c_int),
         ("tile", ctypes.c_int * 4),
-        ("reserved", ctypes.c_int * 3),
+        ("tbc_bot", ctypes.c_int),
+        ("reserved", ctypes.c_int * 2),
     ]
 
 
@@ -129,6 +130,9 @@ class Params:
     # kernel tile shapes (0 = automatic)
     precision: int = PREC_FP64
     tile: List[int] = field(default_factory=lambda: [0, 0, 0, 0])
+    # bottom temperature condition: 0 the wall temperature tbot (the reference's
+    # only one), 1 the fixed wall gradient dT/dz = tbot (a fixed heat flux)
+    tbc_bot: int = 0
 
     def to_c(self) -> HcParams:
         c = HcParams()
@@ -160,6 +164,8 @@ def check_parameters(p: Params) -> None:
         raise ValueError("ny and nz are not divisible by p_col! Quit!")
     if p.nx % 2 or p.ny % 2:
         raise ValueError("Please use even numbers for nx and ny! Quit!")
+    if p.tbc_bot not in (0, 1):
+        raise ValueError("tbc_bot must be 0 (fixed bottom temperature) or 1 (fixed bottom gradient)")
 
 
 _NML_GROUP = re.compile(r"&(\w+)(.*?)/", re.S)
@@ -219,11 +225,12 @@ def config_channel_fd(nx=96, ny=64, nz=64, precision=PREC_FP64) -> Params:
 
 def config_open_channel_spectral(nx=256, ny=256, nz=128, got=0.1, precision=PREC_FP64) -> Params:
     """Stably stratified open channel, pseudo-spectral horizontal derivatives,
-    Pr=0.71, Dirichlet temperature (tbot=-1, ttop=0)."""
+    Pr=0.71, a fixed bottom-cooling flux (dT/dz = 1 at the bottom wall,
+    tbc_bot = 1) and T = 0 at the top."""
     nu = 1.0 / 180.0
     return Params(lx=4 * PI, ly=2 * PI, lz=1.0, nx=nx, ny=ny, nz=nz, zstretch=1.0,
                   ochannel=1, dp_opt=1, cds=3, issk=1, dts=2, nu=nu, alpha=nu / 0.71,
-                  got=got, dt=1e-3, imax=1000, isscalar=1, tbot=-1.0, ttop=0.0,
+                  got=got, dt=1e-3, imax=1000, isscalar=1, tbc_bot=1, tbot=1.0, ttop=0.0,
                   precision=precision)
 
 
@@ -233,6 +240,15 @@ def config_ekman(nx=64, ny=64, nz=65, precision=PREC_FP64) -> Params:
                   ochannel=1, dp_opt=3, cds=2, dts=2, nu=0.0025, alpha=0.0025 / 0.71,
                   fc=0.005, ug=1.0, vg=0.0, dt=0.1, imax=50, isscalar=0, isdamp=0,
                   precision=precision)
+
+
+def t_line(p: Params, z):
+    """The linear temperature between the walls that the bottom condition allows:
+    from tbot at z = 0 to ttop at z = lz (fixed wall temperatures), or with the
+    wall gradient dT/dz = tbot up to ttop at z = lz (tbc_bot = 1)."""
+    if p.tbc_bot:
+        return p.ttop - p.tbot * (p.lz - z)
+    return p.tbot + (p.ttop - p.tbot) * z / p.lz
 
 
 def mesh(p: Params):

@@ -70,16 +70,23 @@ def wall_friction(prof: Dict[str, np.ndarray], p: Params) -> Dict[str, float]:
 def heat_flux(prof: Dict[str, np.ndarray], p: Params) -> Dict[str, np.ndarray]:
     """Wall-normal heat flux: the turbulent part <t'w'> per level, the molecular part
     -alpha dT/dz at the faces between levels, and the wall fluxes through the
-    Dirichlet ghosts t(0) = 2 tbot - t(1), t(nz+1) = 2 ttop - t(nz)
-    (src/module_boundary.f90:176-183)."""
+    ghosts t(0) = 2 tbot - t(1), t(nz+1) = 2 ttop - t(nz) (src/module_boundary.f90:
+    176-183); with a fixed bottom gradient (tbc_bot = 1) the bottom flux is the
+    prescribed -alpha tbot and the bottom-wall temperature t(1) - tbot dz(1)/2 is
+    the quantity the flow sets. Also the two wall temperatures."""
     m = mesh(p)
     T = prof["T"]
     dzt = m["dz_t"][2:p.nz + 1]               # distance between centres k and k+1
     mol_faces = -p.alpha * np.diff(T) / dzt
-    q_bot = -p.alpha * (T[0] - p.tbot) / (0.5 * m["dz"][2])
+    if p.tbc_bot:
+        q_bot = -p.alpha * p.tbot
+        t_bot = T[0] - 0.5 * p.tbot * m["dz"][2]
+    else:
+        q_bot = -p.alpha * (T[0] - p.tbot) / (0.5 * m["dz"][2])
+        t_bot = p.tbot
     q_top = -p.alpha * (p.ttop - T[-1]) / (0.5 * m["dz"][p.nz + 1])
     return {"turbulent": prof["tw"].copy(), "molecular_faces": mol_faces, "wall_bottom": float(q_bot),
-            "wall_top": float(q_top)}
+            "wall_top": float(q_top), "t_wall_bottom": float(t_bot), "t_wall_top": float(p.ttop)}
 
 
 def relative_difference(a: Dict[str, np.ndarray], b: Dict[str, np.ndarray], keys=("U", "uu", "vv", "ww", "uw")):

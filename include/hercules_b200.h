@@ -98,7 +98,12 @@ typedef struct hc_params {
      * per column without the coalescing tiles, >= 32 one thread per column with
      * that many threads a block */
     int    tile[4];
-    int    reserved[3];
+    /* bottom temperature condition (not in the reference, which fixes T): 0 the
+     * wall temperature tbot (src/module_boundary.f90:176-183); 1 a fixed
+     * wall-normal gradient dT/dz = tbot at the bottom wall, i.e. the fixed heat
+     * flux alpha*tbot (tbot > 0 cools the fluid from below) */
+    int    tbc_bot;
+    int    reserved[2];
 } hc_params;
 
 /*
@@ -249,12 +254,18 @@ int hc_ensemble_destroy(hc_ensemble* e);
  * may be called again with other seeds. Any call that changes the state
  * (hc_step, hc_upload*, hc_initialize, hc_set_grid, hc_set_body_force)
  * invalidates the checkpoints (HC_ERR_STATE). Built for FP64 storage, cds = 1
- * or 2, dp_opt = 1 or 3, isscalar = 0, isdamp = 0, nz <= 256; else
+ * or 2, dp_opt = 1 or 3, isdamp = 0, nz <= 256, and with temperature
+ * (isscalar = 1) for a constant Richardson number (is_ri_var = 0); else
  * HC_ERR_UNSUPPORTED. With AB2 (dts = 1) the gradient with respect to the
- * starting histories is not returned. hc_adjoint is the two calls in one. */
+ * starting histories is not returned. hc_adjoint is the two calls in one.
+ * hc_adjoint_reverse_t adds the temperature: lt seeds <lt, t_N> in J and gt
+ * receives the gradient with respect to the starting temperature (NULL = none;
+ * either non-NULL without temperature is HC_ERR_ARG). */
 int hc_adjoint_forward(hc_handle* h, int nsteps, int ckpt);
 int hc_adjoint_reverse(hc_handle* h, const double* lu, const double* lv, const double* lw, const double* lp,
                        double* gu, double* gv, double* gw, double* gp, double* gbf);
+int hc_adjoint_reverse_t(hc_handle* h, const double* lu, const double* lv, const double* lw, const double* lp,
+                         const double* lt, double* gu, double* gv, double* gw, double* gp, double* gt, double* gbf);
 int hc_adjoint(hc_handle* h, int nsteps, int ckpt, const double* lu, const double* lv, const double* lw,
                const double* lp, double* gu, double* gv, double* gw, double* gp, double* gbf);
 /* Device time and kernel launches of the last adjoint forward pass and reverse

@@ -64,7 +64,8 @@ module module_gpu
         real(c_double) :: ri_end
         integer(c_int) :: precision
         integer(c_int) :: tile(4)
-        integer(c_int) :: reserved(3)
+        integer(c_int) :: tbc_bot         ! 0: T = tbot at the bottom wall; 1: dT/dz = tbot there
+        integer(c_int) :: reserved(2)
     end type
 
     ! per-step diagnostics (screen_cpu_time, screen_div_error, calculate_ubar)
@@ -230,6 +231,14 @@ module module_gpu
             real(c_double), intent(in) :: lu(*), lv(*), lw(*), lp(*)      ! seeds dJ/d(field at step N)
             real(c_double), intent(out) :: gu(*), gv(*), gw(*), gp(*)     ! dJ/d(field at step 0)
             real(c_double), intent(out) :: gbf(*)                         ! dJ/d(body force), 3*nx*ny*nz
+        end function
+        integer(c_int) function hc_adjoint_reverse_t(h, lu, lv, lw, lp, lt, gu, gv, gw, gp, gt, gbf) &
+                bind(C, name="hc_adjoint_reverse_t")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: lu(*), lv(*), lw(*), lp(*), lt(*)   ! seeds, t included
+            real(c_double), intent(out) :: gu(*), gv(*), gw(*), gp(*), gt(*)  ! gradients, t included
+            real(c_double), intent(out) :: gbf(*)
         end function
         integer(c_int) function hc_adjoint(h, n, ckpt, lu, lv, lw, lp, gu, gv, gw, gp, gbf) &
                 bind(C, name="hc_adjoint")

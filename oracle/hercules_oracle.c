@@ -403,7 +403,10 @@ static void get_t_eqn_coeff(or_state* s, double* aa, cplx* bb, double* cc)
             for (int i = 1; i <= s->nx; ++i) {
                 cplx kx = tb.x[i], ky = tb.y[j];
                 C(bb, i, j, k) = -kx - ky - aa[k] - cc[k];
-                if (k == s->kstr3) { C(bb, i, j, k) = C(bb, i, j, k) - aa[k]; aa[k] = 0.0; }
+                /* the ghost T(ks-1) folds into the diagonal with -1 (fixed T) or +1
+                 * (fixed gradient); aa is cleared inside the loop, so only the first
+                 * mode, the mean, receives the fold (as in the reference) */
+                if (k == s->kstr3) { C(bb, i, j, k) = C(bb, i, j, k) + (s->prm.tbc_bot ? aa[k] : -aa[k]); aa[k] = 0.0; }
                 if (k == s->kend3) { C(bb, i, j, k) = C(bb, i, j, k) - cc[k]; cc[k] = 0.0; }
             }
     }
@@ -505,13 +508,16 @@ static void update_boundary_p(or_state* s, double* p)
     if (s->prm.cds != 3) comm_bound(s, p);
 }
 
-/* update_boundary_t :167-196 */
+/* update_boundary_t :167-196. tbc_bot = 1 (not in the reference): the bottom
+ * ghost continues T with the fixed wall gradient tbot, T(ks-1) = T(ks) - tbot dz_b(ks). */
 static void update_boundary_t(or_state* s, double* t)
 {
+    const double gb = s->prm.tbot * s->dz_b[s->kstr3];
     for (int j = s->jstr3; j <= s->jend3; ++j)
         for (int i = s->istr3; i <= s->iend3; ++i) {
             F(t, i, j, s->kend3 + 1) = 2.0 * s->prm.ttop - F(t, i, j, s->kend3);
-            F(t, i, j, s->kstr3 - 1) = 2.0 * s->prm.tbot - F(t, i, j, s->kstr3);
+            F(t, i, j, s->kstr3 - 1) = s->prm.tbc_bot ? F(t, i, j, s->kstr3) - gb
+                                                      : 2.0 * s->prm.tbot - F(t, i, j, s->kstr3);
         }
     if (s->prm.cds != 3) comm_bound(s, t);
 }
@@ -581,11 +587,18 @@ static void update_boundary_thxyz(or_state* s)
             F(s->thz, i, j, ke) = tt;
             F(s->thz, i, j, ke + 1) = -F(s->thz, i, j, ke - 1) + 2.0 * tt;
         }
+    const double gb = tb * s->dz_b[ks];
     for (int j = s->jstr3; j <= s->jend3; ++j)
         for (int i = s->istr3; i <= s->iend3; ++i) {
-            F(s->thx, i, j, ks - 1) = -F(s->thx, i, j, ks) + 2.0 * tb;
-            F(s->thy, i, j, ks - 1) = -F(s->thy, i, j, ks) + 2.0 * tb;
-            F(s->thz, i, j, ks - 1) = tb;
+            if (s->prm.tbc_bot) {   /* fixed gradient: the ghost and the wall value continue T linearly */
+                F(s->thx, i, j, ks - 1) = F(s->thx, i, j, ks) - gb;
+                F(s->thy, i, j, ks - 1) = F(s->thy, i, j, ks) - gb;
+                F(s->thz, i, j, ks - 1) = F(s->t, i, j, ks) - 0.5 * gb;
+            } else {
+                F(s->thx, i, j, ks - 1) = -F(s->thx, i, j, ks) + 2.0 * tb;
+                F(s->thy, i, j, ks - 1) = -F(s->thy, i, j, ks) + 2.0 * tb;
+                F(s->thz, i, j, ks - 1) = tb;
+            }
         }
     if (s->prm.cds != 3) { comm_bound(s, s->thx); comm_bound(s, s->thy); comm_bound(s, s->thz); }
 }
@@ -857,7 +870,10 @@ static void thomas_with_flags(or_state* s, cplx* c_src, cplx* c_out, int zstagge
     }
     if (tbnd == 1) {
         double aa_t_zstr = -0.5 * s->rk_c * s->prm.dt * s->prm.alpha / s->dz[s->kstr3] / s->dz_b[s->kstr3];
-        C(c_src, 1, 1, 1) = C(c_src, 1, 1, 1) - 2.0 * aa_t_zstr * s->prm.tbot;
+        if (s->prm.tbc_bot)   /* T(ks-1) = T(ks) - tbot dz_b(ks): the constant part moves to the source */
+            C(c_src, 1, 1, 1) = C(c_src, 1, 1, 1) + aa_t_zstr * s->prm.tbot * s->dz_b[s->kstr3];
+        else
+            C(c_src, 1, 1, 1) = C(c_src, 1, 1, 1) - 2.0 * aa_t_zstr * s->prm.tbot;
         double cc_t_zend = -0.5 * s->rk_c * s->prm.dt * s->prm.alpha / s->dz[s->kend3] / s->dz_t[s->kend3];
         C(c_src, 1, 1, nz) = C(c_src, 1, 1, nz) - 2.0 * cc_t_zend * s->prm.ttop;
     }
@@ -1508,7 +1524,7 @@ or_state* or_create(const hc_params* prm, int* err)
     /* initiate_parameters checks (src/module_parameters.f90:266-270) */
     if (prm->nx % 2 != 0 || prm->ny % 2 != 0 || prm->nx < 4 || prm->ny < 4 || prm->nz < 3 ||
         (prm->cds < 1 || prm->cds > 3) || (prm->dts != 1 && prm->dts != 2) ||
-        (prm->isscalar != 0 && prm->isscalar != 1)) {
+        (prm->isscalar != 0 && prm->isscalar != 1) || (prm->tbc_bot != 0 && prm->tbc_bot != 1)) {
         if (err) *err = HC_ERR_PARAM;
         return NULL;
     }

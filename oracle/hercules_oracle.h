@@ -9,7 +9,8 @@
  * MPI + FFTW 3.3.4 + 2DECOMP&FFT) cannot be compiled in this image (no gfortran,
  * no MPI) and ships no golden vectors or tests. The restatement is pinned instead
  * by analytic known-answer tests derived from the reference's own discretisation
- * (tests/test_oracle_kat.py) and by the fixtures in tests/golden/.
+ * (tests/test_oracle_kat.py); the fixtures in tests/golden/ (written by this
+ * oracle) guard it against regressions.
  */
 #ifndef HERCULES_ORACLE_H
 #define HERCULES_ORACLE_H

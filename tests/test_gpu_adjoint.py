@@ -215,3 +215,98 @@ def test_adjoint_matches_torch_autograd(engine, case):
         ref = x.grad.numpy()
         err = np.max(np.abs(g[k] - ref)) / np.max(np.abs(ref))
         assert err <= 1e-10, (k, err)
+
+
+FIELDS_T = FIELDS + ("t",)
+
+
+def _run_t(engine, p, fields, bf, nsteps):
+    c = engine.Channel(p)
+    c.load(fields)
+    c.set_body_force(*bf)
+    c.initialize()
+    c.step(nsteps)
+    out = {f: c.download(f) for f in FIELDS_T}
+    c.close()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [
+    dict(cds=2, dts=2, dp_opt=1, ochannel=0, got=0.8),
+    dict(cds=1, dts=2, dp_opt=3, ochannel=1, got=0.5, fc=0.5, ug=1.0, vg=0.2),
+    dict(cds=2, dts=1, dp_opt=1, ochannel=0, got=0.8, u_mrf=0.3),
+    dict(cds=1, dts=1, dp_opt=1, ochannel=1, got=-0.4),
+    dict(cds=2, dts=2, dp_opt=1, ochannel=1, got=0.6, tbc_bot=1, tbot=0.4, ttop=0.0),
+], ids=["fd4_rk3_closed", "fd2_rk3_ekman", "fd4_ab2_mrf", "fd2_ab2_unstable", "fd4_rk3_wall_flux"])
+def test_adjoint_with_temperature_matches_central_differences(engine, case):
+    """Stratified channels (constant Richardson number, buoyancy got T in the w
+    equation): the gradient of <seeds, (u, v, w, p, T)_N> with respect to the
+    starting u, v, w, p, T and the body force against FP64 central differences in
+    random directions of all of them."""
+    p = Params(**{**SMALL, **case, "isscalar": 1})
+    fields = inputs.small_random(p, seed=51)
+    fields = {f: fields[f] for f in FIELDS_T}
+    bf = inputs.gaussian_body_force(p, seed=52, amp=0.02)
+    seeds = _random_seeds(p, 53)
+    seeds["t"] = np.random.default_rng(54).standard_normal((p.nz, p.ny, p.nx))
+    nsteps, eps = 5, 1e-6
+    c = engine.Channel(p)
+    c.load(fields)
+    c.set_body_force(*bf)
+    c.initialize()
+    g = c.adjoint(nsteps, seeds, ckpt=2)
+    c.close()
+    assert set(g) >= set(FIELDS_T)
+    rng = np.random.default_rng(55)
+    errs = []
+    for _ in range(3):
+        d = _direction(p, rng)
+        d["t"] = rng.standard_normal((p.nz, p.ny, p.nx))
+        plus = {f: fields[f] + eps * d[f] for f in FIELDS_T}
+        minus = {f: fields[f] - eps * d[f] for f in FIELDS_T}
+        bfp = tuple(bf[q] + eps * d[k] for q, k in enumerate(("fx", "fy", "fz")))
+        bfm = tuple(bf[q] - eps * d[k] for q, k in enumerate(("fx", "fy", "fz")))
+        jp = _objective(_run_t(engine, p, plus, bfp, nsteps), seeds)
+        jm = _objective(_run_t(engine, p, minus, bfm, nsteps), seeds)
+        fd = (jp - jm) / (2 * eps)
+        ad = sum(float(np.sum(g[k] * d[k])) for k in FIELDS_T + ("fx", "fy", "fz"))
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    assert max(errs) <= 1e-6, errs
+
+
+@pytest.mark.gpu
+def test_adjoint_wall_heat_flux_per_field(engine):
+    """The mean bottom-wall heat flux after 8 steps of a stably stratified closed
+    channel: each of the T- and velocity-parts of the gradient separately against
+    central differences (a direction in T alone, then in u, v, w alone), and the
+    same gradient from two checkpoint spacings."""
+    p = Params(**{**SMALL, "cds": 2, "dts": 2, "dp_opt": 1, "ochannel": 0, "got": 1.0, "isscalar": 1})
+    fields = inputs.small_random(p, seed=61)
+    fields = {f: fields[f] for f in FIELDS_T}
+    bf = inputs.gaussian_body_force(p, seed=62, amp=0.02)
+    seeds = {"t": adjoint.wall_heat_flux_seed(p)}
+    gs = []
+    for ckpt in (3, 8):
+        c = engine.Channel(p)
+        c.load(fields)
+        c.set_body_force(*bf)
+        c.initialize()
+        gs.append(c.adjoint(8, seeds, ckpt=ckpt))
+        c.close()
+    for k in gs[0]:
+        assert np.allclose(gs[0][k], gs[1][k], rtol=1e-12, atol=1e-16), k
+    g = gs[0]
+    rng = np.random.default_rng(63)
+    eps = 1e-6
+    for part in (("t",), ("u", "v", "w")):
+        d = {f: (rng.standard_normal((p.nz, p.ny, p.nx)) if f in part else np.zeros((p.nz, p.ny, p.nx)))
+             for f in FIELDS_T}
+        d["w"][-1] = 0.0
+        plus = {f: fields[f] + eps * d[f] for f in FIELDS_T}
+        minus = {f: fields[f] - eps * d[f] for f in FIELDS_T}
+        jp = adjoint.wall_heat_flux(_run_t(engine, p, plus, bf, 8)["t"], p)
+        jm = adjoint.wall_heat_flux(_run_t(engine, p, minus, bf, 8)["t"], p)
+        fd = (jp - jm) / (2 * eps)
+        ad = sum(float(np.sum(g[k] * d[k])) for k in part)
+        assert abs(ad - fd) <= 1e-6 * abs(fd), (part, ad, fd)

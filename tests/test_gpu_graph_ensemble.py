@@ -57,6 +57,7 @@ def test_ensemble_members_equal_individual_runs(engine):
     for c in ref_ch:
         c.step(6)
     for q, (x, y) in enumerate(zip(ens_ch, ref_ch)):
+        prec = members[q].precision
         for f in ("u", "v", "w", "p", "t", "mean_u"):
             a, b = x.download(f), y.download(f)
             if prec == PREC_MIXED:

@@ -38,6 +38,10 @@ CASES = {
     "fd4_open_damp_scalar": small(ochannel=1, isscalar=1, got=0.3, tbot=-1.0, ttop=0.0,
                                   isdamp=1, nzdamp=6, cdamp=0.7),
     "fd2_closed_damp_full_depth": small(cds=1, isdamp=1, nzdamp=16, cdamp=1.0, isscalar=1, got=0.2),
+    # fixed bottom-cooling flux (dT/dz = tbot at the wall) instead of a fixed wall temperature
+    "fd4_open_scalar_wall_flux": small(ochannel=1, isscalar=1, got=0.5, tbc_bot=1, tbot=0.6, ttop=0.0),
+    "fd2_ab2_damp_wall_flux": small(cds=1, dts=1, isscalar=1, got=0.3, tbc_bot=1, tbot=-0.2, ttop=0.5,
+                                    isdamp=1, nzdamp=5, cdamp=0.6, u_mrf=0.2),
     "fd4_ab2_damp_umrf": small(dts=1, u_mrf=0.3, isdamp=1, nzdamp=3, cdamp=0.5),
 }
 
@@ -88,7 +92,7 @@ def test_config1_full_size_fp64_10_steps(oracle_lib, engine):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["fd4_closed_dp2", "fd4_open_scalar", "fd4_open_damp_scalar"])
+@pytest.mark.parametrize("name", ["fd4_closed_dp2", "fd4_open_scalar", "fd4_open_damp_scalar", "fd4_open_scalar_wall_flux"])
 def test_fd_mixed_precision_10_steps(name, oracle_lib, engine):
     p = CASES[name].replace(precision=PREC_MIXED)
     fields = inputs.small_random(p, seed=3)

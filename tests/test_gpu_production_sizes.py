@@ -167,6 +167,7 @@ STRIP = {
     "fd2_open_scalar": _fd(64, 48, 17, cds=1, ochannel=1, isscalar=1, got=0.7, tbot=-1.0, ttop=0.0),
     "fd4_ab2_scalar_partial_tiles": _fd(160, 40, 9, dts=1, isscalar=1, got=0.3, tile=[0, 0, 4, 0]),
     "fd4_open_dp1": _fd(64, 32, 12, ochannel=1),
+    "fd4_closed_scalar_wall_flux": _fd(64, 32, 17, isscalar=1, got=0.4, tbc_bot=1, tbot=0.5, ttop=1.0),
 }
 
 

@@ -38,6 +38,10 @@ SP_CASES = {
     "sp_ab2_skew_scalar": sp(dts=1, issk=1, isscalar=1, got=0.3),
     "sp_radix_3_5": sp(nx=40, ny=36, nz=9, isscalar=1, got=0.1),
     "sp_ri_var": sp(ochannel=1, isscalar=1, is_ri_var=1, ri_str=0.1, ri_end=1.0, imax=20),
+    # fixed bottom-cooling flux (dT/dz = tbot at the wall), the stratified open channel
+    "sp_open_scalar_wall_flux": config_open_channel_spectral(nx=32, ny=24, nz=17).replace(
+        tbc_bot=1, tbot=0.6, ttop=0.0),
+    "sp_closed_ab2_wall_flux_umrf": sp(dts=1, isscalar=1, got=0.3, tbc_bot=1, tbot=0.3, ttop=0.5, u_mrf=0.2),
 }
 
 
@@ -95,7 +99,7 @@ def test_spectral_state_is_truncated(engine):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["sp_open_scalar_skew", "sp_open_damp_scalar"])
+@pytest.mark.parametrize("name", ["sp_open_scalar_skew", "sp_open_damp_scalar", "sp_open_scalar_wall_flux"])
 def test_spectral_mixed_precision_10_steps(name, oracle_lib, engine):
     p = SP_CASES[name].replace(precision=PREC_MIXED)
     o, od, rc, c, gd = run_pair(p, _fields(p, 3), 10, oracle_lib, engine)

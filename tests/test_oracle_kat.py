@@ -192,3 +192,67 @@ def test_nan_input_stops_with_error(oracle_lib):
     o.initialize()
     rc, d = o.step(2)
     assert rc == -5
+
+
+def _linear_t(p, g, t0=0.3):
+    """A wall-normal T profile with the discrete gradient g between all centres,
+    T(k+1) = T(k) + g dz_t(k), and the top-wall value ttop that makes the ghost
+    2 ttop - T(nz-1) continue it."""
+    m = mesh(p)
+    dzt = m["dz_t"][2:p.nz + 2]
+    tz = t0 + g * np.concatenate([[0.0], np.cumsum(dzt[:-1])])
+    return tz, tz[-1] + 0.5 * g * dzt[-1]
+
+
+@pytest.mark.parametrize("dts", [1, 2])
+@pytest.mark.parametrize("tbc_bot", [0, 1])
+def test_conduction_profile_with_wall_gradient_is_steady(oracle_lib, dts, tbc_bot):
+    """Poiseuille flow over a linear temperature profile on a stretched grid: the
+    nonlinear terms vanish, the discrete diffusion of a linear profile vanishes
+    at every level once the bottom ghost continues it, and the buoyancy of a
+    horizontally uniform T is balanced by the pressure, so the step must leave
+    T unchanged. tbc_bot = 1 prescribes the gradient itself (tbot = dT/dz), the
+    reference's fixed wall temperature the wall value of the same line."""
+    g = 0.8
+    p = small(dts=dts, dp_opt=1, zstretch=1.5, isscalar=1, got=0.5, tbc_bot=tbc_bot)
+    tz, ttop = _linear_t(p, g)
+    dzb0 = mesh(p)["dz_b"][2]
+    p = p.replace(ttop=ttop, tbot=g if tbc_bot else tz[0] - 0.5 * g * dzb0)
+    uz = _discrete_poiseuille(p)
+    shape = (p.nz, p.ny, p.nx)
+    f = {"u": np.broadcast_to(uz[:, None, None], shape).copy(), "v": np.zeros(shape),
+         "w": np.zeros(shape), "p": np.zeros(shape), "t": np.broadcast_to(tz[:, None, None], shape).copy()}
+    if dts == 1:
+        f.update(ff=np.ones(shape), gg=np.zeros(shape), hh=np.zeros(shape), ss=np.zeros(shape))
+    o = oracle_lib.Oracle(p)
+    o.load(f)
+    o.initialize()
+    rc, d = o.step(4)
+    assert rc == 0
+    assert np.abs(o.get("t") - f["t"]).max() < 1e-12 * np.abs(f["t"]).max()
+    assert np.abs(o.get("w")).max() < 1e-10
+    o.close()
+
+
+def test_wall_gradient_condition_changes_the_mean_temperature(oracle_lib):
+    """A uniform temperature under the two bottom conditions: a fixed wall value
+    below it cools the first level, a fixed gradient g > 0 (heat leaving through
+    the wall) cools it too, by a different amount, and levels far from the wall
+    stay untouched after one step in both."""
+    shape_p = small(isscalar=1, got=0.0, nz=17, ttop=1.0)
+    shape = (shape_p.nz, shape_p.ny, shape_p.nx)
+    f = {"u": np.zeros(shape), "v": np.zeros(shape), "w": np.zeros(shape), "p": np.zeros(shape),
+         "t": np.ones(shape)}
+    out = {}
+    for tbc_bot, tbot in ((0, 0.0), (1, 0.5)):
+        o = oracle_lib.Oracle(shape_p.replace(tbc_bot=tbc_bot, tbot=tbot, dp_opt=1))
+        o.load(f)
+        o.initialize()
+        rc, _ = o.step(1)
+        assert rc == 0
+        out[tbc_bot] = o.get("t").mean(axis=(1, 2))
+        o.close()
+    for t in out.values():
+        assert t[0] < 1.0 - 1e-6
+        assert np.abs(t[6:11] - 1.0).max() < 1e-12
+    assert abs(out[0][0] - out[1][0]) > 1e-6
