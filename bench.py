@@ -164,14 +164,19 @@ ALG_WORDS_SUB = {
     # FD path, neutral: RHS reads u,v,w,p,ff,gg,hh, writes qu,qv,qw,ff,gg,hh; the
     # column kernel reads 3 spectra, writes u,v,w,psi; the x inverse also reads p (+=)
     "fd": {"rhs_momentum": 13, "fft_x_r2c": 6, "fft_y_fwd": 6, "column_fd": 7, "fft_y_inv": 8,
-           "fft_x_c2r": 9, "div_check": 3},
+           "fft_x_c2r": 9, "div_check": 3,
+           # the fused 2-D transforms: forward 3 physical fields in, 3 half spectra
+           # out; inverse 4 spectra and p in, u, v, w, p out
+           "fft2d_fwd": 6, "fft2d_inv": 9},
     # spectral path (issk=1, scalar): products read u,v,w,t + 6 derivative images,
     # write 8 (+ 7 for T); assembly reads 4 spectra, 8 product spectra, 3 histories,
     # writes 3 histories + 3 RHS (+ 7 for T); the column kernel reads 3 RHS + p,
     # writes u,v,w,p,phi,div; transforms: 6 derivative + 4 state + 1 T inverse,
     # 8 + 3 forward, each pass reads and writes every field
     "sp": {"spec_products": 25, "fft_x_r2c": 22, "fft_y_fwd": 22, "spec_assemble": 28, "column_fd": 10,
-           "column_t": 2, "fft_y_inv": 22, "fft_x_c2r": 22, "div_check": 4, "aux": 9},
+           "column_t": 2, "fft_y_inv": 22, "fft_x_c2r": 22, "div_check": 4, "aux": 9,
+           # fused 2-D transforms: 11 fields each way, one word in and one out
+           "fft2d_fwd": 22, "fft2d_inv": 22},
 }
 
 
@@ -191,22 +196,26 @@ TRAFFIC = {(w, k): v * (WORKLOADS[w][0] * WORKLOADS[w][1] * WORKLOADS[w][2]) / (
 STATS_WINDOW = 16
 
 
-def stats_bytes_per_point(kind: str, wbytes: int) -> float:
+def stats_bytes_per_point(kind: str, wbytes: int, with_t: bool = True) -> float:
     """Bytes per point and step the statistics kernel must move: u, v, w, t (and the
     uhx, vhy snapshots on the FD path) in the storage type, and the 11 accumulators
     read and written -- FP64 sums with FP64 storage; with FP32 storage FP32 window
     sums, plus once a window the fold (window read, FP64 sum read and written,
-    window cleared)."""
-    reads = (6 if kind == "fd" else 4) * wbytes
+    window cleared). Without a temperature equation T is frozen: its three terms
+    are added on request from T and mean_w, and a step moves 8 accumulators and
+    no T."""
+    nacc = 11 if with_t else 8
+    reads = ((6 if kind == "fd" else 4) - (0 if with_t else 1)) * wbytes
     if wbytes == 8:
-        return reads + 11 * 2 * 8
-    return reads + 11 * 2 * 4 + 11 * (4 + 16 + 4) / STATS_WINDOW
+        return reads + nacc * 2 * 8
+    return reads + nacc * 2 * 4 + nacc * (4 + 16 + 4) / STATS_WINDOW
 
 
 def alg_bytes_step(kernel: str, npts: int, wbytes: int, kind: str, nsub: int = 3) -> float:
-    """Algorithmic bytes of one time step in one kernel category."""
+    """Algorithmic bytes of one time step in one kernel category (the FD workloads
+    are neutral, the spectral ones carry temperature)."""
     if kernel == "stats":
-        return npts * stats_bytes_per_point(kind, wbytes)
+        return npts * stats_bytes_per_point(kind, wbytes, with_t=kind != "fd")
     if kind == "fd" and kernel == "div_check":
         # sub-steps 1 and 2 check the divergence inside the next momentum RHS; the
         # separate check runs once a step, after the last sub-step
@@ -602,7 +611,8 @@ def main():
                      "dtype": "f32 fields/FFT + f64 Thomas",
                      "config": {"workload": "ensemble64", "members": 64, "total_points": r[PREC_MIXED]["npts"],
                                 "physics": "stratified closed channels, FD4, RK3, dp_opt=1, one CUDA graph per step",
-                                "parallelism": "one GPU, members as concurrent graph branches"},
+                                "parallelism": "one GPU: each kernel of a stage launched once over all members "
+                                               "(grouped launches), one CUDA graph per step"},
                      "fp64": {"value": r[PREC_FP64]["value"], "ms_per_step": r[PREC_FP64]["ms_per_step"]},
                      "mixed_speedup_vs_fp64": r[PREC_FP64]["ms_per_step"] / r[PREC_MIXED]["ms_per_step"],
                      "gpu_launches": int(r[PREC_MIXED]["launches"]), "clocks": r[PREC_MIXED]["clocks"],

@@ -468,13 +468,15 @@ __global__ void __launch_bounds__(256) k_t_adj_interp(AdjTArgs m)
     const double dta = m.ph.dt * m.rk_a;
     auto L = [&](long long q) { return dta * __ldg(m.lqt + q) + __ldg(m.lss_out + q); };
     m.lss_prev[id] = m.ph.dt * m.rk_b * m.lqt[id];
-    // the x (y) differences at i - off read the flux of face i
+    // the T fluxes sit one point lower than the momentum ones the Dif offsets
+    // describe: tux(i) = (-F(i+1) + 27 F(i) - 27 F(i-1) + F(i-2)) / 24 dx, so the
+    // difference at i + 1 - off reads the flux of face i
     double sx = 0.0, sy = 0.0;
 #pragma unroll
     for (int q = 0; q < Dif<CDS>::n; ++q) {
-        const int o = Dif<CDS>::off(q);
-        sx += Dif<CDS>::c(q) / g.dx * L(N.at(-o, 0));
-        sy += Dif<CDS>::c(q) / g.dy * L(N.at(0, -o));
+        const int o = 1 - Dif<CDS>::off(q);
+        sx += Dif<CDS>::c(q) / g.dx * L(N.at(o, 0));
+        sy += Dif<CDS>::c(q) / g.dy * L(N.at(0, o));
     }
     const Acc<double>& A = m.a;
     const double thx = A.template thx<CDS>(i, j, k), thy = A.template thy<CDS>(i, j, k);

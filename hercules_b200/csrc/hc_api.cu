@@ -20,6 +20,7 @@
 #include "hc_common.cuh"
 #include "hc_fd.cuh"
 #include "hc_fft_t.cuh"
+#include "hc_fft2d.cuh"
 #include "hc_column.cuh"
 #include "hc_rhs_tiled.cuh"
 #include "hc_rhs_tiled2.cuh"
@@ -195,11 +196,11 @@ enum { F_U, F_V, F_W, F_P, F_T, F_FF, F_GG, F_HH, F_SS, F_QU, F_QV, F_QW, F_UHX,
 // kernel categories for the optional per-launch CUDA-event profile
 enum { K_BEGIN, K_RHS_MOM, K_FFT_X_FWD, K_FFT_Y_FWD, K_COLUMN, K_FFT_Y_INV, K_FFT_X_INV,
        K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_SPEC_PROD, K_SPEC_ASM, K_SPEC_AUX, K_ADJ_COLUMN,
-       K_ADJ_RHS, K_NCAT };
+       K_ADJ_RHS, K_FFT2D_FWD, K_FFT2D_INV, K_NCAT };
 static const char* K_NAMES[K_NCAT] = {"substep_begin", "rhs_momentum", "fft_x_r2c", "fft_y_fwd", "column_fd",
                                       "fft_y_inv", "fft_x_c2r", "rhs_temperature", "column_t", "div_check",
                                       "stats", "finalize", "spec_products", "spec_assemble", "aux", "adj_column",
-                                      "adj_rhs"};
+                                      "adj_rhs", "fft2d_fwd", "fft2d_inv"};
 
 // spectral-path buffers (cds = 3), each n values of the storage type: the half
 // spectra of the state and histories, phi, the divergence, the assembled
@@ -249,6 +250,10 @@ struct hc_handle {
     double* mean[11];
     float* win[11];          // FP32 storage: the FP32 window sums of the mean accumulators
     double* mtmp;            // FP32 storage: FP64 sums + window, assembled for a download
+    // no temperature equation and no damping: T never changes, so the statistics
+    // kernel leaves out mean_t, mean_tt, mean_tw and tstat_flush adds them on request
+    int tdefer;
+    double* mw0;             // mean_w sums at the last flush
     double* zbuf;            // 5*(nz+4) doubles, then zm5d (5*nz doubles) and zm5 (5*nz floats)
     double* zm5d;            // FP64 per-level metrics of the strip RHS
     float* zm5;              // FP32 per-level metrics of the strip RHS
@@ -270,6 +275,7 @@ struct hc_handle {
     double2* twbuf;
     void* twt;               // the same tables in the storage precision (FP64: twbuf)
     int fft_tx, fft_ty;      // 1: the compile-time-length kernels serve x / y
+    int fft2d;               // 1: the fused 2-D transform kernels (hc_fft2d.cuh) serve both
     FftPlan px, py;
     double2* wpack;
     int rows_x, tl_y, col_threads, col_warp;
@@ -617,6 +623,58 @@ template <typename R> static int fft_t_dispatch(hc_handle* h, int n, int op, con
     return HC_ERR_UNSUPPORTED;
 }
 
+// ---------------------------------------------------------------------------
+// fused 2-D transforms (hc_fft2d.cuh): one cluster of C CTAs a (field, plane).
+// Shapes: nx/2, ny, C, threads a CTA, resident CTAs an SM with FP32 / FP64 storage
+// ---------------------------------------------------------------------------
+#define HC_FFT2D_SHAPES(X) X(256, 384, 16, 384, 2, 1) X(128, 256, 8, 256, 3, 1) X(128, 192, 8, 256, 3, 1)
+
+template <typename R, int NXH, int NY, int C, int NT, int MINB>
+static int fft2d_op(hc_handle* h, int op, const F2Args<R>* a, int nf)
+{
+    typedef F2Shape<R, NXH, NY, C, NT, MINB> S;
+    void (*fwd)(F2Args<R>) = k_fft2d_fwd<R, NXH, NY, C, NT, MINB>;
+    void (*inv)(F2Args<R>) = k_fft2d_inv<R, NXH, NY, C, NT, MINB>;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = S::smem;
+    cfg.stream = h->st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (op == 0) {
+        // shared-memory limit and cluster size; usable only if a cluster fits the device
+        for (int q = 0; q < 2; ++q) {
+            const void* k = (const void*)(q == 0 ? fwd : inv);
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem) != cudaSuccess) return HC_ERR_UNSUPPORTED;
+            if (C > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return HC_ERR_UNSUPPORTED;
+            int ncl = 0;
+            cfg.gridDim = dim3(C);
+            if (cudaOccupancyMaxActiveClusters(&ncl, k, &cfg) != cudaSuccess || ncl < 1) {
+                cudaGetLastError();
+                return HC_ERR_UNSUPPORTED;
+            }
+        }
+        return HC_OK;
+    }
+    cfg.gridDim = dim3((unsigned)((long long)nf * h->g.nz * C));
+    CK(cudaLaunchKernelEx(&cfg, op == 1 ? fwd : inv, *a));
+    return HC_OK;
+}
+
+// op 0: set up (HC_ERR_UNSUPPORTED: no fused shape for this grid); 1 forward; 2 inverse
+template <typename R> static int fft2d_dispatch(hc_handle* h, int op, const F2Args<R>* a, int nf)
+{
+    const int nxh = h->g.nxh, ny = h->g.ny;
+#define HC_F2_CASE(NXH, NY, C, NT, M32, M64) \
+    if (nxh == NXH && ny == NY) return fft2d_op<R, NXH, NY, C, NT, sizeof(R) == sizeof(float) ? M32 : M64>(h, op, a, nf);
+    HC_FFT2D_SHAPES(HC_F2_CASE)
+#undef HC_F2_CASE
+    return HC_ERR_UNSUPPORTED;
+}
+
 template <typename R> static int fft_t_setup(hc_handle* h)
 {
     int rc = HC_OK;
@@ -675,6 +733,12 @@ static int build_fft(hc_handle* h)
     if (h->fft_tx || h->fft_ty) {
         int rc = h->rsz == sizeof(double) ? fft_t_setup<double>(h) : fft_t_setup<float>(h);
         if (rc != HC_OK) return rc;
+    }
+    // the fused transforms where a shape exists (and no explicit tile asks for the others)
+    h->fft2d = 0;
+    if (h->fft_tx && h->fft_ty) {
+        const int rc = h->rsz == sizeof(double) ? fft2d_dispatch<double>(h, 0, nullptr, 0) : fft2d_dispatch<float>(h, 0, nullptr, 0);
+        h->fft2d = rc == HC_OK;
     }
     const size_t c2 = 2 * h->rsz;     // bytes of one complex
     h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : (h->rsz == sizeof(double) ? 1024 : 2048) / nxh;
@@ -785,6 +849,19 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
     typedef typename V2<R>::T T2;
     const int* halt = &h->sc->nan_flag;
     if (nf < 1 || nf > HC_FFT_MAXF) return HC_ERR_ARG;
+    if (h->fft2d && !h->rec && nf <= HC_FFT_TMAXF) {
+        F2Args<R> a;
+        memset(&a, 0, sizeof(a));
+        for (int f = 0; f < nf; ++f) { a.in[f] = in[f]; a.out[f] = out[f]; }
+        a.nz = h->g.nz;
+        a.twx = fft_tw<R>(h, 0); a.wp = fft_tw<R>(h, 2); a.twy = fft_tw<R>(h, 1);
+        a.scale_x = (R)(1.0 / h->p.nx); a.scale_y = (R)(1.0 / h->p.ny); a.halt = halt;
+        prof_begin(h, K_FFT2D_FWD);
+        int rc = fft2d_dispatch<R>(h, 1, &a, nf);
+        if (rc) return rc;
+        CKL();
+        return HC_OK;
+    }
     if (h->fft_tx) {
         FxArgs<R> a;
         memset(&a, 0, sizeof(a));
@@ -837,6 +914,20 @@ template <typename R> static int fft_inverse(hc_handle* h, typename V2<R>::T* co
 {
     const int* halt = &h->sc->nan_flag;
     if (nf < 1 || nf > HC_FFT_MAXF) return HC_ERR_ARG;
+    if (h->fft2d && !h->rec && nf <= HC_FFT_TMAXF) {
+        // reads the spectra (ysrc, else in) and leaves them as they are
+        F2Args<R> a;
+        memset(&a, 0, sizeof(a));
+        for (int f = 0; f < nf; ++f) { a.in[f] = ysrc ? ysrc[f] : in[f]; a.out[f] = out[f]; a.add[f] = add[f]; }
+        a.nz = h->g.nz;
+        a.twx = fft_tw<R>(h, 0); a.wp = fft_tw<R>(h, 2); a.twy = fft_tw<R>(h, 1);
+        a.scale_x = (R)1; a.scale_y = (R)1; a.halt = halt;
+        prof_begin(h, K_FFT2D_INV);
+        int rc = fft2d_dispatch<R>(h, 2, &a, nf);
+        if (rc) return rc;
+        CKL();
+        return HC_OK;
+    }
     if (h->fft_ty) {
         FyArgs<R> a;
         memset(&a, 0, sizeof(a));
@@ -896,6 +987,7 @@ template <typename R> static int launch_stats(hc_handle* h, int accumulate)
     s.step = &h->sc->step;
     s.window = STATS_WINDOW;
     s.accumulate = accumulate;
+    s.tdefer = h->tdefer ? &h->sc->tstat_n : nullptr;
     s.um = h->p.u_mrf; s.dt = h->p.dt;
     s.part = h->part_st;
     prof_begin(h, K_STATS);
@@ -1894,6 +1986,7 @@ static void free_all(hc_handle* h)
     for (int q = 0; q < 11; ++q) if (h->mean[q]) cudaFree(h->mean[q]);
     for (int q = 0; q < 11; ++q) if (h->win[q]) cudaFree(h->win[q]);
     if (h->mtmp) cudaFree(h->mtmp);
+    if (h->mw0) cudaFree(h->mw0);
     if (h->zbuf) cudaFree(h->zbuf);
     if (h->coef) cudaFree(h->coef);
     if (h->scratch) cudaFree(h->scratch);
@@ -1939,6 +2032,8 @@ int hc_create(const hc_params* p, hc_handle** out)
     h->use_graph = 0; h->gexec = nullptr; h->graph_launches = 0; h->rec = nullptr; h->rhs_strip = 0;
     for (int q = 0; q < 11; ++q) { h->mean[q] = nullptr; h->win[q] = nullptr; }
     h->mtmp = nullptr;
+    h->mw0 = nullptr;
+    h->tdefer = 0;
     h->zbuf = nullptr; h->zm5 = nullptr; h->zm5d = nullptr; h->coef = nullptr; h->scratch = nullptr; h->part_div = nullptr; h->part_st = nullptr;
     h->sc = nullptr; h->diag_dev = nullptr; h->twbuf = nullptr; h->twt = nullptr; h->e0 = nullptr; h->e1 = nullptr; h->st = nullptr;
     h->diag_cap = 0; h->last_ms = 0.0; h->launches = 0; h->initialized = 0;
@@ -1977,6 +2072,11 @@ int hc_create(const hc_params* p, hc_handle** out)
                 if (cudaMalloc(&h->win[q], n * sizeof(float)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
                 if (cudaMemset(h->win[q], 0, n * sizeof(float)) != cudaSuccess) FAIL(HC_ERR_CUDA);
             }
+        }
+        if (p->isscalar == 0 && p->isdamp == 0) {
+            if (cudaMalloc(&h->mw0, n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_NOMEM);
+            if (cudaMemset(h->mw0, 0, n * sizeof(double)) != cudaSuccess) FAIL(HC_ERR_CUDA);
+            h->tdefer = 1;
         }
         if (p->cds == 3) {
             const int nsp = SP_W0 + (p->issk == 1 ? 14 : 8);
@@ -2166,6 +2266,26 @@ static __global__ void k_float_to_double(double* __restrict__ dst, const float* 
 // An interior-only host array (ghost 0, leading dimensions nx, ny) is copied as
 // it is -- straight from the caller's memory, pinned or not -- and converted to
 // the storage type on the device; ghosted arrays are packed on the host first.
+// Adds the deferred temperature terms of the statistics (no temperature
+// equation) to mean_t, mean_tt, mean_tw and restarts the deferral from the
+// current mean_w sums.
+static int tstat_flush(hc_handle* h)
+{
+    if (!h->tdefer) return HC_OK;
+    const long long n = h->g.n;
+    const float* ww = h->win[2];
+    if (h->rsz == sizeof(float))
+        k_tstat_flush<float><<<RED_BLOCKS, 256, 0, h->st>>>((const float*)h->fld[F_T], h->mean[3], h->mean[9], h->mean[10],
+                                                           h->mean[2], ww, h->mw0, &h->sc->tstat_n, h->g.nxy, n);
+    else
+        k_tstat_flush<double><<<RED_BLOCKS, 256, 0, h->st>>>((const double*)h->fld[F_T], h->mean[3], h->mean[9], h->mean[10],
+                                                            h->mean[2], ww, h->mw0, &h->sc->tstat_n, h->g.nxy, n);
+    CK(cudaGetLastError());
+    k_tstat_snap<<<RED_BLOCKS, 256, 0, h->st>>>(h->mw0, h->mean[2], ww, &h->sc->tstat_n, n);
+    CK(cudaGetLastError());
+    return HC_OK;
+}
+
 int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, int ghost)
 {
     if (h) h->adj_ready = 0;     // the adjoint checkpoints no longer describe the state
@@ -2174,6 +2294,8 @@ int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, 
     int is_mean;
     void* d = field_dev(h, field_id, &is_mean);
     if (!d) return HC_ERR_ARG;
+    // deferred temperature statistics are added with the T they were taken with
+    if (field_id == HC_FIELD_T || is_mean) { const int frc = tstat_flush(h); if (frc) return frc; }
     const int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
     const long long n = (long long)nx * ny * nz;
     const bool contiguous = ghost == 0 && ld1 == nx && ld2 == ny;
@@ -2197,6 +2319,10 @@ int hc_upload(hc_handle* h, int field_id, const double* host, int ld1, int ld2, 
         if (!st) return HC_ERR_NOMEM;
         CK(cudaMemcpyAsync(st, src, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
         k_double_to_float<<<RED_BLOCKS, 256, 0, h->st>>>((float*)d, st, n);
+        CK(cudaGetLastError());
+    }
+    if (field_id == HC_FIELD_MEAN_W && h->tdefer) {
+        k_tstat_snap<<<RED_BLOCKS, 256, 0, h->st>>>(h->mw0, h->mean[2], h->win[2], &h->sc->tstat_n, n);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(h->st));
@@ -2224,6 +2350,9 @@ static int spec_source(hc_handle* h, int field_id)
 static void* download_source(hc_handle* h, int field_id, int* is_mean, int* rc)
 {
     *rc = HC_OK;
+    if (field_id == HC_FIELD_MEAN_T || field_id == HC_FIELD_MEAN_TT || field_id == HC_FIELD_MEAN_TW) {
+        if ((*rc = tstat_flush(h)) != HC_OK) return nullptr;
+    }
     const int sid = spec_source(h, field_id);
     if (sid >= 0) {
         *is_mean = 0;
@@ -2311,9 +2440,14 @@ int hc_upload_dev(hc_handle* h, int field_id, const void* dev)
     int is_mean;
     void* d = field_dev(h, field_id, &is_mean);
     if (!d) return HC_ERR_ARG;
+    if (field_id == HC_FIELD_T || is_mean) { const int frc = tstat_flush(h); if (frc) return frc; }
     const size_t bytes = h->g.n * (is_mean ? sizeof(double) : h->rsz);
     CK(cudaMemcpyAsync(d, dev, bytes, cudaMemcpyDeviceToDevice, h->st));
     if (is_mean && h->win[0]) CK(cudaMemsetAsync(h->win[field_id - HC_FIELD_MEAN_U], 0, h->g.n * sizeof(float), h->st));
+    if (field_id == HC_FIELD_MEAN_W && h->tdefer) {
+        k_tstat_snap<<<RED_BLOCKS, 256, 0, h->st>>>(h->mw0, h->mean[2], h->win[2], &h->sc->tstat_n, h->g.n);
+        CK(cudaGetLastError());
+    }
     CK(cudaStreamSynchronize(h->st));
     return HC_OK;
 }

@@ -60,6 +60,7 @@ struct DevScalars {
     double div_max[3];
     int step;            // completed steps
     int nan_flag;
+    int tstat_n;         // statistics steps whose temperature terms are deferred (no temperature equation)
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }

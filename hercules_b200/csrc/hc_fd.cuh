@@ -557,9 +557,44 @@ template <typename R> struct StatsArgs {
     const int* step;                     // completed steps, this one included
     int window;
     int accumulate;
+    // non-null (no temperature equation, T frozen): the temperature terms (mean_t,
+    // mean_tt, mean_tw) are not accumulated; the kernel counts the steps here and
+    // k_tstat_flush adds them later from T and the growth of mean_w
+    int* tdefer;
     double um, dt;
     double* part;                        // per block: sum u*dz, CFL max
 };
+
+// accumulators of the temperature terms (mean_t, mean_tt, mean_tw)
+__host__ __device__ constexpr bool stats_is_t(int a) { return a == 3 || a == 9 || a == 10; }
+
+// The deferred temperature terms of n statistics steps with T frozen:
+// mean_t += n T, mean_tt += n T^2, mean_tw += T (Sw(k) + Sw(k-1)) / 2, where Sw is
+// the growth of the mean_w sums since the last flush (w below the wall is 0).
+template <typename R>
+__global__ void k_tstat_flush(const R* __restrict__ t, double* mt, double* mtt, double* mtw,
+                              const double* __restrict__ mw, const float* __restrict__ ww,
+                              const double* __restrict__ mw0, const int* cnt, long long nxy, long long n)
+{
+    const double nd = (double)*cnt;
+    if (nd == 0.0) return;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const double tv = (double)t[q];
+        const double s0 = mw[q] + (ww ? (double)ww[q] : 0.0) - mw0[q];
+        const double s1 = q >= nxy ? mw[q - nxy] + (ww ? (double)ww[q - nxy] : 0.0) - mw0[q - nxy] : 0.0;
+        mt[q] += nd * tv;
+        mtt[q] += nd * (tv * tv);
+        mtw[q] += tv * 0.5 * (s0 + s1);
+    }
+}
+// after a flush: the mean_w sums it started from, and no step pending
+static __global__ void k_tstat_snap(double* mw0, const double* __restrict__ mw, const float* __restrict__ ww,
+                                    int* cnt, long long n)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        mw0[q] = mw[q] + (ww ? (double)ww[q] : 0.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *cnt = 0;
+}
 
 // FP64 sums plus the pending FP32 window: what the mean accumulators hold
 static __global__ void k_mean_combine(double* __restrict__ dst, const double* __restrict__ tot,
@@ -599,6 +634,8 @@ __device__ __forceinline__ void k_stats_body(const StatsArgs<R>& s, const uint3 
             auto l2 = [](const float* p, long long q) { return *reinterpret_cast<const float2*>(p + q); };
             const double um = s.um;
             const bool fold = s.accumulate && (*s.step % s.window) == 0;
+            const bool skt = s.tdefer != nullptr;
+            if (skt && s.accumulate && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) ++*s.tdefer;
             // ceil(nz / gridDim.y) levels a chunk: the last chunks can start at or past
             // nz, and then read nothing (w below the chunk included)
             float2 wm = (k0 > 0 && k0 < k1) ? l2(s.f.w, (long long)(k0 - 1) * g.nxy + p2) : make_float2(0.0f, 0.0f);
@@ -612,7 +649,7 @@ __device__ __forceinline__ void k_stats_body(const StatsArgs<R>& s, const uint3 
                 ub += (double)u.y * dzk;
                 cfl = fmax(cfl, s.dt * fabs((double)u.y) * rdx + s.dt * fabs((double)v.y) * rdy + s.dt * fabs((double)w.y) / dzk);
                 if (s.accumulate) {
-                    const float2 t = l2(s.f.t, q);
+                    const float2 t = skt ? make_float2(0.0f, 0.0f) : l2(s.f.t, q);
                     const float2 ux = s.uhx_s ? l2(s.uhx_s, q) : u;
                     const float2 vy = s.vhy_s ? l2(s.vhy_s, q) : v;
                     auto c = [&](int a, int e) -> double {
@@ -636,15 +673,18 @@ __device__ __forceinline__ void k_stats_body(const StatsArgs<R>& s, const uint3 
                     if (!fold) {
                         float2 m[11];
 #pragma unroll
-                        for (int a = 0; a < 11; ++a) m[a] = l2(s.win[a], q);
+                        for (int a = 0; a < 11; ++a)
+                            if (!(skt && stats_is_t(a))) m[a] = l2(s.win[a], q);
 #pragma unroll
                         for (int a = 0; a < 11; ++a)
-                            *reinterpret_cast<float2*>(s.win[a] + q) =
-                                make_float2((float)((double)m[a].x + c(a, 0)), (float)((double)m[a].y + c(a, 1)));
+                            if (!(skt && stats_is_t(a)))
+                                *reinterpret_cast<float2*>(s.win[a] + q) =
+                                    make_float2((float)((double)m[a].x + c(a, 0)), (float)((double)m[a].y + c(a, 1)));
                     } else {
                         // end of a window: FP64 sum += window + this step, the window restarts at 0
 #pragma unroll
                         for (int a = 0; a < 11; ++a) {
+                            if (skt && stats_is_t(a)) continue;
                             double2* mp = reinterpret_cast<double2*>(s.mean[a] + q);
                             const float2 wv = l2(s.win[a], q);
                             double2 mv = *mp;
@@ -665,6 +705,8 @@ __device__ __forceinline__ void k_stats_body(const StatsArgs<R>& s, const uint3 
         const double um = s.um;
         // FP32 storage always keeps the FP32 window sums (allocated with the handle)
         const bool fold = sizeof(R) == sizeof(float) && s.accumulate && (*s.step % s.window) == 0;
+        const bool skt = s.tdefer != nullptr;
+        if (skt && s.accumulate && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) ++*s.tdefer;
         double wm = (k0 > 0 && k0 < k1) ? (double)fw[(long long)(k0 - 1) * g.nxy + ij] : 0.0;
         for (int kb = k0; kb < k1; kb += G) {
             // the fields stay in the storage type in registers; products in FP64
@@ -676,7 +718,7 @@ __device__ __forceinline__ void k_stats_body(const StatsArgs<R>& s, const uint3 
                 const long long q = (long long)(in[e] ? kb + e : kb) * g.nxy + ij;
                 u[e] = fu[q]; v[e] = fv[q]; w[e] = fw[q];
                 if (s.accumulate) {
-                    t[e] = ft[q];
+                    t[e] = skt ? R(0) : ft[q];
                     ux[e] = fux ? fux[q] : u[e];
                     vy[e] = fvy ? fvy[q] : v[e];
                 } else {
@@ -721,31 +763,31 @@ __device__ __forceinline__ void k_stats_body(const StatsArgs<R>& s, const uint3 
                 for (int a = 0; a < 11; ++a)
 #pragma unroll
                     for (int e = 0; e < G; ++e)
-                        if (in[e]) m[a][e] = s.mean[a][(long long)(kb + e) * g.nxy + ij];
+                        if (in[e] && !(skt && stats_is_t(a))) m[a][e] = s.mean[a][(long long)(kb + e) * g.nxy + ij];
 #pragma unroll
                 for (int a = 0; a < 11; ++a)
 #pragma unroll
                     for (int e = 0; e < G; ++e)
-                        if (in[e]) s.mean[a][(long long)(kb + e) * g.nxy + ij] = m[a][e] + c(a, e);
+                        if (in[e] && !(skt && stats_is_t(a))) s.mean[a][(long long)(kb + e) * g.nxy + ij] = m[a][e] + c(a, e);
             } else if (!fold) {
                 float m[11][G];
 #pragma unroll
                 for (int a = 0; a < 11; ++a)
 #pragma unroll
                     for (int e = 0; e < G; ++e)
-                        if (in[e]) m[a][e] = s.win[a][(long long)(kb + e) * g.nxy + ij];
+                        if (in[e] && !(skt && stats_is_t(a))) m[a][e] = s.win[a][(long long)(kb + e) * g.nxy + ij];
 #pragma unroll
                 for (int a = 0; a < 11; ++a)
 #pragma unroll
                     for (int e = 0; e < G; ++e)
-                        if (in[e]) s.win[a][(long long)(kb + e) * g.nxy + ij] = (float)((double)m[a][e] + c(a, e));
+                        if (in[e] && !(skt && stats_is_t(a))) s.win[a][(long long)(kb + e) * g.nxy + ij] = (float)((double)m[a][e] + c(a, e));
             } else {
                 // end of a window: FP64 sum += window + this step, the window restarts at 0
 #pragma unroll
                 for (int a = 0; a < 11; ++a)
 #pragma unroll
                     for (int e = 0; e < G; ++e)
-                        if (in[e]) {
+                        if (in[e] && !(skt && stats_is_t(a))) {
                             const long long q = (long long)(kb + e) * g.nxy + ij;
                             s.mean[a][q] += (double)s.win[a][q] + c(a, e);
                             s.win[a][q] = 0.0f;

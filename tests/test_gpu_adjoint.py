@@ -280,7 +280,9 @@ def test_adjoint_wall_heat_flux_per_field(engine):
     """The mean bottom-wall heat flux after 8 steps of a stably stratified closed
     channel: each of the T- and velocity-parts of the gradient separately against
     central differences (a direction in T alone, then in u, v, w alone), and the
-    same gradient from two checkpoint spacings."""
+    same gradient from two checkpoint spacings. The velocities move the wall flux
+    about 1e-4 as much as T does, so their central difference takes eps = 1e-5
+    (round-off of J over 2 eps |dJ| is then about 4e-6 of it) and a 1e-4 bound."""
     p = Params(**{**SMALL, "cds": 2, "dts": 2, "dp_opt": 1, "ochannel": 0, "got": 1.0, "isscalar": 1})
     fields = inputs.small_random(p, seed=61)
     fields = {f: fields[f] for f in FIELDS_T}
@@ -298,8 +300,7 @@ def test_adjoint_wall_heat_flux_per_field(engine):
         assert np.allclose(gs[0][k], gs[1][k], rtol=1e-12, atol=1e-16), k
     g = gs[0]
     rng = np.random.default_rng(63)
-    eps = 1e-6
-    for part in (("t",), ("u", "v", "w")):
+    for part, eps, tol in ((("t",), 1e-6, 1e-6), (("u", "v", "w"), 1e-5, 1e-4)):
         d = {f: (rng.standard_normal((p.nz, p.ny, p.nx)) if f in part else np.zeros((p.nz, p.ny, p.nx)))
              for f in FIELDS_T}
         d["w"][-1] = 0.0
@@ -309,4 +310,4 @@ def test_adjoint_wall_heat_flux_per_field(engine):
         jm = adjoint.wall_heat_flux(_run_t(engine, p, minus, bf, 8)["t"], p)
         fd = (jp - jm) / (2 * eps)
         ad = sum(float(np.sum(g[k] * d[k])) for k in part)
-        assert abs(ad - fd) <= 1e-6 * abs(fd), (part, ad, fd)
+        assert abs(ad - fd) <= tol * abs(fd), (part, ad, fd)

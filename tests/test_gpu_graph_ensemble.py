@@ -6,6 +6,7 @@ import pytest
 
 from hercules_b200 import inputs
 from hercules_b200.params import PREC_MIXED, Params, config_channel_fd
+from parity_util import MIXED_P_TOL
 
 PI = 3.1415926535897932
 
@@ -61,7 +62,8 @@ def test_ensemble_members_equal_individual_runs(engine):
         for f in ("u", "v", "w", "p", "t", "mean_u"):
             a, b = x.download(f), y.download(f)
             if prec == PREC_MIXED:
-                assert np.max(np.abs(a - b)) <= 1e-5 * max(float(np.max(np.abs(b))), 1e-30), (q, f)
+                tol = MIXED_P_TOL if f == "p" else 1e-5
+                assert np.max(np.abs(a - b)) <= tol * max(float(np.max(np.abs(b))), 1e-30), (q, f)
             else:
                 assert np.array_equal(a, b), (q, f)
         if prec != PREC_MIXED:
@@ -127,7 +129,10 @@ def test_grouped_ensemble_equals_individual_runs(engine, prec):
         for f in ("u", "v", "w", "p", "t", "ff", "mean_u", "mean_tw"):
             a, b = x.download(f), y.download(f)
             if prec == PREC_MIXED:
-                assert np.max(np.abs(a - b)) <= 1e-5 * max(float(np.max(np.abs(b))), 1e-30), (q, f)
+                # FP32 round-off of u* reaches p through phi = P^-1 div(u*) / dt,
+                # amplified as in the mixed-vs-FP64 comparison (MIXED_P_TOL)
+                tol = MIXED_P_TOL if f == "p" else 1e-5
+                assert np.max(np.abs(a - b)) <= tol * max(float(np.max(np.abs(b))), 1e-30), (q, f)
             else:
                 assert np.array_equal(a, b), (q, f)
         if prec != PREC_MIXED:
