@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--graph", action="store_true", help="replay each step from a captured CUDA graph")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing leg")
     ap.add_argument("--no-tune", action="store_true", help="ensemble: default tile shapes, no autotuner")
+    ap.add_argument("--tile", type=int, nargs=4, default=None,
+                    help="single-channel workloads: the tile shapes (hc_params.tile), default automatic")
     ap.add_argument("--stats-gate", choices=["config3", "config2"], default=None,
                     help="run the mixed-vs-FP64 statistics gate (long runs) and print its lines")
     ap.add_argument("--adjoint-only", action="store_true",
@@ -74,16 +76,18 @@ def is_spectral(workload: str) -> bool:
     return workload.startswith("open_spectral")
 
 
-def make_case(workload: str, prec: int):
-    """Parameters and seeded initial fields of a workload."""
+def make_case(workload: str, prec: int, tile=None):
+    """Parameters and seeded initial fields of a workload (tile: hc_params.tile)."""
     from hercules_b200 import inputs
     from hercules_b200.params import config_channel_fd, config_open_channel_spectral
     nx, ny, nz = WORKLOADS[workload]
     if is_spectral(workload):
         p = config_open_channel_spectral(nx, ny, nz, got=0.1, precision=prec)
-        return p, inputs.loglaw_stratified(p, seed=10)
-    p = config_channel_fd(nx, ny, nz, precision=prec)
-    return p, inputs.poiseuille_noise(p, seed=3)
+        f = inputs.loglaw_stratified(p, seed=10)
+    else:
+        p = config_channel_fd(nx, ny, nz, precision=prec)
+        f = inputs.poiseuille_noise(p, seed=3)
+    return (p.replace(tile=list(tile)) if tile else p), f
 
 
 def dist_env():
@@ -253,7 +257,7 @@ def run_gpu(args, ws, rank, hbm):
     chans = {}
     precs = {"both": (PREC_FP64, PREC_MIXED), "fp64": (PREC_FP64,), "mixed": (PREC_MIXED,)}[args.precision]
     for prec in precs:
-        p, fields = make_case(args.workload, prec)
+        p, fields = make_case(args.workload, prec, args.tile)
         c = engine.Channel(p)
         c.load(fields)
         c.initialize()
@@ -321,7 +325,7 @@ def run_gpu(args, ws, rank, hbm):
     # end-to-end through the public API with host buffers (mixed)
     e2e = None
     if not args.no_e2e:
-        p, host = make_case(args.workload, PREC_MIXED)
+        p, host = make_case(args.workload, PREC_MIXED, args.tile)
         host = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in host.items()}
         res = {f: torch.empty((p.nz, p.ny, p.nx), dtype=torch.float64).pin_memory().numpy()
                for f in ("u", "v", "w", "p", "t")}
@@ -568,6 +572,8 @@ def main():
     fb = nx * ny * nz * 8
     cfg = {"workload": args.workload, "grid": [nx, ny, nz], "physics": physics, "parallelism": f"replicas x{args.gpus}",
            "l2": f"working set larger than L2 (one FP64 field {fb / 1e6:.0f} MB, FP32 {fb / 2e6:.0f} MB)"}
+    if args.tile:
+        cfg["tile"] = list(args.tile)
 
     if args.impl == "reference":
         if rank != 0:

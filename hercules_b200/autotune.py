@@ -32,13 +32,16 @@ from .params import Params
 from . import inputs
 
 CANDIDATES = {
-    0: ("fft_x", [0, 1, 2, 4, 8, 16]),
+    # tile[0]: -1 the fused 2-D transform instead of the separate x and y kernels
+    0: ("fft_x", [0, -1, 1, 2, 4, 8, 16]),
     1: ("fft_y", [0, 1, 2, 4, 8, 16]),
     2: ("rhs_momentum", [0, 4, 8, 16, 32, 64]),
     3: ("column", [0, 2, 1]),
 }
-KERNELS = {0: ("fft_x_r2c", "fft_x_c2r"), 1: ("fft_y_fwd", "fft_y_inv"), 2: ("rhs_momentum",),
-           3: ("column_fd", "column_t")}
+# the x slot is scored on every transform kernel: its choice can replace the
+# separate x and y kernels by the fused 2-D transforms
+KERNELS = {0: ("fft_x_r2c", "fft_x_c2r", "fft_y_fwd", "fft_y_inv", "fft2d_fwd", "fft2d_inv"),
+           1: ("fft_y_fwd", "fft_y_inv"), 2: ("rhs_momentum",), 3: ("column_fd", "column_t")}
 
 
 def _fields(p: Params):

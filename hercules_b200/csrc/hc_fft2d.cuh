@@ -45,14 +45,25 @@ template <typename R, int NXH, int NY, int C, int NT, int MINB> struct F2Shape {
     typedef typename V2<R>::T T2;
     static constexpr int RMAX = 16;
     static constexpr int G = FPad<R>::G;
-    static constexpr int LSX = FLine<NXH, G>::stride, LSY = FLine<NY, G>::stride;
+    static constexpr int LSX = FLine<NXH, G>::stride;
     static constexpr int LX = NY / C, LY = NXH / C;           // rows, columns a CTA
-    static constexpr int BUF = LX * LSX > LY * LSY ? LX * LSX : LY * LSY;
+    // x buffers: row-major with padded rows; y buffers: element-major ([m][column]),
+    // so that the lanes of a warp, which take consecutive columns, touch
+    // consecutive words (column-major rows of 384 padded elements put 16 columns
+    // on two bank offsets)
+    static constexpr int BUF = LX * LSX > LY * NY ? LX * LSX : LY * NY;
     static constexpr size_t smem = (size_t)2 * BUF * sizeof(T2);
     typedef FPlan<NXH, RMAX> PX;
     typedef FPlan<NY, RMAX> PY;
     static_assert(NXH % C == 0 && NY % C == 0, "the cluster divides the plane");
     static_assert(PX::valid && PY::valid && PX::npass == 2 && PY::npass == 2, "two passes a direction");
+};
+
+// y buffer of a CTA: element e of its column `line` at b[e * LD + line]
+template <typename T2, int LD> struct F2Cols {
+    T2* b;
+    __device__ __forceinline__ T2 ld(int line, int e) const { return b[e * LD + line]; }
+    __device__ __forceinline__ void st(int line, int e, T2 v) const { b[e * LD + line] = v; }
 };
 
 // element m of column l0 + line, read from the CTA of the cluster that holds row m
@@ -79,7 +90,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fft2d_fwd(const __grid_constant__ 
 {
     typedef F2Shape<R, NXH, NY, C, NT, MINB> S;
     typedef typename V2<R>::T T2;
-    constexpr int G = S::G, LSX = S::LSX, LSY = S::LSY, LX = S::LX, LY = S::LY;
+    constexpr int G = S::G, LSX = S::LSX, LX = S::LX, LY = S::LY;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
     T2* P0 = reinterpret_cast<T2*>(smem_raw);
@@ -112,7 +123,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fft2d_fwd(const __grid_constant__ 
     // ---- y: columns l0.. ; the first pass reads row m from the CTA that holds it
     const int l0 = c * LY;
     const F2RemoteRows<T2, LX, LSX, G, C> cols{P0, l0};
-    const SmemIO<T2, LSY, G> y1{P1};
+    const F2Cols<T2, LY> y1{P1};
     stock_pass<R, NY, -1, S::PY::rad(0), S::PY::span(0), LY, NT, true>(cols, y1, a.twy);
     // no CTA reads another's P0 after this barrier (it also orders P1)
     f2_cluster_sync<C>();
@@ -126,7 +137,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fft2d_inv(const __grid_constant__ 
 {
     typedef F2Shape<R, NXH, NY, C, NT, MINB> S;
     typedef typename V2<R>::T T2;
-    constexpr int G = S::G, LSX = S::LSX, LSY = S::LSY, LX = S::LX, LY = S::LY;
+    constexpr int G = S::G, LSX = S::LSX, LX = S::LX, LY = S::LY;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
     T2* P0 = reinterpret_cast<T2*>(smem_raw);
@@ -137,7 +148,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fft2d_inv(const __grid_constant__ 
     // ---- y: columns l0.. of plane k (Nyquist row zeroed before), P0 -> P1
     const int l0 = c * LY;
     const YColsIn<T2, NY, 1> src{reinterpret_cast<const T2*>(a.in[f]) + (long long)k * NY * NXH, l0, NXH};
-    const SmemIO<T2, LSY, G> y0{P0}, y1{P1};
+    const F2Cols<T2, LY> y0{P0}, y1{P1};
     stock_pass<R, NY, 1, S::PY::rad(0), S::PY::span(0), LY, NT, true>(src, y0, a.twy);
     __syncthreads();
     stock_pass<R, NY, 1, S::PY::rad(1), S::PY::span(1), LY, NT, true>(y0, y1, a.twy);
@@ -151,7 +162,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fft2d_inv(const __grid_constant__ 
     auto ldx = [&](int line, int l) -> T2 {     // X(l) of row m0 + line
         const int own = l / LY;
         const T2* b = C > 1 ? cooperative_groups::this_cluster().map_shared_rank(P1, own) : P1;
-        return b[(l - own * LY) * LSY + fpi<G>(m0 + line)];
+        return b[(m0 + line) * LY + (l - own * LY)];
     };
     auto zsplit = [&](T2 a0, T2 b0, int ll) {
         T2 bc = b0; bc.y = -bc.y;

@@ -166,16 +166,19 @@ static int build_fft(hc_handle* h)
         CK(cudaMalloc(&h->twt, tf.size() * sizeof(float2)));
         CK(cudaMemcpy(h->twt, tf.data(), tf.size() * sizeof(float2), cudaMemcpyHostToDevice));
     }
-    // explicit tile sizes (tile[0], tile[1]) select the runtime-length kernels
-    h->fft_tx = h->p.tile[0] == 0 && fft_t_length_ok(nxh);
+    // explicit tile sizes (tile[0], tile[1] > 0) select the runtime-length kernels;
+    // tile[0] = -1 the fused 2-D transforms where a shape exists (measured slower
+    // than the separate kernels at 512 x 384 x 256, so not the default)
+    if (h->p.tile[0] < -1) return HC_ERR_PARAM;
+    h->fft_tx = h->p.tile[0] <= 0 && fft_t_length_ok(nxh);
     h->fft_ty = h->p.tile[1] == 0 && fft_t_length_ok(ny);
     if (h->fft_tx || h->fft_ty) {
         int rc = h->rsz == sizeof(double) ? fft_t_setup<double>(h) : fft_t_setup<float>(h);
         if (rc != HC_OK) return rc;
     }
-    // the fused transforms where a shape exists (and no explicit tile asks for the others)
+    // the fused transforms where a shape exists, when tile[0] = -1 asks for them
     h->fft2d = 0;
-    if (h->fft_tx && h->fft_ty) {
+    if (h->fft_tx && h->fft_ty && h->p.tile[0] == -1) {
         const int rc = h->rsz == sizeof(double) ? fft2d_dispatch<double>(h, 0, nullptr, 0) : fft2d_dispatch<float>(h, 0, nullptr, 0);
         h->fft2d = rc == HC_OK;
     }

@@ -92,8 +92,9 @@ typedef struct hc_params {
     double ri_str, ri_end;
     int    precision;
     /* tile shapes, 0 = automatic (the autotuner in hercules_b200/autotune.py
-     * writes these): [0] x-FFT rows per block, [1] y-FFT lines per block (a
-     * positive value selects the runtime-plan transforms), [2] momentum-RHS
+     * writes these): [0] x-FFT rows per block (-1: the fused 2-D transform
+     * kernels where a shape exists), [1] y-FFT lines per
+     * block (a positive value selects the runtime-plan transforms), [2] momentum-RHS
      * levels per block, [3] column solve: 1 one thread per column, 2 one warp
      * per column without the coalescing tiles, >= 32 one thread per column with
      * that many threads a block */

@@ -108,6 +108,24 @@ def test_production_planes(name, oracle_lib, engine):
     _compare(p, inputs.small_random(p, seed=5), 4, oracle_lib, engine)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(PLANES) + ["fd4_256x192x9"])
+def test_fused_2d_transforms(name, oracle_lib, engine):
+    """tile[0] = -1: the fused 2-D transforms (thread-block clusters, the plane
+    exchanged in distributed shared memory) on the planes that have a shape
+    (512 x 384, 256 x 256, 256 x 192) against the oracle, FP64 and mixed."""
+    p = PLANES[name] if name in PLANES else _fd(256, 192, 9, isscalar=1, got=0.3)
+    p = p.replace(tile=[-1, 0, 0, 0])
+    _compare(p, inputs.small_random(p, seed=6), 4, oracle_lib, engine)
+    c = engine.Channel(p)
+    c.load(inputs.small_random(p, seed=6))
+    c.initialize()
+    c.set_profiling(True)
+    c.step(1)
+    assert c.kernel_profile().get("fft2d_fwd", {}).get("launches", 0) > 0
+    c.close()
+
+
 DEPTHS = {
     # warp-per-column solves, K = ceil(nz/32) rows a lane
     "fd4_nz128": _fd(32, 24, 128, isscalar=1, got=0.3),
