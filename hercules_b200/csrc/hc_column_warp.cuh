@@ -293,14 +293,23 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_fd_warp(ColArgs<R> 
 // Columns of CT_COLS adjacent wavenumber pairs staged in shared memory, so that
 // every global load and store is a coalesced row segment of CT_COLS modes
 // instead of one scattered access per lane. Tile layout per column: [i][lane]
-// (row r = lane*K + i), rows of CT_RP = 32 slots (aligned for the per-lane
-// accesses of the solves), columns padded by one slot so that the row-wise
-// global loads spread over the banks.
+// (row r = lane*K + i), rows of RP slots (the per-lane accesses of the solves
+// are consecutive), columns padded so that the row-wise global loads, whose 32
+// lanes write 4 rows r of 8 columns, spread over the banks: 16-byte elements
+// (FP64) rows of 32 and one pad slot a column; 8-byte elements (FP32) rows of 33
+// and two (rows of 32 put the 4 rows on one bank group: 4-way conflicts in every
+// load and store of the tiles, 2-way with 33).
 // ---------------------------------------------------------------------------
 #define CT_COLS 8
-#define CT_RP 32
 
-template <int K> __host__ __device__ constexpr int ct_stride() { return K * CT_RP + 1; }
+template <typename TT> struct CtLayout {
+    static constexpr int rp = sizeof(TT) == 8 ? 33 : 32;
+    template <int K> __host__ __device__ static constexpr int stride() { return K * rp + (sizeof(TT) == 8 ? 2 : 1); }
+};
+template <int K> __host__ __device__ constexpr int ct_stride_e(size_t elem)
+{
+    return elem == 8 ? CtLayout<float2>::stride<K>() : CtLayout<double2>::stride<K>();
+}
 
 // ---------------------------------------------------------------------------
 // The partition + PCR solve on a chosen arithmetic type T (float or double):
@@ -439,7 +448,7 @@ __device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename 
 // of each column
 template <int K> __host__ size_t column_tile_smem_r(size_t elem)
 {
-    return (size_t)3 * CT_COLS * ct_stride<K>() * elem +
+    return (size_t)3 * CT_COLS * ct_stride_e<K>(elem) * elem +
            (elem == sizeof(float2) ? (size_t)6 * K * 32 * (sizeof(float) + sizeof(double)) +
                                          (size_t)CT_COLS * 16 * sizeof(double) : 0);
 }
@@ -456,7 +465,8 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
     const long long c = c0 + wp;
     const bool active = c < ncol;
     const int nz = a.g.nz;
-    constexpr int STR = ct_stride<K>();
+    constexpr int STR = CtLayout<TT>::template stride<K>();
+    constexpr int RP = CtLayout<TT>::rp;
     TT* TU = reinterpret_cast<TT*>(smem_raw);
     TT* TV = TU + CT_COLS * STR;
     TT* TW = TV + CT_COLS * STR;
@@ -507,14 +517,14 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
         for (int it = 0; it < K; ++it) {
             const int idx = threadIdx.x + it * CT_COLS * 32;
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
-            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * CT_RP + r / K] = v[it];
+            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * RP + r / K] = v[it];
         }
     };
     auto store = [&](TT* __restrict__ q, const TT* T, int nrows) {
         for (int idx = threadIdx.x; idx < nrows * CT_COLS; idx += blockDim.x) {
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
             const long long cc = c0 + cb;
-            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * CT_RP + r / K];
+            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * RP + r / K];
         }
     };
     load(a.qu, TU, nz);
@@ -583,7 +593,7 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
                 for (int i = 0; i < K; ++i) {
                     const int r = r0 + i;
                     if (r < nz) {
-                        const TT xu = SU[i * CT_RP + ln], xv = SV[i * CT_RP + ln];
+                        const TT xu = SU[i * RP + ln], xv = SV[i * RP + ln];
                         double ux = (double)xu.x;
                         if (is00 && r == 0) ux += a.bcu0;
                         if (is00 && r == nz - 1) ux += a.bcu1;
@@ -610,15 +620,15 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
                 warp_partition_solve_t<T, K, 2>(cf, d, ln);
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
-                    SU[i * CT_RP + ln] = mk2<R>((R)d[0][i].x, (R)d[0][i].y);
-                    SV[i * CT_RP + ln] = mk2<R>((R)d[1][i].x, (R)d[1][i].y);
+                    SU[i * RP + ln] = mk2<R>((R)d[0][i].x, (R)d[0][i].y);
+                    SV[i * RP + ln] = mk2<R>((R)d[1][i].x, (R)d[1][i].y);
                 }
             }
             {
                 T2 dw[1][K];
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
-                    const TT x = SW[i * CT_RP + ln];
+                    const TT x = SW[i * RP + ln];
                     dw[0][i] = r0 + i < nz - 1 ? mk2<T>((T)x.x, (T)x.y) : mk2<T>(T(0), T(0));
                 }
                 const float rlam = (float)(rk * lam);
@@ -636,7 +646,7 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
                 };
                 warp_partition_solve_t<T, K, 1>(cf, dw, ln);
 #pragma unroll
-                for (int i = 0; i < K; ++i) SW[i * CT_RP + ln] = mk2<R>((R)dw[0][i].x, (R)dw[0][i].y);
+                for (int i = 0; i < K; ++i) SW[i * RP + ln] = mk2<R>((R)dw[0][i].x, (R)dw[0][i].y);
             }
         };
         if (is00) helmholtz(double(0)); else helmholtz(R(0));
@@ -647,15 +657,15 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
         const double rdt = 1.0 / dt;
         {
             auto ldt = [&](const TT* S, int idx) { const TT x = S[idx]; return make_double2((double)x.x, (double)x.y); };
-            const double2 wlast = ldt(SW, (K - 1) * CT_RP + ln);
+            const double2 wlast = ldt(SW, (K - 1) * RP + ln);
             double2 wprev0 = shfl_up2(wlast, 1);
             if (ln == 0) wprev0 = make_double2(0, 0);
 #pragma unroll
             for (int i = 0; i < K; ++i) {
                 const int r = r0 + i;
                 if (r < nz) {
-                    const double2 us = ldt(SU, i * CT_RP + ln), vs = ldt(SV, i * CT_RP + ln), ws = ldt(SW, i * CT_RP + ln);
-                    const double2 wm = i > 0 ? ldt(SW, (i - 1) * CT_RP + ln) : wprev0;
+                    const double2 us = ldt(SU, i * RP + ln), vs = ldt(SV, i * RP + ln), ws = ldt(SW, i * RP + ln);
+                    const double2 wm = i > 0 ? ldt(SW, (i - 1) * RP + ln) : wprev0;
                     const double rdz = dtab(3, r);
                     double2 div = zadd(zmul(DX, us), zmul(DY, vs));
                     div = zadd(div, make_double2((ws.x - wm.x) * rdz, (ws.y - wm.y) * rdz));
@@ -690,12 +700,12 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
                 if (r >= nz) continue;
                 const double2 pc = ph[0][i];
                 const double2 pu = (r == nz - 1) ? pc : (i < K - 1 ? ph[0][i + 1] : nxt0);
-                const TT us = SU[i * CT_RP + ln], vs = SV[i * CT_RP + ln], ws = SW[i * CT_RP + ln];
+                const TT us = SU[i * RP + ln], vs = SV[i * RP + ln], ws = SW[i * RP + ln];
                 const double rdzt = dtab(4, r);
                 const double2 gu = zmul(GX, pc), gv = zmul(GY, pc);
-                SU[i * CT_RP + ln] = mk2<R>((R)((double)us.x - cpr * gu.x), (R)((double)us.y - cpr * gu.y));
-                SV[i * CT_RP + ln] = mk2<R>((R)((double)vs.x - cpr * gv.x), (R)((double)vs.y - cpr * gv.y));
-                SW[i * CT_RP + ln] = r <= nz - 2 ? mk2<R>((R)((double)ws.x - cpr * (pu.x - pc.x) * rdzt),
+                SU[i * RP + ln] = mk2<R>((R)((double)us.x - cpr * gu.x), (R)((double)us.y - cpr * gu.y));
+                SV[i * RP + ln] = mk2<R>((R)((double)vs.x - cpr * gv.x), (R)((double)vs.y - cpr * gv.y));
+                SW[i * RP + ln] = r <= nz - 2 ? mk2<R>((R)((double)ws.x - cpr * (pu.x - pc.x) * rdzt),
                                                        (R)((double)ws.y - cpr * (pu.y - pc.y) * rdzt))
                                               : mk2<R>(R(0), R(0));
             }
@@ -727,7 +737,7 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
                 double2 lz;
                 lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
                 lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
-                SU[i * CT_RP + ln] = mk2<R>((R)(pc.x - cps * (lxy * pc.x + lz.x)), (R)(pc.y - cps * (lxy * pc.y + lz.y)));
+                SU[i * RP + ln] = mk2<R>((R)(pc.x - cps * (lxy * pc.x + lz.x)), (R)(pc.y - cps * (lxy * pc.y + lz.y)));
             }
         }
     }
@@ -746,7 +756,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
 // solution may overwrite q_t. (One warp per column reading and writing a row a
 // lane: 76 -> 67 us mixed, 91 -> 68 us FP64 a launch at 256 x 256 x 128.)
 // ---------------------------------------------------------------------------
-template <int K> __host__ size_t column_t_tile_smem(size_t elem) { return (size_t)CT_COLS * ct_stride<K>() * elem; }
+template <int K> __host__ size_t column_t_tile_smem(size_t elem) { return (size_t)CT_COLS * ct_stride_e<K>(elem) * elem; }
 
 template <typename R, int K>
 __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
@@ -759,7 +769,8 @@ __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const
     const long long c0 = (long long)blockIdx.x * CT_COLS;
     const long long c = c0 + wp;
     const int nz = a.g.nz;
-    constexpr int STR = ct_stride<K>();
+    constexpr int STR = CtLayout<TT>::template stride<K>();
+    constexpr int RP = CtLayout<TT>::rp;
     TT* TQ = reinterpret_cast<TT*>(smem_raw);
     {
         TT v[K];
@@ -774,7 +785,7 @@ __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const
         for (int it = 0; it < K; ++it) {
             const int idx = threadIdx.x + it * CT_COLS * 32;
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
-            if (idx < nz * CT_COLS) TQ[cb * STR + (r % K) * CT_RP + r / K] = v[it];
+            if (idx < nz * CT_COLS) TQ[cb * STR + (r % K) * RP + r / K] = v[it];
         }
     }
     __syncthreads();
@@ -791,7 +802,7 @@ __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const
         for (int i = 0; i < K; ++i) {
             const int r = r0 + i;
             if (r < nz) {
-                const TT x = SQ[i * CT_RP + ln];
+                const TT x = SQ[i * RP + ln];
                 d[0][i] = make_double2((double)x.x, (double)x.y);
                 if (is00 && r == 0) d[0][i].x += a.bct0;
                 if (is00 && r == nz - 1) d[0][i].x += a.bct1;
@@ -811,14 +822,14 @@ __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             const double2 v = tr ? make_double2(0, 0) : d[0][i];
-            SQ[i * CT_RP + ln] = mk2<R>((R)v.x, (R)v.y);
+            SQ[i * RP + ln] = mk2<R>((R)v.x, (R)v.y);
         }
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < nz * CT_COLS; idx += blockDim.x) {
         const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
         const long long cc = c0 + cb;
-        if (cc < ncol) a.out[(long long)r * ncol + cc] = TQ[cb * STR + (r % K) * CT_RP + r / K];
+        if (cc < ncol) a.out[(long long)r * ncol + cc] = TQ[cb * STR + (r % K) * RP + r / K];
     }
 }
 template <typename R, int K>

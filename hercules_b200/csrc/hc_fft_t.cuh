@@ -219,13 +219,15 @@ __device__ __forceinline__ void stock_pass(const SRC& src, const DST& dst, const
 // Passes P..npass-1. Pass P reads SRC; passes after the first read shared
 // buffer A (ping-pong with B); the last pass writes DST. Every pass but the last
 // ends with a barrier.
-template <typename R, int N, int S, int RMAX, int LINES, int NT, bool LMINOR, int P, bool FF = false, class SRC, class DST>
+// LSO: the shared lines' stride (0: FLine's).
+template <typename R, int N, int S, int RMAX, int LINES, int NT, bool LMINOR, int P, bool FF = false, int LSO = 0,
+          class SRC, class DST>
 __device__ __forceinline__ void run_passes(const SRC& src, const DST& dst, typename V2<R>::T* A, typename V2<R>::T* B,
                                            const typename V2<R>::T* tw)
 {
     typedef FPlan<N, RMAX, FF> PL;
     typedef typename V2<R>::T T2;
-    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride;
+    constexpr int G = FPad<R>::G, LS = LSO ? LSO : FLine<N, G>::stride;
     if constexpr (P == PL::npass - 1) {
         stock_pass<R, N, S, PL::rad(P), PL::span(P), LINES, NT, LMINOR>(src, dst, tw);
     } else {
@@ -233,7 +235,7 @@ __device__ __forceinline__ void run_passes(const SRC& src, const DST& dst, typen
         stock_pass<R, N, S, PL::rad(P), PL::span(P), LINES, NT, LMINOR>(src, out, tw);
         __syncthreads();
         const SmemIO<T2, LS, G> in{A};
-        run_passes<R, N, S, RMAX, LINES, NT, LMINOR, P + 1, FF>(in, dst, B, A, tw);
+        run_passes<R, N, S, RMAX, LINES, NT, LMINOR, P + 1, FF, LSO>(in, dst, B, A, tw);
     }
 }
 
@@ -293,9 +295,83 @@ template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_
 {
     return (size_t)FBufs<N, RMAX>::x * FxLines<R, N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
 }
+// y tiles in FP32 put the folded pass first where the other order would start
+// with a pass of fewer than 16 points: 192 = 24 x 8 then reads 24 elements a
+// thread in one round instead of 8 elements in 1.5 rounds (forward 85 -> 70 us,
+// inverse 107 -> 97 us at 256 x 192 x 256, 3 and 4 fields). 384 = 16 x 24 keeps
+// radix 16 first: radix 24 first gained nothing forward and spilled inverse
+// there, and in FP64 it was slower in both directions.
+template <typename R, int N, int RMAX> struct FyFoldFirst {
+    typedef FPlan<N, RMAX> PL;
+    static constexpr bool v = sizeof(R) == sizeof(float) && PL::nfold == 1 && PL::rad(0) < 16;
+};
+
+// Shared-memory wavefronts of one warp's access to elements at a[0..31] (-1: lane
+// idle) of W per 128 bytes: the most distinct elements that fall on one of the W
+// bank groups (8-byte elements: 16 groups of two banks; 16-byte: 8 of four).
+template <int W> __host__ __device__ constexpr int f_wavefronts(const int (&a)[32])
+{
+    int cnt[W] = {};
+    for (int l = 0; l < 32; ++l) {
+        if (a[l] < 0) continue;
+        bool first = true;
+        for (int t = 0; t < l; ++t)
+            if (a[t] == a[l]) first = false;
+        if (first) ++cnt[a[l] % W];
+    }
+    int m = 0;
+    for (int q = 0; q < W; ++q) m = cnt[q] > m ? cnt[q] : m;
+    return m;
+}
+// Wavefronts of the first warp's shared-memory reads and writes over the plan's
+// passes (radix slots r = 0, 1; the others repeat them shifted) for y lines of
+// stride LS: consecutive lanes take consecutive lines, then the next item
+// (stock_pass with LMINOR); padded index e + e / G.
+template <int N, int RMAX, bool FF, int LINES, int G, int W> __host__ __device__ constexpr int f_ycost(int LS)
+{
+    typedef FPlan<N, RMAX, FF> PL;
+    int cost = 0;
+    for (int p = 0; p < PL::npass; ++p) {
+        const int RAD = PL::rad(p), NS = PL::span(p), NR = N / RAD;
+        for (int r = 0; r < 2 && r < RAD; ++r) {
+            int rd[32] = {}, wr[32] = {};
+            for (int it = 0; it < 32; ++it) {
+                const int j = it / LINES, line = it % LINES;
+                if (j >= NR) { rd[it] = -1; wr[it] = -1; continue; }
+                const int er = j + r * NR;
+                const int ew = (j / NS) * NS * RAD + (NS == 1 ? 0 : j % NS) + r * NS;
+                rd[it] = line * LS + er + er / G;
+                wr[it] = line * LS + ew + ew / G;
+            }
+            if (p > 0) cost += f_wavefronts<W>(rd);
+            if (p < PL::npass - 1) cost += f_wavefronts<W>(wr);
+        }
+    }
+    return cost;
+}
+// y line stride: FLine's stride plus the pad in [0, W) with the fewest
+// wavefronts. With FLine's own stride (408 for 384 FP32 points) the 8 lines a warp
+// touches sit on two bank offsets and every access of the passes is 4-way
+// conflicted (8-way in FP64).
+template <typename R, int N, int RMAX> struct FyStride {
+    static constexpr int G = FPad<R>::G, W = 128 / (2 * (int)sizeof(R)), base = FLine<N, G>::stride;
+    static constexpr int LINES = FyLines<R, N>::v;
+    static constexpr bool FF = FyFoldFirst<R, N, RMAX>::v;
+    static constexpr int pick()
+    {
+        int best = 0, bc = 1 << 30;
+        for (int q = 0; q < W; ++q) {
+            const int c = f_ycost<N, RMAX, FF, LINES, G, W>(base + q);
+            if (c < bc) { bc = c; best = q; }
+        }
+        return base + best;
+    }
+    static constexpr int v = pick();
+};
+
 template <typename R, int N, int RMAX> __host__ __device__ constexpr size_t fft_y_smem()
 {
-    return (size_t)FBufs<N, RMAX>::y * FyLines<R, N>::v * FLine<N, FPad<R>::G>::stride * sizeof(typename V2<R>::T);
+    return (size_t)FBufs<N, RMAX>::y * FyLines<R, N>::v * FyStride<R, N, RMAX>::v * sizeof(typename V2<R>::T);
 }
 // y kernels in FP32: registers sized for as many resident blocks as the shared
 // memory allows, at 64 registers a thread at least (1024 threads an SM)
@@ -487,21 +563,11 @@ __global__ void __launch_bounds__(FxThreads<R, N>::v) k_fft_x_c2r_t(FxArgs<R> a)
 // y direction on the half spectrum [k][m][l]: tiles of FyLines<R, N> columns l of
 // one plane k; grid (ceil(nxh/TL), nz, fields)
 // ----------------------------------------------------------------------------
-// y tiles in FP32 put the folded pass first where the other order would start
-// with a pass of fewer than 16 points: 192 = 24 x 8 then reads 24 elements a
-// thread in one round instead of 8 elements in 1.5 rounds (forward 85 -> 70 us,
-// inverse 107 -> 97 us at 256 x 192 x 256, 3 and 4 fields). 384 = 16 x 24 keeps
-// radix 16 first: radix 24 first gained nothing forward and spilled inverse
-// there, and in FP64 it was slower in both directions.
-template <typename R, int N, int RMAX> struct FyFoldFirst {
-    typedef FPlan<N, RMAX> PL;
-    static constexpr bool v = sizeof(R) == sizeof(float) && PL::nfold == 1 && PL::rad(0) < 16;
-};
 template <typename R, int N, int S, int RMAX>
 __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a, const uint3 blockIdx)
 {
     typedef typename V2<R>::T T2;
-    constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride, TL = FyLines<R, N>::v, NT = FyThreads<R, N>::v;
+    constexpr int G = FPad<R>::G, LS = FyStride<R, N, RMAX>::v, TL = FyLines<R, N>::v, NT = FyThreads<R, N>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.halt && *a.halt) return;
     T2* A = reinterpret_cast<T2*>(smem_raw);
@@ -515,8 +581,7 @@ __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a, const uint3 block
     if constexpr (FPlan<N, RMAX>::npass == 1) {
         // one pass: in place is safe only through a barrier between reads and writes
         if (s == d) {
-            constexpr int LSz = FLine<N, G>::stride;
-            const SmemIO<T2, LSz, G> stage{A};
+            const SmemIO<T2, LS, G> stage{A};
             for (int idx = threadIdx.x; idx < TL * N; idx += NT) {
                 const int m = idx / TL, lt = idx - m * TL;
                 stage.st(lt, m, src.ld(lt, m));
@@ -528,7 +593,7 @@ __device__ __forceinline__ void fft_y_tile(const FyArgs<R>& a, const uint3 block
     }
     // in place (s == d) with two or more passes: the first pass reads every
     // element of the tile before its barrier, and only the last pass writes it
-    run_passes<R, N, S, RMAX, TL, NT, true, 0, FyFoldFirst<R, N, RMAX>::v>(src, dst, A, B, a.tw);
+    run_passes<R, N, S, RMAX, TL, NT, true, 0, FyFoldFirst<R, N, RMAX>::v, LS>(src, dst, A, B, a.tw);
 }
 
 template <typename R, int N, int S, int RMAX>

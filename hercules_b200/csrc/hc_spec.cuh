@@ -813,7 +813,7 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_sp_warp(SpColArgs<R
 // its column with one access per lane (32 rows of one column per instruction).
 template <int K> __host__ size_t column_sp_tile_smem(size_t elem)
 {
-    return (size_t)4 * CT_COLS * ct_stride<K>() * elem;
+    return (size_t)4 * CT_COLS * ct_stride_e<K>(elem) * elem;
 }
 
 template <typename R, int K>
@@ -829,12 +829,13 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
     const long long c = c0 + wp;
     const bool active = c < ncol;
     const int nz = a.g.nz;
-    constexpr int STR = ct_stride<K>();
+    constexpr int STR = CtLayout<TT>::template stride<K>();
+    constexpr int RP = CtLayout<TT>::rp;
     TT* TU = reinterpret_cast<TT*>(smem_raw);
     TT* TV = TU + CT_COLS * STR;
     TT* TW = TV + CT_COLS * STR;
     TT* TP = TW + CT_COLS * STR;
-    // element (column cb, row r) at cb * STR + (r % K) * CT_RP + r / K: lane ln of
+    // element (column cb, row r) at cb * STR + (r % K) * RP + r / K: lane ln of
     // a warp holds rows ln K .. ln K + K - 1 of its column
     auto load = [&](const TT* __restrict__ q, TT* T, int nrows) {
         TT v[K];
@@ -849,14 +850,14 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
         for (int it = 0; it < K; ++it) {
             const int idx = threadIdx.x + it * CT_COLS * 32;
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
-            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * CT_RP + r / K] = v[it];
+            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * RP + r / K] = v[it];
         }
     };
     auto store = [&](TT* __restrict__ q, const TT* T) {
         for (int idx = threadIdx.x; idx < nz * CT_COLS; idx += blockDim.x) {
             const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
             const long long cc = c0 + cb;
-            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * CT_RP + r / K];
+            if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * RP + r / K];
         }
     };
     load(a.qu, TU, nz);
@@ -892,8 +893,8 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
             for (int i = 0; i < K; ++i) {
                 const int r = r0 + i;
                 if (r < nz) {
-                    d[0][i] = dbl(SU[i * CT_RP + ln]);
-                    d[1][i] = dbl(SV[i * CT_RP + ln]);
+                    d[0][i] = dbl(SU[i * RP + ln]);
+                    d[1][i] = dbl(SV[i * RP + ln]);
                     if (is00 && r == 0) d[0][i].x += a.bcu0;
                     if (is00 && r == nz - 1) d[0][i].x += a.bcu1;
                 } else {
@@ -917,7 +918,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
 #pragma unroll
             for (int i = 0; i < K; ++i) {
                 const int r = r0 + i;
-                dw[0][i] = r < nz - 1 ? dbl(SW[i * CT_RP + ln]) : make_double2(0, 0);
+                dw[0][i] = r < nz - 1 ? dbl(SW[i * RP + ln]) : make_double2(0, 0);
             }
             auto cf = [&](int r, double& aa, double& bb, double& cc) {
                 if (r < nz - 1) {
@@ -983,26 +984,26 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
                 lz.x = ((pu.x - pc.x) * rdzt - (pc.x - pd.x) * rdzb) * rdz;
                 lz.y = ((pu.y - pc.y) * rdzt - (pc.y - pd.y) * rdzb) * rdz;
                 const double2 psi = make_double2(pc.x - cps * (lxy * pc.x + lz.x), pc.y - cps * (lxy * pc.y + lz.y));
-                double2 fp = zadd(A.dt.at(dbl(SP[i * CT_RP + ln]), 3, r, nz), psi);
+                double2 fp = zadd(A.dt.at(dbl(SP[i * RP + ln]), 3, r, nz), psi);
                 if (tr) { fu = make_double2(0, 0); fv = fu; fw = fu; fp = fu; }
-                put(SU, i * CT_RP + ln, fu);
-                put(SV, i * CT_RP + ln, fv);
-                put(SW, i * CT_RP + ln, fw);
-                put(SP, i * CT_RP + ln, fp);
+                put(SU, i * RP + ln, fu);
+                put(SV, i * RP + ln, fv);
+                put(SW, i * RP + ln, fw);
+                put(SP, i * RP + ln, fp);
             }
         }
         __syncwarp();
         // ---- divergence spectrum of the stored fields (the physical w is 0 below
         //      the bottom wall and on the top wall)
-        const double2 wlast = dbl(SW[(K - 1) * CT_RP + ln]);
+        const double2 wlast = dbl(SW[(K - 1) * RP + ln]);
         double2 wbelow0 = shfl_up2(wlast, 1);
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             const int r = r0 + i;
             double2 dv = make_double2(0, 0);
             if (r < nz && !nyq) {
-                const double2 fu = dbl(SU[i * CT_RP + ln]), fv = dbl(SV[i * CT_RP + ln]), fw = dbl(SW[i * CT_RP + ln]);
-                const double2 fwm = r == 0 ? make_double2(0, 0) : (i > 0 ? dbl(SW[(i - 1) * CT_RP + ln]) : wbelow0);
+                const double2 fu = dbl(SU[i * RP + ln]), fv = dbl(SV[i * RP + ln]), fw = dbl(SW[i * RP + ln]);
+                const double2 fwm = r == 0 ? make_double2(0, 0) : (i > 0 ? dbl(SW[(i - 1) * RP + ln]) : wbelow0);
                 const double rdz = __ldg(a.c.rdz + r);
                 dv = zadd(zmul(DX, fu), zmul(DY, fv));
                 dv = zadd(dv, make_double2((fw.x - fwm.x) * rdz, (fw.y - fwm.y) * rdz));
@@ -1020,8 +1021,8 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
     if (active) {
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            put(SU, i * CT_RP + ln, ph[0][i]);
-            put(SV, i * CT_RP + ln, dvr[i]);
+            put(SU, i * RP + ln, ph[0][i]);
+            put(SV, i * RP + ln, dvr[i]);
         }
     }
     __syncthreads();
