@@ -485,6 +485,14 @@ __device__ __forceinline__ void k_fft_x_c2r_t_body(const FxArgs<R>& a, const uin
     const long long row0 = (long long)blockIdx.x * L;
     const int nr = (int)min((long long)L, a.nrows - row0);
     const T2* in = reinterpret_cast<const T2*>(a.in[f]) + row0 * N;
+    if (a.add[f]) {
+        // the rows this block adds to (p += psi) are read only in the last pass:
+        // bring their 128-byte lines into L2 now, so that read does not wait on HBM
+        const char* pb = reinterpret_cast<const char*>(reinterpret_cast<const T2*>(a.out[f]) + row0 * N);
+        const int nbytes = nr * N * (int)sizeof(T2);
+        for (int o = threadIdx.x * 128; o < nbytes; o += NTX * 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(pb + o));
+    }
     // pre-split straight from global: Z(l) = (X(l) + conj X(N-l)) + i conj(W_l) (X(l) - conj X(N-l));
     // the partner of l = 0 is the x Nyquist mode (zero, not stored). FP32: one
     // thread per pair (l, N-l), so every mode is read once.
