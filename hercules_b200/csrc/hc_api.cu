@@ -283,6 +283,7 @@ struct hc_handle {
     void* twt;               // the same tables in the storage precision (FP64: twbuf)
     int fft_tx, fft_ty;      // 1: the compile-time-length kernels serve x / y
     int fft2d;               // 1: the fused 2-D transform kernels (hc_fft2d.cuh) serve both
+    int f2_ncl[2];           // their persistent clusters resident at once: forward, inverse
     FftPlan px, py;
     double2* wpack;
     int rows_x, tl_y, col_threads, col_warp;

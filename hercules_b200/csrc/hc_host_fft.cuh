@@ -63,7 +63,7 @@ template <typename R> static int fft_t_dispatch(hc_handle* h, int n, int op, con
 }
 
 // ---------------------------------------------------------------------------
-// fused 2-D transforms (hc_fft2d.cuh): one cluster of C CTAs a (field, plane).
+// fused 2-D transforms (hc_fft2d.cuh): persistent clusters of C CTAs over the (field, plane) pairs.
 // Shapes: nx/2, ny, C, threads a CTA, resident CTAs an SM with FP32 / FP64 storage
 // ---------------------------------------------------------------------------
 #define HC_FFT2D_SHAPES(X) X(256, 384, 16, 384, 2, 1) X(128, 256, 8, 256, 3, 1) X(128, 192, 8, 256, 3, 1)
@@ -87,19 +87,31 @@ static int fft2d_op(hc_handle* h, int op, const F2Args<R>* a, int nf)
         // shared-memory limit and cluster size; usable only if a cluster fits the device
         for (int q = 0; q < 2; ++q) {
             const void* k = (const void*)(q == 0 ? fwd : inv);
-            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem) != cudaSuccess) return HC_ERR_UNSUPPORTED;
-            if (C > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return HC_ERR_UNSUPPORTED;
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem) != cudaSuccess) {
+                cudaGetLastError();
+                return HC_ERR_UNSUPPORTED;
+            }
+            if (C > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+                cudaGetLastError();
+                return HC_ERR_UNSUPPORTED;
+            }
             int ncl = 0;
             cfg.gridDim = dim3(C);
             if (cudaOccupancyMaxActiveClusters(&ncl, k, &cfg) != cudaSuccess || ncl < 1) {
                 cudaGetLastError();
                 return HC_ERR_UNSUPPORTED;
             }
+            h->f2_ncl[q] = ncl;
         }
         return HC_OK;
     }
-    cfg.gridDim = dim3((unsigned)((long long)nf * h->g.nz * C));
-    CK(cudaLaunchKernelEx(&cfg, op == 1 ? fwd : inv, *a));
+    // persistent clusters: as many as are resident at once, at most one a plane
+    const long long np = (long long)nf * h->g.nz;
+    const long long ncl = std::min<long long>(np, h->f2_ncl[op == 1 ? 0 : 1]);
+    F2Args<R> b = *a;
+    b.nplanes = (int)np;
+    cfg.gridDim = dim3((unsigned)(ncl * C));
+    CK(cudaLaunchKernelEx(&cfg, op == 1 ? fwd : inv, b));
     return HC_OK;
 }
 
