@@ -342,67 +342,75 @@ template <typename T> __device__ __forceinline__ typename V2<T>::T t2shfl_dn(typ
     return mk2<T>(__shfl_down_sync(0xffffffffu, v.x, s), __shfl_down_sync(0xffffffffu, v.y, s));
 }
 
-template <typename T, int K, int NR, typename CF>
-__device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename V2<T>::T (&d)[NR][K], int ln)
-{
+// The partition + PCR solve of one system on the arithmetic type T (float or
+// double), in three phases: the lane's local elimination and the reduced row of
+// its last unknown (elim), one PCR level (pcr), the back-substitution (finish).
+// warp_partition_solve_t runs them for one system; warp_partition_solve2_t for two
+// independent systems phase by phase, so that the dependent chains of the one
+// fill the latency of the other's.
+template <typename T, int K, int NR> struct PartSys {
     typedef typename V2<T>::T T2;
-    const int r0 = ln * K;
     T vv[K], ww[K], ib[K];
-    if (K >= 2) {
-        T a0, b0, c0;
-        coef(r0, a0, b0, c0);
-        ib[0] = rcp_t(b0);
-        vv[0] = -a0;
-        ww[0] = (K == 2) ? -c0 : T(0);
-        T cprev = c0;
-#pragma unroll
-        for (int i = 1; i <= K - 2; ++i) {
-            T ai, bi, ci;
-            coef(r0 + i, ai, bi, ci);
-            const T mlt = ai * ib[i - 1];
-            ib[i] = rcp_t(bi - mlt * cprev);
-#pragma unroll
-            for (int q = 0; q < NR; ++q) d[q][i] = t2axpy<T>(d[q][i], d[q][i - 1], mlt);
-            vv[i] = -mlt * vv[i - 1];
-            ww[i] = (i == K - 2 ? -ci : T(0)) - mlt * ww[i - 1];
-            cprev = ci;
-        }
-#pragma unroll
-        for (int q = 0; q < NR; ++q) d[q][K - 2] = t2scale<T>(d[q][K - 2], ib[K - 2]);
-        vv[K - 2] *= ib[K - 2];
-        ww[K - 2] *= ib[K - 2];
-#pragma unroll
-        for (int i = K - 3; i >= 0; --i) {
-            T ai, bi, ci;
-            coef(r0 + i, ai, bi, ci);
-#pragma unroll
-            for (int q = 0; q < NR; ++q) d[q][i] = t2scale<T>(t2axpy<T>(d[q][i], d[q][i + 1], ci), ib[i]);
-            vv[i] = (vv[i] - ci * vv[i + 1]) * ib[i];
-            ww[i] = (ww[i] - ci * ww[i + 1]) * ib[i];
-        }
-    }
-    T aK, bK, cK;
-    coef(r0 + K - 1, aK, bK, cK);
-    const T xm_v = K >= 2 ? vv[K - 2] : T(1);
-    const T xm_w = K >= 2 ? ww[K - 2] : T(0);
-    const T f_v = K >= 2 ? vv[0] : T(0);
-    const T f_w = K >= 2 ? ww[0] : T(1);
-    const T nf_v = __shfl_down_sync(0xffffffffu, f_v, 1);
-    const T nf_w = __shfl_down_sync(0xffffffffu, f_w, 1);
-    T A = aK * xm_v;
-    T B = aK * xm_w + bK + cK * nf_v;
-    T C = cK * nf_w;
+    T A, B, C;
     T2 D[NR];
+    template <typename CF> __device__ __forceinline__ void elim(const CF& coef, T2 (&d)[NR][K], int ln)
+    {
+        const int r0 = ln * K;
+        if (K >= 2) {
+            T a0, b0, c0;
+            coef(r0, a0, b0, c0);
+            ib[0] = rcp_t(b0);
+            vv[0] = -a0;
+            ww[0] = (K == 2) ? -c0 : T(0);
+            T cprev = c0;
 #pragma unroll
-    for (int q = 0; q < NR; ++q) {
-        const T2 z = mk2<T>(T(0), T(0));
-        const T2 xm_g = K >= 2 ? d[q][K - 2 < 0 ? 0 : K - 2] : z;
-        const T2 f_g = K >= 2 ? d[q][0] : z;
-        const T2 nf_g = t2shfl_dn<T>(f_g, 1);
-        D[q] = t2axpy<T>(t2axpy<T>(d[q][K - 1], xm_g, aK), nf_g, cK);
+            for (int i = 1; i <= K - 2; ++i) {
+                T ai, bi, ci;
+                coef(r0 + i, ai, bi, ci);
+                const T mlt = ai * ib[i - 1];
+                ib[i] = rcp_t(bi - mlt * cprev);
+#pragma unroll
+                for (int q = 0; q < NR; ++q) d[q][i] = t2axpy<T>(d[q][i], d[q][i - 1], mlt);
+                vv[i] = -mlt * vv[i - 1];
+                ww[i] = (i == K - 2 ? -ci : T(0)) - mlt * ww[i - 1];
+                cprev = ci;
+            }
+#pragma unroll
+            for (int q = 0; q < NR; ++q) d[q][K - 2] = t2scale<T>(d[q][K - 2], ib[K - 2]);
+            vv[K - 2] *= ib[K - 2];
+            ww[K - 2] *= ib[K - 2];
+#pragma unroll
+            for (int i = K - 3; i >= 0; --i) {
+                T ai, bi, ci;
+                coef(r0 + i, ai, bi, ci);
+#pragma unroll
+                for (int q = 0; q < NR; ++q) d[q][i] = t2scale<T>(t2axpy<T>(d[q][i], d[q][i + 1], ci), ib[i]);
+                vv[i] = (vv[i] - ci * vv[i + 1]) * ib[i];
+                ww[i] = (ww[i] - ci * ww[i + 1]) * ib[i];
+            }
+        }
+        T aK, bK, cK;
+        coef(r0 + K - 1, aK, bK, cK);
+        const T xm_v = K >= 2 ? vv[K - 2] : T(1);
+        const T xm_w = K >= 2 ? ww[K - 2] : T(0);
+        const T f_v = K >= 2 ? vv[0] : T(0);
+        const T f_w = K >= 2 ? ww[0] : T(1);
+        const T nf_v = __shfl_down_sync(0xffffffffu, f_v, 1);
+        const T nf_w = __shfl_down_sync(0xffffffffu, f_w, 1);
+        A = aK * xm_v;
+        B = aK * xm_w + bK + cK * nf_v;
+        C = cK * nf_w;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            const T2 z = mk2<T>(T(0), T(0));
+            const T2 xm_g = K >= 2 ? d[q][K - 2 < 0 ? 0 : K - 2] : z;
+            const T2 f_g = K >= 2 ? d[q][0] : z;
+            const T2 nf_g = t2shfl_dn<T>(f_g, 1);
+            D[q] = t2axpy<T>(t2axpy<T>(d[q][K - 1], xm_g, aK), nf_g, cK);
+        }
     }
-#pragma unroll
-    for (int s = 1; s < 32; s <<= 1) {
+    __device__ __forceinline__ void pcr(int s, int ln)
+    {
         T Am = __shfl_up_sync(0xffffffffu, A, s), Bm = __shfl_up_sync(0xffffffffu, B, s);
         T Cm = __shfl_up_sync(0xffffffffu, C, s);
         T Ap = __shfl_down_sync(0xffffffffu, A, s), Bp = __shfl_down_sync(0xffffffffu, B, s);
@@ -421,17 +429,44 @@ __device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename 
         const T nA = -Am * k1, nC = -Cp * k2, nB = B - Cm * k1 - Ap * k2;
         A = nA; B = nB; C = nC;
     }
-    const T iB = rcp_t(B);
+    __device__ __forceinline__ void finish(T2 (&d)[NR][K], int ln)
+    {
+        const T iB = rcp_t(B);
 #pragma unroll
-    for (int q = 0; q < NR; ++q) {
-        const T2 y = t2scale<T>(D[q], iB);
-        T2 yp = t2shfl_up<T>(y, 1);
-        if (ln == 0) yp = mk2<T>(T(0), T(0));
+        for (int q = 0; q < NR; ++q) {
+            const T2 y = t2scale<T>(D[q], iB);
+            T2 yp = t2shfl_up<T>(y, 1);
+            if (ln == 0) yp = mk2<T>(T(0), T(0));
 #pragma unroll
-        for (int i = 0; i < K - 1; ++i)
-            d[q][i] = mk2<T>(d[q][i].x + vv[i] * yp.x + ww[i] * y.x, d[q][i].y + vv[i] * yp.y + ww[i] * y.y);
-        d[q][K - 1] = y;
+            for (int i = 0; i < K - 1; ++i)
+                d[q][i] = mk2<T>(d[q][i].x + vv[i] * yp.x + ww[i] * y.x, d[q][i].y + vv[i] * yp.y + ww[i] * y.y);
+            d[q][K - 1] = y;
+        }
     }
+};
+
+template <typename T, int K, int NR, typename CF>
+__device__ __forceinline__ void warp_partition_solve_t(const CF& coef, typename V2<T>::T (&d)[NR][K], int ln)
+{
+    PartSys<T, K, NR> a;
+    a.elim(coef, d, ln);
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) a.pcr(s, ln);
+    a.finish(d, ln);
+}
+
+template <typename T, int K, int NR1, int NR2, typename CF1, typename CF2>
+__device__ __forceinline__ void warp_partition_solve2_t(const CF1& coef1, typename V2<T>::T (&d1)[NR1][K],
+                                                        const CF2& coef2, typename V2<T>::T (&d2)[NR2][K], int ln)
+{
+    PartSys<T, K, NR1> a;
+    PartSys<T, K, NR2> b;
+    a.elim(coef1, d1, ln);
+    b.elim(coef2, d2, ln);
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) { a.pcr(s, ln); b.pcr(s, ln); }
+    a.finish(d1, ln);
+    b.finish(d2, ln);
 }
 
 // ---------------------------------------------------------------------------
@@ -587,8 +622,35 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
             typedef typename V2<T>::T T2;
             const double* dgu = is00 ? a.c.d0u : a.c.dgu;
             const double* dgw = is00 ? a.c.d0w : a.c.dgw;
-            {
-                T2 d[2][K];
+            // u*, v* (two right-hand sides of one matrix) and w* (its own matrix):
+            // two independent systems; in FP32 solved phase by phase side by side,
+            // in FP64 one after the other (side by side they would not fit the registers)
+            const float rlam = (float)(rk * lam);
+            auto cf = [&](int r, T& aa, T& bb, T& cc) {
+                if (r < nz) {
+                    if constexpr (sizeof(T) == sizeof(float)) {
+                        const int t = tpos(r);
+                        aa = HT[t]; cc = HT[K * 32 + t]; bb = HT[2 * K * 32 + t] - rlam;
+                    } else {
+                        aa = (T)(rk * __ldg(a.c.au + r));
+                        cc = (T)(rk * __ldg(a.c.cu + r));
+                        bb = (T)(1.0 + rk * (-lam + __ldg(dgu + r)));
+                    }
+                } else { aa = T(0); bb = T(1); cc = T(0); }
+            };
+            auto cfw = [&](int r, T& aa, T& bb, T& cc) {
+                if (r < nz - 1) {
+                    if constexpr (sizeof(T) == sizeof(float)) {
+                        const int t = tpos(r);
+                        aa = HT[3 * K * 32 + t]; cc = HT[4 * K * 32 + t]; bb = HT[5 * K * 32 + t] - rlam;
+                    } else {
+                        aa = (T)(rk * __ldg(a.c.aw + r));
+                        cc = (T)(rk * __ldg(a.c.cw + r));
+                        bb = (T)(1.0 + rk * (-lam + __ldg(dgw + r)));
+                    }
+                } else { aa = T(0); bb = T(1); cc = T(0); }
+            };
+            auto load_uv = [&](T2 (&d)[2][K]) {
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
                     const int r = r0 + i;
@@ -604,49 +666,45 @@ __device__ __forceinline__ void k_column_fd_tile_r_body(const ColArgs<R>& a, con
                         d[1][i] = mk2<T>(T(0), T(0));
                     }
                 }
-                const float rlam = (float)(rk * lam);
-                auto cf = [&](int r, T& aa, T& bb, T& cc) {
-                    if (r < nz) {
-                        if constexpr (sizeof(T) == sizeof(float)) {
-                            const int t = tpos(r);
-                            aa = HT[t]; cc = HT[K * 32 + t]; bb = HT[2 * K * 32 + t] - rlam;
-                        } else {
-                            aa = (T)(rk * __ldg(a.c.au + r));
-                            cc = (T)(rk * __ldg(a.c.cu + r));
-                            bb = (T)(1.0 + rk * (-lam + __ldg(dgu + r)));
-                        }
-                    } else { aa = T(0); bb = T(1); cc = T(0); }
-                };
-                warp_partition_solve_t<T, K, 2>(cf, d, ln);
-#pragma unroll
-                for (int i = 0; i < K; ++i) {
-                    SU[i * RP + ln] = mk2<R>((R)d[0][i].x, (R)d[0][i].y);
-                    SV[i * RP + ln] = mk2<R>((R)d[1][i].x, (R)d[1][i].y);
-                }
-            }
-            {
-                T2 dw[1][K];
+            };
+            auto load_w = [&](T2 (&dw)[1][K]) {
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
                     const TT x = SW[i * RP + ln];
                     dw[0][i] = r0 + i < nz - 1 ? mk2<T>((T)x.x, (T)x.y) : mk2<T>(T(0), T(0));
                 }
-                const float rlam = (float)(rk * lam);
-                auto cf = [&](int r, T& aa, T& bb, T& cc) {
-                    if (r < nz - 1) {
-                        if constexpr (sizeof(T) == sizeof(float)) {
-                            const int t = tpos(r);
-                            aa = HT[3 * K * 32 + t]; cc = HT[4 * K * 32 + t]; bb = HT[5 * K * 32 + t] - rlam;
-                        } else {
-                            aa = (T)(rk * __ldg(a.c.aw + r));
-                            cc = (T)(rk * __ldg(a.c.cw + r));
-                            bb = (T)(1.0 + rk * (-lam + __ldg(dgw + r)));
-                        }
-                    } else { aa = T(0); bb = T(1); cc = T(0); }
-                };
-                warp_partition_solve_t<T, K, 1>(cf, dw, ln);
+            };
+            auto store_uv = [&](const T2 (&d)[2][K]) {
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    SU[i * RP + ln] = mk2<R>((R)d[0][i].x, (R)d[0][i].y);
+                    SV[i * RP + ln] = mk2<R>((R)d[1][i].x, (R)d[1][i].y);
+                }
+            };
+            auto store_w = [&](const T2 (&dw)[1][K]) {
 #pragma unroll
                 for (int i = 0; i < K; ++i) SW[i * RP + ln] = mk2<R>((R)dw[0][i].x, (R)dw[0][i].y);
+            };
+            if constexpr (sizeof(T) == sizeof(float)) {
+                T2 d[2][K], dw[1][K];
+                load_uv(d);
+                load_w(dw);
+                warp_partition_solve2_t<T, K, 2, 1>(cf, d, cfw, dw, ln);
+                store_uv(d);
+                store_w(dw);
+            } else {
+                {
+                    T2 d[2][K];
+                    load_uv(d);
+                    warp_partition_solve_t<T, K, 2>(cf, d, ln);
+                    store_uv(d);
+                }
+                {
+                    T2 dw[1][K];
+                    load_w(dw);
+                    warp_partition_solve_t<T, K, 1>(cfw, dw, ln);
+                    store_w(dw);
+                }
             }
         };
         if (is00) helmholtz(double(0)); else helmholtz(R(0));
