@@ -30,6 +30,8 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     "channel_fd4_512x384x256": (512, 384, 256),
+    # the same channel with temperature (stable stratification, Ri_b = 0.1)
+    "channel_fd4_512x384x256_ri0.1": (512, 384, 256),
     "channel_fd4_256x256x128": (256, 256, 128),
     "channel_fd4_96x64x64": (96, 64, 64),
     # profiling size: production nz with a few GB on the device
@@ -86,7 +88,13 @@ def make_case(workload: str, prec: int, tile=None):
         f = inputs.loglaw_stratified(p, seed=10)
     else:
         p = config_channel_fd(nx, ny, nz, precision=prec)
+        if workload.endswith("_ri0.1"):
+            p = p.replace(isscalar=1, got=0.1, tbot=0.0, ttop=1.0)
         f = inputs.poiseuille_noise(p, seed=3)
+        if p.isscalar:
+            from hercules_b200.params import mesh, t_line
+            import numpy as np
+            f["t"] = np.broadcast_to(t_line(p, mesh(p)["zc"])[:, None, None], (p.nz, p.ny, p.nx)).copy()
     return (p.replace(tile=list(tile)) if tile else p), f
 
 
@@ -569,6 +577,8 @@ def main():
         base["data"] = "synthetic (seeded log-law + 5% Gaussian noise, linear T + 1% noise)"
     else:
         physics = "neutral closed channel, FD4 horizontal, FD2 vertical, RK3, dp_opt=2, nu=1/2800, dt=1e-3, zstretch=1"
+        if args.workload.endswith("_ri0.1"):
+            physics = physics.replace("neutral", "stably stratified (Ri_b = 0.1, T from 0 to 1, Pr = 0.71)")
     fb = nx * ny * nz * 8
     cfg = {"workload": args.workload, "grid": [nx, ny, nz], "physics": physics, "parallelism": f"replicas x{args.gpus}",
            "l2": f"working set larger than L2 (one FP64 field {fb / 1e6:.0f} MB, FP32 {fb / 2e6:.0f} MB)"}

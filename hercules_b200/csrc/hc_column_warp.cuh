@@ -814,7 +814,12 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_fd_tile_r(ColArgs<R>
 // solution may overwrite q_t. (One warp per column reading and writing a row a
 // lane: 76 -> 67 us mixed, 91 -> 68 us FP64 a launch at 256 x 256 x 128.)
 // ---------------------------------------------------------------------------
-template <int K> __host__ size_t column_t_tile_smem(size_t elem) { return (size_t)CT_COLS * ct_stride_e<K>(elem) * elem; }
+// FP32 storage: the tile and, after it, the per-level matrix rows of the sub-step
+// in FP32 (rk at, rk ct, 1 + rk dgt) in the [i][lane] order of the solves
+template <int K> __host__ size_t column_t_tile_smem(size_t elem)
+{
+    return (size_t)CT_COLS * ct_stride_e<K>(elem) * elem + (elem == sizeof(float2) ? (size_t)3 * K * 32 * sizeof(float) : 0);
+}
 
 template <typename R, int K>
 __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const uint3 blockIdx, const dim3 gridDim)
@@ -830,6 +835,17 @@ __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const
     constexpr int STR = CtLayout<TT>::template stride<K>();
     constexpr int RP = CtLayout<TT>::rp;
     TT* TQ = reinterpret_cast<TT*>(smem_raw);
+    // FP32 storage: the sub-step's matrix rows in FP32 after the tile
+    float* TB = reinterpret_cast<float*>(TQ + CT_COLS * STR);
+    if constexpr (sizeof(R) == sizeof(float)) {
+        const double rk = a.rk_c;
+        for (int r = threadIdx.x; r < nz; r += blockDim.x) {
+            const int t = (r % K) * 32 + r / K;
+            TB[t] = (float)(rk * __ldg(a.c.at + r));
+            TB[K * 32 + t] = (float)(rk * __ldg(a.c.ct + r));
+            TB[2 * K * 32 + t] = (float)(1.0 + rk * __ldg(a.c.dgt + r));
+        }
+    }
     {
         TT v[K];
 #pragma unroll
@@ -855,32 +871,54 @@ __device__ __forceinline__ void k_column_t_tile_body(const ColTArgs<R>& a, const
         const double lam = __ldg(a.c.hxt + l) + __ldg(a.c.hyt + m);
         const double* dg = is00 ? a.c.d0t : a.c.dgt;
         const int r0 = ln * K;
-        double2 d[1][K];
-#pragma unroll
-        for (int i = 0; i < K; ++i) {
-            const int r = r0 + i;
-            if (r < nz) {
-                const TT x = SQ[i * RP + ln];
-                d[0][i] = make_double2((double)x.x, (double)x.y);
-                if (is00 && r == 0) d[0][i].x += a.bct0;
-                if (is00 && r == nz - 1) d[0][i].x += a.bct1;
-            } else {
-                d[0][i] = make_double2(0, 0);
-            }
-        }
-        auto cf = [&](int r, double& aa, double& bb, double& cc) {
-            if (r < nz) {
-                aa = rk * __ldg(a.c.at + r);
-                cc = rk * __ldg(a.c.ct + r);
-                bb = 1.0 + rk * (-lam + __ldg(dg + r));
-            } else { aa = 0.0; bb = 1.0; cc = 0.0; }
-        };
-        warp_partition_solve<K, 1>(cf, d, ln);
         const bool tr = spec_truncated(l, m, a.g.ny, a.ltr, a.mtr);
+        if (sizeof(R) == sizeof(float) && !is00) {
+            // FP32 storage, every mode but the mean: the diagonally dominant
+            // Helmholtz system in FP32, as the momentum ones (the mean mode keeps
+            // FP64 with the wall constants)
+            const float rlam = (float)(rk * lam);
+            float2 df[1][K];
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            const double2 v = tr ? make_double2(0, 0) : d[0][i];
-            SQ[i * RP + ln] = mk2<R>((R)v.x, (R)v.y);
+            for (int i = 0; i < K; ++i) {
+                const TT x = SQ[i * RP + ln];
+                df[0][i] = r0 + i < nz ? make_float2((float)x.x, (float)x.y) : make_float2(0.0f, 0.0f);
+            }
+            auto cf = [&](int r, float& aa, float& bb, float& cc) {
+                if (r < nz) {
+                    const int t = (r % K) * 32 + r / K;
+                    aa = TB[t]; cc = TB[K * 32 + t]; bb = TB[2 * K * 32 + t] - rlam;
+                } else { aa = 0.0f; bb = 1.0f; cc = 0.0f; }
+            };
+            warp_partition_solve_t<float, K, 1>(cf, df, ln);
+#pragma unroll
+            for (int i = 0; i < K; ++i) SQ[i * RP + ln] = tr ? mk2<R>(R(0), R(0)) : mk2<R>((R)df[0][i].x, (R)df[0][i].y);
+        } else {
+            double2 d[1][K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                if (r < nz) {
+                    const TT x = SQ[i * RP + ln];
+                    d[0][i] = make_double2((double)x.x, (double)x.y);
+                    if (is00 && r == 0) d[0][i].x += a.bct0;
+                    if (is00 && r == nz - 1) d[0][i].x += a.bct1;
+                } else {
+                    d[0][i] = make_double2(0, 0);
+                }
+            }
+            auto cf = [&](int r, double& aa, double& bb, double& cc) {
+                if (r < nz) {
+                    aa = rk * __ldg(a.c.at + r);
+                    cc = rk * __ldg(a.c.ct + r);
+                    bb = 1.0 + rk * (-lam + __ldg(dg + r));
+                } else { aa = 0.0; bb = 1.0; cc = 0.0; }
+            };
+            warp_partition_solve<K, 1>(cf, d, ln);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const double2 v = tr ? make_double2(0, 0) : d[0][i];
+                SQ[i * RP + ln] = mk2<R>((R)v.x, (R)v.y);
+            }
         }
     }
     __syncthreads();
