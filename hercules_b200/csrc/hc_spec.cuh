@@ -887,6 +887,41 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
         //      registers until the projection, as the warp kernel keeps them in
         //      FP64 shared memory (the tiles hold the storage type)
         double2 us_[K], vs_[K], ws_[K];
+        if (sizeof(R) == sizeof(float) && !is00) {
+            // FP32 storage, every mode but the mean: the two diagonally dominant
+            // Helmholtz systems in FP32, side by side (as the FD column kernel);
+            // the results join the FP64 projection
+            float2 d[2][K], dw[1][K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                const int r = r0 + i;
+                const TT xu = SU[i * RP + ln], xv = SV[i * RP + ln], xw = SW[i * RP + ln];
+                d[0][i] = r < nz ? make_float2((float)xu.x, (float)xu.y) : make_float2(0.0f, 0.0f);
+                d[1][i] = r < nz ? make_float2((float)xv.x, (float)xv.y) : make_float2(0.0f, 0.0f);
+                dw[0][i] = r < nz - 1 ? make_float2((float)xw.x, (float)xw.y) : make_float2(0.0f, 0.0f);
+            }
+            auto cfu = [&](int r, float& aa, float& bb, float& cc) {
+                if (r < nz) {
+                    aa = (float)(rk * __ldg(a.c.au + r));
+                    cc = (float)(rk * __ldg(a.c.cu + r));
+                    bb = (float)(1.0 + rk * (-lam + __ldg(dgu + r)));
+                } else { aa = 0.0f; bb = 1.0f; cc = 0.0f; }
+            };
+            auto cfw = [&](int r, float& aa, float& bb, float& cc) {
+                if (r < nz - 1) {
+                    aa = (float)(rk * __ldg(a.c.aw + r));
+                    cc = (float)(rk * __ldg(a.c.cw + r));
+                    bb = (float)(1.0 + rk * (-lam + __ldg(dgw + r)));
+                } else { aa = 0.0f; bb = 1.0f; cc = 0.0f; }
+            };
+            warp_partition_solve2_t<float, K, 2, 1>(cfu, d, cfw, dw, ln);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                us_[i] = make_double2((double)d[0][i].x, (double)d[0][i].y);
+                vs_[i] = make_double2((double)d[1][i].x, (double)d[1][i].y);
+                ws_[i] = make_double2((double)dw[0][i].x, (double)dw[0][i].y);
+            }
+        } else {
         {
             double2 d[2][K];
 #pragma unroll
@@ -930,6 +965,7 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
             warp_partition_solve<K, 1>(cf, dw, ln);
 #pragma unroll
             for (int i = 0; i < K; ++i) ws_[i] = dw[0][i];
+        }
         }
         // ---- phi: source (i kx u* + i ky v* + dw*/dz) / dt, zero on the Nyquist row
         const double2 DX = __ldg(a.c.dx + l), DY = __ldg(a.c.dy + m);
