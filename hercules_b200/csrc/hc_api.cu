@@ -203,11 +203,11 @@ enum { F_U, F_V, F_W, F_P, F_T, F_FF, F_GG, F_HH, F_SS, F_QU, F_QV, F_QW, F_UHX,
 // kernel categories for the optional per-launch CUDA-event profile
 enum { K_BEGIN, K_RHS_MOM, K_FFT_X_FWD, K_FFT_Y_FWD, K_COLUMN, K_FFT_Y_INV, K_FFT_X_INV,
        K_RHS_T, K_COLUMN_T, K_DIV, K_STATS, K_FINAL, K_SPEC_PROD, K_SPEC_ASM, K_SPEC_AUX, K_ADJ_COLUMN,
-       K_ADJ_RHS, K_FFT2D_FWD, K_FFT2D_INV, K_NCAT };
+       K_ADJ_RHS, K_FFT2D_FWD, K_FFT2D_INV, K_SPEC_PRODFX, K_NCAT };
 static const char* K_NAMES[K_NCAT] = {"substep_begin", "rhs_momentum", "fft_x_r2c", "fft_y_fwd", "column_fd",
                                       "fft_y_inv", "fft_x_c2r", "rhs_temperature", "column_t", "div_check",
                                       "stats", "finalize", "spec_products", "spec_assemble", "aux", "adj_column",
-                                      "adj_rhs", "fft2d_fwd", "fft2d_inv"};
+                                      "adj_rhs", "fft2d_fwd", "fft2d_inv", "spec_products_fx"};
 
 // spectral-path buffers (cds = 3), each n values of the storage type: the half
 // spectra of the state and histories, phi, the divergence, the assembled
@@ -284,6 +284,8 @@ struct hc_handle {
     int fft_tx, fft_ty;      // 1: the compile-time-length kernels serve x / y
     int fft2d;               // 1: the fused 2-D transform kernels (hc_fft2d.cuh) serve both
     int f2_ncl[2];           // their persistent clusters resident at once: forward, inverse
+    int spx;                 // 1: the spectral products and their x transform in one kernel (k_spec_products_fx)
+    int spx_minb;            // its blocks resident an SM
     FftPlan px, py;
     double2* wpack;
     int rows_x, tl_y, col_threads, col_warp;

@@ -126,6 +126,64 @@ template <typename R> static int fft2d_dispatch(hc_handle* h, int op, const F2Ar
     return HC_ERR_UNSUPPORTED;
 }
 
+// ---------------------------------------------------------------------------
+// the spectral products fused with their forward x transform (hc_spec.cuh):
+// x half lengths with an instantiation
+// ---------------------------------------------------------------------------
+#define HC_SPX_LENGTHS(X) X(16) X(32) X(64) X(128) X(256)
+
+// op 0: raise the shared-memory limit, note the resident blocks; 1: launch
+template <typename R, int N> static int spx_op(hc_handle* h, int op, const ProdFxArgs<R>* a, dim3 grid)
+{
+    constexpr size_t sm = SpxCfg<R, N, HC_FFT_T_RMAX>::smem;
+    // above 100 KB of shared memory (FP64 at nx/2 = 256) fewer than two blocks
+    // fit an SM: the separate kernels run
+    if constexpr (sm > 100 * 1024) {
+        return HC_ERR_UNSUPPORTED;
+    } else {
+        void (*k)(ProdFxArgs<R>) = k_spec_products_fx<R, N, HC_FFT_T_RMAX>;
+        if (op == 0) {
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->spx_minb, k, SpxCfg<R, N, HC_FFT_T_RMAX>::NT, sm) != cudaSuccess ||
+                h->spx_minb < 1) {
+                cudaGetLastError();
+                return HC_ERR_UNSUPPORTED;
+            }
+            return HC_OK;
+        }
+        k<<<grid, SpxCfg<R, N, HC_FFT_T_RMAX>::NT, sm, h->st>>>(*a);
+        return HC_OK;
+    }
+}
+
+template <typename R> static int spx_dispatch(hc_handle* h, int op, const ProdFxArgs<R>* a, dim3 grid)
+{
+    switch (h->g.nxh) {
+#define HC_SPX_CASE(N) case N: return spx_op<R, N>(h, op, a, grid);
+    HC_SPX_LENGTHS(HC_SPX_CASE)
+#undef HC_SPX_CASE
+    }
+    return HC_ERR_UNSUPPORTED;
+}
+
+// Levels a block of k_spec_products_fx: the chunk (4..SPEC_KCHUNK_MAX) whose
+// grid of ny x chunks blocks fills its last wave best, each chunk's two extra
+// start-up levels counted as extra reads
+static int spx_kchunk(const hc_handle* h)
+{
+    const int nz = h->p.nz, ny = h->g.ny;
+    const double slots = 148.0 * h->spx_minb;
+    int best = nz < SPEC_KCHUNK_MAX ? nz : SPEC_KCHUNK_MAX;
+    double bcost = 1e300;
+    for (int kc = 4; kc <= SPEC_KCHUNK_MAX && kc <= nz; ++kc) {
+        const double nb = (double)ny * ((nz + kc - 1) / kc);
+        const double waves = nb / slots;
+        const double cost = ceil(waves) / waves * (1.0 + 2.0 / kc);
+        if (cost < bcost - 1e-12) { bcost = cost; best = kc; }
+    }
+    return best;
+}
+
 template <typename R> static int fft_t_setup(hc_handle* h)
 {
     int rc = HC_OK;
@@ -193,6 +251,14 @@ static int build_fft(hc_handle* h)
     if (h->fft_tx && h->fft_ty && h->p.tile[0] == -1) {
         const int rc = h->rsz == sizeof(double) ? fft2d_dispatch<double>(h, 0, nullptr, 0) : fft2d_dispatch<float>(h, 0, nullptr, 0);
         h->fft2d = rc == HC_OK;
+    }
+    // the spectral products with their x transform in one kernel: templated x
+    // transforms of an instantiated length, the separate y transform after them
+    h->spx = 0;
+    if (h->p.cds == 3 && h->fft_tx && !h->fft2d) {
+        const int rc = h->rsz == sizeof(double) ? spx_dispatch<double>(h, 0, nullptr, dim3())
+                                                : spx_dispatch<float>(h, 0, nullptr, dim3());
+        h->spx = rc == HC_OK;
     }
     const size_t c2 = 2 * h->rsz;     // bytes of one complex
     h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : (h->rsz == sizeof(double) ? 1024 : 2048) / nxh;

@@ -11,7 +11,7 @@ static int spec_kchunk(const hc_handle* h, long long columns)
     const long long blocks = (columns + 255) / 256;
     long long kc = blocks * h->p.nz / (8LL * 148);
     if (kc < 4) kc = 4;
-    if (kc > 32) kc = 32;
+    if (kc > SPEC_KCHUNK_MAX) kc = SPEC_KCHUNK_MAX;
     if (kc > h->p.nz) kc = h->p.nz;
     return (int)kc;
 }
@@ -115,14 +115,32 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         t_ghost_bottom(h, pa.tbs, pa.tba);
         pa.inv_coe = 1.0 / (p.issk == 1 ? 0.5 : 1.0);
         pa.closed = p.ochannel == 0; pa.dp3 = p.dp_opt == 3; pa.scalar = p.isscalar == 1; pa.skew = p.issk == 1;
-        pa.kchunk = spec_kchunk(h, g.nxy); pa.halt = halt;
-        prof_begin(h, K_SPEC_PROD);
-        k_spec_products<R><<<dim3((unsigned)((g.nxy + 255) / 256), (p.nz + pa.kchunk - 1) / pa.kchunk), 256, 0, h->st>>>(pa);
-        CKL();
+        pa.halt = halt;
         const R* fin[8];
         T2* fout[8];
         for (int f = 0; f < 8; ++f) { fin[f] = Q[SP_W0 + f]; fout[f] = S[SP_W0 + f]; }
-        if ((rc = fft_forward<R>(h, fin, fout, 8))) return rc;
+        // pairs of points: the fields must be aligned to two values
+        bool fx = h->spx && !h->rec;
+        auto al = [&](const void* q) { return ((uintptr_t)q & (2 * sizeof(R) - 1)) == 0; };
+        fx = fx && al(pa.u) && al(pa.v) && al(pa.w) && al(pa.t);
+        for (int f = 0; f < 6; ++f) fx = fx && (!pa.d[f] || al(pa.d[f]));
+        if (fx) {
+            ProdFxArgs<R> fa;
+            fa.p = pa;
+            for (int f = 0; f < 8; ++f) fa.p.out[f] = (R*)S[SP_W0 + f];
+            fa.p.kchunk = spx_kchunk(h);
+            fa.tw = fft_tw<R>(h, 0); fa.wp = fft_tw<R>(h, 2); fa.scale = (R)(1.0 / p.nx);
+            prof_begin(h, K_SPEC_PRODFX);
+            if ((rc = spx_dispatch<R>(h, 1, &fa, dim3((unsigned)g.ny, (p.nz + fa.p.kchunk - 1) / fa.p.kchunk)))) return rc;
+            CKL();
+            if ((rc = fft_forward<R>(h, fin, fout, 8, true))) return rc;
+        } else {
+            pa.kchunk = spec_kchunk(h, g.nxy);
+            prof_begin(h, K_SPEC_PROD);
+            k_spec_products<R><<<dim3((unsigned)((g.nxy + 255) / 256), (p.nz + pa.kchunk - 1) / pa.kchunk), 256, 0, h->st>>>(pa);
+            CKL();
+            if ((rc = fft_forward<R>(h, fin, fout, 8))) return rc;
+        }
     }
     // right-hand sides and new histories, mode by mode
     {
@@ -205,7 +223,13 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
     fi.u = (const R*)h->fld[F_U]; fi.v = (const R*)h->fld[F_V]; fi.w = (const R*)h->fld[F_W];
     fi.p = nullptr; fi.t = nullptr;
     prof_begin(h, K_DIV);
-    k_spec_div_reduce<R><<<(unsigned)h->nbd, 256, 0, h->st>>>(Q[SP_W0 + 3], fi, g.n, h->part_div + (long long)sub * h->pd_stride * 3);
+    const R* dv = Q[SP_W0 + 3];
+    double* dp = h->part_div + (long long)sub * h->pd_stride * 3;
+    auto a16 = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
+    if (a16(dv) && a16(fi.u) && a16(fi.v) && a16(fi.w))
+        k_spec_div_reduce<R, 16 / sizeof(R)><<<(unsigned)h->nbd, 256, 0, h->st>>>(dv, fi, g.n, dp);
+    else
+        k_spec_div_reduce<R, 1><<<(unsigned)h->nbd, 256, 0, h->st>>>(dv, fi, g.n, dp);
     CKL();
     return HC_OK;
 }

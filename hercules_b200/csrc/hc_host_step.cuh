@@ -50,12 +50,15 @@ template <typename R> static const typename V2<R>::T* fft_tw(hc_handle* h, int w
     return which == 0 ? t : (which == 1 ? t + h->g.nxh : t + h->g.nxh + h->g.ny);
 }
 
-// x then y forward transform of nf physical fields into half spectra
-template <typename R> static int fft_forward(hc_handle* h, const R* const* in, typename V2<R>::T* const* out, int nf)
+// x then y forward transform of nf physical fields into half spectra (x_done:
+// out already holds the x half spectra, only the y transform runs)
+template <typename R> static int fft_forward(hc_handle* h, const R* const* in, typename V2<R>::T* const* out, int nf,
+                                             bool x_done = false)
 {
     typedef typename V2<R>::T T2;
     const int* halt = &h->sc->nan_flag;
     if (nf < 1 || nf > HC_FFT_MAXF) return HC_ERR_ARG;
+    if (x_done && h->fft2d) return HC_ERR_ARG;
     if (h->fft2d && !h->rec && nf <= HC_FFT_TMAXF) {
         F2Args<R> a;
         memset(&a, 0, sizeof(a));
@@ -69,7 +72,8 @@ template <typename R> static int fft_forward(hc_handle* h, const R* const* in, t
         CKL();
         return HC_OK;
     }
-    if (h->fft_tx) {
+    if (x_done) {
+    } else if (h->fft_tx) {
         FxArgs<R> a;
         memset(&a, 0, sizeof(a));
         for (int f = 0; f < nf; ++f) { a.in[f] = in[f]; a.out[f] = out[f]; }

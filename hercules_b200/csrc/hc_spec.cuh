@@ -186,15 +186,79 @@ template <typename R> struct ProdArgs {
 // us; bounded to two blocks it spilled and took 211 us)
 template <typename R> struct AsmMinBlocks { static constexpr int v = sizeof(R) == sizeof(float) ? 2 : 1; };
 
+// The eight products of one point (the arithmetic both product kernels share):
+// z neighbours of u, v, w (m: level below, k, p: above) and t (k, p) with their
+// ghost values, the six skew derivatives at level k (skew), the body force (bf,
+// null: none) and the z factors l_t, l_b, 1/dz, 1/dz_t of level k.
 template <typename R>
-__global__ void __launch_bounds__(256, 3) k_spec_products(ProdArgs<R> a)
+__device__ __forceinline__ void spec_point_products(const ProdArgs<R>& a, double dpx, double got, double ic,
+                                                    double um_, double uk, double up, double vm, double vk, double vp,
+                                                    double wm, double wk, double wp, double tk, double tp,
+                                                    const R* dd, const double* bf, double lt, double lb, double rdz,
+                                                    double rdzt, double o[8])
+{
+    const double um = a.um;
+    const double a1u = up * lt + uk * (1.0 - lt), a2u = um_ * lb + uk * (1.0 - lb);
+    const double a1v = vp * lt + vk * (1.0 - lt), a2v = vm * lb + vk * (1.0 - lb);
+    double cu = ic * (a.dp3 ? a.fc * (vk - a.vg) : dpx) - (a1u * wk - a2u * wm) * rdz;
+    double cv = ic * (a.dp3 ? a.fc * (a.ug - uk - um) : 0.0) - (a1v * wk - a2v * wm) * rdz;
+    const double hp = 0.5 * (wk + wp), hm = 0.5 * (wk + wm);
+    const double tmpw = (hp * hp - hm * hm) * rdzt;
+    double cw = a.scalar ? ic * (got * ((1.0 - lt) * tk + lt * tp - a.t_ref)) - tmpw : -tmpw;
+    if (a.skew) {
+        const double wc = 0.5 * (wk + wm);
+        cu -= uk * (double)dd[0] + vk * (double)dd[1] + (a1u - a2u) * rdz * wc;
+        cv -= uk * (double)dd[2] + vk * (double)dd[3] + (a1v - a2v) * rdz * wc;
+        cw -= a1u * (double)dd[4] + a1v * (double)dd[5] + wk * ((hp - hm) * rdzt);
+    }
+    if (bf) {
+        cu += ic * bf[0];
+        cv += ic * bf[1];
+        cw += ic * bf[2];
+    }
+    o[0] = uk * uk; o[1] = uk * vk; o[2] = vk * vk; o[3] = a1u * wk; o[4] = a1v * wk;
+    o[5] = cu; o[6] = cv; o[7] = cw;
+}
+
+// k_spec_products stages what a level reads (u, v, w, t one level up and the six
+// skew derivatives) in shared memory with per-thread cp.async copies, D levels
+// ahead of use: three with FP32 storage, one with FP64. Each thread copies and
+// reads only its own words, so the ring needs no block barrier; a slot is
+// refilled one level after it was read. Held in registers one level ahead, the
+// FP32 loads carried half the bytes of the FP64 ones and the kernel held 0.58 of
+// the HBM bandwidth at 256 x 256 x 128. The z factors of the chunk sit in shared
+// memory too (a chunk has at most SPEC_KCHUNK_MAX levels).
+#define SPEC_KCHUNK_MAX 32
+template <typename R> struct ProdAhead { static constexpr int v = sizeof(R) == sizeof(float) ? 3 : 1; };
+constexpr int PROD_NT = 256, PROD_NW = 10;   // threads a block, words a level
+
+template <int B> __device__ __forceinline__ void sp_cp(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void sp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void sp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <typename R>
+__global__ void __launch_bounds__(PROD_NT, 3) k_spec_products(ProdArgs<R> a)
 {
     if (a.halt && *a.halt) return;
     const Geo& g = a.g;
-    const long long ij = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ij >= g.nxy) return;
     const int nz = g.nz;
     const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    constexpr int D = ProdAhead<R>::v, NS = D + 1;
+    // l_t, l_b, 1/dz, 1/dz_t of the chunk's levels; the ring [slot][word][thread]
+    __shared__ double zs[4][SPEC_KCHUNK_MAX];
+    __shared__ R ring[NS][PROD_NW][PROD_NT];
+    for (int i = threadIdx.x; i < 4 * (k1 - k0); i += blockDim.x) {
+        const int f = i / (k1 - k0), k = k0 + i % (k1 - k0);
+        zs[f][k - k0] = f == 0 ? ldz(g.z.l_t, k) : f == 1 ? ldz(g.z.l_b, k) : f == 2 ? a.rdz[k] : a.rdzt[k];
+    }
+    __syncthreads();
+    const int tid = threadIdx.x;
+    const long long ij = (long long)blockIdx.x * PROD_NT + tid;
+    if (ij >= g.nxy) return;
     const long long nxy = g.nxy;
     const double um = a.um;
     // stored value of the level a vertical neighbour reads (clamped; w reads
@@ -212,77 +276,244 @@ __global__ void __launch_bounds__(256, 3) k_spec_products(ProdArgs<R> a)
         if (!a.scalar) return 0.0;
         return k < 0 ? a.tbs * (double)r + a.tba : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
     };
-    // the four fields at level L, in the storage type
-    struct Lv { R u, v, w, t; };
-    auto fetch = [&](int L, Lv& o) {
-        o.u = raw(a.u, iC(L)); o.v = raw(a.v, iC(L)); o.w = raw(a.w, iW(L));
-        o.t = a.scalar ? raw(a.t, iC(L)) : R(0);
+    // the copies of level k (u, v, w, t at level k+1; derivatives at level k) into
+    // a slot, as one commit group (empty past the chunk, so that the group count
+    // stays one a level)
+    auto issue = [&](int k, int slot) {
+        if (k < k1) {
+            const int L = k + 1;
+            sp_cp<sizeof(R)>(&ring[slot][0][tid], a.u + (long long)iC(L) * nxy + ij);
+            sp_cp<sizeof(R)>(&ring[slot][1][tid], a.v + (long long)iC(L) * nxy + ij);
+            sp_cp<sizeof(R)>(&ring[slot][2][tid], a.w + (long long)iW(L) * nxy + ij);
+            if (a.scalar) sp_cp<sizeof(R)>(&ring[slot][3][tid], a.t + (long long)iC(L) * nxy + ij);
+            if (a.skew) {
+#pragma unroll
+                for (int f = 0; f < 6; ++f) sp_cp<sizeof(R)>(&ring[slot][4 + f][tid], a.d[f] + (long long)k * nxy + ij);
+            }
+        }
+        sp_commit();
     };
+#pragma unroll
+    for (int s = 0; s < D; ++s) issue(k0 + s, s);
     const double dpx = a.sc->dpx_drive, got = a.sc->got, ic = a.inv_coe;
-    Lv l0, l1;
-    fetch(k0 - 1, l0); fetch(k0, l1);
-    double um_ = gU(l0.u, k0 - 1), uk = gU(l1.u, k0), vm = gV(l0.v, k0 - 1), vk = gV(l1.v, k0);
-    double wm = gW(l0.w, k0 - 1), wk = gW(l1.w, k0), tk = gT(l1.t, k0);
-    // the loads a level needs (level k+1 of the fields, level k of the skew
-    // derivatives and of the z factors) are issued one level ahead, in the
-    // storage type, so that their latency overlaps the previous level's
-    // arithmetic and stores
-    Lv lp;
-    fetch(k0 + 1, lp);
-    R dd[6] = {0, 0, 0, 0, 0, 0};
-    auto ld_d = [&](int k, R* o) {
-        if (a.skew) {
-#pragma unroll
-            for (int f = 0; f < 6; ++f) o[f] = a.d[f][(long long)k * nxy + ij];
-        }
-    };
-    ld_d(k0, dd);
-    double zf[4] = {ldz(g.z.l_t, k0), ldz(g.z.l_b, k0), a.rdz[k0], a.rdzt[k0]};
-    for (int k = k0; k < k1; ++k) {
-        Lv ln;
-        R dn[6] = {0, 0, 0, 0, 0, 0};
-        double zn[4] = {0, 0, 0, 0};
-        if (k + 1 < k1) {
-            fetch(k + 2, ln);
-            ld_d(k + 1, dn);
-            zn[0] = ldz(g.z.l_t, k + 1); zn[1] = ldz(g.z.l_b, k + 1); zn[2] = a.rdz[k + 1]; zn[3] = a.rdzt[k + 1];
-        }
-        const double up = gU(lp.u, k + 1), vp = gV(lp.v, k + 1), wp = gW(lp.w, k + 1), tp = gT(lp.t, k + 1);
-        const double lt = zf[0], lb = zf[1], rdz = zf[2], rdzt = zf[3];
-        const long long q = (long long)k * nxy + ij;
-        const double a1u = up * lt + uk * (1.0 - lt), a2u = um_ * lb + uk * (1.0 - lb);
-        const double a1v = vp * lt + vk * (1.0 - lt), a2v = vm * lb + vk * (1.0 - lb);
-        double cu = ic * (a.dp3 ? a.fc * (vk - a.vg) : dpx) - (a1u * wk - a2u * wm) * rdz;
-        double cv = ic * (a.dp3 ? a.fc * (a.ug - uk - um) : 0.0) - (a1v * wk - a2v * wm) * rdz;
-        const double hp = 0.5 * (wk + wp), hm = 0.5 * (wk + wm);
-        const double tmpw = (hp * hp - hm * hm) * rdzt;
-        double cw = a.scalar ? ic * (got * ((1.0 - lt) * tk + lt * tp - a.t_ref)) - tmpw : -tmpw;
-        if (a.skew) {
-            const double wc = 0.5 * (wk + wm);
-            cu -= uk * (double)dd[0] + vk * (double)dd[1] + (a1u - a2u) * rdz * wc;
-            cv -= uk * (double)dd[2] + vk * (double)dd[3] + (a1v - a2v) * rdz * wc;
-            cw -= a1u * (double)dd[4] + a1v * (double)dd[5] + wk * ((hp - hm) * rdzt);
-        }
-        a.out[0][q] = (R)(uk * uk);
-        a.out[1][q] = (R)(uk * vk);
-        a.out[2][q] = (R)(vk * vk);
-        a.out[3][q] = (R)(a1u * wk);
-        a.out[4][q] = (R)(a1v * wk);
-        if (a.bf[0]) {
-            cu += ic * (double)a.bf[0][q];
-            cv += ic * (double)a.bf[1][q];
-            cw += ic * (double)a.bf[2][q];
-        }
-        a.out[5][q] = (R)cu;
-        a.out[6][q] = (R)cv;
-        a.out[7][q] = (R)cw;
-        um_ = uk; uk = up; vm = vk; vk = vp; wm = wk; wk = wp; tk = tp;
-        lp = ln;
-#pragma unroll
-        for (int f = 0; f < 6; ++f) dd[f] = dn[f];
-#pragma unroll
-        for (int f = 0; f < 4; ++f) zf[f] = zn[f];
+    double um_, uk, vm, vk, wm, wk, tk;
+    {
+        const R u0 = raw(a.u, iC(k0 - 1)), v0 = raw(a.v, iC(k0 - 1)), w0 = raw(a.w, iW(k0 - 1));
+        const R u1 = raw(a.u, iC(k0)), v1 = raw(a.v, iC(k0)), w1 = raw(a.w, iW(k0));
+        const R t1 = a.scalar ? raw(a.t, iC(k0)) : R(0);
+        um_ = gU(u0, k0 - 1); uk = gU(u1, k0); vm = gV(v0, k0 - 1); vk = gV(v1, k0);
+        wm = gW(w0, k0 - 1); wk = gW(w1, k0); tk = gT(t1, k0);
     }
+    // slot s of the unrolled inner loop holds level kb + s
+    for (int kb = k0; kb < k1; kb += NS) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int k = kb + s;
+            if (k >= k1) break;
+            sp_wait<D - 1>();      // level k's group (D - 1 newer ones may still run)
+            R cur[PROD_NW];
+#pragma unroll
+            for (int f = 0; f < PROD_NW; ++f) cur[f] = ring[s][f][tid];
+            issue(k + D, (s + D) % NS);   // refills the slot of level k - 1
+            const double up = gU(cur[0], k + 1), vp = gV(cur[1], k + 1), wp = gW(cur[2], k + 1), tp = gT(cur[3], k + 1);
+            const long long q = (long long)k * nxy + ij;
+            double bfv[3], o[8];
+            if (a.bf[0]) { bfv[0] = (double)a.bf[0][q]; bfv[1] = (double)a.bf[1][q]; bfv[2] = (double)a.bf[2][q]; }
+            spec_point_products<R>(a, dpx, got, ic, um_, uk, up, vm, vk, vp, wm, wk, wp, tk, tp, cur + 4,
+                                   a.bf[0] ? bfv : nullptr, zs[0][k - k0], zs[1][k - k0], zs[2][k - k0], zs[3][k - k0], o);
+#pragma unroll
+            for (int f = 0; f < 8; ++f) a.out[f][q] = (R)o[f];
+            um_ = uk; uk = up; vm = vk; vk = vp; wm = wk; wk = wp; tk = tp;
+        }
+    }
+    sp_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// k_spec_products_fx: the products of k_spec_products and their forward x
+// transform (the x half of dev_fft_nonlinear_cmplx / real_2_cmplx) in one pass.
+// A block of 128 threads takes one y row j and a chunk of levels. Per level each
+// thread forms the eight products at its x pairs (2e, 2e+1), rounded to the
+// storage type as the separate kernel stores them; the eight rows then go
+// through the shared-memory passes of k_fft_x_r2c_t (same plan, same arithmetic)
+// and leave as x half spectra, row k ny + j of nx/2 modes, which the y transform
+// takes in place. The physical products never reach HBM: a point moves 10 words
+// in and 8 out, against 10 + 8 for the products and 8 + 8 for the transform.
+// What level k+1 reads is copied (cp.async, each thread its own pairs) into the
+// other of two shared slots while level k is formed and transformed; a slot is
+// refilled one level after it was read, two block barriers later.
+// ---------------------------------------------------------------------------
+template <typename R> struct ProdFxArgs {
+    ProdArgs<R> p;                     // p.out[f]: the x half spectra (complex rows)
+    const typename V2<R>::T* tw;       // exp(-2 pi i e / (nx/2)), e < nx/2
+    const typename V2<R>::T* wp;       // exp(-2 pi i l / nx), l < nx/2
+    R scale;                           // 1/nx
+};
+template <typename R, int N, int RMAX> struct SpxCfg {
+    static constexpr int NT = 128, L = 8, EPT = (N + NT - 1) / NT;
+    static constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride;
+    // the passes' two buffers (the product rows share the second when there are
+    // two passes or more: the first pass has read them before it is written),
+    // two slots of 10 rows of pairs
+    static constexpr int np = FPlan<N, RMAX>::npass;
+    static constexpr size_t smem = ((size_t)(np >= 2 ? 2 : 3) * L * LS + (size_t)2 * PROD_NW * N) *
+                                   sizeof(typename V2<R>::T);
+    // FP32 up to nx/2 = 128: four blocks an SM (128 registers a thread; bounded
+    // to five, with the column values carried in the storage type, it took 11 %
+    // more instructions and 184 against 165 us at 256 x 256 x 128)
+    static constexpr int minb = sizeof(R) == sizeof(float) && N <= 128 ? 4 : 1;
+};
+
+template <typename R, int N, int RMAX>
+__global__ void __launch_bounds__(128, (SpxCfg<R, N, RMAX>::minb)) k_spec_products_fx(ProdFxArgs<R> A)
+{
+    typedef typename V2<R>::T T2;
+    typedef SpxCfg<R, N, RMAX> CF;
+    constexpr int NT = CF::NT, L = CF::L, EPT = CF::EPT, G = CF::G, LS = CF::LS;
+    const ProdArgs<R>& a = A.p;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (a.halt && *a.halt) return;
+    const Geo& g = a.g;
+    const int nz = g.nz, j = blockIdx.x;
+    const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    // C: the product rows; A, B: the passes' buffers (the last pass lands in Z);
+    // slot [2][word][pair]: u, v, w, t of level k+1 and the derivatives of level k
+    constexpr int np = FPlan<N, RMAX>::npass;
+    static_assert(np == CF::np, "plan of the shared-memory layout");
+    T2* Ab = reinterpret_cast<T2*>(smem_raw);
+    T2* Bb = Ab + L * LS;
+    T2* Cb = np >= 2 ? Bb : Bb + L * LS;
+    T2* slot = Bb + (np >= 2 ? 1 : 2) * L * LS;
+    T2* Z = (np % 2 == 1) ? Ab : Bb;
+    __shared__ double zs[4][SPEC_KCHUNK_MAX];
+    for (int i = threadIdx.x; i < 4 * (k1 - k0); i += blockDim.x) {
+        const int f = i / (k1 - k0), k = k0 + i % (k1 - k0);
+        zs[f][k - k0] = f == 0 ? ldz(g.z.l_t, k) : f == 1 ? ldz(g.z.l_b, k) : f == 2 ? a.rdz[k] : a.rdzt[k];
+    }
+    const int tid = threadIdx.x;
+    const long long nxy = g.nxy, row = (long long)j * g.nx;
+    const double um = a.um;
+    const int nz1 = nz - 1;
+    auto iC = [&](int k) { return k < 0 ? 0 : (k > nz1 ? nz1 : k); };
+    auto iW = [&](int k) { return k < 0 ? 0 : (k > nz1 ? nz - 2 : k); };
+    auto gU = [&](R r, int k) -> double {
+        return (k < 0 || (k >= nz && a.closed)) ? -(double)r - 2.0 * um : (double)r;
+    };
+    auto gV = [&](R r, int k) -> double { return (k < 0 || (k >= nz && a.closed)) ? -(double)r : (double)r; };
+    auto gW = [&](R r, int k) -> double { return k < 0 ? 0.0 : (k >= nz ? -(double)r : (double)r); };
+    auto gT = [&](R r, int k) -> double {
+        if (!a.scalar) return 0.0;
+        return k < 0 ? a.tbs * (double)r + a.tba : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
+    };
+    // the pair (2e, 2e+1) of a field at a stored level
+    auto gp = [&](const R* f, int kk, int e) { return f + (long long)kk * nxy + row + 2 * e; };
+    auto ld2 = [&](const R* f, int kk, int e) -> T2 { return *reinterpret_cast<const T2*>(gp(f, kk, e)); };
+    // copies of what level k reads into slot sl, one commit group
+    auto issue = [&](int k, int sl) {
+        T2* S = slot + sl * PROD_NW * N;
+        const int Lk = k + 1;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = tid + i * NT;
+            if (e >= N) continue;
+            sp_cp<sizeof(T2)>(S + 0 * N + e, gp(a.u, iC(Lk), e));
+            sp_cp<sizeof(T2)>(S + 1 * N + e, gp(a.v, iC(Lk), e));
+            sp_cp<sizeof(T2)>(S + 2 * N + e, gp(a.w, iW(Lk), e));
+            if (a.scalar) sp_cp<sizeof(T2)>(S + 3 * N + e, gp(a.t, iC(Lk), e));
+            if (a.skew) {
+#pragma unroll
+                for (int f = 0; f < 6; ++f) sp_cp<sizeof(T2)>(S + (4 + f) * N + e, gp(a.d[f], k, e));
+            }
+        }
+        sp_commit();
+    };
+    issue(k0, 0);
+    __syncthreads();                 // zs
+    auto cx = [](T2 v, int c) -> R { return c == 0 ? v.x : v.y; };
+    const double dpx = a.sc->dpx_drive, got = a.sc->got, ic = a.inv_coe;
+    // the columns' carried values: [element][x of the pair]
+    double um_[EPT][2], uk[EPT][2], vm[EPT][2], vk[EPT][2], wm[EPT][2], wk[EPT][2], tk[EPT][2];
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+        const int e = tid + i * NT;
+        if (e >= N) continue;
+        const T2 u0 = ld2(a.u, iC(k0 - 1), e), v0 = ld2(a.v, iC(k0 - 1), e), w0 = ld2(a.w, iW(k0 - 1), e);
+        const T2 u1 = ld2(a.u, iC(k0), e), v1 = ld2(a.v, iC(k0), e), w1 = ld2(a.w, iW(k0), e);
+        const T2 t1 = a.scalar ? ld2(a.t, iC(k0), e) : mk2<R>(R(0), R(0));
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            um_[i][c] = gU(cx(u0, c), k0 - 1); uk[i][c] = gU(cx(u1, c), k0);
+            vm[i][c] = gV(cx(v0, c), k0 - 1); vk[i][c] = gV(cx(v1, c), k0);
+            wm[i][c] = gW(cx(w0, c), k0 - 1); wk[i][c] = gW(cx(w1, c), k0); tk[i][c] = gT(cx(t1, c), k0);
+        }
+    }
+    const SmemIO<T2, LS, G> cin{Cb}, zout{Z};
+    const R zero = R(0);
+    for (int k = k0; k < k1; ++k) {
+        const int sl = (k - k0) & 1;
+        sp_wait<0>();
+        const T2* S = slot + sl * PROD_NW * N;
+        // the thread's own pairs of level k, then level k+1's copies into the other slot
+        T2 cur[EPT][PROD_NW];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = tid + i * NT;
+#pragma unroll
+            for (int f = 0; f < PROD_NW; ++f) cur[i][f] = e < N ? S[f * N + e] : mk2<R>(zero, zero);
+        }
+        if (k + 1 < k1) issue(k + 1, sl ^ 1);
+        const double lt = zs[0][k - k0], lb = zs[1][k - k0], rdz = zs[2][k - k0], rdzt = zs[3][k - k0];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = tid + i * NT;
+            if (e >= N) continue;
+            R pr[8][2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const double up = gU(cx(cur[i][0], c), k + 1), vp = gV(cx(cur[i][1], c), k + 1);
+                const double wp = gW(cx(cur[i][2], c), k + 1), tp = gT(cx(cur[i][3], c), k + 1);
+                R dd[6];
+#pragma unroll
+                for (int f = 0; f < 6; ++f) dd[f] = cx(cur[i][4 + f], c);
+                double bfv[3], o[8];
+                if (a.bf[0]) {
+                    const long long q = (long long)k * nxy + row + 2 * e + c;
+                    bfv[0] = (double)a.bf[0][q]; bfv[1] = (double)a.bf[1][q]; bfv[2] = (double)a.bf[2][q];
+                }
+                spec_point_products<R>(a, dpx, got, ic, um_[i][c], uk[i][c], up, vm[i][c], vk[i][c], vp,
+                                       wm[i][c], wk[i][c], wp, tk[i][c], tp, dd, a.bf[0] ? bfv : nullptr,
+                                       lt, lb, rdz, rdzt, o);
+#pragma unroll
+                for (int f = 0; f < 8; ++f) pr[f][c] = (R)o[f];
+                um_[i][c] = uk[i][c]; uk[i][c] = up; vm[i][c] = vk[i][c]; vk[i][c] = vp;
+                wm[i][c] = wk[i][c]; wk[i][c] = wp; tk[i][c] = tp;
+            }
+#pragma unroll
+            for (int f = 0; f < 8; ++f) cin.st(f, e, mk2<R>(pr[f][0], pr[f][1]));
+        }
+        __syncthreads();
+        run_passes<R, N, -1, RMAX, L, NT, false, 0>(cin, zout, Ab, Bb, A.tw);
+        __syncthreads();
+        // unpack the half-length transform into the nx/2 modes, as k_fft_x_r2c_t
+        // (a thread keeps its modes l and their twiddle over the eight rows)
+        const long long orow = ((long long)k * g.ny + j) * N;
+        const R sc = A.scale;
+        for (int l = tid; l < N; l += NT) {
+            const T2 w = __ldg(A.wp + l);
+            const int i0 = fpi<G>(l), i1 = fpi<G>(l == 0 ? 0 : N - l);
+#pragma unroll
+            for (int line = 0; line < L; ++line) {
+                const T2 z = Z[line * LS + i0];
+                T2 zc = Z[line * LS + i1];
+                zc.y = -zc.y;
+                const T2 ev = mk2<R>(R(0.5) * (z.x + zc.x), R(0.5) * (z.y + zc.y));
+                const T2 dv = mk2<R>(R(0.5) * (z.x - zc.x), R(0.5) * (z.y - zc.y));
+                const T2 wd = cmulc(w, dv);
+                reinterpret_cast<T2*>(a.out[line])[orow + l] = mk2<R>((ev.x + wd.y) * sc, (ev.y - wd.x) * sc);
+            }
+        }
+    }
+    sp_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -449,47 +680,70 @@ template <typename R> struct ProdTArgs {
 };
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_spec_products_t(ProdTArgs<R> a)
+__global__ void __launch_bounds__(PROD_NT) k_spec_products_t(ProdTArgs<R> a)
 {
     if (a.halt && *a.halt) return;
     const Geo& g = a.g;
-    const long long ij = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ij >= g.nxy) return;
     const int nz = g.nz;
     const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    // t one level up and u, v, w of a level staged D levels ahead in a
+    // per-thread cp.async ring, the z factors of the chunk in shared memory
+    // (see k_spec_products)
+    constexpr int D = ProdAhead<R>::v, NS = D + 1, NW = 4;
+    __shared__ double zs[3][SPEC_KCHUNK_MAX];
+    __shared__ R ring[NS][NW][PROD_NT];
+    for (int i = threadIdx.x; i < 3 * (k1 - k0); i += blockDim.x) {
+        const int f = i / (k1 - k0), k = k0 + i % (k1 - k0);
+        zs[f][k - k0] = ldz(f == 0 ? g.z.l_t : f == 1 ? g.z.l_b : g.z.dz, k);
+    }
+    __syncthreads();
+    const int tid = threadIdx.x;
+    const long long ij = (long long)blockIdx.x * PROD_NT + tid;
+    if (ij >= g.nxy) return;
     const long long nxy = g.nxy;
     // stored t of the level a neighbour reads (clamped) and the ghost rule of
-    // update_boundary_t on it; everything a level reads is loaded one level ahead
-    // in the storage type (see k_spec_products)
+    // update_boundary_t on it
     const int nz1 = nz - 1;
-    auto rawt = [&](int k) -> R { return a.t[(long long)(k < 0 ? 0 : (k > nz1 ? nz1 : k)) * nxy + ij]; };
+    auto tq = [&](int k) { return (long long)(k < 0 ? 0 : (k > nz1 ? nz1 : k)) * nxy + ij; };
     auto gT = [&](R r, int k) -> double {
         return k < 0 ? a.tbs * (double)r + a.tba : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
     };
-    struct Lv { R tp, u, v, w; double lt, lb, dz; };
-    auto fetch = [&](int k, Lv& L) {
-        const long long q = (long long)k * nxy + ij;
-        L.tp = rawt(k + 1); L.u = a.u[q]; L.v = a.v[q]; L.w = a.w[q];
-        L.lt = ldz(g.z.l_t, k); L.lb = ldz(g.z.l_b, k); L.dz = ldz(g.z.dz, k);
+    auto issue = [&](int k, int slot) {
+        if (k < k1) {
+            const long long q = (long long)k * nxy + ij;
+            sp_cp<sizeof(R)>(&ring[slot][0][tid], a.t + tq(k + 1));
+            sp_cp<sizeof(R)>(&ring[slot][1][tid], a.u + q);
+            sp_cp<sizeof(R)>(&ring[slot][2][tid], a.v + q);
+            sp_cp<sizeof(R)>(&ring[slot][3][tid], a.w + q);
+        }
+        sp_commit();
     };
-    double tm = gT(rawt(k0 - 1), k0 - 1), tk = gT(rawt(k0), k0);
+#pragma unroll
+    for (int s = 0; s < D; ++s) issue(k0 + s, s);
+    double tm = gT(a.t[tq(k0 - 1)], k0 - 1), tk = gT(a.t[tq(k0)], k0);
     double wm = k0 > 0 ? (double)a.w[(long long)(k0 - 1) * nxy + ij] : 0.0;
-    Lv cur;
-    fetch(k0, cur);
-    for (int k = k0; k < k1; ++k) {
-        Lv nxt;
-        if (k + 1 < k1) fetch(k + 1, nxt);
-        const double tp = gT(cur.tp, k + 1);
-        const long long q = (long long)k * nxy + ij;
-        const double uk = (double)cur.u, vk = (double)cur.v, wk = (double)cur.w;
-        const double lt = cur.lt, lb = cur.lb;
-        const double a1 = tp * lt + tk * (1.0 - lt), a2 = tm * lb + tk * (1.0 - lb);
-        a.out[0][q] = (R)(uk * tk);
-        a.out[1][q] = (R)(tk * vk);
-        a.out[2][q] = (R)((a1 * wk - a2 * wm) / cur.dz);
-        tm = tk; tk = tp; wm = wk;
-        cur = nxt;
+    for (int kb = k0; kb < k1; kb += NS) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int k = kb + s;
+            if (k >= k1) break;
+            sp_wait<D - 1>();
+            R cur[NW];
+#pragma unroll
+            for (int f = 0; f < NW; ++f) cur[f] = ring[s][f][tid];
+            issue(k + D, (s + D) % NS);
+            const double tp = gT(cur[0], k + 1);
+            const long long q = (long long)k * nxy + ij;
+            const double uk = (double)cur[1], vk = (double)cur[2], wk = (double)cur[3];
+            const double lt = zs[0][k - k0], lb = zs[1][k - k0];
+            const double a1 = tp * lt + tk * (1.0 - lt), a2 = tm * lb + tk * (1.0 - lb);
+            a.out[0][q] = (R)(uk * tk);
+            a.out[1][q] = (R)(tk * vk);
+            a.out[2][q] = (R)((a1 * wk - a2 * wm) / zs[2][k - k0]);
+            tm = tk; tk = tp; wm = wk;
+        }
     }
+    sp_wait<0>();
 }
 
 template <typename R> struct AsmTArgs {
@@ -571,8 +825,12 @@ __global__ void __launch_bounds__(256) k_spec_assemble_t(AsmTArgs<R> a)
 
 // screen_div_error_spec (src/module_spectral.f90:899-1007) on the physical image
 // of the divergence spectrum: per block sum |div|, the div of largest magnitude
-// and a NaN flag over u, v, w (same partial layout as k_div_check).
-template <typename R>
+// and a NaN flag over u, v, w (same partial layout as k_div_check). V points a
+// thread and load (16-byte loads when the host finds the fields aligned; the
+// n % V points past the last full vector are taken one a thread).
+template <typename R, int V> struct alignas(sizeof(R) * V) DivVec { R x[V]; };
+
+template <typename R, int V>
 __global__ void __launch_bounds__(256) k_spec_div_reduce(const R* div, FieldsIn<R> f, long long n, double* part)
 {
     __shared__ double s_sum[8], s_max[8];
@@ -582,13 +840,23 @@ __global__ void __launch_bounds__(256) k_spec_div_reduce(const R* div, FieldsIn<
     __syncthreads();
     double sm = 0.0, mx = 0.0;
     int nan = 0;
-    for (long long q = (long long)blockIdx.x * blockDim.x + tid; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const double d = (double)div[q];
-        const double uc = (double)f.u[q], vc = (double)f.v[q], wc = (double)f.w[q];
-        if (uc != uc || vc != vc || wc != wc || d != d) { nan = 1; continue; }
+    auto point = [&](R dr, R ur, R vr, R wr) {
+        const double d = (double)dr, uc = (double)ur, vc = (double)vr, wc = (double)wr;
+        if (uc != uc || vc != vc || wc != wc || d != d) { nan = 1; return; }
         sm += fabs(d);
         mx = absmax_pick(mx, d);
+    };
+    typedef DivVec<R, V> Vt;
+    const long long nv = n / V, stride = (long long)gridDim.x * blockDim.x;
+    const long long i0 = (long long)blockIdx.x * blockDim.x + tid;
+#pragma unroll 2
+    for (long long i = i0; i < nv; i += stride) {
+        const Vt d = reinterpret_cast<const Vt*>(div)[i], u = reinterpret_cast<const Vt*>(f.u)[i];
+        const Vt v = reinterpret_cast<const Vt*>(f.v)[i], w = reinterpret_cast<const Vt*>(f.w)[i];
+#pragma unroll
+        for (int e = 0; e < V; ++e) point(d.x[e], u.x[e], v.x[e], w.x[e]);
     }
+    for (long long q = nv * V + i0; q < n; q += stride) point(div[q], f.u[q], f.v[q], f.w[q]);
     if (nan) s_nan = 1;
     sm = warp_sum(sm);
     mx = warp_absmax(mx);

@@ -148,3 +148,37 @@ def test_spectral_body_force_parity(name, oracle_lib, engine):
         assert e <= FP64_TOL, f"{name}: field {f} rel err {e:.3e}"
     c.close()
 
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [0, PREC_MIXED])
+def test_products_fused_with_x_transform(prec, oracle_lib, engine):
+    """The products and their forward x transform run as one kernel
+    (spec_products_fx) where nx/2 has an instantiation (32 x 24 here), and as the
+    separate kernels otherwise (the radix-5 grid, and tile[0] = -1 with its fused
+    2-D transforms); both paths against the oracle, skew form with body force."""
+    for name, fused in (("sp_open_scalar_skew", True), ("sp_radix_3_5", False)):
+        p = SP_CASES[name].replace(issk=1, precision=prec)
+        fields = _fields(p, 13)
+        bf = inputs.gaussian_body_force(p, seed=2, amp=0.05)
+        o = oracle_lib.Oracle(p)
+        o.load(fields)
+        o.set_body_force(*bf)
+        o.initialize()
+        rc, od = o.step(6)
+        assert rc == 0
+        c = engine.Channel(p)
+        c.load(fields)
+        c.set_body_force(*bf)
+        c.initialize()
+        c.set_profiling(True)
+        c.step(6)
+        prof = c.kernel_profile()
+        assert (prof.get("spec_products_fx", {}).get("launches", 0) > 0) == fused, name
+        assert (prof.get("spec_products", {}).get("launches", 0) > 0)   # the temperature products
+        tol = FP64_TOL if prec == 0 else MIXED_TOL
+        for f in ["u", "v", "w", "t"]:
+            e = rel_err(c.download(f), o.get(f))
+            assert e <= tol, f"{name}: field {f} rel err {e:.3e}"
+        c.close()
+        o.close()
