@@ -29,8 +29,8 @@ template <typename R> static DampTab spec_damp_tab(hc_handle* h)
 template <typename R, int K> static int col_sp_k(hc_handle* h, const SpColArgs<R>& a)
 {
     if constexpr (K <= 4) {
-        const unsigned nb = (unsigned)((h->g.ncol + CT_COLS - 1) / CT_COLS);
-        k_column_sp_tile<R, K><<<nb, CT_COLS * 32, column_sp_tile_smem<K>(sizeof(typename V2<R>::T)), h->st>>>(a);
+        const unsigned nb = (unsigned)((h->g.ncol + SP_COLS - 1) / SP_COLS);
+        k_column_sp_tile<R, K><<<nb, SP_COLS * 32, column_sp_tile_smem<K>(sizeof(typename V2<R>::T)), h->st>>>(a);
     } else {
         const unsigned nb = (unsigned)((h->g.ncol + CW_WARPS - 1) / CW_WARPS);
         k_column_sp_warp<R, K><<<nb, CW_WARPS * 32, column_warp_smem<K>(), h->st>>>(a);

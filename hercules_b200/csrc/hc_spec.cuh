@@ -353,8 +353,9 @@ template <typename R, int N, int RMAX> struct SpxCfg {
     static constexpr int NT = 128, L = 8, EPT = (N + NT - 1) / NT;
     static constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride;
     // the passes' two buffers (the product rows share the second when there are
-    // two passes or more: the first pass has read them before it is written),
-    // two slots of 10 rows of pairs
+    // two passes or more: the first pass has read them before it is written;
+    // the last pass of an even count lands there too, and the next level's
+    // products wait for a barrier after the unpacking), two slots of 10 rows of pairs
     static constexpr int np = FPlan<N, RMAX>::npass;
     static constexpr size_t smem = ((size_t)(np >= 2 ? 2 : 3) * L * LS + (size_t)2 * PROD_NW * N) *
                                    sizeof(typename V2<R>::T);
@@ -512,6 +513,9 @@ __global__ void __launch_bounds__(128, (SpxCfg<R, N, RMAX>::minb)) k_spec_produc
                 reinterpret_cast<T2*>(a.out[line])[orow + l] = mk2<R>((ev.x + wd.y) * sc, (ev.y - wd.x) * sc);
             }
         }
+        // with an even number of passes the last one lands in B, where the next
+        // level's products go: every thread must be done unpacking first
+        if constexpr (np >= 2 && np % 2 == 0) __syncthreads();
     }
     sp_wait<0>();
 }
@@ -1073,19 +1077,22 @@ __global__ void __launch_bounds__(CW_WARPS * 32, 4) k_column_sp_warp(SpColArgs<R
 }
 
 // The same column work as k_column_sp_warp with the coalescing tiles of
-// k_column_fd_tile_r: a block of CT_COLS warps stages the rows of CT_COLS
+// k_column_fd_tile_r: a block of SP_COLS warps stages the rows of SP_COLS
 // adjacent columns (q_u, q_v, q_w and the old pressure spectrum) in shared
 // memory with row-contiguous loads, each warp solves one column from the tiles,
 // and the results (u, v, w, p, phi, the divergence spectrum) leave through the
 // tiles with row-contiguous stores; the warp kernel read and wrote every row of
 // its column with one access per lane (32 rows of one column per instruction).
+// columns a block (8 warps); 4 columns of 4 warps, at 4 resident blocks, took
+// 216 against 212 us a launch mixed and 294 against 275 us FP64 at 256 x 256 x 128
+#define SP_COLS 8
 template <int K> __host__ size_t column_sp_tile_smem(size_t elem)
 {
-    return (size_t)4 * CT_COLS * ct_stride_e<K>(elem) * elem;
+    return (size_t)4 * SP_COLS * ct_stride_e<K>(elem) * elem;
 }
 
 template <typename R, int K>
-__global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R> A)
+__global__ void __launch_bounds__(SP_COLS * 32, 16 / SP_COLS) k_column_sp_tile(SpColArgs<R> A)
 {
     typedef typename V2<R>::T TT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1093,37 +1100,37 @@ __global__ void __launch_bounds__(CT_COLS * 32, 2) k_column_sp_tile(SpColArgs<R>
     if (a.halt && *a.halt) return;
     const int ln = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const long long ncol = a.g.ncol;
-    const long long c0 = (long long)blockIdx.x * CT_COLS;
+    const long long c0 = (long long)blockIdx.x * SP_COLS;
     const long long c = c0 + wp;
     const bool active = c < ncol;
     const int nz = a.g.nz;
     constexpr int STR = CtLayout<TT>::template stride<K>();
     constexpr int RP = CtLayout<TT>::rp;
     TT* TU = reinterpret_cast<TT*>(smem_raw);
-    TT* TV = TU + CT_COLS * STR;
-    TT* TW = TV + CT_COLS * STR;
-    TT* TP = TW + CT_COLS * STR;
+    TT* TV = TU + SP_COLS * STR;
+    TT* TW = TV + SP_COLS * STR;
+    TT* TP = TW + SP_COLS * STR;
     // element (column cb, row r) at cb * STR + (r % K) * RP + r / K: lane ln of
     // a warp holds rows ln K .. ln K + K - 1 of its column
     auto load = [&](const TT* __restrict__ q, TT* T, int nrows) {
         TT v[K];
 #pragma unroll
         for (int it = 0; it < K; ++it) {
-            const int idx = threadIdx.x + it * CT_COLS * 32;
-            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+            const int idx = threadIdx.x + it * SP_COLS * 32;
+            const int r = idx / SP_COLS, cb = idx - r * SP_COLS;
             const long long cc = c0 + cb;
-            v[it] = (idx < nrows * CT_COLS && cc < ncol) ? q[(long long)r * ncol + cc] : mk2<R>(R(0), R(0));
+            v[it] = (idx < nrows * SP_COLS && cc < ncol) ? q[(long long)r * ncol + cc] : mk2<R>(R(0), R(0));
         }
 #pragma unroll
         for (int it = 0; it < K; ++it) {
-            const int idx = threadIdx.x + it * CT_COLS * 32;
-            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
-            if (idx < nrows * CT_COLS) T[cb * STR + (r % K) * RP + r / K] = v[it];
+            const int idx = threadIdx.x + it * SP_COLS * 32;
+            const int r = idx / SP_COLS, cb = idx - r * SP_COLS;
+            if (idx < nrows * SP_COLS) T[cb * STR + (r % K) * RP + r / K] = v[it];
         }
     };
     auto store = [&](TT* __restrict__ q, const TT* T) {
-        for (int idx = threadIdx.x; idx < nz * CT_COLS; idx += blockDim.x) {
-            const int r = idx / CT_COLS, cb = idx - r * CT_COLS;
+        for (int idx = threadIdx.x; idx < nz * SP_COLS; idx += blockDim.x) {
+            const int r = idx / SP_COLS, cb = idx - r * SP_COLS;
             const long long cc = c0 + cb;
             if (cc < ncol) q[(long long)r * ncol + cc] = T[cb * STR + (r % K) * RP + r / K];
         }
