@@ -190,10 +190,13 @@ ALG_WORDS_SUB = {
            # fused 2-D transforms: 11 fields each way, one word in and one out
            "fft2d_fwd": 22, "fft2d_inv": 22},
 }
-# spectral path with the products fused with their x transform: that kernel reads
-# the products' 10 inputs and writes 8 x half spectra; the separate products and
-# x forward kernels are left with the temperature's 7 and 3 + 3 words
-ALG_WORDS_SP_FUSED = {"spec_products_fx": 18, "spec_products": 7, "fft_x_r2c": 6}
+# spectral path with the products fused with their x transform: the momentum
+# kernel reads the products' 10 inputs and writes 8 x half spectra; the
+# temperature kernel reads 4 and writes 3 (fused too unless a separate temperature
+# products kernel shows in the profile, which then keeps 7 words and the x
+# forward kernel 3 + 3)
+ALG_WORDS_SP_FUSED = {"spec_products_fx": 25, "spec_products": 0, "fft_x_r2c": 0}
+ALG_WORDS_SP_FUSED_MOM = {"spec_products_fx": 18, "spec_products": 7, "fft_x_r2c": 6}
 
 
 # DRAM bytes (read + write) of one launch per kernel category, FP32-mixed, measured
@@ -227,10 +230,19 @@ def stats_bytes_per_point(kind: str, wbytes: int, with_t: bool = True) -> float:
     return reads + nacc * 2 * 4 + nacc * (4 + 16 + 4) / STATS_WINDOW
 
 
-def alg_bytes_step(kernel: str, npts: int, wbytes: int, kind: str, nsub: int = 3, fused: bool = False) -> float:
+def fused_mode(prof) -> str:
+    """Which spectral products ran fused with their x transform, from the kernel
+    categories of a profile."""
+    if "spec_products_fx" not in prof:
+        return ""
+    return "mom" if "spec_products" in prof else "all"
+
+
+def alg_bytes_step(kernel: str, npts: int, wbytes: int, kind: str, nsub: int = 3, fused: str = "") -> float:
     """Algorithmic bytes of one time step in one kernel category (the FD workloads
-    are neutral, the spectral ones carry temperature; fused: the spectral products
-    ran fused with their x transform)."""
+    are neutral, the spectral ones carry temperature; fused: "all" when the
+    spectral products ran fused with their x transform, "mom" when only the
+    momentum ones did)."""
     if kernel == "stats":
         return npts * stats_bytes_per_point(kind, wbytes, with_t=kind != "fd")
     if kind == "fd" and kernel == "div_check":
@@ -239,7 +251,7 @@ def alg_bytes_step(kernel: str, npts: int, wbytes: int, kind: str, nsub: int = 3
         nsub = 1
     words = ALG_WORDS_SUB[kind].get(kernel, 0)
     if kind == "sp" and fused:
-        words = ALG_WORDS_SP_FUSED.get(kernel, words)
+        words = (ALG_WORDS_SP_FUSED if fused == "all" else ALG_WORDS_SP_FUSED_MOM).get(kernel, words)
     return words * nsub * npts * wbytes
 
 
@@ -330,7 +342,7 @@ def run_gpu(args, ws, rank, hbm):
         kern[tag] = {}
         for k, v in prof.items():
             avg = v["total_ms"] / max(v["launches"], 1)
-            b = alg_bytes_step(k, npts, wb, kind, fused="spec_products_fx" in prof) * nprof
+            b = alg_bytes_step(k, npts, wb, kind, fused=fused_mode(prof)) * nprof
             gbs = (b / (v["total_ms"] * 1e-3) / 1e9) if b and v["total_ms"] > 0 else None
             kern[tag][k] = {"launches": v["launches"], "avg_ms": avg, "total_ms": v["total_ms"],
                             "alg_bytes_per_launch": b / max(v["launches"], 1) if b else None,
@@ -667,7 +679,7 @@ def main():
     roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
             "frac": ach / hbm if ach else None, "peak_kind": peak_kind, "traffic": TRAFFIC.get((args.workload, dom)),
             "traffic_capture": TRAFFIC_CAPTURE if (args.workload, dom) in TRAFFIC else None,
-            "alg_bytes_per_launch": alg_bytes_step(dom, npts, 4, kind, fused="spec_products_fx" in km)
+            "alg_bytes_per_launch": alg_bytes_step(dom, npts, 4, kind, fused=fused_mode(km))
             / max(km[dom]["launches"] / 2, 1)}
     # whole-step HBM fraction with the fixed per-point accounting of an ideally
     # fused step: FD neutral RK3 131 words (117 field words + 14 FP64 mean words);

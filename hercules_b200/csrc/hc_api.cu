@@ -286,6 +286,7 @@ struct hc_handle {
     int f2_ncl[2];           // their persistent clusters resident at once: forward, inverse
     int spx;                 // 1: the spectral products and their x transform in one kernel (k_spec_products_fx)
     int spx_minb;            // its blocks resident an SM
+    int spx_t;               // 1: the temperature products too (k_spec_products_t_fx)
     FftPlan px, py;
     double2* wpack;
     int rows_x, tl_y, col_threads, col_warp;

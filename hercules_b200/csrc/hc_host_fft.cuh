@@ -166,6 +166,36 @@ template <typename R> static int spx_dispatch(hc_handle* h, int op, const ProdFx
     return HC_ERR_UNSUPPORTED;
 }
 
+// the temperature products fused with their x transform: op 0 set up, 1 launch
+template <typename R, int N> static int spx_t_op(hc_handle* h, int op, const ProdTFxArgs<R>* a, dim3 grid)
+{
+    constexpr size_t sm = SpxTCfg<R, N, HC_FFT_T_RMAX>::smem;
+    if constexpr (sm > 100 * 1024) {
+        return HC_ERR_UNSUPPORTED;
+    } else {
+        void (*k)(ProdTFxArgs<R>) = k_spec_products_t_fx<R, N, HC_FFT_T_RMAX>;
+        if (op == 0) {
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
+                cudaGetLastError();
+                return HC_ERR_UNSUPPORTED;
+            }
+            return HC_OK;
+        }
+        k<<<grid, SpxTCfg<R, N, HC_FFT_T_RMAX>::NT, sm, h->st>>>(*a);
+        return HC_OK;
+    }
+}
+
+template <typename R> static int spx_t_dispatch(hc_handle* h, int op, const ProdTFxArgs<R>* a, dim3 grid)
+{
+    switch (h->g.nxh) {
+#define HC_SPX_CASE(N) case N: return spx_t_op<R, N>(h, op, a, grid);
+    HC_SPX_LENGTHS(HC_SPX_CASE)
+#undef HC_SPX_CASE
+    }
+    return HC_ERR_UNSUPPORTED;
+}
+
 // Levels a block of k_spec_products_fx: the chunk (4..SPEC_KCHUNK_MAX) whose
 // grid of ny x chunks blocks fills its last wave best, each chunk's two extra
 // start-up levels counted as extra reads
@@ -259,6 +289,12 @@ static int build_fft(hc_handle* h)
         const int rc = h->rsz == sizeof(double) ? spx_dispatch<double>(h, 0, nullptr, dim3())
                                                 : spx_dispatch<float>(h, 0, nullptr, dim3());
         h->spx = rc == HC_OK;
+    }
+    h->spx_t = 0;
+    if (h->spx && h->p.isscalar == 1) {
+        const int rc = h->rsz == sizeof(double) ? spx_t_dispatch<double>(h, 0, nullptr, dim3())
+                                                : spx_t_dispatch<float>(h, 0, nullptr, dim3());
+        h->spx_t = rc == HC_OK;
     }
     const size_t c2 = 2 * h->rsz;     // bytes of one complex
     h->rows_x = h->p.tile[0] > 0 ? h->p.tile[0] : (h->rsz == sizeof(double) ? 1024 : 2048) / nxh;

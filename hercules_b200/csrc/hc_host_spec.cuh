@@ -188,13 +188,27 @@ template <typename R> static int substep_sp(hc_handle* h, int sub)
         pt.u = (const R*)h->fld[F_U]; pt.v = (const R*)h->fld[F_V]; pt.w = (const R*)h->fld[F_W]; pt.t = (const R*)h->fld[F_T];
         for (int f = 0; f < 3; ++f) pt.out[f] = Q[SP_W0 + 4 + f];
         t_ghost_bottom(h, pt.tbs, pt.tba);
-        pt.g = g; pt.ttop = p.ttop; pt.kchunk = spec_kchunk(h, g.nxy); pt.halt = halt;
-        prof_begin(h, K_SPEC_PROD);
-        k_spec_products_t<R><<<dim3((unsigned)((g.nxy + 255) / 256), (p.nz + pt.kchunk - 1) / pt.kchunk), 256, 0, h->st>>>(pt);
-        CKL();
+        pt.g = g; pt.ttop = p.ttop; pt.halt = halt;
         const R* fin[3] = {Q[SP_W0 + 4], Q[SP_W0 + 5], Q[SP_W0 + 6]};
         T2* fout[3] = {S[SP_W0 + 4], S[SP_W0 + 5], S[SP_W0 + 6]};
-        if ((rc = fft_forward<R>(h, fin, fout, 3))) return rc;
+        auto al = [&](const void* q) { return ((uintptr_t)q & (2 * sizeof(R) - 1)) == 0; };
+        if (h->spx_t && !h->rec && al(pt.u) && al(pt.v) && al(pt.w) && al(pt.t)) {
+            ProdTFxArgs<R> ta;
+            ta.p = pt;
+            for (int f = 0; f < 3; ++f) ta.p.out[f] = (R*)S[SP_W0 + 4 + f];
+            ta.p.kchunk = spx_kchunk(h);
+            ta.tw = fft_tw<R>(h, 0); ta.wp = fft_tw<R>(h, 2); ta.scale = (R)(1.0 / p.nx);
+            prof_begin(h, K_SPEC_PRODFX);
+            if ((rc = spx_t_dispatch<R>(h, 1, &ta, dim3((unsigned)g.ny, (p.nz + ta.p.kchunk - 1) / ta.p.kchunk)))) return rc;
+            CKL();
+            if ((rc = fft_forward<R>(h, fin, fout, 3, true))) return rc;
+        } else {
+            pt.kchunk = spec_kchunk(h, g.nxy);
+            prof_begin(h, K_SPEC_PROD);
+            k_spec_products_t<R><<<dim3((unsigned)((g.nxy + 255) / 256), (p.nz + pt.kchunk - 1) / pt.kchunk), 256, 0, h->st>>>(pt);
+            CKL();
+            if ((rc = fft_forward<R>(h, fin, fout, 3))) return rc;
+        }
         AsmTArgs<R> at;
         at.st = S[SP_T];
         for (int f = 0; f < 3; ++f) at.F[f] = S[SP_W0 + 4 + f];

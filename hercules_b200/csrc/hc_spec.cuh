@@ -750,6 +750,143 @@ __global__ void __launch_bounds__(PROD_NT) k_spec_products_t(ProdTArgs<R> a)
     sp_wait<0>();
 }
 
+// k_spec_products_t_fx: the three temperature products of k_spec_products_t and
+// their forward x transform in one pass, as k_spec_products_fx (three rows a
+// level; t one level up and u, v, w of the level arrive by cp.async one level
+// ahead; the products are rounded to the storage type before the passes).
+template <typename R> struct ProdTFxArgs {
+    ProdTArgs<R> p;                    // p.out[f]: the x half spectra (complex rows)
+    const typename V2<R>::T* tw;       // exp(-2 pi i e / (nx/2)), e < nx/2
+    const typename V2<R>::T* wp;       // exp(-2 pi i l / nx), l < nx/2
+    R scale;                           // 1/nx
+};
+template <typename R, int N, int RMAX> struct SpxTCfg {
+    static constexpr int NT = 128, L = 3, NW = 4;
+    static constexpr int G = FPad<R>::G, LS = FLine<N, G>::stride;
+    static constexpr int np = FPlan<N, RMAX>::npass;
+    static constexpr size_t smem = ((size_t)(np >= 2 ? 2 : 3) * L * LS + (size_t)2 * NW * N) *
+                                   sizeof(typename V2<R>::T);
+};
+
+template <typename R, int N, int RMAX>
+__global__ void __launch_bounds__(128) k_spec_products_t_fx(ProdTFxArgs<R> A)
+{
+    typedef typename V2<R>::T T2;
+    typedef SpxTCfg<R, N, RMAX> CF;
+    constexpr int NT = CF::NT, L = CF::L, NW = CF::NW, G = CF::G, LS = CF::LS, EPT = (N + NT - 1) / NT;
+    const ProdTArgs<R>& a = A.p;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (a.halt && *a.halt) return;
+    const Geo& g = a.g;
+    const int nz = g.nz, j = blockIdx.x;
+    const int k0 = blockIdx.y * a.kchunk, k1 = min(nz, k0 + a.kchunk);
+    constexpr int np = CF::np;
+    T2* Ab = reinterpret_cast<T2*>(smem_raw);
+    T2* Bb = Ab + L * LS;
+    T2* Cb = np >= 2 ? Bb : Bb + L * LS;
+    T2* slot = Bb + (np >= 2 ? 1 : 2) * L * LS;
+    T2* Z = (np % 2 == 1) ? Ab : Bb;
+    __shared__ double zs[3][SPEC_KCHUNK_MAX];
+    for (int i = threadIdx.x; i < 3 * (k1 - k0); i += blockDim.x) {
+        const int f = i / (k1 - k0), k = k0 + i % (k1 - k0);
+        zs[f][k - k0] = ldz(f == 0 ? g.z.l_t : f == 1 ? g.z.l_b : g.z.dz, k);
+    }
+    const int tid = threadIdx.x;
+    const long long nxy = g.nxy, row = (long long)j * g.nx;
+    const int nz1 = nz - 1;
+    auto tq = [&](int k) { return (long long)(k < 0 ? 0 : (k > nz1 ? nz1 : k)) * nxy + row; };
+    auto gT = [&](R r, int k) -> double {
+        return k < 0 ? a.tbs * (double)r + a.tba : (k >= nz ? 2.0 * a.ttop - (double)r : (double)r);
+    };
+    auto issue = [&](int k, int sl) {
+        T2* S = slot + sl * NW * N;
+        const long long q = (long long)k * nxy + row;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = tid + i * NT;
+            if (e >= N) continue;
+            sp_cp<sizeof(T2)>(S + 0 * N + e, a.t + tq(k + 1) + 2 * e);
+            sp_cp<sizeof(T2)>(S + 1 * N + e, a.u + q + 2 * e);
+            sp_cp<sizeof(T2)>(S + 2 * N + e, a.v + q + 2 * e);
+            sp_cp<sizeof(T2)>(S + 3 * N + e, a.w + q + 2 * e);
+        }
+        sp_commit();
+    };
+    issue(k0, 0);
+    __syncthreads();                 // zs
+    auto cx = [](T2 v, int c) -> R { return c == 0 ? v.x : v.y; };
+    double tm[EPT][2], tk[EPT][2], wm[EPT][2];
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+        const int e = tid + i * NT;
+        if (e >= N) continue;
+        const T2 t0 = *reinterpret_cast<const T2*>(a.t + tq(k0 - 1) + 2 * e);
+        const T2 t1 = *reinterpret_cast<const T2*>(a.t + tq(k0) + 2 * e);
+        const T2 w0 = k0 > 0 ? *reinterpret_cast<const T2*>(a.w + (long long)(k0 - 1) * nxy + row + 2 * e)
+                             : mk2<R>(R(0), R(0));
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            tm[i][c] = gT(cx(t0, c), k0 - 1); tk[i][c] = gT(cx(t1, c), k0);
+            wm[i][c] = k0 > 0 ? (double)cx(w0, c) : 0.0;
+        }
+    }
+    const SmemIO<T2, LS, G> cin{Cb}, zout{Z};
+    const R zero = R(0);
+    for (int k = k0; k < k1; ++k) {
+        const int sl = (k - k0) & 1;
+        sp_wait<0>();
+        const T2* S = slot + sl * NW * N;
+        T2 cur[EPT][NW];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = tid + i * NT;
+#pragma unroll
+            for (int f = 0; f < NW; ++f) cur[i][f] = e < N ? S[f * N + e] : mk2<R>(zero, zero);
+        }
+        if (k + 1 < k1) issue(k + 1, sl ^ 1);
+        const double lt = zs[0][k - k0], lb = zs[1][k - k0], dz = zs[2][k - k0];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = tid + i * NT;
+            if (e >= N) continue;
+            R pr[3][2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const double tp = gT(cx(cur[i][0], c), k + 1);
+                const double uk = (double)cx(cur[i][1], c), vk = (double)cx(cur[i][2], c), wk = (double)cx(cur[i][3], c);
+                const double a1 = tp * lt + tk[i][c] * (1.0 - lt), a2 = tm[i][c] * lb + tk[i][c] * (1.0 - lb);
+                pr[0][c] = (R)(uk * tk[i][c]);
+                pr[1][c] = (R)(tk[i][c] * vk);
+                pr[2][c] = (R)((a1 * wk - a2 * wm[i][c]) / dz);
+                tm[i][c] = tk[i][c]; tk[i][c] = tp; wm[i][c] = wk;
+            }
+#pragma unroll
+            for (int f = 0; f < 3; ++f) cin.st(f, e, mk2<R>(pr[f][0], pr[f][1]));
+        }
+        __syncthreads();
+        run_passes<R, N, -1, RMAX, L, NT, false, 0>(cin, zout, Ab, Bb, A.tw);
+        __syncthreads();
+        const long long orow = ((long long)k * g.ny + j) * N;
+        const R sc = A.scale;
+        for (int l = tid; l < N; l += NT) {
+            const T2 w = __ldg(A.wp + l);
+            const int i0 = fpi<G>(l), i1 = fpi<G>(l == 0 ? 0 : N - l);
+#pragma unroll
+            for (int line = 0; line < L; ++line) {
+                const T2 z = Z[line * LS + i0];
+                T2 zc = Z[line * LS + i1];
+                zc.y = -zc.y;
+                const T2 ev = mk2<R>(R(0.5) * (z.x + zc.x), R(0.5) * (z.y + zc.y));
+                const T2 dv = mk2<R>(R(0.5) * (z.x - zc.x), R(0.5) * (z.y - zc.y));
+                const T2 wd = cmulc(w, dv);
+                reinterpret_cast<T2*>(a.out[line])[orow + l] = mk2<R>((ev.x + wd.y) * sc, (ev.y - wd.x) * sc);
+            }
+        }
+        if constexpr (np >= 2 && np % 2 == 0) __syncthreads();   // C shares Z (see k_spec_products_fx)
+    }
+    sp_wait<0>();
+}
+
 template <typename R> struct AsmTArgs {
     const typename V2<R>::T* st;
     const typename V2<R>::T* F[3];

@@ -153,10 +153,10 @@ def test_spectral_body_force_parity(name, oracle_lib, engine):
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", [0, PREC_MIXED])
 def test_products_fused_with_x_transform(prec, oracle_lib, engine):
-    """The products and their forward x transform run as one kernel
-    (spec_products_fx) where nx/2 has an instantiation (32 x 24 here), and as the
-    separate kernels otherwise (the radix-5 grid, and tile[0] = -1 with its fused
-    2-D transforms); both paths against the oracle, skew form with body force."""
+    """The products (momentum and temperature) and their forward x transforms
+    run as fused kernels (spec_products_fx) where nx/2 has an instantiation
+    (32 x 24 here), and as the separate kernels otherwise (the radix-5 grid);
+    both paths against the oracle, skew form with body force and temperature."""
     for name, fused in (("sp_open_scalar_skew", True), ("sp_radix_3_5", False)):
         p = SP_CASES[name].replace(issk=1, precision=prec)
         fields = _fields(p, 13)
@@ -174,8 +174,9 @@ def test_products_fused_with_x_transform(prec, oracle_lib, engine):
         c.set_profiling(True)
         c.step(6)
         prof = c.kernel_profile()
+        # fused: the momentum and the temperature products both run fused
         assert (prof.get("spec_products_fx", {}).get("launches", 0) > 0) == fused, name
-        assert (prof.get("spec_products", {}).get("launches", 0) > 0)   # the temperature products
+        assert (prof.get("spec_products", {}).get("launches", 0) > 0) == (not fused), name
         tol = FP64_TOL if prec == 0 else MIXED_TOL
         for f in ["u", "v", "w", "t"]:
             e = rel_err(c.download(f), o.get(f))
