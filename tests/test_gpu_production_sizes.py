@@ -246,3 +246,27 @@ def test_strip_rhs_reports_nan(engine):
         c.step(2)
     assert ei.value.code == -5
     c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,prec", [("spectral_256x256x8", 0), ("spectral_256x256x8", PREC_MIXED),
+                                       ("spectral_512x384x8", PREC_MIXED)])
+def test_fused_products_are_deterministic(name, prec, engine):
+    """The fused products + x transform kernels on production planes, where the
+    product rows share a shared-memory buffer with the passes: two channels from
+    the same state end bit-equal after 5 steps (a race between a level's
+    unpacking and the next level's products would make them differ)."""
+    p = PLANES[name].replace(precision=prec)
+    fields = inputs.small_random(p, seed=17)
+    out = []
+    for _ in range(2):
+        c = engine.Channel(p)
+        c.load(fields)
+        c.initialize()
+        c.set_profiling(True)
+        c.step(5)
+        assert c.kernel_profile().get("spec_products_fx", {}).get("launches", 0) > 0
+        out.append({f: c.download(f) for f in ("u", "v", "w", "p") + (("t",) if p.isscalar else ())})
+        c.close()
+    for f in out[0]:
+        assert np.array_equal(out[0][f], out[1][f]), f
